@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""Benchmark of the self-gravity FMG Poisson solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload jeans6|nested5|uniform64]
+
+A step is one complete solve (zero initial guess) to relative residual
+<= 1e-10 on the 6-level Jeans-refined hierarchy (128^3 periodic base of 8^3
+blocks, 133,856 blocks, 60.2M leaf cells).  `value` is the mixed-precision
+solves/s with inputs resident in HBM (device-timed with CUDA events on the
+solve's stream); `fp64` repeats it for the plain FP64 path; `e2e` is the same
+metric through the host-buffer C ABI call (sfm_solve) with pinned buffers,
+the host<->device copies inside the timed region.  Inputs (>= 1 GB per field)
+exceed the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: the path runs as independent replicas (one hierarchy per GPU, no
+collective in the data path); value = all ranks' solves / max-over-ranks time.
+
+--impl reference times the CPU restatement of the reference algorithm
+(oracle/, the reference itself cannot be built here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "AMR Poisson solves/s & Gcell-updates/s at rel. resid ≤1e-10, mixed vs plain FP64"
+REL_TOL = 1e-10
+MAX_OUTER = 30
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="jeans6")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    return ap.parse_args()
+
+
+def load_workload(name):
+    """(hierarchy, rho array [nb,G,G,G] with 2 ghost layers, bc), cached on local disk."""
+    import numpy as np
+    from code_only_b200 import workloads as w
+    cache = os.path.join("/tmp", f"sfmg_{name}_v1.npz")
+    h, fn, bc = None, None, None
+    if os.path.exists(cache):
+        try:
+            z = np.load(cache)
+            h = w.Hierarchy(ni=int(z["ni"]), ngb=tuple(z["ngb"].tolist()), nlev=int(z["nlev"]),
+                            periodic=bool(z["periodic"]), box_lo=z["box_lo"], box_size=float(z["box_size"]),
+                            level=z["level"], ijk=z["ijk"], parent=z["parent"], child=z["child"],
+                            nbr=z["nbr"], touch=z["touch"], cellwidth=z["cellwidth"], x0=z["x0"])
+            return h.contiguous(), z["rho"], int(z["bc"])
+        except Exception:
+            pass
+    h, fn, bc = w.config_hierarchy(name)
+    rho = w.block_field(h, 2, fn)
+    try:
+        np.savez(cache, ni=h.ni, ngb=np.array(h.ngb), nlev=h.nlev, periodic=h.periodic, box_lo=h.box_lo,
+                 box_size=h.box_size, level=h.level, ijk=h.ijk, parent=h.parent, child=h.child, nbr=h.nbr,
+                 touch=h.touch, cellwidth=h.cellwidth, x0=h.x0, rho=rho, bc=bc)
+    except Exception:
+        pass
+    return h, rho, bc
+
+
+def params_for(bc, precision, profile=0):
+    from code_only_b200 import abi
+    kw = dict(rel_tol=REL_TOL, max_outer=MAX_OUTER, precision=precision, profile=profile)
+    if bc == abi.SFM_BC_SPHERE:
+        kw["zero_mean"] = 0
+        kw["lmax"] = 4
+    return abi.default_params(bc, **kw)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n):
+    if n <= 1 and "RANK" not in os.environ:
+        return 0, 1, 0
+    import datetime
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    import torch
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def time_device(solver, rho_d, psi_d, g_d, steps, warmup, world):
+    """Device-timed solves (CUDA events on the solve's stream).  Returns
+    (ms per solve over all ranks' max, last stats, launches, smoother stats)."""
+    import torch
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    st = None
+    for _ in range(warmup):
+        psi_d.zero_()
+        st = solver.solve_device(rho_d.data_ptr(), psi_d.data_ptr(), g_d.data_ptr(), sptr)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches, sm_ms, sm_n, sm_cells, iters = 0, 0.0, 0, 0, []
+    e0.record(stream)
+    for _ in range(steps):
+        psi_d.zero_()
+        st = solver.solve_device(rho_d.data_ptr(), psi_d.data_ptr(), g_d.data_ptr(), sptr)
+        launches += st.kernel_launches
+        sm_ms += st.smoother_ms
+        sm_n += st.smoother_launches
+        sm_cells += st.smoother_cells
+        iters.append(st.outer_iters)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1) / steps
+    return max_over_ranks(ms, world), st, launches, (sm_ms, sm_n, sm_cells), iters
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from code_only_b200 import abi, build as b
+    from code_only_b200.solver import FMGPoisson
+
+    rank, world, local = dist_setup(args.gpus)
+    if rank == 0:
+        b.build(verbose=False)
+    barrier(world)
+    h, rho, bc = load_workload(args.workload)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    rho_d = torch.from_numpy(rho).to(dev)
+    psi_d = torch.zeros_like(rho_d)
+    G = rho.shape[1]
+    g_d = torch.zeros((h.nblocks, 3, G, G, G), dtype=torch.float64, device=dev)
+    leaf_cells = h.leaf_cells()
+
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    results = {}
+    for prec, key in ((abi.SFM_PREC_MIXED, "mixed"), (abi.SFM_PREC_FP64, "fp64")):
+        with FMGPoisson(h, params=params_for(bc, prec, profile=1)) as s:
+            if key == "mixed" and sampler:
+                sampler.start()
+            ms, st, launches, smo, iters = time_device(s, rho_d, psi_d, g_d, args.steps, args.warmup, world)
+            if key == "mixed" and sampler:
+                clocks = sampler.stop()
+            results[key] = dict(ms=ms, st=st, launches=launches, smo=smo, iters=iters,
+                                resid=st.true_rel_residual, info=s.info())
+    # end to end through the host-buffer ABI (pinned host memory)
+    e2e = None
+    if not args.no_e2e:
+        with FMGPoisson(h, params=params_for(bc, abi.SFM_PREC_MIXED)) as s:
+            rho_h = torch.from_numpy(rho).pin_memory().numpy()
+            psi_h = torch.zeros(rho.shape, dtype=torch.float64).pin_memory().numpy()
+            g_h = torch.zeros((h.nblocks, 3, G, G, G), dtype=torch.float64).pin_memory().numpy()
+            for _ in range(max(1, args.warmup // 2)):
+                psi_h[...] = 0.0
+                s.solve(rho_h, psi_h)
+            barrier(world)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                psi_h[...] = 0.0
+                out = s.lib.sfm_solve(s.ctx, rho_h.ctypes.data, psi_h.ctypes.data, g_h.ctypes.data, None)
+                if out not in (abi.SFM_OK, abi.SFM_ENOTCONVERGED):
+                    raise RuntimeError(f"sfm_solve failed {out}")
+            t1 = time.perf_counter()
+            barrier(world)
+            ms_e2e = max_over_ranks((t1 - t0) * 1e3 / args.steps, world)
+            nbytes = rho.nbytes
+            e2e = {"value": world * 1e3 / ms_e2e, "unit": "solves/s",
+                   "h2d_bytes_per_step": 5 * nbytes,   # rho, psi (warm start), g (kept outside interiors)
+                   "d2h_bytes_per_step": 4 * nbytes,   # psi, g
+                   "timing": "host wall clock around blocking sfm_solve calls"}
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    mx, fp = results["mixed"], results["fp64"]
+    value = world * 1e3 / mx["ms"]
+    # roofline of the dominant kernel: level-0 red-black colour launch
+    sm_ms, sm_n, sm_cells = mx["smo"]
+    elem = mx["st"].elem_bytes or 4
+    alg_bytes_per_launch = (sm_cells / max(sm_n, 1)) * 2 * elem   # u read + rhs/2 read + u/2 written
+    launch_s = (sm_ms / max(sm_n, 1)) * 1e-3
+    achieved = alg_bytes_per_launch / launch_s / 1e9 if launch_s > 0 else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = prof.get(args.workload, {}).get("bytes_per_launch")
+    except Exception:
+        pass
+    cells_updates = leaf_cells * 1.0
+    sweeps = mx["smo"][1] / max(args.steps, 1) / 2   # full red+black sweeps at level 0 per solve
+    line = {
+        "metric": METRIC,
+        "value": round(value, 4),
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(mx["ms"], 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 inner / f64 outer",
+        "data": "synthetic",
+        "config": {
+            "workload": args.workload,
+            "hierarchy": f"{h.nlev} AMR levels, {h.nblocks} blocks of {h.ni}^3, {leaf_cells} leaf cells",
+            "level_blocks": [int(v) for v in h.level_counts()],
+            "bc": "periodic" if bc == 0 else "isolated sphere (multipole l<=4)",
+            "rel_tol": REL_TOL,
+            "l2": "inputs larger than L2 (>= 1 GB per field), no flush",
+            "parallelism": f"replicas x{world}",
+        },
+        "gcell_updates_per_s": round(value * sweeps * cells_updates / 1e9, 3),
+        "outer_iterations": {"mixed": mx["iters"][-1], "fp64": fp["iters"][-1]},
+        "true_rel_residual": {"mixed": mx["resid"], "fp64": fp["resid"]},
+        "fp64": {"value": round(world * 1e3 / fp["ms"], 4), "unit": "solves/s", "ms_per_step": round(fp["ms"], 4)},
+        "mixed_over_fp64": round(fp["ms"] / mx["ms"], 3),
+        "roofline": {
+            "kernel": "red-black colour sweep, fmg level 0 (OpRelax<float>)",
+            "bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4) if achieved else None,
+            "traffic": traffic,
+            "alg_bytes_per_launch": alg_bytes_per_launch,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+        },
+        "gpu_launches": int(mx["launches"]),
+        "clocks": clocks,
+        "device_bytes": mx["info"]["device_bytes"],
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(h, rho, bc, fp["iters"][-1], sample_iters=1)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(h, rho, bc, n_outer, sample_iters=1):
+    """Times the oracle (CPU restatement) on a bounded sample: one solve with
+    max_outer = 0 (set-up and finish) and one with max_outer = 1; a full
+    solve is set-up + n_outer x one outer iteration."""
+    from tests.oracle_lib import load_oracle, oracle_solve
+    lib = load_oracle()
+    threads = lib.oracle_threads()
+    p0 = params_for(bc, 0)
+    p0.max_outer = 0
+    p1 = params_for(bc, 0)
+    p1.max_outer = sample_iters
+    p1.stagnation_exit = 0
+    t = time.perf_counter()
+    oracle_solve(h, rho, p0, want_g=True)
+    t0 = time.perf_counter() - t
+    t = time.perf_counter()
+    oracle_solve(h, rho, p1, want_g=True)
+    t1 = time.perf_counter() - t
+    t_iter = max(t1 - t0, 1e-9) / sample_iters
+    t_solve = t0 + n_outer * t_iter
+    return {"value": round(1.0 / t_solve, 6), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"oracle FP64 restatement, OpenMP {threads} threads: set-up+finish {t0:.2f} s and "
+                      f"{sample_iters} outer iteration {t_iter:.2f} s measured; solve = set-up + "
+                      f"{n_outer} iterations (the FP64 solve's count to 1e-10)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    import numpy as np
+    h, rho, bc = load_workload(args.workload)
+    from tests.oracle_lib import load_oracle, oracle_solve
+    lib = load_oracle()
+    threads = lib.oracle_threads()
+    # one full FP64 solve gives the outer-iteration count to 1e-10
+    p_full = params_for(bc, 0)
+    t = time.perf_counter()
+    rc, psi, g, st, _ = oracle_solve(h, rho, p_full, want_g=True)
+    t_full = time.perf_counter() - t
+    n_outer = st.outer_iters
+    p0 = params_for(bc, 0)
+    p0.max_outer = 0
+    p1 = params_for(bc, 0)
+    p1.max_outer = 1
+    p1.stagnation_exit = 0
+    samples = []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        oracle_solve(h, rho, p0)
+        a = time.perf_counter() - t
+        t = time.perf_counter()
+        oracle_solve(h, rho, p1)
+        b_ = time.perf_counter() - t
+        if i >= args.warmup:
+            samples.append(a + n_outer * max(b_ - a, 1e-9))
+    t_solve = statistics.median(samples)
+    value = 1.0 / t_solve
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_solve * 1e3, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "rel_tol": REL_TOL,
+                   "hierarchy": f"{h.nlev} AMR levels, {h.nblocks} blocks of {h.ni}^3"},
+        "cpu_baseline": {"value": round(value, 6), "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"each step: oracle set-up+finish and one outer iteration, projected to "
+                                   f"{n_outer} iterations; one full solve took {t_full:.1f} s"},
+        "e2e": {"value": round(value, 6), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_note": "the Fortran/MPI reference cannot be built in this image; the CPU restatement of "
+                          "its algorithm (oracle/) is timed",
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -1,0 +1,367 @@
+// sfm_kernels_misc.cuh -- set-up, boundary, reduction and base-grid kernels.
+#pragma once
+#include "sfm_device.cuh"
+
+namespace sfm {
+
+// ---------------------------------------------------------------------------
+// fmg_make_physvar / fmg_prepare_interp (fmg_data_if.F90:13-84,176-217):
+// U := psi (warm start), RHO := rho * 4 pi G on (-1:n)^3, from the caller's
+// arrays with `g` ghost layers.  Non-finite inputs raise *bad.
+// ---------------------------------------------------------------------------
+template <class TR>
+struct OpPhysvar {
+    double *U; TR *R; const double *rho; const double *psi; int n, G, g; int64_t V; double fourpiG; int *bad;
+    __device__ void operator()(int64_t idx) const {
+        int64_t b = idx / V;
+        int r = (int)(idx % V);
+        int i = r % G - 1, j = (r / G) % G - 1, k = r / (G * G) - 1;
+        const int Gi = n + 2 * g;
+        int64_t s = b * (int64_t)Gi * Gi * Gi + ((int64_t)(k + g) * Gi + (j + g)) * Gi + (i + g);
+        double rv = rho[s], pv = psi ? psi[s] : 0.0;
+        if (!isfinite(rv) || !isfinite(pv)) *bad = 1;
+        U[idx] = pv;
+        R[idx] = (TR)(rv * fourpiG);
+    }
+};
+
+// per-block interior sum, sequential in (i fastest) order as Fortran SUM
+template <class T>
+struct OpBlockSum {
+    const T *a; const int32_t *blocks; double *out; int n, G; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        const T *ab = a + (int64_t)blocks[idx] * V;
+        double s = 0.0;
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) s = s + (double)ab[cidx(G, i, j, k)];
+        out[idx] = s;
+    }
+};
+
+// leaf-volume mean of RHO (fmg_data_if.F90:59-77): mass and volume summed
+// block after block in level order, then rho_ave -> *out
+__global__ void k_mean_combine(const double *psum, const int32_t *blocks, int nblk, const int32_t *level,
+                               const double *h0, int n, double *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double mass = 0.0, vol = 0.0;
+    for (int q = 0; q < nblk; q++) {
+        double hd = h0[level[blocks[q]]];
+        double dv = hd * hd * hd;
+        mass = mass + psum[q] * dv;
+        vol = vol + (double)(n * n * n) * dv;
+    }
+    *out = mass / vol;
+}
+
+// vmg_zeroAverage (vmg.F90:900-916) via fmg_ave (fmg_data.F90:730-769)
+__global__ void k_ave_combine(const double *psum, int nblk, int n, double *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double ave = 0.0;
+    for (int q = 0; q < nblk; q++) ave = ave + psum[q];
+    *out = nblk == 0 ? 0.0 : ave / (double)(n * n * n * nblk);
+}
+
+template <class T>
+struct OpSubScalarAll {      // a := a - *s over whole arrays
+    T *a; const double *s;
+    __device__ void operator()(int64_t idx) const { a[idx] = a[idx] - (T)(*s); }
+};
+template <class T>
+struct OpSubScalarInterior { // a := a - *s on the interior of consecutive blocks
+    T *a; const double *s; int first, n, G; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        const int per = n * n * n;
+        int b = first + (int)(idx / per);
+        int r = (int)(idx % per);
+        int64_t c = (int64_t)b * V + cidx(G, r % n, (r / n) % n, r / (n * n));
+        a[c] = a[c] - (T)(*s);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// isolated boundary (fmg_boundary_phys_sphere.F90:81-354)
+// ---------------------------------------------------------------------------
+struct OpSphereMask {        // rho := 0 where x^2+y^2+z^2 >= rad2, all cells of all blocks
+    double *R; const double *x0; const double *h0; const int32_t *level; int n, G; int64_t V; double rad2;
+    __device__ void operator()(int64_t idx) const {
+        int64_t b = idx / V;
+        int r = (int)(idx % V);
+        int i = r % G - 1, j = (r / G) % G - 1, k = r / (G * G) - 1;
+        double h = h0[level[b]];
+        double x = x0[3 * b] + (double)i * h, y = x0[3 * b + 1] + (double)j * h, z = x0[3 * b + 2] + (double)k * h;
+        if (x * x + y * y + z * z >= rad2) R[idx] = 0.0;
+    }
+};
+
+// moments of one base block: one CTA per block, fixed-order tree reduction
+__global__ void k_moments_block(const double *R, const double *x0, const double *h0, int n, int G, int64_t V,
+                                int lmax, double *part /* [nbase][25] */) {
+    __shared__ double red[25][128];   // blockDim.x == 128
+    const int b = blockIdx.x;
+    const double h = h0[0], dv = h * h * h;
+    double a[25];
+    for (int m = 0; m < 25; m++) a[m] = 0.0;
+    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
+        int i = c % n, j = (c / n) % n, k = c / (n * n);
+        double x = x0[3 * b] + (double)i * h, y = x0[3 * b + 1] + (double)j * h, z = x0[3 * b + 2] + (double)k * h;
+        double r2 = x * x + y * y + z * z;
+        double r = sqrt(r2);
+        double r3 = r2 * r;
+        double rc = sqrt(x * x + y * y);
+        double ri = 1 / r, rci = 1 / rc;
+        double cost = z * ri, sint = rc * ri, cosp = x * rci, sinp = y * rci;
+        double rhodv = R[(int64_t)b * V + cidx(G, i, j, k)] * dv;
+        a[0] += rhodv;
+        a[1] += rhodv * r * cost;
+        a[2] += rhodv * r * sint * cosp;
+        a[3] += rhodv * r * sint * sinp;
+        a[4] += rhodv * r2 * (3 * (cost * cost) - 1);
+        a[5] += rhodv * r2 * sint * cost * cosp;
+        a[6] += rhodv * r2 * sint * cost * sinp;
+        a[7] += rhodv * r2 * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
+        a[8] += rhodv * r2 * (sint * sint) * 2 * sinp * cosp;
+        a[9] += rhodv * r3 * cost * (5 * (cost * cost) - 3);
+        a[10] += rhodv * r3 * sint * (5 * (cost * cost) - 1) * cosp;
+        a[11] += rhodv * r3 * sint * (5 * (cost * cost) - 1) * sinp;
+        a[12] += rhodv * r3 * cost * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
+        a[13] += rhodv * r3 * cost * (sint * sint) * 2 * sinp * cosp;
+        a[14] += rhodv * r3 * (sint * sint * sint) * cosp * ((cosp * cosp) - 3 * (sinp * sinp));
+        a[15] += rhodv * r3 * (sint * sint * sint) * sinp * (3 * (cosp * cosp) - (sinp * sinp));
+        if (lmax >= 4) {
+            double r4 = r2 * r2, c2 = cost * cost, s2 = sint * sint;
+            double cos2p = (cosp * cosp) - (sinp * sinp), sin2p = 2 * sinp * cosp;
+            double cos3p = cosp * ((cosp * cosp) - 3 * (sinp * sinp));
+            double sin3p = sinp * (3 * (cosp * cosp) - (sinp * sinp));
+            double cos4p = cos2p * cos2p - sin2p * sin2p, sin4p = 2 * sin2p * cos2p;
+            a[16] += rhodv * r4 * (35 * (c2 * c2) - 30 * c2 + 3);
+            a[17] += rhodv * r4 * sint * cost * (7 * c2 - 3) * cosp;
+            a[18] += rhodv * r4 * sint * cost * (7 * c2 - 3) * sinp;
+            a[19] += rhodv * r4 * s2 * (7 * c2 - 1) * cos2p;
+            a[20] += rhodv * r4 * s2 * (7 * c2 - 1) * sin2p;
+            a[21] += rhodv * r4 * s2 * sint * cost * cos3p;
+            a[22] += rhodv * r4 * s2 * sint * cost * sin3p;
+            a[23] += rhodv * r4 * (s2 * s2) * cos4p;
+            a[24] += rhodv * r4 * (s2 * s2) * sin4p;
+        }
+    }
+    for (int m = 0; m < 25; m++) red[m][threadIdx.x] = a[m];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int m = 0; m < 25; m++) red[m][threadIdx.x] = red[m][threadIdx.x] + red[m][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 25) part[(int64_t)b * 25 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// sum of the per-block moments in block order, then the normalisations of
+// sphere.F90:227-242 (and of the l = 4 extension)
+__global__ void k_moments_combine(const double *part, int nbase, double *mom) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a[25];
+    for (int m = 0; m < 25; m++) a[m] = 0.0;
+    for (int b = 0; b < nbase; b++)
+        for (int m = 0; m < 25; m++) a[m] = a[m] + part[(int64_t)b * 25 + m];
+    const double pi = 3.141592653589793;
+    mom[0] = -a[0] / (4.0 * pi);
+    mom[1] = -a[1] / (4.0 * pi);
+    mom[2] = -a[2] / (8.0 * pi);
+    mom[3] = -a[3] / (8.0 * pi);
+    mom[4] = -a[4] / (16.0 * pi);
+    mom[5] = -a[5] / (8.0 * pi) * 3.0;
+    mom[6] = -a[6] / (8.0 * pi) * 3.0;
+    mom[7] = -a[7] / (32.0 * pi) * 3.0;
+    mom[8] = -a[8] / (32.0 * pi) * 3.0;
+    mom[9] = -a[9] / (16.0 * pi);
+    mom[10] = -a[10] / (64.0 * pi) * 3.0;
+    mom[11] = -a[11] / (64.0 * pi) * 3.0;
+    mom[12] = -a[12] / (32.0 * pi) * 15.0;
+    mom[13] = -a[13] / (32.0 * pi) * 15.0;
+    mom[14] = -a[14] / (64.0 * pi) * 5.0;
+    mom[15] = -a[15] / (64.0 * pi) * 5.0;
+    mom[16] = -a[16] / (4.0 * pi) * (1.0 / 64.0);
+    mom[17] = -a[17] / (4.0 * pi) * (5.0 / 8.0);
+    mom[18] = -a[18] / (4.0 * pi) * (5.0 / 8.0);
+    mom[19] = -a[19] / (4.0 * pi) * (5.0 / 16.0);
+    mom[20] = -a[20] / (4.0 * pi) * (5.0 / 16.0);
+    mom[21] = -a[21] / (4.0 * pi) * (35.0 / 8.0);
+    mom[22] = -a[22] / (4.0 * pi) * (35.0 / 8.0);
+    mom[23] = -a[23] / (4.0 * pi) * (35.0 / 64.0);
+    mom[24] = -a[24] / (4.0 * pi) * (35.0 / 64.0);
+}
+
+// U00..U33 (sphere.F90:267-293) and the l = 4 terms
+__device__ __forceinline__ double multipole_eval(const double *m, int lmax, double x, double y, double z) {
+    double r2i = 1 / (x * x + y * y + z * z);
+    double ri = sqrt(r2i);
+    double r3i = r2i * ri;
+    double r4i = r2i * r2i;
+    double rc = sqrt(x * x + y * y);
+    double rci = 1 / rc;
+    double cost = z * ri, sint = rc * ri, cosp = x * rci, sinp = y * rci;
+    double U00 = ri * m[0];
+    double U10 = r2i * cost * m[1];
+    double U11 = r2i * sint * (cosp * m[2] + sinp * m[3]) * 2;
+    double U20 = r3i * (3 * (cost * cost) - 1) * m[4];
+    double U21 = r3i * sint * cost * (cosp * m[5] + sinp * m[6]) * 2;
+    double U22 = r3i * (sint * sint) * (((cosp * cosp) - (sinp * sinp)) * m[7] + 2 * sinp * cosp * m[8]) * 2;
+    double U30 = r4i * cost * (5 * (cost * cost) - 3) * m[9];
+    double U31 = r4i * sint * (5 * (cost * cost) - 1) * (cosp * m[10] + sinp * m[11]) * 2;
+    double U32 = r4i * cost * (sint * sint) * (((cosp * cosp) - (sinp * sinp)) * m[12] + 2 * sinp * cosp * m[13]) * 2;
+    double U33 = r4i * (sint * sint * sint) * (cosp * ((cosp * cosp) - 3 * (sinp * sinp)) * m[14]
+                                              + sinp * (3 * (cosp * cosp) - (sinp * sinp)) * m[15]) * 2;
+    double ub = U00 + U10 + U11 + U20 + U21 + U22 + U30 + U31 + U32 + U33;
+    if (lmax >= 4) {
+        double r5i = r4i * ri, c2 = cost * cost, s2 = sint * sint;
+        double cos2p = (cosp * cosp) - (sinp * sinp), sin2p = 2 * sinp * cosp;
+        double cos3p = cosp * ((cosp * cosp) - 3 * (sinp * sinp));
+        double sin3p = sinp * (3 * (cosp * cosp) - (sinp * sinp));
+        double cos4p = cos2p * cos2p - sin2p * sin2p, sin4p = 2 * sin2p * cos2p;
+        double U40 = r5i * (35 * (c2 * c2) - 30 * c2 + 3) * m[16];
+        double U41 = r5i * sint * cost * (7 * c2 - 3) * (cosp * m[17] + sinp * m[18]);
+        double U42 = r5i * s2 * (7 * c2 - 1) * (cos2p * m[19] + sin2p * m[20]);
+        double U43 = r5i * s2 * sint * cost * (cos3p * m[21] + sin3p * m[22]);
+        double U44 = r5i * (s2 * s2) * (cos4p * m[23] + sin4p * m[24]);
+        ub = ub + U40 + U41 + U42 + U43 + U44;
+    }
+    return ub;
+}
+
+struct OpSphereGhost {       // potential on the first ghost layer of boundary faces
+    double *U; const BFace *faces; const double *mom; const double *x0; const double *h0; const int32_t *level;
+    int n, G; int64_t V; int lmax;
+    __device__ void operator()(int64_t idx) const {
+        const int GT = n + 2;
+        int64_t it = idx / (GT * GT);
+        int r = (int)(idx - it * GT * GT);
+        BFace bf = faces[it];
+        int dir = bf.face >> 1, lr = bf.face & 1, i, j, k;
+        put3(dir, lr == 0 ? -1 : n, r % GT - 1, r / GT - 1, i, j, k);
+        double h = h0[level[bf.b]];
+        const double *xb = x0 + 3 * (int64_t)bf.b;
+        U[(int64_t)bf.b * V + cidx(G, i, j, k)] =
+            multipole_eval(mom, lmax, xb[0] + (double)i * h, xb[1] + (double)j * h, xb[2] + (double)k * h);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// fmg_psi2g (fmg_poisson.F90:4-49) into the caller's layout, and
+// fmg_restore_u (fmg_data_if.F90:275-294)
+// ---------------------------------------------------------------------------
+struct OpPsi2g {
+    double *g; const double *U; const int8_t *skip; const int32_t *level; const double *h0;
+    const int32_t *rslot; const double *rbuf; int n, G, gw; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        const int per = n * n * n;
+        int b = (int)(idx / per);
+        int r = (int)(idx % per);
+        int i = r % n, j = (r / n) % n, k = r / (n * n);
+        const int Gi = n + 2 * gw;
+        const int64_t Vi = (int64_t)Gi * Gi * Gi;
+        int64_t s = ((int64_t)(k + gw) * Gi + (j + gw)) * Gi + (i + gw);
+        double *gx = g + (int64_t)b * 3 * Vi, *gy = gx + Vi, *gz = gy + Vi;
+        double hi = 1.0 / hlev(h0, level[b], 0);
+        const double *ub = U + (int64_t)b * V;
+        if (skip[b]) {
+            gx[s] = -((ub[cidx(G, i + 1, j, k)] - ub[cidx(G, i - 1, j, k)]) * hi * 0.5);
+            gy[s] = -((ub[cidx(G, i, j + 1, k)] - ub[cidx(G, i, j - 1, k)]) * hi * 0.5);
+            gz[s] = -((ub[cidx(G, i, j, k + 1)] - ub[cidx(G, i, j, k - 1)]) * hi * 0.5);
+        } else {
+            Flux<double> F{ub, G, n, hi, rslot, rbuf, b};
+            gx[s] = -((F(0, i, j, k) + F(0, i - 1, j, k)) * 0.5);
+            gy[s] = -((F(1, i, j, k) + F(1, i, j - 1, k)) * 0.5);
+            gz[s] = -((F(2, i, j, k) + F(2, i, j, k - 1)) * 0.5);
+        }
+    }
+};
+struct OpRestore {
+    double *psi; const double *U; int n, G, gw; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        int64_t b = idx / V;
+        int r = (int)(idx % V);
+        int i = r % G - 1, j = (r / G) % G - 1, k = r / (G * G) - 1;
+        const int Gi = n + 2 * gw;
+        psi[b * (int64_t)Gi * Gi * Gi + ((int64_t)(k + gw) * Gi + (j + gw)) * Gi + (i + gw)] = U[idx];
+    }
+};
+
+// ---------------------------------------------------------------------------
+// vmg_tau_crop (vmg.F90:463-505): zero the parent's boundary plane behind
+// every face of a child whose neighbour is one level up
+// ---------------------------------------------------------------------------
+template <class T>
+struct OpTauCrop {
+    T *tau; const BFace *faces; const int32_t *parent; int n, G; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        const int GT = n + 2;
+        int64_t it = idx / (GT * GT);
+        int r = (int)(idx - it * GT * GT);
+        BFace bf = faces[it];
+        int dir = bf.face >> 1, lr = bf.face & 1, i, j, k;
+        put3(dir, lr == 0 ? 0 : n - 1, r % GT - 1, r / GT - 1, i, j, k);
+        tau[(int64_t)parent[bf.b] * V + cidx(G, i, j, k)] = (T)0;
+    }
+};
+
+// tau on fine blocks: 0 everywhere, -(div F)/h inside (vmg_poisson.F90:18-35)
+template <class T>
+struct OpTauFine {
+    T *tau; const T *u; int first, n, G; int64_t V; T hi;
+    __device__ void operator()(int64_t idx) const {
+        int b = first + (int)(idx / V);
+        int r = (int)(idx % V);
+        int i = r % G - 1, j = (r / G) % G - 1, k = r / (G * G) - 1;
+        T v = (T)0;
+        if (i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n) {
+            Flux<T> F{u + (int64_t)b * V, G, n, hi, nullptr, nullptr, b};
+            v = -(F.div(i, j, k) * hi);
+        }
+        tau[(int64_t)b * V + r] = v;
+    }
+};
+// tau += (div F)/h on parents with children (vmg_poisson.F90:40-57)
+template <class T>
+struct OpTauParent {
+    T *tau; const T *u; const int32_t *blocks; int n, G; int64_t V; T hi;
+    __device__ void operator()(int64_t idx) const {
+        const int per = n * n * n;
+        int b = blocks[idx / per];
+        int r = (int)(idx % per);
+        int i = r % n, j = (r / n) % n, k = r / (n * n);
+        Flux<T> F{u + (int64_t)b * V, G, n, hi, nullptr, nullptr, b};
+        int64_t c = (int64_t)b * V + cidx(G, i, j, k);
+        tau[c] = tau[c] + F.div(i, j, k) * hi;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// base grid <-> base blocks (mg_dataPrepare / mg_dataRestore,
+// mg_data.F90:179-330)
+// ---------------------------------------------------------------------------
+template <class T>
+struct OpMgGather {
+    double *S, *P; const T *rhs, *u; const int32_t *baseIdx; int ngb0, ngb1, n, G, N; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        int N3 = N;   // cells per base-grid edge
+        int I = (int)(idx % N3), J = (int)((idx / N3) % N3), K = (int)(idx / ((int64_t)N3 * N3));
+        int ib = I / n, jb = J / n, kb = K / n;
+        int b = baseIdx[((int64_t)kb * ngb1 + jb) * ngb0 + ib];
+        int64_t c = (int64_t)b * V + cidx(G, I - ib * n, J - jb * n, K - kb * n);
+        int64_t m = cidx(N + 2, I, J, K);
+        S[m] = (double)rhs[c];
+        P[m] = (double)u[c];
+    }
+};
+template <class T>
+struct OpMgScatter {
+    T *u; const double *P; const int32_t *baseIdx; int ngb0, ngb1, n, G, N; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        int I = (int)(idx % N), J = (int)((idx / N) % N), K = (int)(idx / ((int64_t)N * N));
+        int ib = I / n, jb = J / n, kb = K / n;
+        int b = baseIdx[((int64_t)kb * ngb1 + jb) * ngb0 + ib];
+        u[(int64_t)b * V + cidx(G, I - ib * n, J - jb * n, K - kb * n)] = (T)P[cidx(N + 2, I, J, K)];
+    }
+};
+
+}  // namespace sfm

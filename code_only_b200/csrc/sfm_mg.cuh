@@ -1,0 +1,224 @@
+// sfm_mg.cuh -- the uniform base-grid multigrid (mg.F90, mg_poisson.F90,
+// mg_interpol_cubic.F90) as one persistent CTA.
+//
+// The reference gathers the base level to rank 0 and runs mg_cycle there
+// serially (vmg.F90:407-428, mg_data.F90:179-330).  Here the whole cycle
+// (<= 10 defect corrections of an FMG with Ncycle 2, 2/2 smoothing) runs in
+// one CTA of 1024 threads on a base grid of at most 64^3 cells, its levels
+// resident in global memory (L2), every operation separated by
+// __syncthreads; nothing returns to the host.  FP64 throughout (the
+// coarsest-level solve stays in FP64 in the mixed-precision path).
+#pragma once
+#include "sfm_device.cuh"
+
+namespace sfm {
+
+constexpr int MG_MAXLEV = 8;
+
+struct MgData {
+    double *U[MG_MAXLEV], *RES[MG_MAXLEV], *RHS[MG_MAXLEV], *RHO[MG_MAXLEV];
+    double *SRC, *PSI;   // level 0 only
+    int N;               // cells per edge on level 0
+    int MMax;            // coarsest level (1 cell)
+    double hbase;        // cell width on level 0 (fmg_get_h(Lmin, FMG_LevelMax))
+    int periodic;        // mg_boundary_u wraps (periodic module) or is a no-op (sphere)
+    int touch[6];        // TouchBoundary of the base grid (mg_data.F90:77-83)
+};
+
+__device__ __forceinline__ int mgN(const MgData &d, int m) { return d.N >> m; }
+__device__ __forceinline__ double mgH(const MgData &d, int m) { return d.hbase * (double)(1 << m); }
+
+__device__ double mg_block_max(double v, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+        double t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = t > v ? t : v;
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = sh[w] > m ? sh[w] : m;
+    __syncthreads();
+    return m;
+}
+
+// periodic wrap of one ghost layer, x then y then z
+// (fmg_boundary_phys_periodic.F90:71-104)
+__device__ void mg_boundary_u(const MgData &d, int m, double *a) {
+    if (!d.periodic) return;
+    const int n = mgN(d, m), G = n + 2;
+    for (int dir = 0; dir < 3; dir++) {
+        for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
+            int p = t % G - 1, q = t / G - 1, i, j, k, is, js, ks;
+            put3(dir, -1, p, q, i, j, k); put3(dir, n - 1, p, q, is, js, ks);
+            a[cidx(G, i, j, k)] = a[cidx(G, is, js, ks)];
+            put3(dir, n, p, q, i, j, k); put3(dir, 0, p, q, is, js, ks);
+            a[cidx(G, i, j, k)] = a[cidx(G, is, js, ks)];
+        }
+        __syncthreads();
+    }
+}
+__device__ void mg_boundary_fill0(const MgData &d, int m, double *a) {   // mg.F90:735-750
+    const int n = mgN(d, m), G = n + 2;
+    for (int f = 0; f < 6; f++) {
+        if (!d.touch[f]) continue;
+        for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
+            int i, j, k;
+            put3(f >> 1, (f & 1) ? n : -1, t % G - 1, t / G - 1, i, j, k);
+            a[cidx(G, i, j, k)] = 0.0;
+        }
+    }
+    __syncthreads();
+}
+__device__ void mg_boundary_extrap(const MgData &d, int m, double *a) {  // mg.F90:754-771
+    const int n = mgN(d, m), G = n + 2;
+    for (int dir = 0; dir < 3; dir++) {
+        for (int lr = 0; lr < 2; lr++) {
+            if (!d.touch[lr + 2 * dir]) continue;
+            for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
+                int i, j, k, ii, jj, kk;
+                put3(dir, lr ? n : -1, t % G - 1, t / G - 1, i, j, k);
+                put3(dir, lr ? n - 1 : 0, t % G - 1, t / G - 1, ii, jj, kk);
+                a[cidx(G, i, j, k)] = -a[cidx(G, ii, jj, kk)];
+            }
+        }
+        __syncthreads();
+    }
+}
+__device__ __forceinline__ double mg_lap_sum(const double *u, int G, int i, int j, int k) {
+    double s = u[cidx(G, i + 1, j, k)] + u[cidx(G, i - 1, j, k)];
+    s = s + u[cidx(G, i, j + 1, k)];
+    s = s + u[cidx(G, i, j - 1, k)];
+    s = s + u[cidx(G, i, j, k + 1)];
+    s = s + u[cidx(G, i, j, k - 1)];
+    s = s - 6.0 * u[cidx(G, i, j, k)];
+    return s;
+}
+__device__ void mg_resid(const MgData &d, int m, double *res, double *u, const double *rhs) {   // mg_poisson.F90:5-28
+    const int n = mgN(d, m), G = n + 2;
+    double hh = mgH(d, m);
+    double h2i = 1.0 / (hh * hh);
+    mg_boundary_u(d, m, u);
+    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
+        int i = c % n, j = (c / n) % n, k = c / (n * n);
+        res[cidx(G, i, j, k)] = -h2i * mg_lap_sum(u, G, i, j, k) + rhs[cidx(G, i, j, k)];
+    }
+    __syncthreads();
+}
+// returns Resmaxg = max|resh2| / h^2 over both colours (mg_poisson.F90:32-79)
+__device__ double mg_relax(const MgData &d, int m, double *u, const double *rhs, double *sh) {
+    const int n = mgN(d, m), G = n + 2;
+    double hh = mgH(d, m), h2 = hh * hh, rm = 0.0;
+    const int half = (n * n * n + 1) / 2;
+    for (int ipass = 1; ipass <= 2; ipass++) {
+        mg_boundary_u(d, m, u);
+        for (int c = threadIdx.x; c < half; c += blockDim.x) {
+            int i2, j, k, i;
+            if (n == 1) { if (((ipass) & 1) != 0) continue; i = 0; j = 0; k = 0; }
+            else {
+                int hn = n / 2;
+                i2 = c % hn; j = (c / hn) % n; k = c / (hn * n);
+                i = 2 * i2 + ((j + k + ipass) & 1);
+            }
+            double resh2 = mg_lap_sum(u, G, i, j, k) - h2 * rhs[cidx(G, i, j, k)];
+            u[cidx(G, i, j, k)] = u[cidx(G, i, j, k)] + (1.0 / 6.0) * resh2;
+            double a = fabs(resh2);
+            rm = a > rm ? a : rm;
+        }
+        __syncthreads();
+    }
+    return mg_block_max(rm, sh) / h2;
+}
+__device__ void mg_rstrct(const MgData &d, int m, double *uc, const double *uf) {   // linear (mg.F90:581-602)
+    const int n = mgN(d, m), G = n + 2, Gf = 2 * n + 2;
+    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
+        int i = c % n, j = (c / n) % n, k = c / (n * n);
+        uc[cidx(G, i, j, k)] = rstrct_linear(uf, Gf, 2 * i, 2 * j, 2 * k);
+    }
+    __syncthreads();
+}
+__device__ void mg_interp(const MgData &d, int m, double *uf, double *uc, bool cubic) {   // mg.F90:608-633
+    const int lc = m + 1, n = mgN(d, m), G = n + 2, nc = mgN(d, lc), Gc = nc + 2;
+    mg_boundary_extrap(d, lc, uc);
+    mg_boundary_u(d, lc, uc);
+    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
+        int i = c % n, j = (c / n) % n, k = c / (n * n);
+        uf[cidx(G, i, j, k)] = (cubic && nc + 2 >= 4) ? tricubic_cell(uc, Gc, i, j, k, -1, nc)
+                                                      : trilinear_cell(uc, Gc, i, j, k, 0, 0, 0);
+    }
+    __syncthreads();
+    mg_boundary_fill0(d, m, uf);
+    mg_boundary_fill0(d, lc, uc);
+    mg_boundary_u(d, m, uf);
+    mg_boundary_u(d, lc, uc);
+}
+__device__ void mg_fill0(const MgData &d, int m, double *a) {
+    const int G = mgN(d, m) + 2;
+    for (int c = threadIdx.x; c < G * G * G; c += blockDim.x) a[c] = 0.0;
+    __syncthreads();
+}
+__device__ void mg_copy(const MgData &d, int m, double *o, const double *a) {
+    const int G = mgN(d, m) + 2;
+    for (int c = threadIdx.x; c < G * G * G; c += blockDim.x) o[c] = a[c];
+    __syncthreads();
+}
+__device__ void mg_addw(const MgData &d, int m, double *a, const double *da) {
+    const int G = mgN(d, m) + 2;
+    for (int c = threadIdx.x; c < G * G * G; c += blockDim.x) a[c] = a[c] + da[c];
+    __syncthreads();
+}
+
+// mg_lin (mg.F90:106-218); returns the last Resmaxg
+__device__ double mg_lin(const MgData &d, double *sh) {
+    double res = 0.0;
+    for (int m = 1; m <= d.MMax; m++) mg_rstrct(d, m, d.RHO[m], d.RHO[m - 1]);
+    mg_fill0(d, d.MMax, d.U[d.MMax]);
+    for (int q = 0; q < 2; q++) res = mg_relax(d, d.MMax, d.U[d.MMax], d.RHO[d.MMax], sh);
+    for (int m = d.MMax - 1; m >= 0; m--) {
+        mg_interp(d, m, d.U[m], d.U[m + 1], true);
+        mg_copy(d, m, d.RHS[m], d.RHO[m]);
+        for (int jc = 1; jc <= 2; jc++) {
+            for (int v = m; v <= d.MMax - 1; v++) {
+                for (int q = 0; q < 2; q++) res = mg_relax(d, v, d.U[v], d.RHS[v], sh);
+                mg_resid(d, v, d.RES[v], d.U[v], d.RHS[v]);
+                mg_rstrct(d, v + 1, d.RHS[v + 1], d.RES[v]);
+                mg_fill0(d, v + 1, d.U[v + 1]);
+            }
+            for (int q = 0; q < 2; q++) res = mg_relax(d, d.MMax, d.U[d.MMax], d.RHS[d.MMax], sh);
+            for (int v = d.MMax - 1; v >= m; v--) {
+                mg_interp(d, v, d.RES[v], d.U[v + 1], false);
+                mg_addw(d, v, d.U[v], d.RES[v]);
+                for (int q = 0; q < 2; q++) res = mg_relax(d, v, d.U[v], d.RHS[v], sh);
+            }
+        }
+    }
+    return res;
+}
+
+// mg_cycle (mg.F90:42-94) with ju = PSI, jrho = SRC; one CTA
+__global__ void __launch_bounds__(1024) k_mg_cycle(MgData d, int *iters_out) {
+    __shared__ double sh[32];
+    const double errmax = (double)1.e-2f;   // default-real literal (mg.F90:50)
+    mg_boundary_fill0(d, 0, d.PSI);
+    mg_boundary_u(d, 0, d.PSI);
+    double rhomax = 0.0;
+    int it;
+    for (it = 1; it <= 10; it++) {
+        mg_resid(d, 0, d.RHO[0], d.PSI, d.SRC);
+        if (it == 1) {
+            const int n = d.N, G = n + 2;
+            double v = 0.0;
+            for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
+                double a = fabs(d.RHO[0][cidx(G, c % n, (c / n) % n, c / (n * n))]);
+                v = a > v ? a : v;
+            }
+            rhomax = mg_block_max(v, sh);
+        }
+        double res = mg_lin(d, sh);
+        mg_addw(d, 0, d.PSI, d.U[0]);
+        if (res / rhomax < errmax) break;
+    }
+    if (threadIdx.x == 0 && iters_out) *iters_out = it > 10 ? 10 : it;
+}
+
+}  // namespace sfm

@@ -1,0 +1,1020 @@
+// sfm_solver.cu -- host driver of the B200 FMG Poisson solve and the C ABI
+// of include/sfmg.h.
+//
+// The driver issues, in the reference's order, one batched kernel per
+// operation of fmg_cycle / fmg_lin / vmg_fas (fmg.F90:134-377, vmg.F90:116-243):
+// every block of a level (or of all levels) is updated by one launch driven
+// from device-resident block, face and reflux tables; the base-grid solve
+// (mg.F90:42-218) is one persistent CTA.  All fields of all levels stay in
+// HBM for the whole solve and across calls.
+//
+// Precision: Solver<double> is the plain FP64 path (bit-identical
+// expressions to the reference's); Solver<float> runs fmg_lin and vmg_fas in
+// FP32 inside the FP64 defect-correction loop, with the outer residual, the
+// accumulation into phi, the reflux flux sums and the base-grid solve in FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/sfmg.h"
+#include "sfm_device.cuh"
+#include "sfm_kernels_misc.cuh"
+#include "sfm_mg.cuh"
+
+namespace sfm {
+
+constexpr int Undef = -1;
+
+// ---------------------------------------------------------------------------
+// host copy of the hierarchy, links and invariants
+// (fmg_make_linklist fmg_data_if.F90:298-411, fmg_check_linklist :415-568)
+// ---------------------------------------------------------------------------
+struct HostHier {
+    int nb = 0, nlev = 0, NI = 0, FMax = 0, ngb[3] = {0, 0, 0};
+    std::vector<int> lstart, level, parent, child, nbr, nbrGid, baseIdx;
+    std::vector<int8_t> oct, touch, sameLev, parLev, skip;
+    std::vector<double> h0, x0;
+
+    int build(const sfm_hier_desc *hd) {
+        nb = hd->nblocks; nlev = hd->nlev; NI = hd->ni;
+        if (nb <= 0 || nlev <= 0 || nlev > 30) return SFM_EINVAL;
+        if (NI < 4 || (NI & (NI - 1)) || hd->nj != NI || hd->nk != NI || NI > 64) return SFM_EINVAL;
+        if (!hd->level || !hd->ijk || !hd->parent || !hd->child || !hd->nbr || !hd->touch || !hd->cellwidth || !hd->x0)
+            return SFM_EINVAL;
+        for (int d = 0; d < 3; d++) { ngb[d] = hd->ngb[d]; if (ngb[d] <= 0) return SFM_EINVAL; }
+        FMax = 0; while ((2 << FMax) < NI) FMax++;
+        level.assign(hd->level, hd->level + nb);
+        parent.assign(hd->parent, hd->parent + nb);
+        child.assign(hd->child, hd->child + 8 * (size_t)nb);
+        nbr.assign(hd->nbr, hd->nbr + 6 * (size_t)nb);
+        touch.resize(6 * (size_t)nb);
+        for (size_t i = 0; i < touch.size(); i++) touch[i] = hd->touch[i] ? 1 : 0;
+        h0.assign(hd->cellwidth, hd->cellwidth + nlev);
+        x0.assign(hd->x0, hd->x0 + 3 * (size_t)nb);
+        for (double v : h0) if (!(v > 0) || !std::isfinite(v)) return SFM_EINVAL;
+        for (double v : x0) if (!std::isfinite(v)) return SFM_EINVAL;
+        lstart.assign(nlev + 1, 0);
+        for (int b = 0; b < nb; b++) {
+            if (level[b] < 0 || level[b] >= nlev) return SFM_EHIER;
+            if (b > 0 && level[b] < level[b - 1]) return SFM_EHIER;
+            lstart[level[b] + 1]++;
+        }
+        for (int L = 0; L < nlev; L++) {
+            lstart[L + 1] += lstart[L];
+            if (lstart[L + 1] == lstart[L]) return SFM_EHIER;   // every level populated
+        }
+        for (int v : parent) if (v < -1 || v >= nb) return SFM_EHIER;
+        for (int v : child) if (v < -1 || v >= nb) return SFM_EHIER;
+        for (int v : nbr) if (v < -1 || v >= nb) return SFM_EHIER;
+        // same-level and parent-level links
+        nbrGid.assign(6 * (size_t)nb, Undef);
+        sameLev.assign(6 * (size_t)nb, 0);
+        parLev.assign(6 * (size_t)nb, 0);
+        for (int b = 0; b < nb; b++)
+            for (int f = 0; f < 6; f++)
+                if (nbr[6 * b + f] != Undef) { nbrGid[6 * b + f] = nbr[6 * b + f]; sameLev[6 * b + f] = 1; }
+        for (int L = 1; L < nlev; L++)
+            for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+                int p = parent[b];
+                if (p < 0) return SFM_EHIER;
+                for (int f = 0; f < 6; f++) {
+                    if (sameLev[6 * b + f]) continue;
+                    int np = nbrGid[6 * p + f];
+                    if (np == Undef) continue;
+                    nbrGid[6 * b + f] = np;
+                    parLev[6 * b + f] = 1;
+                }
+            }
+        oct.assign(3 * (size_t)nb, 0);
+        for (int b = 0; b < nb; b++) {
+            if (level[b] == 0) { if (parent[b] != Undef) return SFM_EHIER; continue; }
+            int p = parent[b], found = 0;
+            for (int c = 0; c < 8; c++)
+                if (child[8 * p + c] == b) {
+                    oct[3 * b] = c & 1; oct[3 * b + 1] = (c >> 1) & 1; oct[3 * b + 2] = (c >> 2) & 1;
+                    found++;
+                }
+            if (found != 1) return SFM_EHIER;
+        }
+        // invariants
+        for (int b = 0; b < nb; b++) {
+            int L = level[b];
+            if (L > 0 && level[parent[b]] != L - 1) return SFM_EHIER;
+            if (child[8 * b] != Undef) {
+                if (L == nlev - 1) return SFM_EHIER;
+                for (int c = 0; c < 8; c++) {
+                    int cb = child[8 * b + c];
+                    if (cb < 0 || parent[cb] != b || level[cb] != L + 1) return SFM_EHIER;
+                }
+            } else {
+                for (int c = 1; c < 8; c++) if (child[8 * b + c] != Undef) return SFM_EHIER;
+            }
+            for (int f = 0; f < 6; f++) {
+                int nbb = nbrGid[6 * b + f];
+                if (sameLev[6 * b + f]) {
+                    int fs = (f ^ 1);
+                    if (level[nbb] != L || nbr[6 * nbb + fs] != b) return SFM_EHIER;
+                    if (touch[6 * b + f]) return SFM_EHIER;
+                }
+                if (parLev[6 * b + f] && level[nbb] != L - 1) return SFM_EHIER;
+                if ((int)sameLev[6 * b + f] + (int)parLev[6 * b + f] + (int)touch[6 * b + f] != 1) return SFM_EHIER;
+            }
+        }
+        skip.assign(nb, 0);
+        for (int b = 0; b < nb; b++) skip[b] = (level[b] != nlev - 1 && child[8 * b] != Undef) ? 1 : 0;
+        baseIdx.assign((size_t)ngb[0] * ngb[1] * ngb[2], -1);
+        if (lstart[1] != ngb[0] * ngb[1] * ngb[2]) return SFM_EHIER;
+        for (int b = lstart[0]; b < lstart[1]; b++) {
+            int i = hd->ijk[3 * b], j = hd->ijk[3 * b + 1], k = hd->ijk[3 * b + 2];
+            if (i < 0 || j < 0 || k < 0 || i >= ngb[0] || j >= ngb[1] || k >= ngb[2]) return SFM_EHIER;
+            int &slot = baseIdx[((size_t)k * ngb[1] + j) * ngb[0] + i];
+            if (slot != -1) return SFM_EHIER;
+            slot = b;
+        }
+        return SFM_OK;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// device memory bookkeeping
+// ---------------------------------------------------------------------------
+struct DevMem {
+    std::vector<void *> ptrs;
+    int64_t bytes = 0;
+    cudaError_t err = cudaSuccess;
+    template <class T>
+    T *alloc(size_t count) {
+        if (count == 0) count = 1;
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) { err = e; return nullptr; }
+        ptrs.push_back(p);
+        bytes += (int64_t)(count * sizeof(T));
+        return (T *)p;
+    }
+    template <class T>
+    T *upload(const std::vector<T> &v) {
+        T *p = alloc<T>(v.size());
+        if (p && !v.empty()) {
+            cudaError_t e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) err = e;
+        }
+        return p;
+    }
+    void release() {
+        for (void *p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+};
+
+struct Field {     // one element type, one fmg level, all blocks
+    void *p = nullptr; int n = 0, G = 0; int64_t V = 0;
+};
+
+class SolverBase {
+public:
+    virtual ~SolverBase() {}
+    virtual int solve(const double *rho, double *psi, double *g, sfm_stats *st, cudaStream_t s, int stop_stage,
+                      double *dump) = 0;
+    virtual int64_t device_bytes() const = 0;
+    virtual int fmg_levels() const = 0;
+    std::string last_error;
+};
+
+template <class T>
+class Solver : public SolverBase {
+public:
+    HostHier H;
+    sfm_params P;
+    DevMem mem;
+    cudaStream_t own_ = nullptr;   // the context's stream
+    cudaStream_t st_ = nullptr;    // stream of the current call (caller's or own_)
+    int64_t launches = 0;
+    int maxBlocks = 148 * 16;
+
+    // device tables
+    int32_t *d_level = nullptr, *d_parent = nullptr, *d_rslot = nullptr, *d_all = nullptr, *d_leaves = nullptr;
+    int32_t *d_withChild = nullptr, *d_baseIdx = nullptr;
+    int8_t *d_oct = nullptr, *d_skip = nullptr;
+    double *d_h0 = nullptr, *d_x0 = nullptr;
+    FaceItem *d_faces = nullptr;
+    RefluxItem *d_reflux = nullptr;
+    BFace *d_tfL = nullptr, *d_tfDL = nullptr, *d_crop = nullptr;
+    std::vector<int64_t> faceOff, tfLOff, tfDLOff, cropOff, wcOff;
+    int nLeaves = 0, nReflux = 0, nSlots = 0;
+    std::vector<int> leafList;
+
+    // fields: inner precision T at every fmg level, FP64 outer fields at level 0
+    std::vector<T *> U, RES, RHS, RHO;
+    T *RUF = nullptr;
+    double *SRC0 = nullptr, *PSI0 = nullptr, *PHI0 = nullptr, *RES0d = nullptr;
+    std::vector<double *> rbuf;
+    std::vector<int> nf, Gf;
+    std::vector<int64_t> Vf;
+    // scalars
+    unsigned long long *d_max = nullptr;   // [8]
+    double *d_scal = nullptr;              // [8]
+    int *d_bad = nullptr;
+    double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
+    int *d_mgit = nullptr;
+    // base grid
+    MgData mg;
+    bool useSerialMg = false;
+    int NBc = 0;
+    std::vector<std::pair<void *, size_t>> zeroList;   // re-zeroed at every solve
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    int FmgLevel_fill0 = Undef;
+
+    ~Solver() override {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_) cudaStreamDestroy(own_);
+        mem.release();
+    }
+    int64_t device_bytes() const override { return mem.bytes; }
+    int fmg_levels() const override { return H.FMax + 1; }
+
+    // -----------------------------------------------------------------
+    int init(const sfm_hier_desc *hd, const sfm_params *p) {
+        int rc = H.build(hd);
+        if (rc) return rc;
+        P = *p;
+        if (cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking) != cudaSuccess) return SFM_ECUDA;
+        st_ = own_;
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        const int nb = H.nb, nlev = H.nlev, FMax = H.FMax;
+        // ---- tables
+        std::vector<int32_t> all(nb);
+        for (int b = 0; b < nb; b++) all[b] = b;
+        for (int b = 0; b < nb; b++) if (!H.skip[b]) leafList.push_back(b);
+        nLeaves = (int)leafList.size();
+        std::vector<int32_t> withChild;
+        wcOff.assign(nlev + 1, 0);
+        for (int L = 0; L < nlev; L++) {
+            wcOff[L] = (int64_t)withChild.size();
+            for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++) if (H.child[8 * b] != Undef) withChild.push_back(b);
+        }
+        wcOff[nlev] = (int64_t)withChild.size();
+        // ghost pass faces per (level, dir)
+        std::vector<FaceItem> faces;
+        faceOff.assign(nlev * 3 + 1, 0);
+        for (int L = 0; L < nlev; L++)
+            for (int dir = 0; dir < 3; dir++) {
+                faceOff[L * 3 + dir] = (int64_t)faces.size();
+                for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                    for (int lr = 0; lr < 2; lr++) {
+                        int f = lr + 2 * dir;
+                        if (!H.sameLev[6 * b + f] && !(L > 0 && H.parLev[6 * b + f])) continue;
+                        FaceItem it;
+                        it.dst = b; it.src = H.nbrGid[6 * b + f]; it.lr = (int8_t)lr;
+                        it.type = H.sameLev[6 * b + f] ? 0 : 1;
+                        it.oa = H.oct[3 * b + tra(dir)]; it.ob = H.oct[3 * b + trb(dir)];
+                        faces.push_back(it);
+                    }
+            }
+        faceOff[nlev * 3] = (int64_t)faces.size();
+        // reflux: coarse faces covered by finer blocks get a slot
+        std::vector<int32_t> rslot(6 * (size_t)nb, -1);
+        std::vector<RefluxItem> refl;
+        for (int L = 1; L < nlev; L++)
+            for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                for (int dir = 0; dir < 3; dir++)
+                    for (int lr = 0; lr < 2; lr++) {
+                        int f = lr + 2 * dir;
+                        if (!H.parLev[6 * b + f]) continue;
+                        int cb = H.nbrGid[6 * b + f];
+                        int cf = (1 - lr) + 2 * dir;   // the coarse block's face
+                        if (rslot[6 * cb + cf] < 0) rslot[6 * cb + cf] = nSlots++;
+                        RefluxItem it;
+                        it.fine = b; it.slot = rslot[6 * cb + cf]; it.dir = (int8_t)dir; it.lr = (int8_t)lr;
+                        it.oa = H.oct[3 * b + tra(dir)]; it.ob = H.oct[3 * b + trb(dir)];
+                        refl.push_back(it);
+                    }
+        nReflux = (int)refl.size();
+        // physical-boundary faces, by level then dir, and by dir then level
+        std::vector<BFace> tfL, tfDL;
+        tfLOff.assign(nlev + 1, 0);
+        for (int L = 0; L < nlev; L++) {
+            tfLOff[L] = (int64_t)tfL.size();
+            for (int dir = 0; dir < 3; dir++)
+                for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                    for (int lr = 0; lr < 2; lr++)
+                        if (H.touch[6 * b + lr + 2 * dir]) { BFace x{}; x.b = b; x.face = (int8_t)(lr + 2 * dir); tfL.push_back(x); }
+        }
+        tfLOff[nlev] = (int64_t)tfL.size();
+        tfDLOff.assign(3 * nlev + 1, 0);
+        for (int dir = 0; dir < 3; dir++)
+            for (int L = 0; L < nlev; L++) {
+                tfDLOff[dir * nlev + L] = (int64_t)tfDL.size();
+                for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                    for (int lr = 0; lr < 2; lr++)
+                        if (H.touch[6 * b + lr + 2 * dir]) { BFace x{}; x.b = b; x.face = (int8_t)(lr + 2 * dir); tfDL.push_back(x); }
+            }
+        tfDLOff[3 * nlev] = (int64_t)tfDL.size();
+        // tau crop faces per child level
+        std::vector<BFace> crop;
+        cropOff.assign(nlev + 1, 0);
+        for (int L = 0; L < nlev; L++) {
+            cropOff[L] = (int64_t)crop.size();
+            if (L == 0) continue;
+            for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                for (int f = 0; f < 6; f++)
+                    if (H.parLev[6 * b + f]) { BFace x{}; x.b = b; x.face = (int8_t)f; crop.push_back(x); }
+        }
+        cropOff[nlev] = (int64_t)crop.size();
+
+        d_level = mem.upload(std::vector<int32_t>(H.level.begin(), H.level.end()));
+        d_parent = mem.upload(std::vector<int32_t>(H.parent.begin(), H.parent.end()));
+        d_oct = mem.upload(H.oct);
+        d_skip = mem.upload(H.skip);
+        d_rslot = mem.upload(rslot);
+        d_h0 = mem.upload(H.h0);
+        d_x0 = mem.upload(H.x0);
+        d_all = mem.upload(all);
+        d_leaves = mem.upload(std::vector<int32_t>(leafList.begin(), leafList.end()));
+        d_withChild = mem.upload(withChild);
+        d_faces = mem.upload(faces);
+        d_reflux = mem.upload(refl);
+        d_tfL = mem.upload(tfL);
+        d_tfDL = mem.upload(tfDL);
+        d_crop = mem.upload(crop);
+        d_baseIdx = mem.upload(std::vector<int32_t>(H.baseIdx.begin(), H.baseIdx.end()));
+        // ---- fields
+        nf.resize(FMax + 1); Gf.resize(FMax + 1); Vf.resize(FMax + 1);
+        for (int f = 0; f <= FMax; f++) { nf[f] = H.NI >> f; Gf[f] = nf[f] + 2; Vf[f] = (int64_t)Gf[f] * Gf[f] * Gf[f]; }
+        auto fieldT = [&](int f) { T *p = mem.alloc<T>((size_t)nb * Vf[f]); zeroList.push_back({p, (size_t)nb * Vf[f] * sizeof(T)}); return p; };
+        auto fieldD = [&](int f) { double *p = mem.alloc<double>((size_t)nb * Vf[f]); zeroList.push_back({p, (size_t)nb * Vf[f] * sizeof(double)}); return p; };
+        for (int f = 0; f <= FMax; f++) {
+            U.push_back(fieldT(f)); RES.push_back(fieldT(f)); RHS.push_back(fieldT(f)); RHO.push_back(fieldT(f));
+            rbuf.push_back(mem.alloc<double>((size_t)std::max(nSlots, 1) * nf[f] * nf[f]));
+        }
+        RUF = fieldT(FMax);
+        SRC0 = fieldD(0); PSI0 = fieldD(0); PHI0 = fieldD(0); RES0d = fieldD(0);
+        d_max = mem.alloc<unsigned long long>(8);
+        d_scal = mem.alloc<double>(8);
+        d_bad = mem.alloc<int>(1);
+        d_mom = mem.alloc<double>(32);
+        d_part = mem.alloc<double>((size_t)(H.lstart[1]) * 25);
+        d_psum = mem.alloc<double>((size_t)nb);
+        d_mgit = mem.alloc<int>(1);
+        // ---- base grid (mg_data_init, mg_data.F90:45-90)
+        auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+        int NBx = (H.ngb[0] * H.NI) >> FMax, NBy = (H.ngb[1] * H.NI) >> FMax, NBz = (H.ngb[2] * H.NI) >> FMax;
+        useSerialMg = pow2(H.ngb[0]) && pow2(H.ngb[1]) && pow2(H.ngb[2]) && NBx == NBy && NBy == NBz;
+        std::memset(&mg, 0, sizeof(mg));
+        if (useSerialMg) {
+            NBc = NBx;
+            int MMax = 0; while ((1 << MMax) < NBc) MMax++;
+            if (MMax + 1 > MG_MAXLEV) return SFM_ESIZE;
+            mg.N = NBc; mg.MMax = MMax;
+            mg.hbase = hlev(H.h0.data(), 0, FMax);
+            mg.periodic = P.bc == SFM_BC_PERIODIC ? 1 : 0;
+            for (int f = 0; f < 6; f++) {
+                mg.touch[f] = 0;
+                for (int b = H.lstart[0]; b < H.lstart[1]; b++) mg.touch[f] |= H.touch[6 * b + f];
+            }
+            for (int m = 0; m <= MMax; m++) {
+                size_t G = (size_t)(NBc >> m) + 2, V = G * G * G;
+                mg.U[m] = mem.alloc<double>(V); mg.RES[m] = mem.alloc<double>(V);
+                mg.RHS[m] = mem.alloc<double>(V); mg.RHO[m] = mem.alloc<double>(V);
+                for (double *q : {mg.U[m], mg.RES[m], mg.RHS[m], mg.RHO[m]}) zeroList.push_back({q, V * sizeof(double)});
+            }
+            size_t G0 = (size_t)NBc + 2, V0 = G0 * G0 * G0;
+            mg.SRC = mem.alloc<double>(V0); mg.PSI = mem.alloc<double>(V0);
+            zeroList.push_back({mg.SRC, V0 * sizeof(double)});
+            zeroList.push_back({mg.PSI, V0 * sizeof(double)});
+        }
+        if (mem.err != cudaSuccess) {
+            last_error = cudaGetErrorString(mem.err);
+            return mem.err == cudaErrorMemoryAllocation ? SFM_ENOMEM : SFM_ECUDA;
+        }
+        return SFM_OK;
+    }
+
+    // -----------------------------------------------------------------
+    // launch helpers
+    template <class Op>
+    void run(const Op &op, int64_t n) {
+        if (n <= 0) return;
+        int64_t blocks = (n + 255) / 256;
+        if (blocks > maxBlocks) blocks = maxBlocks;
+        k_apply<Op><<<(unsigned)blocks, 256, 0, st_>>>(op, n);
+        ++launches;
+    }
+    template <class Op>
+    void runMax(const Op &op, int64_t n, unsigned long long *out) {
+        if (n <= 0) return;
+        int64_t blocks = (n + 255) / 256;
+        if (blocks > maxBlocks) blocks = maxBlocks;
+        k_apply_max<Op><<<(unsigned)blocks, 256, 0, st_>>>(op, n, out);
+        ++launches;
+    }
+    int cnt(int L) const { return H.lstart[L + 1] - H.lstart[L]; }
+
+    // -----------------------------------------------------------------
+    // ghost cells, convergence, boundary (any element type)
+    template <class TT>
+    void ghostcell_fix(int f, TT *u, bool cubic) {
+        for (int L = 0; L < H.nlev; L++)
+            for (int dir = 0; dir < 3; dir++) ghost_pass(L, f, dir, u, cubic);
+    }
+    template <class TT>
+    void ghost_pass(int L, int f, int dir, TT *u, bool cubic) {   // parentlev + samelev of (L, dir)
+        int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
+        if (c <= 0) return;
+        int GT = nf[f] + 2;
+        run(OpGhostPass<TT>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, -1}, c * GT * GT);
+    }
+    template <class TT>
+    void converge_c2p_lev(int Lc, int f, TT *u, bool cubic) {
+        int Lf = Lc + 1, h = nf[f] / 2;
+        run(OpConverge<TT>{u, d_parent, d_oct, H.lstart[Lf], nf[f], Gf[f], Vf[f], cubic ? 1 : 0},
+            (int64_t)cnt(Lf) * h * h * h);
+    }
+    template <class TT>
+    void converge_c2p(int f, TT *u, bool cubic = false) {
+        for (int Lc = H.nlev - 2; Lc >= 0; Lc--) converge_c2p_lev(Lc, f, u, cubic);
+    }
+    template <class TT>
+    void boundary_fill0(int f, TT *u) {   // all blocks
+        int64_t c = tfLOff[H.nlev];
+        int GT = nf[f] + 2;
+        run(OpFill0Faces<TT>{u, d_tfL, nf[f], Gf[f], Vf[f]}, c * GT * GT);
+    }
+    template <class TT>
+    void boundary_fill0_level(int L, int f, TT *u) {
+        int64_t o = tfLOff[L], c = tfLOff[L + 1] - o;
+        int GT = nf[f] + 2;
+        run(OpFill0Faces<TT>{u, d_tfL + o, nf[f], Gf[f], Vf[f]}, c * GT * GT);
+    }
+    template <class TT>
+    void boundary_extrap(int f, TT *u) {   // all blocks, directions in order
+        int GT = nf[f] + 2;
+        for (int dir = 0; dir < 3; dir++) {
+            int64_t o = tfDLOff[dir * H.nlev], c = tfDLOff[(dir + 1) * H.nlev] - o;
+            run(OpExtrapFaces<TT>{u, d_tfDL + o, nf[f], Gf[f], Vf[f]}, c * GT * GT);
+        }
+    }
+    template <class TT>
+    void boundary_extrap_level(int L, int f, TT *u) {
+        int GT = nf[f] + 2;
+        for (int dir = 0; dir < 3; dir++) {
+            int64_t o = tfDLOff[dir * H.nlev + L], c = tfDLOff[dir * H.nlev + L + 1] - o;
+            run(OpExtrapFaces<TT>{u, d_tfDL + o, nf[f], Gf[f], Vf[f]}, c * GT * GT);
+        }
+    }
+    template <class TT>
+    void reflux(int f, const TT *u) {
+        int h = nf[f] / 2;
+        run(OpReflux<TT>{u, d_reflux, rbuf[f], d_h0, d_level, f, nf[f], Gf[f], Vf[f]}, (int64_t)nReflux * h * h);
+    }
+    // fmg_poisson_flux (fmg_poisson.F90:53-124)
+    template <class TT>
+    void poisson_flux(int f, TT *u, bool bf0) {
+        if (FmgLevel_fill0 != f) {
+            converge_c2p(f, u);
+            ghostcell_fix(f, u, false);
+            if (bf0) boundary_fill0(f, u);
+        }
+        FmgLevel_fill0 = Undef;
+        reflux(f, u);
+    }
+
+    // -----------------------------------------------------------------
+    // fmg level operations on the inner fields
+    void relax(int f, T *u, T *rhs, bool bf0, int slot) {   // fmg_poisson_relax
+        cudaMemsetAsync(d_max + slot, 0, sizeof(unsigned long long), st_);
+        const int n = nf[f];
+        for (int ipass = 1; ipass <= 2; ipass++) {
+            poisson_flux(f, u, bf0);
+            bool prof = P.profile && f == 0 && profEv.size() < 2 * kMaxProf;
+            if (prof) { profEv.push_back(nullptr); cudaEventCreate(&profEv.back()); cudaEventRecord(profEv.back(), st_); }
+            runMax(OpRelax<T, T>{u, rhs, d_leaves, d_h0, d_level, d_rslot, rbuf[f], f, n, Gf[f], Vf[f], ipass},
+                   (int64_t)nLeaves * n * n * n / 2, d_max + slot);
+            if (prof) { profEv.push_back(nullptr); cudaEventCreate(&profEv.back()); cudaEventRecord(profEv.back(), st_); }
+        }
+    }
+    static constexpr size_t kMaxProf = 4096;
+    std::vector<cudaEvent_t> profEv;
+    void prof_collect(sfm_stats *stats) {
+        double ms = 0.0;
+        for (size_t q = 0; q + 1 < profEv.size(); q += 2) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, profEv[q], profEv[q + 1]);
+            ms += t;
+        }
+        if (stats) {
+            stats->smoother_ms = ms;
+            stats->smoother_launches = (int64_t)(profEv.size() / 2);
+            stats->smoother_cells = (int64_t)(profEv.size() / 2) * nLeaves * H.NI * H.NI * H.NI;
+        }
+        for (auto e : profEv) cudaEventDestroy(e);
+        profEv.clear();
+    }
+    template <class TU, class TR, class TO>
+    void resid(int f, TO *res, TU *u, const TR *rhs, bool bf0) {   // fmg_poisson_resid
+        poisson_flux(f, u, bf0);
+        const int n = nf[f];
+        run(OpResid<TU, TR, TO>{res, u, rhs, d_leaves, d_h0, d_level, d_rslot, rbuf[f], f, n, Gf[f], Vf[f]},
+            (int64_t)nLeaves * n * n * n);
+    }
+    void fmg_rstrct(int f, T *uc, const T *uf) {
+        int nc = nf[f];
+        run(OpRstrct<T, T>{uc, uf, d_leaves, nc, Gf[f], Gf[f - 1], Vf[f], Vf[f - 1]}, (int64_t)nLeaves * nc * nc * nc);
+    }
+    void fill0(int f, T *u) { run(OpZero<T>{u, d_leaves, Vf[f]}, (int64_t)nLeaves * Vf[f]); }
+    template <class TO, class TI>
+    void copy(int f, TO *o, const TI *a, bool noskip) {
+        run(OpCopy<TO, TI>{o, a, noskip ? d_all : d_leaves, Vf[f]}, (int64_t)(noskip ? H.nb : nLeaves) * Vf[f]);
+    }
+    template <class TA, class TD>
+    void add(int f, TA *a, const TD *d) { run(OpAdd<TA, TD>{a, d, d_leaves, Vf[f]}, (int64_t)nLeaves * Vf[f]); }
+
+    // fmg_interp (fmg.F90:786-822)
+    void fmg_interp(int f, T *uf, T *uc, bool cubic) {
+        int lc = f + 1;
+        converge_c2p(lc, uc, cubic);
+        ghostcell_fix(lc, uc, cubic);
+        boundary_extrap(lc, uc);
+        const int n = nf[f];
+        run(OpInterp<T>{uf, uc, d_leaves, n, Gf[f], Gf[lc], Vf[f], Vf[lc], cubic ? 1 : 0}, (int64_t)nLeaves * n * n * n);
+        boundary_fill0(lc, uc);
+        boundary_fill0(f, uf);
+    }
+
+    // fmg_lin (fmg.F90:270-377)
+    void fmg_lin() {
+        const int FMax = H.FMax;
+        for (int f = 1; f <= FMax; f++) fmg_rstrct(f, RHO[f], RHO[f - 1]);
+        fill0(FMax, U[FMax]);
+        vmg_fas(false);
+        for (int f = FMax - 1; f >= 0; f--) {
+            fmg_interp(f, U[f], U[f + 1], true);
+            copy(f, RHS[f], RHO[f], false);
+            for (int jc = 1; jc <= 2; jc++) {
+                for (int v = f; v <= FMax - 1; v++) {
+                    for (int q = 0; q < 2; q++) relax(v, U[v], RHS[v], true, 0);
+                    resid(v, RES[v], U[v], RHS[v], true);
+                    fmg_rstrct(v + 1, RHS[v + 1], RES[v]);
+                    fill0(v + 1, U[v + 1]);
+                    FmgLevel_fill0 = v + 1;
+                }
+                vmg_fas(true);
+                for (int v = FMax - 1; v >= f; v--) {
+                    fmg_interp(v, RES[v], U[v + 1], false);   // fmg_addint
+                    add(v, U[v], RES[v]);
+                    for (int q = 0; q < 2; q++) relax(v, U[v], RHS[v], true, 0);
+                }
+            }
+        }
+        converge_c2p(0, U[0]);
+    }
+
+    // -----------------------------------------------------------------
+    // vmg (vmg.F90) at fmg level FMax
+    void vmg_ghostcell(int L, T *u) {
+        const int F = H.FMax;
+        for (int dir = 0; dir < 3; dir++) ghost_pass_same(L, F, dir, u);
+        boundary_fill0_level(L, F, u);
+    }
+    // same-level face copies of (L, dir) only (fmg_ghfix_samelev)
+    void ghost_pass_same(int L, int f, int dir, T *u) {
+        int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
+        if (c <= 0) return;
+        int GT = nf[f] + 2;
+        run(OpGhostPass<T>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, 0, 0}, c * GT * GT);
+    }
+    // coarse-fine faces of (L, dir) only (fmg_ghfix_parentlev)
+    void ghost_pass_parent(int L, int f, int dir, T *u, bool cubic) {
+        if (L <= 0) return;
+        int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
+        if (c <= 0) return;
+        int GT = nf[f] + 2;
+        run(OpGhostPass<T>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, 1}, c * GT * GT);
+    }
+    void vmg_gridboundary(int L, T *u) {
+        const int F = H.FMax;
+        for (int dir = 0; dir < 3; dir++) ghost_pass_parent(L, F, dir, u, false);
+        boundary_fill0_level(L, F, u);
+    }
+    void vmg_relax(int L, T *u, const T *rhs) {
+        const int F = H.FMax, n = nf[F];
+        for (int ipass = 1; ipass <= 2; ipass++) {
+            vmg_ghostcell(L, u);
+            runMax(OpRelax<T, T>{u, rhs, d_all + H.lstart[L], d_h0, d_level, nullptr, nullptr, F, n, Gf[F], Vf[F], ipass},
+                   (int64_t)cnt(L) * n * n * n / 2, d_max + 1);
+        }
+    }
+    void vmg_rstrct(int Lc, T *u, bool cubic) {
+        const int F = H.FMax;
+        if (cubic)
+            for (int dir = 0; dir < 3; dir++) {
+                ghost_pass_parent(Lc + 1, F, dir, u, true);
+                ghost_pass_same(Lc + 1, F, dir, u);
+            }
+        converge_c2p_lev(Lc, F, u, cubic);
+    }
+    void vmg_copy_level(int L, T *o, const T *a) {
+        const int F = H.FMax;
+        run(OpCopy<T, T>{o, a, d_all + H.lstart[L], Vf[F]}, (int64_t)cnt(L) * Vf[F]);
+    }
+    void vmg_tau(int L) {   // vmg_poisson_tau + vmg_tau_crop, tau in RES
+        const int F = H.FMax, n = nf[F];
+        int Lf = L + 1;
+        if (Lf > H.nlev - 1) return;
+        vmg_ghostcell(Lf, U[F]);
+        run(OpTauFine<T>{RES[F], U[F], H.lstart[Lf], n, Gf[F], Vf[F], (T)(1.0 / hlev(H.h0.data(), Lf, F))},
+            (int64_t)cnt(Lf) * Vf[F]);
+        converge_c2p_lev(L, F, RES[F], false);
+        vmg_ghostcell(L, U[F]);
+        int64_t wc = wcOff[L + 1] - wcOff[L];
+        run(OpTauParent<T>{RES[F], U[F], d_withChild + wcOff[L], n, Gf[F], Vf[F], (T)(1.0 / hlev(H.h0.data(), L, F))},
+            wc * n * n * n);
+        int64_t co = cropOff[Lf], cc = cropOff[Lf + 1] - co;
+        int GT = n + 2;
+        run(OpTauCrop<T>{RES[F], d_crop + co, d_parent, n, Gf[F], Vf[F]}, cc * GT * GT);
+    }
+    void vmg_interp(int Lf, T *uf, T *uc) {   // vmg_interp (vmg.F90:592-601)
+        const int F = H.FMax, n = nf[F];
+        int Lc = Lf - 1;
+        vmg_ghostcell(Lc, uc);
+        boundary_extrap_level(Lc, F, uc);
+        run(OpP2C<T>{uf, uc, d_parent, d_oct, H.lstart[Lf], n, Gf[F], Vf[F]}, (int64_t)cnt(Lf) * n * n * n);
+        boundary_fill0_level(Lc, F, uc);
+    }
+    void vmg_zeroAverage(T *a) {
+        const int F = H.FMax, n = nf[F];
+        run(OpBlockSum<T>{a, d_all, d_psum, n, Gf[F], Vf[F]}, (int64_t)cnt(0));
+        k_ave_combine<<<1, 1, 0, st_>>>(d_psum, cnt(0), n, d_scal + 1);
+        ++launches;
+        run(OpSubScalarInterior<T>{a, d_scal + 1, 0, n, Gf[F], Vf[F]}, (int64_t)cnt(0) * n * n * n);
+    }
+    void vmg_slvsml(T *u, T *rhs) {
+        if (!useSerialMg) {
+            for (int q = 0; q < 10; q++) vmg_relax(0, u, rhs);
+            return;
+        }
+        const int F = H.FMax;
+        int64_t N3 = (int64_t)NBc * NBc * NBc;
+        run(OpMgGather<T>{mg.SRC, mg.PSI, rhs, u, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
+        k_mg_cycle<<<1, 1024, 0, st_>>>(mg, d_mgit);
+        ++launches;
+        run(OpMgScatter<T>{u, mg.PSI, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
+    }
+    // vmg_fas (vmg.F90:116-243); jrho = IRHS when copy_rhs (second and later calls)
+    void vmg_fas(bool copy_rhs) {
+        const int F = H.FMax, nlev = H.nlev;
+        if (copy_rhs)
+            for (int L = 0; L < nlev; L++) vmg_copy_level(L, RHO[F], RHS[F]);
+        converge_c2p(F, U[F]);
+        converge_c2p(F, RHO[F]);
+        boundary_fill0(F, U[F]);
+        for (int L = 0; L < nlev; L++) vmg_copy_level(L, RHS[F], RHO[F]);
+        for (int v = nlev - 1; v >= 1; v--) {
+            vmg_gridboundary(v, U[F]);
+            for (int q = 0; q < 2; q++) vmg_relax(v, U[F], RHS[F]);
+            vmg_rstrct(v - 1, U[F], true);
+            vmg_copy_level(v - 1, RUF, U[F]);
+            vmg_rstrct(v - 1, RHS[F], false);
+            vmg_tau(v - 1);
+            int64_t wc = wcOff[v] - wcOff[v - 1];
+            run(OpAdd<T, T>{RHS[F], RES[F], d_withChild + wcOff[v - 1], Vf[F]}, wc * Vf[F]);
+        }
+        if (P.zero_mean) vmg_zeroAverage(RHS[F]);
+        vmg_slvsml(U[F], RHS[F]);
+        for (int v = 1; v <= nlev - 1; v++) {
+            run(OpSub<T>{RES[F], U[F], RUF, d_all + H.lstart[v - 1], Vf[F]}, (int64_t)cnt(v - 1) * Vf[F]);
+            vmg_interp(v, RES[F], RES[F]);
+            run(OpAdd<T, T>{U[F], RES[F], d_all + H.lstart[v], Vf[F]}, (int64_t)cnt(v) * Vf[F]);
+            vmg_gridboundary(v, U[F]);
+            for (int q = 0; q < 2; q++) vmg_relax(v, U[F], RHS[F]);
+        }
+    }
+
+    // -----------------------------------------------------------------
+    // outer FP64 stages
+    void boundary_physical_grid() {   // sphere: mask SRC0, moments, multipole ghosts of PSI0
+        if (P.bc != SFM_BC_SPHERE) return;
+        const int n = H.NI;
+        int bmin = H.baseIdx.front(), bmax = H.baseIdx.back();
+        auto X = [&](int b, int d, int i) { return H.x0[3 * b + d] + (double)i * H.h0[H.level[b]]; };
+        double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
+        double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
+        double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        double rad2 = rr * rr;
+        run(OpSphereMask{SRC0, d_x0, d_h0, d_level, n, Gf[0], Vf[0], rad2}, (int64_t)H.nb * Vf[0]);
+        k_moments_block<<<cnt(0), 128, 0, st_>>>(SRC0, d_x0, d_h0, n, Gf[0], Vf[0], P.lmax, d_part);
+        k_moments_combine<<<1, 1, 0, st_>>>(d_part, cnt(0), d_mom);
+        launches += 2;
+        int GT = n + 2;
+        run(OpSphereGhost{PSI0, d_tfL, d_mom, d_x0, d_h0, d_level, n, Gf[0], Vf[0], P.lmax}, tfLOff[H.nlev] * GT * GT);
+    }
+
+    double read_max(int slot) {
+        unsigned long long v = 0;
+        cudaMemcpyAsync(&v, d_max + slot, sizeof(v), cudaMemcpyDeviceToHost, st_);
+        cudaStreamSynchronize(st_);
+        double d;
+        std::memcpy(&d, &v, sizeof(d));
+        return d;
+    }
+    void h2absmax(const double *a, int slot) {
+        const int n = nf[0];
+        cudaMemsetAsync(d_max + slot, 0, sizeof(unsigned long long), st_);
+        runMax(OpH2Abs<double>{a, d_leaves, d_h0, d_level, 0, n, Gf[0], Vf[0]}, (int64_t)nLeaves * n * n * n, d_max + slot);
+    }
+
+    int check(const char *where) {
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+        if (e != cudaSuccess) {
+            last_error = std::string(where) + ": " + cudaGetErrorString(e);
+            return SFM_ECUDA;
+        }
+        return SFM_OK;
+    }
+
+    // fmg_cycle (fmg.F90:134-233) on device arrays
+    int solve(const double *rho, double *psi, double *g, sfm_stats *stats, cudaStream_t s, int stop_stage,
+              double *dump) override {
+        st_ = s ? s : own_;   // all work of this call is ordered on the caller's stream
+        launches = 0;
+        const int nb = H.nb, gw = P.ngh_io;
+        cudaEventRecord(ev0, st_);
+        // fresh, zero-filled arrays as fmg_alloc_arr gives (fmg_data.F90:393)
+        for (auto &z : zeroList) cudaMemsetAsync(z.first, 0, z.second, st_);
+        cudaMemsetAsync(d_bad, 0, sizeof(int), st_);
+        FmgLevel_fill0 = Undef;
+        // fmg_make_physvar
+        run(OpPhysvar<double>{PHI0, RES0d, rho, psi, H.NI, Gf[0], gw, Vf[0], P.four_pi_G, d_bad}, (int64_t)nb * Vf[0]);
+        if (P.zero_mean) {
+            run(OpBlockSum<double>{RES0d, d_leaves, d_psum, H.NI, Gf[0], Vf[0]}, (int64_t)nLeaves);
+            k_mean_combine<<<1, 1, 0, st_>>>(d_psum, d_leaves, nLeaves, d_level, d_h0, H.NI, d_scal);
+            ++launches;
+            run(OpSubScalarAll<double>{RES0d, d_scal}, (int64_t)nb * Vf[0]);
+        } else {
+            cudaMemsetAsync(d_scal, 0, sizeof(double), st_);
+        }
+        copy(0, RHO[0], RES0d, true);   // IRHO(f0) as the reference holds it
+        copy(0, U[0], PHI0, true);      // IU(f0)
+        copy(0, PSI0, PHI0, false);     // fmg_copy(IPSI, IU)
+        copy(0, SRC0, RES0d, false);    // fmg_copy(ISRC, IRHO)
+        converge_c2p(0, SRC0);
+        converge_c2p(0, PSI0);
+        boundary_physical_grid();
+        h2absmax(SRC0, 2);
+        int rc = check("setup");
+        if (rc) return rc;
+        int bad = 0;
+        cudaMemcpy(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost);
+        if (bad) return SFM_ENONFINITE;
+        double resh2max = read_max(2), rhoave = 0.0;
+        cudaMemcpy(&rhoave, d_scal, sizeof(double), cudaMemcpyDeviceToHost);
+        if (stop_stage == 1) return dumpd(SRC0, dump);
+        if (stats) { std::memset(stats, 0, sizeof(*stats)); stats->resh2max = resh2max; stats->rho_mean = rhoave; }
+        double ratio_prev = std::numeric_limits<double>::max();
+        int nmax = P.max_outer;
+        if (std::fabs(resh2max) <= std::numeric_limits<double>::min()) nmax = 0;
+        bool conv = true, reached = (nmax == 0);
+        int iters = 0;
+        for (int it = 1; it <= nmax; it++) {
+            resid<double, double, T>(0, RHO[0], PSI0, SRC0, false);
+            if (stop_stage == 2) { rc = check("resid"); return rc ? rc : dumpT(RHO[0], dump); }
+            fmg_lin();
+            if (stop_stage == 3) { rc = check("fmg_lin"); return rc ? rc : dumpT(U[0], dump); }
+            add(0, PSI0, U[0]);
+            rc = check("outer");
+            if (rc) return rc;
+            iters = it;
+            double ratio = read_max(0) / resh2max;
+            if (stats && it <= SFM_MAX_HISTORY) stats->ratio[it - 1] = ratio;
+            if (ratio < P.rel_tol) { reached = true; break; }
+            if (it == nmax) conv = false;
+            if (P.stagnation_exit && ratio > ratio_prev * 0.5) conv = false;
+            if (!conv) break;
+            ratio_prev = ratio;
+        }
+        if (stop_stage == 4) return dumpd(PSI0, dump);
+        copy(0, PHI0, PSI0, true);
+        converge_c2p(0, PHI0);
+        poisson_flux(0, PHI0, false);
+        if (g) run(OpPsi2g{g, PHI0, d_skip, d_level, d_h0, d_rslot, rbuf[0], H.NI, Gf[0], gw, Vf[0]}, (int64_t)nb * H.NI * H.NI * H.NI);
+        if (psi) run(OpRestore{psi, PHI0, H.NI, Gf[0], gw, Vf[0]}, (int64_t)nb * Vf[0]);
+        cudaEventRecord(ev1, st_);
+        double trr = 0.0;
+        if (P.report_residual && resh2max > 0) {
+            FmgLevel_fill0 = Undef;
+            resid<double, double, double>(0, RES0d, PHI0, SRC0, false);
+            h2absmax(RES0d, 3);
+            trr = read_max(3) / resh2max;
+        }
+        rc = check("finish");
+        if (rc) return rc;
+        if (stats) {
+            stats->outer_iters = iters;
+            stats->converged = (conv && reached) ? 1 : 0;
+            stats->true_rel_residual = trr;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            stats->device_ms = ms;
+            stats->kernel_launches = launches;
+            stats->elem_bytes = (int32_t)sizeof(T);
+        }
+        prof_collect(stats);
+        return (conv && reached) ? SFM_OK : SFM_ENOTCONVERGED;
+    }
+    int dumpd(const double *a, double *dump) {
+        int rc = check("dump");
+        if (rc) return rc;
+        if (dump) cudaMemcpy(dump, a, (size_t)H.nb * Vf[0] * sizeof(double), cudaMemcpyDeviceToHost);
+        return SFM_OK;
+    }
+    int dumpT(const T *a, double *dump) {
+        if (!dump) return SFM_OK;
+        std::vector<T> tmp((size_t)H.nb * Vf[0]);
+        cudaMemcpy(tmp.data(), a, tmp.size() * sizeof(T), cudaMemcpyDeviceToHost);
+        for (size_t i = 0; i < tmp.size(); i++) dump[i] = (double)tmp[i];
+        return SFM_OK;
+    }
+};
+
+}  // namespace sfm
+
+// =============================================================================
+// C ABI
+// =============================================================================
+struct sfm_ctx {
+    sfm::SolverBase *s = nullptr;
+    sfm_params p;
+    int device = 0, nb = 0, ni = 0, ngh = 0;
+    double *d_rho = nullptr, *d_psi = nullptr, *d_g = nullptr;   // staging for host calls
+    std::string err;
+};
+
+static int check_device(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return SFM_EDEVICE;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return SFM_EDEVICE;
+    if (prop.major != 10) return SFM_EDEVICE;   // built for sm_100a only
+    return SFM_OK;
+}
+
+extern "C" {
+
+void sfm_default_params(sfm_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->bc = SFM_BC_PERIODIC;
+    p->lmax = 3;
+    p->precision = SFM_PREC_FP64;
+    p->max_outer = 10;
+    p->rel_tol = 1e-3;
+    p->four_pi_G = 4.0 * 3.141592653589793;
+    p->zero_mean = 1;
+    p->ngh_io = 2;
+    p->report_residual = 1;
+    p->stagnation_exit = 1;
+    p->profile = 0;
+}
+
+int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out) {
+    if (!h || !p || !out) return SFM_EINVAL;
+    *out = nullptr;
+    if (p->ngh_io < 1 || p->max_outer < 0 || p->max_outer > 1000 || !(p->rel_tol >= 0) ||
+        (p->bc != SFM_BC_PERIODIC && p->bc != SFM_BC_SPHERE) || (p->lmax != 3 && p->lmax != 4) ||
+        (p->precision != SFM_PREC_FP64 && p->precision != SFM_PREC_MIXED))
+        return SFM_EINVAL;
+    int rc = check_device();
+    if (rc) return rc;
+    sfm_ctx *c = new (std::nothrow) sfm_ctx();
+    if (!c) return SFM_ENOMEM;
+    c->p = *p;
+    cudaGetDevice(&c->device);
+    if (p->precision == SFM_PREC_FP64) {
+        auto *s = new (std::nothrow) sfm::Solver<double>();
+        if (!s) { delete c; return SFM_ENOMEM; }
+        rc = s->init(h, p);
+        c->s = s;
+    } else {
+        auto *s = new (std::nothrow) sfm::Solver<float>();
+        if (!s) { delete c; return SFM_ENOMEM; }
+        rc = s->init(h, p);
+        c->s = s;
+    }
+    if (rc) { delete c->s; delete c; return rc; }
+    c->nb = h->nblocks; c->ni = h->ni; c->ngh = p->ngh_io;
+    *out = c;
+    return SFM_OK;
+}
+
+static int64_t io_elems(const sfm_ctx *c) {
+    int64_t G = c->ni + 2 * c->ngh;
+    return (int64_t)c->nb * G * G * G;
+}
+
+int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g, sfm_stats *st, void *stream) {
+    if (!c || !c->s || !d_rho) return SFM_EINVAL;
+    cudaSetDevice(c->device);
+    return c->s->solve(d_rho, d_psi, d_g, st, (cudaStream_t)stream, 0, nullptr);
+}
+
+int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
+    if (!c || !c->s || !rho) return SFM_EINVAL;
+    cudaSetDevice(c->device);
+    int64_t n = io_elems(c);
+    size_t bytes = (size_t)n * sizeof(double);
+    if (!c->d_rho) {
+        if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess ||
+            cudaMalloc(&c->d_g, 3 * bytes) != cudaSuccess)
+            return SFM_ENOMEM;
+    }
+    if (cudaMemcpy(c->d_rho, rho, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA;
+    if (psi) { if (cudaMemcpy(c->d_psi, psi, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA; }
+    // the solve writes g on block interiors only; the rest of the caller's array is kept
+    if (g) { if (cudaMemcpy(c->d_g, g, 3 * bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA; }
+    int rc = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, g ? c->d_g : nullptr, st, nullptr, 0, nullptr);
+    if (rc != SFM_OK && rc != SFM_ENOTCONVERGED) return rc;
+    if (psi && cudaMemcpy(psi, c->d_psi, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return SFM_ECUDA;
+    if (g && cudaMemcpy(g, c->d_g, 3 * bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return SFM_ECUDA;
+    return rc;
+}
+
+int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st) {
+    (void)st;
+    if (!c || !dJ_dphi || !dJ_drho) return SFM_EINVAL;
+    return SFM_EINVAL;
+}
+
+void sfm_destroy(sfm_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->d_rho) cudaFree(c->d_rho);
+    if (c->d_psi) cudaFree(c->d_psi);
+    if (c->d_g) cudaFree(c->d_g);
+    delete c->s;
+    delete c;
+}
+
+const char *sfm_strerror(int code) {
+    switch (code) {
+        case SFM_OK: return "ok";
+        case SFM_EINVAL: return "invalid argument";
+        case SFM_EHIER: return "hierarchy violates a link-list invariant";
+        case SFM_ECUDA: return "CUDA runtime error";
+        case SFM_ENOMEM: return "out of memory";
+        case SFM_ENOTCONVERGED: return "outer iteration did not reach rel_tol";
+        case SFM_ENONFINITE: return "non-finite input";
+        case SFM_EDEVICE: return "no usable sm_100 CUDA device";
+        case SFM_ETIMEOUT: return "bounded device wait expired";
+        case SFM_ESIZE: return "size exceeds a fixed maximum";
+        default: return "unknown error";
+    }
+}
+
+int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes) {
+    if (!c || !c->s) return SFM_EINVAL;
+    if (fmg_levels) *fmg_levels = c->s->fmg_levels();
+    if (device_bytes) *device_bytes = c->s->device_bytes();
+    return SFM_OK;
+}
+
+// Test hook (not part of include/sfmg.h): like sfm_solve on host arrays, but
+// stops after stage `stop_stage` (1 set-up, 2 first outer residual, 3 first
+// fmg_lin, 4 outer loop) and copies that stage's level-0 field, ghost width 1,
+// into `dump`.
+int sfm_debug_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st, int stop_stage,
+                    double *dump) {
+    if (!c || !c->s || !rho) return SFM_EINVAL;
+    cudaSetDevice(c->device);
+    int64_t n = io_elems(c);
+    size_t bytes = (size_t)n * sizeof(double);
+    if (!c->d_rho) {
+        if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess ||
+            cudaMalloc(&c->d_g, 3 * bytes) != cudaSuccess)
+            return SFM_ENOMEM;
+    }
+    cudaMemcpy(c->d_rho, rho, bytes, cudaMemcpyHostToDevice);
+    if (psi) cudaMemcpy(c->d_psi, psi, bytes, cudaMemcpyHostToDevice);
+    if (g) cudaMemcpy(c->d_g, g, 3 * bytes, cudaMemcpyHostToDevice);
+    int rc = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, g ? c->d_g : nullptr, st, nullptr, stop_stage, dump);
+    if (stop_stage == 0 && (rc == SFM_OK || rc == SFM_ENOTCONVERGED)) {
+        if (psi) cudaMemcpy(psi, c->d_psi, bytes, cudaMemcpyDeviceToHost);
+        if (g) cudaMemcpy(g, c->d_g, 3 * bytes, cudaMemcpyDeviceToHost);
+    }
+    return rc;
+}
+
+}  // extern "C"

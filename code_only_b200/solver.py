@@ -1,0 +1,103 @@
+"""Python mirror of the reference's `fmg_poisson` entry point over the C ABI.
+
+The reference's `fmg_poisson` (fmg.F90:63-74) takes no arguments: it reads the
+hierarchy and the block arrays from module globals, solves
+lap(phi) = 4 pi G (rho - <rho>) by FMG, and writes U(MPSI) (interior + 1
+ghost layer) and U(MGX:MGZ) (interior) back.  Here the same data is passed
+explicitly:
+
+    ctx = FMGPoisson(hierarchy, bc=SFM_BC_SPHERE)        # fmg_data_init + fmg_alloc_LoL
+    psi, g, stats = ctx.solve(rho, psi0)                 # fmg_cycle
+    ctx.close()
+
+``rho``/``psi0`` are float64 arrays [nblocks, G, G, G] (G = ni + 2*ngh_io,
+i fastest in memory), as BlockMem(gid)%u(:,:,:,m) stores one component.
+Errors raise SFMError carrying the library's status code; there is no CPU
+path -- a missing or unloadable CUDA library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+
+
+class SFMError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        lib = abi.load_library()
+        super().__init__(f"{what}: {lib.sfm_strerror(code).decode()} ({code})")
+
+
+class FMGPoisson:
+    def __init__(self, hierarchy, bc: int = abi.SFM_BC_PERIODIC, params: Optional[abi.SfmParams] = None, **kw):
+        self.lib = abi.load_library()
+        self.h = hierarchy
+        self.desc = abi.HierDesc(hierarchy)
+        self.params = params if params is not None else abi.default_params(bc, **kw)
+        self.ctx = C.c_void_p()
+        rc = self.lib.sfm_create(self.desc.ref(), C.byref(self.params), C.byref(self.ctx))
+        if rc != abi.SFM_OK:
+            self.ctx = None
+            raise SFMError(rc, "sfm_create")
+        self.G = hierarchy.ni + 2 * self.params.ngh_io
+
+    @property
+    def shape(self):
+        return (self.h.nblocks, self.G, self.G, self.G)
+
+    def solve(self, rho: np.ndarray, psi: Optional[np.ndarray] = None, want_g: bool = True, allow_unconverged=True):
+        """One solve with host arrays (sfm_solve).  Returns (psi, g, stats)."""
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        if rho.shape != self.shape:
+            raise ValueError(f"rho has shape {rho.shape}, expected {self.shape}")
+        psi = np.zeros(self.shape) if psi is None else np.array(psi, dtype=np.float64, order="C", copy=True)
+        g = np.zeros((self.h.nblocks, 3, self.G, self.G, self.G)) if want_g else None
+        st = abi.SfmStats()
+        rc = self.lib.sfm_solve(self.ctx, rho.ctypes.data, psi.ctypes.data,
+                                g.ctypes.data if g is not None else None, C.byref(st))
+        if rc not in (abi.SFM_OK, abi.SFM_ENOTCONVERGED) or (rc != abi.SFM_OK and not allow_unconverged):
+            raise SFMError(rc, "sfm_solve")
+        return psi, g, st
+
+    def solve_device(self, rho_ptr: int, psi_ptr: int, g_ptr: Optional[int] = None, stream: int = 0):
+        """Solve on device-resident buffers (sfm_solve_device); pointers as ints."""
+        st = abi.SfmStats()
+        rc = self.lib.sfm_solve_device(self.ctx, C.c_void_p(rho_ptr), C.c_void_p(psi_ptr),
+                                       C.c_void_p(g_ptr) if g_ptr else None, C.byref(st),
+                                       C.c_void_p(stream) if stream else None)
+        if rc not in (abi.SFM_OK, abi.SFM_ENOTCONVERGED):
+            raise SFMError(rc, "sfm_solve_device")
+        return st
+
+    def info(self):
+        lv = C.c_int32()
+        by = C.c_int64()
+        self.lib.sfm_info(self.ctx, C.byref(lv), C.byref(by))
+        return {"fmg_levels": lv.value, "device_bytes": by.value}
+
+    def close(self):
+        if self.ctx:
+            self.lib.sfm_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fmg_poisson(hierarchy, rho: np.ndarray, psi: np.ndarray, bc: int = abi.SFM_BC_PERIODIC, **kw):
+    """One-shot form of the reference entry point: returns (psi, g, stats)."""
+    with FMGPoisson(hierarchy, bc=bc, **kw) as s:
+        return s.solve(rho, psi)

@@ -1,0 +1,164 @@
+/*
+ * sfmg.h -- C ABI of the B200 self-gravity FMG Poisson solver.
+ *
+ * The solver is a drop-in for the reference's `fmg_poisson` entry point
+ * (fmg.F90:63-74, public in module `fmg`, fmg.F90:23), which takes no
+ * arguments and reads the block hierarchy from module globals of `grid`
+ * (BlockMem(gid)%u, GidList, ParentGid/ChildGid/NeighborGid, CellWidth,
+ * touch_boundary; grid.F90:19-66, boundary_fixed.F90:217-231).  The
+ * replacement receives the same information explicitly: a hierarchy
+ * descriptor (the link tables of grid.F90:44-52 in fmg-local numbering) and
+ * per-block arrays laid out like BlockMem(gid)%u(:,:,:,m) (Fortran order,
+ * i fastest, `ngh_io` ghost layers).  A Fortran ISO_C_BINDING shim that keeps
+ * the name `fmg_poisson` is shown in INTEGRATION.md.
+ *
+ * Conventions shared by every entry point:
+ *   - blocks are numbered 0..nblocks-1 and must be sorted by AMR level
+ *     (the reference's GidList(n, level), grid.F90:64);
+ *   - face index  f = lr + 2*dir, lr 0 = Left, 1 = Right, dir 0/1/2 = x/y/z
+ *     (NeighborGid(lr, dir), grid.F90:47);
+ *   - child index c = lri + 2*lrj + 4*lrk (ChildGid(lri,lrj,lrk), grid.F90:50);
+ *   - a block array holds (ni+2*ngh_io)^3 doubles, i fastest, so cell
+ *     (i,j,k), -ngh_io <= i,j,k < ni+ngh_io, sits at
+ *     ((k+ngh_io)*(ni+2*ngh_io) + (j+ngh_io))*(ni+2*ngh_io) + (i+ngh_io);
+ *   - every function returns SFM_OK (0) or a negative SFM_E* code and never
+ *     aborts the process (the reference prints and stops, fmg_data.F90:185,575).
+ *
+ * Threading: a context is used by one host thread at a time and owns all of
+ * its device memory; it lives on the CUDA device that was current when it
+ * was created.
+ */
+#ifndef SFMG_H
+#define SFMG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define SFM_OK               0
+#define SFM_EINVAL          -1   /* bad argument (NULL pointer, bad size)      */
+#define SFM_EHIER           -2   /* hierarchy violates a link-list invariant   */
+#define SFM_ECUDA           -3   /* CUDA runtime error                         */
+#define SFM_ENOMEM          -4   /* device or host allocation failed           */
+#define SFM_ENOTCONVERGED   -5   /* outer loop ended without reaching rel_tol  */
+#define SFM_ENONFINITE      -6   /* non-finite density or potential on input   */
+#define SFM_EDEVICE         -7   /* no usable CUDA device / wrong architecture */
+#define SFM_ETIMEOUT        -8   /* a bounded device wait gave up              */
+#define SFM_ESIZE           -9   /* a size exceeds a fixed maximum             */
+
+/* ---- hierarchy ---------------------------------------------------------
+ * Replaces the link tables that fmg_make_linklist (fmg_data_if.F90:298-411)
+ * gathers from module `grid`.  Parent-level neighbour links
+ * (NeighborParentLevel, fmg_data_if.F90:376-395) are derived internally. */
+typedef struct sfm_hier_desc {
+    int32_t nlev;            /* AMR levels present: 0 .. nlev-1 (Lmin .. LevelMax) */
+    int32_t nblocks;
+    int32_t ni, nj, nk;      /* cells per block edge (NI,NJ,NK, config.h:15-17);
+                                must be equal and a power of two >= 4            */
+    int32_t ngb[3];          /* base blocks per dimension (NGI_BASE.., config.h:21-23) */
+    const int32_t *level;    /* [nblocks] AMR level of each block                */
+    const int32_t *ijk;      /* [3*nblocks] block index on its level (Igrid..)   */
+    const int32_t *parent;   /* [nblocks] parent block, -1 on level 0            */
+    const int32_t *child;    /* [8*nblocks] children, -1 for a block without any */
+    const int32_t *nbr;      /* [6*nblocks] same-level face neighbour or -1      */
+    const int8_t  *touch;    /* [6*nblocks] 1 where the face is on the physical
+                                boundary (touch_boundary, boundary_fixed.F90:217) */
+    const double  *cellwidth;/* [nlev] cell width h at fmg level 0 (CellWidth)   */
+    const double  *x0;       /* [3*nblocks] coordinates of the centre of cell
+                                (0,0,0) of each block (BlockMem(gid)%x(Imin)..)  */
+} sfm_hier_desc;
+
+/* ---- solver parameters ------------------------------------------------
+ * The reference hard-codes these (fmg.F90:146,179; config.h:194). */
+#define SFM_BC_PERIODIC 0   /* fmg_boundary_phys_periodic.F90                  */
+#define SFM_BC_SPHERE   1   /* fmg_boundary_phys_sphere.F90 (multipole ghosts)  */
+#define SFM_PREC_FP64   0   /* every operation in FP64, as the reference       */
+#define SFM_PREC_MIXED  1   /* FP32 inner fmg_lin/vmg, FP64 outer loop and base solve */
+
+typedef struct sfm_params {
+    int32_t bc;              /* SFM_BC_*                                        */
+    int32_t lmax;            /* multipole order for SFM_BC_SPHERE: 3 (reference) or 4 */
+    int32_t precision;       /* SFM_PREC_*                                      */
+    int32_t max_outer;       /* nfmgmax (reference: 10)                         */
+    double  rel_tol;         /* errormax (reference: 1e-3)                      */
+    double  four_pi_G;       /* MP_Gconst * Pi4 (fmg_data_if.F90:40)            */
+    int32_t zero_mean;       /* ZERO_AVERAGE_DENSITY (config.h:194): subtract the
+                                leaf-volume mean of rho and zero the base mean  */
+    int32_t ngh_io;          /* ghost layers of the caller's block arrays, >= 1
+                                (N_GHOST_CELL = 2, config.h:135)                */
+    int32_t report_residual; /* 1: compute the true FP64 composite residual of
+                                the returned potential into sfm_stats          */
+    int32_t stagnation_exit; /* 1: stop when the ratio fails to halve, as
+                                fmg.F90:193 does; 0: run until rel_tol/max_outer */
+    int32_t profile;         /* 1: time every smoother launch on fmg level 0
+                                with CUDA events (sfm_stats.smoother_*)        */
+} sfm_params;
+
+/* Fills *p with the reference's defaults (periodic, FP64, 10 outer
+ * iterations, rel_tol 1e-3, 4piG = 4pi, zero_mean on, ngh_io 2). */
+void sfm_default_params(sfm_params *p);
+
+#define SFM_MAX_HISTORY 64
+typedef struct sfm_stats {
+    int32_t outer_iters;         /* fmg_lin calls done                        */
+    int32_t converged;           /* bool_converge of fmg_cycle (fmg.F90:181)  */
+    double  resh2max;            /* max_leaf |h^2 SRC| (fmg.F90:172)          */
+    double  ratio[SFM_MAX_HISTORY]; /* Resh2maxg/resh2max per iteration (fmg.F90:188) */
+    double  true_rel_residual;   /* max_leaf|h^2 (SRC - L phi)| / resh2max    */
+    double  rho_mean;            /* subtracted mean of 4 pi G rho             */
+    double  device_ms;           /* device time of the solve (CUDA events)   */
+    int64_t kernel_launches;     /* kernels launched by this call             */
+    double  smoother_ms;         /* summed duration of the level-0 red-black
+                                    colour launches (params.profile = 1)      */
+    int64_t smoother_launches;   /* number of those launches                  */
+    int64_t smoother_cells;      /* leaf cells swept per launch x launches    */
+    int32_t elem_bytes;          /* bytes per value of the inner solve (8 or 4) */
+} sfm_stats;
+
+typedef struct sfm_ctx sfm_ctx;
+
+/* Builds the device hierarchy, neighbour and work tables and allocates all
+ * device fields (fmg_data_init + fmg_alloc_LoL + fmg_make_linklist,
+ * fmg_data.F90:110-319, fmg_data_if.F90:298-411).  The link invariants of
+ * fmg_check_linklist (fmg_data_if.F90:415-568) are verified; a violation
+ * returns SFM_EHIER. */
+int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out);
+
+/* One solve with HOST arrays: replaces fmg_poisson (fmg.F90:63-74).
+ *   rho [nblocks][(ni+2g)^3]   density (U1(MRHO), fmg_data_if.F90:51), read on (-1:ni)^3
+ *   psi [nblocks][(ni+2g)^3]   in: warm start U(MPSI) (fmg_data_if.F90:46), read on (-1:ni)^3
+ *                              out: potential on (-1:ni)^3 (fmg_restore_u, fmg_data_if.F90:275-294)
+ *   g   [nblocks][3][(ni+2g)^3] out: -grad phi on the interior (fmg_psi2g, fmg_poisson.F90:4-49);
+ *                              may be NULL
+ *   st  may be NULL.
+ * Returns SFM_OK, or SFM_ENOTCONVERGED when the outer loop stopped early
+ * (the outputs are still written, as the reference continues in that case). */
+int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st);
+
+/* Same with DEVICE pointers on the context's device (no host copies).
+ * `stream` is a cudaStream_t or NULL for the context's own stream. */
+int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g,
+                     sfm_stats *st, void *stream);
+
+/* Adjoint of the solve: given dJ/dphi on the interior of every block
+ * (layout as psi; ghost entries ignored), returns dJ/drho on the interior of
+ * every block (layout as rho) for the linear map rho -> phi that sfm_solve
+ * converges to (the transposed composite operator).  No counterpart in the
+ * reference. */
+int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st);
+
+void sfm_destroy(sfm_ctx *c);
+const char *sfm_strerror(int code);
+
+/* Number of fmg sub-block levels (FMG_LevelMax+1, fmg_data.F90:113) and
+ * bytes of device memory held by the context. */
+int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SFMG_H */

@@ -1,0 +1,1541 @@
+// =============================================================================
+// sfmg_oracle.cpp -- CPU FP64 restatement of the reference's self-gravity FMG
+// Poisson solve.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA solver in
+// code_only_b200/: only tests/, __graft_entry__.smoke() and the cpu_baseline
+// leg of bench.py load it.  The product never calls it.
+//
+// Parity status: the reference (Fortran 90 + MPI) cannot be compiled or run in
+// this image (no Fortran compiler, no MPI) and ships no golden vectors or
+// known-answer tests for this path, so this restatement is "parity unpinned"
+// against the reference's own outputs.  It is pinned instead by analytic
+// known answers (discrete eigenmodes, exactness on linear potentials), by the
+// link-list invariants of fmg_check_linklist, and by the reference's own
+// stopping rule.
+//
+// The restatement follows the reference routine by routine, with every
+// array kept per (AMR level, fmg level, block) for the whole solve exactly as
+// GridLevel()%Block()%{U,Res,Rhs,Rho,Src,Psi,F} are (fmg_data.F90:35-43),
+// with the same loop, fill and pass orders, and with Fortran's left-to-right
+// evaluation of every arithmetic expression.  Single process: every MPI
+// exchange of the reference becomes a local copy (NPE = 1 semantics).
+//
+// Routine map (reference file:line -> function here):
+//   fmg_poisson / fmg_cycle       fmg.F90:63-74,134-233   -> Oracle::solve
+//   fmg_lin                       fmg.F90:270-377         -> fmg_lin
+//   fmg_rstrct/interp/addint/...  fmg.F90:750-946         -> fmg_rstrct, fmg_interp, ...
+//   fmg_get_h2absmax              fmg.F90:1017-1039       -> h2absmax
+//   fmg_poisson_flux/relax/resid  fmg_poisson.F90:53-265  -> poisson_flux, relax, resid
+//   fmg_psi2g                     fmg_poisson.F90:4-49    -> psi2g
+//   fmg_make_linklist/physvar     fmg_data_if.F90:13-411  -> build_links, make_physvar
+//   fmg_check_linklist            fmg_data_if.F90:415-568 -> check_linklist
+//   fmg_ghostcell_fix/...         fmg_ghostcell.F90:43-771-> ghostcell_fix, samelev, parentlev
+//   fmg_converge_c2p(_lev)        fmg_converge.F90:73-188 -> converge_c2p(_lev)
+//   fmg_fluxcorrection            fmg_reflux.F90:28-258   -> fluxcorrection
+//   fmg_boundary_fill0/extrap     fmg_boundary.F90:15-146 -> boundary_fill0, boundary_extrap
+//   periodic mg_boundary_u        fmg_boundary_phys_periodic.F90:71-104 -> mg_boundary_u
+//   sphere physical grid          fmg_boundary_phys_sphere.F90:81-354   -> boundary_physical_grid
+//   rstrct_linear/cubic           restriction.F90:22-151  -> rstrct_linear/_cubic
+//   interp_tricubic/trilinear     interpolation.F90:40-247-> interp_tricubic/_trilinear
+//   vmg_*                         vmg.F90:48-916, vmg_poisson.F90:6-145,
+//                                 vmg_interpol.F90:22-164 -> vmg_*
+//   mg_*                          mg.F90:42-804, mg_poisson.F90:5-79,
+//                                 mg_data.F90:45-559, mg_interpol_cubic.F90:89-125 -> mg_*
+// =============================================================================
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "../include/sfmg.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#define OMP_FOR _Pragma("omp parallel for schedule(static)")
+#else
+#define OMP_FOR
+#endif
+
+namespace {
+
+constexpr int Left = 0, Right = 1;
+constexpr int MX = 0, MY = 1, MZ = 2;
+constexpr int Undef = -1;
+
+// field codes (fmg_data.F90:89)
+enum { IU = 0, IRES, IRHS, IRHO, ISRC, IPSI, NCODE };
+
+inline int fdiv2(int i) { return (i >= 0) ? i / 2 : -((-i + 1) / 2); }   // IJKC(i,0) = floor(i/2)
+inline int modulo2(int i) { int r = i % 2; return r < 0 ? r + 2 : r; }   // Fortran MODULO(i,2)
+inline int near_(int nf, int nc) { return nc + 2 * modulo2(nf) - 1; }     // NEAR (interpolation.F90:55)
+
+// One field at one fmg level for every block: (-1:n)^3 per block, i fastest.
+struct Arr {
+    int n = 0, G = 0;
+    size_t V = 0;
+    std::vector<double> d;
+    void init(int nb, int n_) {
+        n = n_; G = n + 2; V = (size_t)G * G * G;
+        d.assign((size_t)nb * V, 0.0);
+    }
+    inline size_t idx(int i, int j, int k) const { return ((size_t)(k + 1) * G + (j + 1)) * G + (i + 1); }
+    inline double &at(int b, int i, int j, int k) { return d[(size_t)b * V + idx(i, j, k)]; }
+    inline double *blk(int b) { return d.data() + (size_t)b * V; }
+};
+
+// component access helper: cell (i,j,k) with coordinate `dir` set to `x`
+// and the two transverse coordinates (a, b): a is the lower axis.
+inline void put3(int dir, int x, int a, int b, int &i, int &j, int &k) {
+    if (dir == MX) { i = x; j = a; k = b; }
+    else if (dir == MY) { i = a; j = x; k = b; }
+    else { i = a; j = b; k = x; }
+}
+
+struct Oracle {
+    // ---------------- hierarchy ----------------
+    int nb = 0, nlev = 0, NI = 0, FMax = 0;
+    int ngb[3] = {0, 0, 0};
+    std::vector<int> lstart;                 // blocks of level L: [lstart[L], lstart[L+1])
+    std::vector<int> level, parent, child, nbr, octant;  // octant: 3 per block
+    std::vector<int> nbrGid;                 // Ancestry NeighborGid (same or parent level)
+    std::vector<char> sameLev, parLev, touch;
+    std::vector<double> h0, x0;
+    std::vector<int> baseIdx;                // GidBase(i,j,k) -> block
+
+    // ---------------- parameters ----------------
+    int bc = SFM_BC_PERIODIC, lmax = 3, zero_mean = 1, nfmgmax = 10, stagnation_exit = 1;
+    double four_pi_G = 4.0 * M_PI, errormax = 1e-3;
+
+    // ---------------- fmg fields ----------------
+    std::vector<Arr> fld;   // [code*(FMax+1) + f]
+    std::vector<Arr> flx;   // [dir*(FMax+1) + f]
+    int FmgLevel_fill0 = Undef;
+    double Resh2maxg = 0.0;
+    std::vector<double> vmgResmaxg;
+
+    // ---------------- mg (base grid) ----------------
+    int MMax = 0, NBc[3] = {0, 0, 0};     // base cells per dim at FMG level FMax
+    std::vector<Arr> mgf;                   // [code*(MMax+1) + m], single "block"
+    double mgResmaxg = 0.0;
+    bool mgTouch[6] = {false, false, false, false, false, false};
+    bool useSerialMg = true;
+
+    Arr &F(int code, int f) { return fld[code * (FMax + 1) + f]; }
+    Arr &FL(int dir, int f) { return flx[dir * (FMax + 1) + f]; }
+    Arr &MG(int code, int m) { return mgf[code * (MMax + 1) + m]; }
+    int nF(int f) const { return NI >> f; }
+    double h(int L, int f) const { return h0[L] * (double)(1 << f); }  // CellWidth*2**n (fmg_data.F90:288)
+    bool isLeaf(int b) const { return child[8 * b] == Undef; }
+    // fmg_skip_grid (fmg_data.F90:618-628)
+    bool skip(int b) const { return level[b] != nlev - 1 && child[8 * b] != Undef; }
+
+    // =====================================================================
+    // set-up
+    // =====================================================================
+    int setup(const sfm_hier_desc *hd, const sfm_params *p) {
+        nb = hd->nblocks; nlev = hd->nlev; NI = hd->ni;
+        if (nb <= 0 || nlev <= 0 || NI < 4 || (NI & (NI - 1)) || hd->nj != NI || hd->nk != NI) return SFM_EINVAL;
+        for (int d = 0; d < 3; d++) ngb[d] = hd->ngb[d];
+        // FMG_LevelMax = log2(min(NI,NJ,NK)) - 1 (fmg_data.F90:113)
+        FMax = 0; while ((2 << FMax) < NI) FMax++;
+        level.assign(hd->level, hd->level + nb);
+        parent.assign(hd->parent, hd->parent + nb);
+        child.assign(hd->child, hd->child + 8 * nb);
+        nbr.assign(hd->nbr, hd->nbr + 6 * nb);
+        touch.resize(6 * nb);
+        for (int i = 0; i < 6 * nb; i++) touch[i] = hd->touch[i] ? 1 : 0;
+        h0.assign(hd->cellwidth, hd->cellwidth + nlev);
+        x0.assign(hd->x0, hd->x0 + 3 * nb);
+        lstart.assign(nlev + 1, 0);
+        for (int b = 0; b < nb; b++) {
+            if (level[b] < 0 || level[b] >= nlev) return SFM_EHIER;
+            if (b > 0 && level[b] < level[b - 1]) return SFM_EHIER;
+            lstart[level[b] + 1]++;
+        }
+        for (int L = 0; L < nlev; L++) lstart[L + 1] += lstart[L];
+        bc = p->bc; lmax = p->lmax; zero_mean = p->zero_mean;
+        nfmgmax = p->max_outer; errormax = p->rel_tol; four_pi_G = p->four_pi_G;
+        stagnation_exit = p->stagnation_exit;
+        int rc = build_links();
+        if (rc) return rc;
+        rc = check_linklist();
+        if (rc) return rc;
+        // allocate all fields zero-initialised (fmg_alloc_arr zeroes, fmg_data.F90:393)
+        fld.resize(NCODE * (FMax + 1));
+        flx.resize(3 * (FMax + 1));
+        for (int c = 0; c < NCODE; c++)
+            for (int f = 0; f <= FMax; f++) F(c, f).init(nb, nF(f));
+        for (int d = 0; d < 3; d++)
+            for (int f = 0; f <= FMax; f++) FL(d, f).init(nb, nF(f));
+        vmgResmaxg.assign(nlev, 0.0);
+        // mg_data_init (mg_data.F90:45-90): base grid at FMG level FMax
+        for (int d = 0; d < 3; d++) NBc[d] = (ngb[d] * NI) >> FMax;
+        int boxsize = std::min(NBc[0], std::min(NBc[1], NBc[2]));
+        MMax = 0; while ((1 << MMax) < boxsize) MMax++;   // log2(boxsize)
+        if ((1 << MMax) != boxsize || NBc[0] != NBc[1] || NBc[1] != NBc[2]) {
+            // non-cubic or non-power-of-two base: UseSerialMg = .FALSE. (vmg.F90:85-91)
+            useSerialMg = false;
+        }
+        auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+        useSerialMg = pow2(ngb[0]) && pow2(ngb[1]) && pow2(ngb[2]) && NBc[0] == NBc[1] && NBc[1] == NBc[2];
+        if (useSerialMg) {
+            mgf.resize(NCODE * (MMax + 1));
+            for (int c = 0; c < NCODE; c++)
+                for (int m = 0; m <= MMax; m++) MG(c, m).init(1, NBc[0] >> m);
+            for (int i = 0; i < 6; i++) mgTouch[i] = false;
+            for (int b = lstart[0]; b < lstart[1]; b++)
+                for (int i = 0; i < 6; i++) mgTouch[i] = mgTouch[i] || touch[6 * b + i];
+        }
+        // GidBase(i,j,k) (grid.F90:54)
+        baseIdx.assign((size_t)ngb[0] * ngb[1] * ngb[2], -1);
+        for (int b = lstart[0]; b < lstart[1]; b++) {
+            int i = hd->ijk[3 * b], j = hd->ijk[3 * b + 1], k = hd->ijk[3 * b + 2];
+            if (i < 0 || j < 0 || k < 0 || i >= ngb[0] || j >= ngb[1] || k >= ngb[2]) return SFM_EHIER;
+            baseIdx[((size_t)k * ngb[1] + j) * ngb[0] + i] = b;
+        }
+        for (int v : baseIdx) if (v < 0) return SFM_EHIER;
+        return SFM_OK;
+    }
+
+    // fmg_make_linklist (fmg_data_if.F90:298-411), single rank.
+    int build_links() {
+        nbrGid.assign(6 * nb, Undef);
+        sameLev.assign(6 * nb, 0);
+        parLev.assign(6 * nb, 0);
+        octant.assign(3 * nb, Undef);
+        for (int b = 0; b < nb; b++)
+            for (int f = 0; f < 6; f++)
+                if (nbr[6 * b + f] != Undef) { nbrGid[6 * b + f] = nbr[6 * b + f]; sameLev[6 * b + f] = 1; }
+        // parent-level links, levels ascending (fmg_data_if.F90:377-395)
+        for (int L = 1; L < nlev; L++)
+            for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+                int p = parent[b];
+                if (p < 0 || p >= nb) return SFM_EHIER;
+                for (int f = 0; f < 6; f++) {
+                    if (sameLev[6 * b + f]) continue;
+                    int np = nbrGid[6 * p + f];
+                    if (np == Undef) continue;
+                    nbrGid[6 * b + f] = np;
+                    parLev[6 * b + f] = 1;
+                }
+            }
+        // octant of every block in its parent (fmg_left_or_right, fmg_data.F90:563-596)
+        for (int b = 0; b < nb; b++) {
+            if (level[b] == 0) continue;
+            int p = parent[b], found = 0;
+            for (int c = 0; c < 8; c++)
+                if (child[8 * p + c] == b) {
+                    octant[3 * b] = c & 1; octant[3 * b + 1] = (c >> 1) & 1; octant[3 * b + 2] = (c >> 2) & 1;
+                    found++;
+                }
+            if (found != 1) return SFM_EHIER;
+        }
+        return SFM_OK;
+    }
+
+    // fmg_check_linklist (fmg_data_if.F90:415-568) plus the proper-nesting
+    // requirement that a parent-level link ends on level L-1 (the reference
+    // indexes that block in level L-1's list, fmg_ghostcell.F90:350).
+    int check_linklist() {
+        for (int b = 0; b < nb; b++) {
+            int L = level[b];
+            if (L > 0) {   // parent -> child -> self
+                int p = parent[b];
+                if (level[p] != L - 1) return SFM_EHIER;
+                bool ok = false;
+                for (int c = 0; c < 8; c++) ok = ok || child[8 * p + c] == b;
+                if (!ok) return SFM_EHIER;
+            }
+            if (child[8 * b] != Undef) {   // child -> parent -> self
+                if (L == nlev - 1) return SFM_EHIER;
+                for (int c = 0; c < 8; c++) {
+                    int cb = child[8 * b + c];
+                    if (cb < 0 || cb >= nb || parent[cb] != b || level[cb] != L + 1) return SFM_EHIER;
+                }
+            } else {
+                for (int c = 1; c < 8; c++) if (child[8 * b + c] != Undef) return SFM_EHIER;
+            }
+            for (int dir = 0; dir < 3; dir++)
+                for (int lr = 0; lr < 2; lr++) {
+                    int f = lr + 2 * dir;
+                    int nbb = nbrGid[6 * b + f];
+                    if (sameLev[6 * b + f]) {   // neighbour symmetry
+                        int fs = (1 - lr) + 2 * dir;
+                        if (nbb < 0 || nbb >= nb || level[nbb] != L || nbr[6 * nbb + fs] != b) return SFM_EHIER;
+                        if (parLev[6 * b + f] || touch[6 * b + f]) return SFM_EHIER;
+                    }
+                    if (parLev[6 * b + f] && (nbb < 0 || level[nbb] != L - 1)) return SFM_EHIER;
+                    int cnt = (int)sameLev[6 * b + f] + (int)parLev[6 * b + f] + (int)touch[6 * b + f];
+                    if (cnt != 1) return SFM_EHIER;
+                }
+        }
+        return SFM_OK;
+    }
+
+    // =====================================================================
+    // fmg_make_physvar (fmg_data_if.F90:13-84) and fmg_prepare_interp
+    // (fmg_data_if.F90:176-217): U := psi_in, RHO := rho_in * 4 pi G on
+    // (-1:n)^3, then the leaf-volume mean of RHO is subtracted everywhere.
+    // =====================================================================
+    double make_physvar(const double *rho, const double *psi, int g) {
+        const int n = NI, Gi = NI + 2 * g;
+        Arr &U = F(IU, 0), &R = F(IRHO, 0);
+        for (int b = 0; b < nb; b++)
+            for (int k = -1; k <= n; k++)
+                for (int j = -1; j <= n; j++)
+                    for (int i = -1; i <= n; i++) {
+                        size_t s = (size_t)b * Gi * Gi * Gi + ((size_t)(k + g) * Gi + (j + g)) * Gi + (i + g);
+                        U.at(b, i, j, k) = psi ? psi[s] : 0.0;
+                        R.at(b, i, j, k) = rho[s] * four_pi_G;
+                    }
+        double rhoave = 0.0;
+        if (zero_mean) {
+            double mass = 0.0, vol = 0.0;
+            for (int L = 0; L < nlev; L++) {
+                double dv = h(L, 0) * h(L, 0) * h(L, 0);   // dv = h**3 (fmg_data.F90:290)
+                for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+                    if (child[8 * b] != Undef) continue;
+                    double s = 0.0;
+                    for (int k = 0; k < n; k++)
+                        for (int j = 0; j < n; j++)
+                            for (int i = 0; i < n; i++) s = s + R.at(b, i, j, k);
+                    mass = mass + s * dv;
+                    vol = vol + (double)(n * n * n) * dv;
+                }
+            }
+            rhoave = mass / vol;
+            for (double &v : R.d) v = v - rhoave;
+        }
+        return rhoave;
+    }
+
+    // =====================================================================
+    // block-wise BLAS-1 (fmg.F90:847-946)
+    // =====================================================================
+    void fill0(int f, int code) {   // fmg_fill0: non-skip grids, whole arrays
+        Arr &A = F(code, f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++)
+            if (!skip(b)) std::fill(A.blk(b), A.blk(b) + A.V, 0.0);
+    }
+    void copy(int f, int out, int in, bool noskip = false) {   // fmg_copy
+        Arr &O = F(out, f), &I = F(in, f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++)
+            if (noskip || !skip(b)) std::copy(I.blk(b), I.blk(b) + I.V, O.blk(b));
+    }
+    void add(int f, int a, int da) {   // fmg_add
+        Arr &A = F(a, f), &D = F(da, f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            double *x = A.blk(b), *y = D.blk(b);
+            for (size_t q = 0; q < A.V; q++) x[q] = x[q] + y[q];
+        }
+    }
+    // fmg_get_h2absmax (fmg.F90:1017-1039)
+    double h2absmax(int f, int code) {
+        Arr &A = F(code, f);
+        const int n = nF(f);
+        double m = 0.0;
+        for (int L = 0; L < nlev; L++) {
+            double h2 = h(L, f) * h(L, f);
+            for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+                if (skip(b)) continue;
+                double bm = 0.0;
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) bm = std::max(bm, std::fabs(A.at(b, i, j, k)));
+                m = std::max(m, bm * h2);
+            }
+        }
+        return m;
+    }
+
+    // =====================================================================
+    // restriction (restriction.F90:22-151)
+    // =====================================================================
+    // rstrct_linear: uc(ic..) for ic in [ics,ice] from uf(2*(ic-ic0)+ic0 ..)
+    static void rstrct_linear_cell(const Arr &Fa, int bf, int i0, int j0, int k0, double &out) {
+        const double rdv = 1.0 / 8.0;
+        auto uf = [&](int i, int j, int k) { return Fa.d[(size_t)bf * Fa.V + Fa.idx(i, j, k)]; };
+        out = (uf(i0, j0, k0) + uf(i0 + 1, j0, k0)
+             + uf(i0, j0 + 1, k0) + uf(i0, j0, k0 + 1)
+             + uf(i0 + 1, j0 + 1, k0) + uf(i0 + 1, j0, k0 + 1)
+             + uf(i0, j0 + 1, k0 + 1) + uf(i0 + 1, j0 + 1, k0 + 1)) * rdv;
+    }
+    static double St(int i, int j, int k) {   // rstrct_cubic_init (restriction.F90:38-63)
+        static const double s1d[4] = {-1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0};
+        return (s1d[i] * s1d[j]) * s1d[k];
+    }
+    static void rstrct_cubic_cell(const Arr &Fa, int bf, int i1, int j1, int k1, double &out) {
+        auto uf = [&](int i, int j, int k) { return Fa.d[(size_t)bf * Fa.V + Fa.idx(i, j, k)]; };
+        double s = 0.0;
+        bool first = true;
+        // same term order as restriction.F90:96-111: i fastest, then j, then k
+        for (int kk = 0; kk < 4; kk++)
+            for (int jj = 0; jj < 4; jj++)
+                for (int ii = 0; ii < 4; ii++) {
+                    double t = uf(i1 - 1 + ii, j1 - 1 + jj, k1 - 1 + kk) * St(ii, jj, kk);
+                    if (first) { s = t; first = false; } else s = s + t;
+                }
+        out = s;
+    }
+
+    // fmg_rstrct (fmg.F90:750-778): coarse fmg level f from f-1 within each
+    // non-skip block (the cubic form is used by the nonlinear path only)
+    void fmg_rstrct(int f, int iuc, int iuf) {
+        Arr &C = F(iuc, f), &Fa = F(iuf, f - 1);
+        const int nc = nF(f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            for (int kc = 0; kc < nc; kc++)
+                for (int jc = 0; jc < nc; jc++)
+                    for (int ic = 0; ic < nc; ic++)
+                        rstrct_linear_cell(Fa, b, 2 * ic, 2 * jc, 2 * kc, C.at(b, ic, jc, kc));
+        }
+    }
+
+    // =====================================================================
+    // fmg_converge_c2p (fmg_converge.F90:73-188)
+    // =====================================================================
+    void converge_c2p_lev(int Lc, int f, int code, bool cubic) {
+        Arr &A = F(code, f);
+        const int n = nF(f), h2n = n / 2;
+        const int Lf = Lc + 1;
+        OMP_FOR
+        for (int b = lstart[Lf]; b < lstart[Lf + 1]; b++) {
+            int p = parent[b];
+            int oi = octant[3 * b] * h2n, oj = octant[3 * b + 1] * h2n, ok = octant[3 * b + 2] * h2n;
+            for (int kc = 0; kc < h2n; kc++)
+                for (int jc = 0; jc < h2n; jc++)
+                    for (int ic = 0; ic < h2n; ic++) {
+                        double v;
+                        if (cubic) rstrct_cubic_cell(A, b, 2 * ic, 2 * jc, 2 * kc, v);
+                        else rstrct_linear_cell(A, b, 2 * ic, 2 * jc, 2 * kc, v);
+                        A.at(p, ic + oi, jc + oj, kc + ok) = v;
+                    }
+        }
+    }
+    void converge_c2p(int f, int code, bool cubic = false) {
+        for (int Lc = nlev - 2; Lc >= 0; Lc--) converge_c2p_lev(Lc, f, code, cubic);
+    }
+
+    // =====================================================================
+    // ghost cells (fmg_ghostcell.F90)
+    // =====================================================================
+    // same-level face copy, full transverse range (fmg_ghfix_samelev, :127-199)
+    void samelev(int L, int f, int dir, int code) {
+        Arr &A = F(code, f);
+        const int n = nF(f);
+        OMP_FOR
+        for (int b = lstart[L]; b < lstart[L + 1]; b++)
+            for (int lr = 0; lr < 2; lr++) {
+                int fc = lr + 2 * dir;
+                if (!sameLev[6 * b + fc]) continue;
+                int s = nbrGid[6 * b + fc];
+                int xr = (lr == Left) ? -1 : n;       // Recv
+                int xs = (lr == Left) ? n - 1 : 0;    // Send
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) {
+                        int i, j, k, is, js, ks;
+                        put3(dir, xr, p, q, i, j, k);
+                        put3(dir, xs, p, q, is, js, ks);
+                        A.at(b, i, j, k) = A.at(s, is, js, ks);
+                    }
+            }
+    }
+
+    // Lagrange weights of interpCubic / interp_tricubic for fine index p,
+    // coarse buffer bounds [lb, ub] (fmg_ghostcell.F90:577-598)
+    static void cubic_weights(int p, int lb, int ub, int c[4], double a[4]) {
+        int cP = fdiv2(p), cN = near_(p, cP);
+        int c1 = std::min(cP, cN), c2 = std::max(cP, cN);
+        int c0 = 2 * c1 - c2, c3 = 2 * c2 - c1;
+        int nshift = 0;
+        if (c3 > ub) nshift = c3 - ub;
+        if (c0 < lb) nshift = c0 - lb;
+        c0 -= nshift; c1 -= nshift; c2 -= nshift; c3 -= nshift;
+        double xc = cP + 0.25 * (double)(2 * modulo2(p) - 1);
+        a[0] = (xc - c1) * (xc - c2) * (xc - c3) / (double)((c0 - c1) * (c0 - c2) * (c0 - c3));
+        a[1] = (xc - c0) * (xc - c2) * (xc - c3) / (double)((c1 - c0) * (c1 - c2) * (c1 - c3));
+        a[2] = (xc - c0) * (xc - c1) * (xc - c3) / (double)((c2 - c0) * (c2 - c1) * (c2 - c3));
+        a[3] = (xc - c0) * (xc - c1) * (xc - c2) / (double)((c3 - c0) * (c3 - c1) * (c3 - c2));
+        c[0] = c0; c[1] = c1; c[2] = c2; c[3] = c3;
+    }
+
+    // coarse-fine ghost (fmg_ghfix_parentlev, :312-757).  `cubic` selects
+    // interpCubic when the transverse buffer has >= 4 cells
+    // (interpCubic_checkSize, :738-756), else interp (bilinear).
+    void parentlev(int L, int f, int dir, int code, bool cubic) {
+        if (L <= 0) return;
+        Arr &A = F(code, f);
+        const int n = nF(f), nb2 = n / 2;
+        const int W = nb2 + 2;           // buffer transverse extent: [-1, n/2]
+        const int GT = n + 2;            // fine transverse extent: [-1, n]
+        OMP_FOR
+        for (int b = lstart[L]; b < lstart[L + 1]; b++)
+            for (int lr = 0; lr < 2; lr++) {
+                int fc = lr + 2 * dir;
+                if (!parLev[6 * b + fc]) continue;
+                int cb = nbrGid[6 * b + fc];
+                // buffer = coarse layer adjacent to the face, octant half +-1
+                int xc = (lr == Left) ? n - 1 : 0;
+                int oa, ob;   // offsets of the two transverse axes from the octant
+                int ta = (dir == MX) ? MY : MX, tb = (dir == MZ) ? MY : MZ;
+                oa = octant[3 * b + ta] * nb2; ob = octant[3 * b + tb] * nb2;
+                std::vector<double> buf((size_t)W * W);
+                auto B = [&](int a, int bb) -> double & { return buf[(size_t)(bb + 1) * W + (a + 1)]; };
+                for (int q = -1; q <= nb2; q++)
+                    for (int p = -1; p <= nb2; p++) {
+                        int i, j, k;
+                        put3(dir, xc, p + oa, q + ob, i, j, k);
+                        B(p, q) = A.at(cb, i, j, k);
+                    }
+                std::vector<double> uH((size_t)GT * GT);
+                auto H = [&](int a, int bb) -> double & { return uH[(size_t)(bb + 1) * GT + (a + 1)]; };
+                bool useCubic = cubic && W >= 4;
+                if (!useCubic) {
+                    // bilinear (fmg_ghostcell.F90:443-465)
+                    for (int q = -1; q <= n; q++)
+                        for (int p = -1; p <= n; p++) {
+                            int pc = fdiv2(p), qc = fdiv2(q);
+                            int p1 = near_(p, pc), q1 = near_(q, qc);
+                            H(p, q) = (9.0 * B(pc, qc) + B(p1, q1) + 3.0 * B(pc, q1) + 3.0 * B(p1, qc)) / 16.0;
+                        }
+                } else {
+                    // bicubic: first along the lower transverse axis, then the
+                    // other (fmg_ghostcell.F90:567-695)
+                    std::vector<double> bx((size_t)GT * W);   // [q coarse][p fine]
+                    for (int q = -1; q <= nb2; q++)
+                        for (int p = -1; p <= n; p++) {
+                            int c[4]; double a[4];
+                            cubic_weights(p, -1, nb2, c, a);
+                            bx[(size_t)(q + 1) * GT + (p + 1)] =
+                                a[0] * B(c[0], q) + a[1] * B(c[1], q) + a[2] * B(c[2], q) + a[3] * B(c[3], q);
+                        }
+                    for (int q = -1; q <= n; q++) {
+                        int c[4]; double a[4];
+                        cubic_weights(q, -1, nb2, c, a);
+                        for (int p = -1; p <= n; p++)
+                            H(p, q) = a[0] * bx[(size_t)(c[0] + 1) * GT + (p + 1)]
+                                    + a[1] * bx[(size_t)(c[1] + 1) * GT + (p + 1)]
+                                    + a[2] * bx[(size_t)(c[2] + 1) * GT + (p + 1)]
+                                    + a[3] * bx[(size_t)(c[3] + 1) * GT + (p + 1)];
+                    }
+                }
+                // quadratic along the normal (fmg_ghostcell.F90:473-495)
+                int xg = (lr == Left) ? -1 : n;
+                int inner = (lr == Left) ? 1 : -1;
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) {
+                        int i, j, k, i0, j0, k0, iN, jN, kN;
+                        put3(dir, xg, p, q, i, j, k);
+                        put3(dir, xg + inner, p, q, i0, j0, k0);
+                        put3(dir, xg + 2 * inner, p, q, iN, jN, kN);
+                        double u0 = A.at(b, i0, j0, k0), uN = A.at(b, iN, jN, kN);
+                        A.at(b, i, j, k) = (10.0 * u0 + 8.0 * H(p, q) - 3.0 * uN) / 15.0;
+                    }
+            }
+    }
+
+    // fmg_ghostcell_fix (fmg_ghostcell.F90:43-55)
+    void ghostcell_fix(int f, int code, bool cubic = false) {
+        for (int L = 0; L < nlev; L++)
+            for (int dir = 0; dir < 3; dir++) {
+                parentlev(L, f, dir, code, cubic);
+                samelev(L, f, dir, code);
+            }
+    }
+
+    // =====================================================================
+    // physical boundary (fmg_boundary.F90)
+    // =====================================================================
+    void fill0_faces_block(Arr &A, int b, int n) {
+        for (int dir = 0; dir < 3; dir++)
+            for (int lr = 0; lr < 2; lr++) {
+                if (!touch[6 * b + lr + 2 * dir]) continue;
+                int x = (lr == Left) ? -1 : n;
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) {
+                        int i, j, k; put3(dir, x, p, q, i, j, k);
+                        A.at(b, i, j, k) = 0.0;
+                    }
+            }
+    }
+    void boundary_fill0(int f, int code) {   // all blocks (fmg_boundary.F90:15-54)
+        Arr &A = F(code, f);
+        const int n = nF(f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++) fill0_faces_block(A, b, n);
+    }
+    void extrap_block(Arr &A, int b, int n) {   // odd reflection, faces in order
+        for (int dir = 0; dir < 3; dir++)
+            for (int lr = 0; lr < 2; lr++) {
+                if (!touch[6 * b + lr + 2 * dir]) continue;
+                int x = (lr == Left) ? -1 : n, xi = (lr == Left) ? 0 : n - 1;
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) {
+                        int i, j, k, ii, jj, kk;
+                        put3(dir, x, p, q, i, j, k);
+                        put3(dir, xi, p, q, ii, jj, kk);
+                        A.at(b, i, j, k) = -A.at(b, ii, jj, kk);
+                    }
+            }
+    }
+    void boundary_extrap(int f, int code) {   // fmg_boundary.F90:89-146
+        Arr &A = F(code, f);
+        const int n = nF(f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++) extrap_block(A, b, n);
+    }
+
+    // fmg_boundary_physical_grid (fmg_boundary_phys_sphere.F90:81-354);
+    // a no-op for periodic (fmg_boundary_phys_periodic.F90:109-112)
+    void boundary_physical_grid(int ju, int jrho) {
+        if (bc != SFM_BC_SPHERE) return;
+        const int f = 0, n = NI;
+        Arr &R = F(jrho, f), &U = F(ju, f);
+        auto X = [&](int b, int d, int i) { return x0[3 * b + d] + (double)i * h0[level[b]]; };
+        // box extent from the corner base blocks' cell centres (fmg_bndp_xyzminmax)
+        int bmin = baseIdx[0], bmax = baseIdx.back();
+        double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
+        double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
+        double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        double rad2 = rr * rr;
+        for (int b = 0; b < nb; b++)
+            for (int k = -1; k <= n; k++)
+                for (int j = -1; j <= n; j++)
+                    for (int i = -1; i <= n; i++) {
+                        double x = X(b, 0, i), y = X(b, 1, j), z = X(b, 2, k);
+                        if (x * x + y * y + z * z >= rad2) R.at(b, i, j, k) = 0.0;
+                    }
+        double mom[25];
+        multipole_moments(R, mom);
+        // potential on the first ghost layer of every boundary-touching block
+        for (int b = 0; b < nb; b++)
+            for (int dir = 0; dir < 3; dir++)
+                for (int lr = 0; lr < 2; lr++) {
+                    if (!touch[6 * b + lr + 2 * dir]) continue;
+                    int xg = (lr == Left) ? -1 : n;
+                    for (int q = -1; q <= n; q++)
+                        for (int p = -1; p <= n; p++) {
+                            int i, j, k; put3(dir, xg, p, q, i, j, k);
+                            U.at(b, i, j, k) = multipole_eval(mom, X(b, 0, i), X(b, 1, j), X(b, 2, k));
+                        }
+                }
+    }
+
+    // moments a_lm over base-level interior cells (sphere.F90:132-242);
+    // l = 4 terms extend the reference (which stops at l = 3).
+    void multipole_moments(Arr &R, double *out) {
+        const int n = NI;
+        double dv = h0[0] * h0[0] * h0[0];
+        double a[25];
+        for (double &v : a) v = 0.0;
+        for (int b = lstart[0]; b < lstart[1]; b++)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) {
+                        double x = x0[3 * b] + (double)i * h0[0];
+                        double y = x0[3 * b + 1] + (double)j * h0[0];
+                        double z = x0[3 * b + 2] + (double)k * h0[0];
+                        double r2 = x * x + y * y + z * z;
+                        double r = std::sqrt(r2);
+                        double r3 = r2 * r;
+                        double rc = std::sqrt(x * x + y * y);
+                        double ri = 1 / r, rci = 1 / rc;
+                        double cost = z * ri, sint = rc * ri, cosp = x * rci, sinp = y * rci;
+                        double rhodv = R.at(b, i, j, k) * dv;
+                        a[0] = a[0] + rhodv;
+                        a[1] = a[1] + rhodv * r * cost;
+                        a[2] = a[2] + rhodv * r * sint * cosp;
+                        a[3] = a[3] + rhodv * r * sint * sinp;
+                        a[4] = a[4] + rhodv * r2 * (3 * (cost * cost) - 1);
+                        a[5] = a[5] + rhodv * r2 * sint * cost * cosp;
+                        a[6] = a[6] + rhodv * r2 * sint * cost * sinp;
+                        a[7] = a[7] + rhodv * r2 * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
+                        a[8] = a[8] + rhodv * r2 * (sint * sint) * 2 * sinp * cosp;
+                        a[9] = a[9] + rhodv * r3 * cost * (5 * (cost * cost) - 3);
+                        a[10] = a[10] + rhodv * r3 * sint * (5 * (cost * cost) - 1) * cosp;
+                        a[11] = a[11] + rhodv * r3 * sint * (5 * (cost * cost) - 1) * sinp;
+                        a[12] = a[12] + rhodv * r3 * cost * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
+                        a[13] = a[13] + rhodv * r3 * cost * (sint * sint) * 2 * sinp * cosp;
+                        a[14] = a[14] + rhodv * r3 * (sint * sint * sint) * cosp * ((cosp * cosp) - 3 * (sinp * sinp));
+                        a[15] = a[15] + rhodv * r3 * (sint * sint * sint) * sinp * (3 * (cosp * cosp) - (sinp * sinp));
+                        if (lmax >= 4) {
+                            double r4 = r2 * r2, c2 = cost * cost, s2 = sint * sint;
+                            double cos2p = (cosp * cosp) - (sinp * sinp), sin2p = 2 * sinp * cosp;
+                            double cos3p = cosp * ((cosp * cosp) - 3 * (sinp * sinp));
+                            double sin3p = sinp * (3 * (cosp * cosp) - (sinp * sinp));
+                            double cos4p = cos2p * cos2p - sin2p * sin2p, sin4p = 2 * sin2p * cos2p;
+                            a[16] = a[16] + rhodv * r4 * (35 * (c2 * c2) - 30 * c2 + 3);
+                            a[17] = a[17] + rhodv * r4 * sint * cost * (7 * c2 - 3) * cosp;
+                            a[18] = a[18] + rhodv * r4 * sint * cost * (7 * c2 - 3) * sinp;
+                            a[19] = a[19] + rhodv * r4 * s2 * (7 * c2 - 1) * cos2p;
+                            a[20] = a[20] + rhodv * r4 * s2 * (7 * c2 - 1) * sin2p;
+                            a[21] = a[21] + rhodv * r4 * s2 * sint * cost * cos3p;
+                            a[22] = a[22] + rhodv * r4 * s2 * sint * cost * sin3p;
+                            a[23] = a[23] + rhodv * r4 * (s2 * s2) * cos4p;
+                            a[24] = a[24] + rhodv * r4 * (s2 * s2) * sin4p;
+                        }
+                    }
+        const double pi = M_PI;
+        // normalisations (sphere.F90:227-242)
+        out[0] = -a[0] / (4.0 * pi);
+        out[1] = -a[1] / (4.0 * pi);
+        out[2] = -a[2] / (8.0 * pi);
+        out[3] = -a[3] / (8.0 * pi);
+        out[4] = -a[4] / (16.0 * pi);
+        out[5] = -a[5] / (8.0 * pi) * 3.0;
+        out[6] = -a[6] / (8.0 * pi) * 3.0;
+        out[7] = -a[7] / (32.0 * pi) * 3.0;
+        out[8] = -a[8] / (32.0 * pi) * 3.0;
+        out[9] = -a[9] / (16.0 * pi);
+        out[10] = -a[10] / (64.0 * pi) * 3.0;
+        out[11] = -a[11] / (64.0 * pi) * 3.0;
+        out[12] = -a[12] / (32.0 * pi) * 15.0;
+        out[13] = -a[13] / (32.0 * pi) * 15.0;
+        out[14] = -a[14] / (64.0 * pi) * 5.0;
+        out[15] = -a[15] / (64.0 * pi) * 5.0;
+        // l = 4: coefficient -(4pi)^-1 (2 - delta_m0) (4-m)!/(4+m)! C_m^2, where
+        // C_m is the constant factor of P_4^m that the sums above leave out
+        // (C = 1/8, 5/2, 15/2, 105, 105): 1/64, 5/8, 5/16, 35/8, 35/64.
+        out[16] = -a[16] / (4.0 * pi) * (1.0 / 64.0);
+        out[17] = -a[17] / (4.0 * pi) * (5.0 / 8.0);
+        out[18] = -a[18] / (4.0 * pi) * (5.0 / 8.0);
+        out[19] = -a[19] / (4.0 * pi) * (5.0 / 16.0);
+        out[20] = -a[20] / (4.0 * pi) * (5.0 / 16.0);
+        out[21] = -a[21] / (4.0 * pi) * (35.0 / 8.0);
+        out[22] = -a[22] / (4.0 * pi) * (35.0 / 8.0);
+        out[23] = -a[23] / (4.0 * pi) * (35.0 / 64.0);
+        out[24] = -a[24] / (4.0 * pi) * (35.0 / 64.0);
+    }
+
+    // U00..U33 (sphere.F90:267-293), plus the l = 4 extension
+    double multipole_eval(const double *m, double x, double y, double z) const {
+        double r2i = 1 / (x * x + y * y + z * z);
+        double ri = std::sqrt(r2i);
+        double r3i = r2i * ri;
+        double r4i = r2i * r2i;
+        double rc = std::sqrt(x * x + y * y);
+        double rci = 1 / rc;
+        double cost = z * ri, sint = rc * ri, cosp = x * rci, sinp = y * rci;
+        double U00 = ri * m[0];
+        double U10 = r2i * cost * m[1];
+        double U11 = r2i * sint * (cosp * m[2] + sinp * m[3]) * 2;
+        double U20 = r3i * (3 * (cost * cost) - 1) * m[4];
+        double U21 = r3i * sint * cost * (cosp * m[5] + sinp * m[6]) * 2;
+        double U22 = r3i * (sint * sint) * (((cosp * cosp) - (sinp * sinp)) * m[7] + 2 * sinp * cosp * m[8]) * 2;
+        double U30 = r4i * cost * (5 * (cost * cost) - 3) * m[9];
+        double U31 = r4i * sint * (5 * (cost * cost) - 1) * (cosp * m[10] + sinp * m[11]) * 2;
+        double U32 = r4i * cost * (sint * sint) * (((cosp * cosp) - (sinp * sinp)) * m[12] + 2 * sinp * cosp * m[13]) * 2;
+        double U33 = r4i * (sint * sint * sint) * (cosp * ((cosp * cosp) - 3 * (sinp * sinp)) * m[14]
+                                                  + sinp * (3 * (cosp * cosp) - (sinp * sinp)) * m[15]) * 2;
+        double ub = U00 + U10 + U11 + U20 + U21 + U22 + U30 + U31 + U32 + U33;
+        if (lmax >= 4) {
+            double r5i = r4i * ri, c2 = cost * cost, s2 = sint * sint;
+            double cos2p = (cosp * cosp) - (sinp * sinp), sin2p = 2 * sinp * cosp;
+            double cos3p = cosp * ((cosp * cosp) - 3 * (sinp * sinp));
+            double sin3p = sinp * (3 * (cosp * cosp) - (sinp * sinp));
+            double cos4p = cos2p * cos2p - sin2p * sin2p, sin4p = 2 * sin2p * cos2p;
+            double U40 = r5i * (35 * (c2 * c2) - 30 * c2 + 3) * m[16];
+            double U41 = r5i * sint * cost * (7 * c2 - 3) * (cosp * m[17] + sinp * m[18]);
+            double U42 = r5i * s2 * (7 * c2 - 1) * (cos2p * m[19] + sin2p * m[20]);
+            double U43 = r5i * s2 * sint * cost * (cos3p * m[21] + sin3p * m[22]);
+            double U44 = r5i * (s2 * s2) * (cos4p * m[23] + sin4p * m[24]);
+            ub = ub + U40 + U41 + U42 + U43 + U44;
+        }
+        return ub;
+    }
+
+    // =====================================================================
+    // Poisson operator (fmg_poisson.F90)
+    // =====================================================================
+    // fmg_poisson_flux (:53-124)
+    void poisson_flux(int f, int ju, bool bf0) {
+        if (FmgLevel_fill0 != f) {
+            converge_c2p(f, ju);
+            ghostcell_fix(f, ju);
+            if (bf0) boundary_fill0(f, ju);
+        }
+        FmgLevel_fill0 = Undef;
+        Arr &U = F(ju, f);
+        const int n = nF(f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            double hi = 1.0 / h(level[b], f);
+            for (int k = -1; k <= n - 1; k++)
+                for (int j = -1; j <= n - 1; j++)
+                    for (int i = -1; i <= n - 1; i++) {
+                        double u = U.at(b, i, j, k);
+                        FL(MX, f).at(b, i, j, k) = (U.at(b, i + 1, j, k) - u) * hi;
+                        FL(MY, f).at(b, i, j, k) = (U.at(b, i, j + 1, k) - u) * hi;
+                        FL(MZ, f).at(b, i, j, k) = (U.at(b, i, j, k + 1) - u) * hi;
+                    }
+        }
+        fluxcorrection(f);
+    }
+
+    // fmg_fluxcorrection (fmg_reflux.F90:28-258): for every fine face whose
+    // neighbour is at the parent level, the coarse flux on the matching face
+    // quarter becomes the mean of the 4 fine fluxes.  All reads precede all
+    // writes, as the reference packs before it unpacks.
+    void fluxcorrection(int f) {
+        const int n = nF(f), h2n = n / 2;
+        struct Item { int cb, dir, xc, ta0, tb0; std::vector<double> v; };
+        std::vector<Item> items;
+        for (int L = 1; L < nlev; L++)
+            for (int b = lstart[L]; b < lstart[L + 1]; b++)
+                for (int dir = 0; dir < 3; dir++)
+                    for (int lr = 0; lr < 2; lr++) {
+                        int fc = lr + 2 * dir;
+                        if (!parLev[6 * b + fc]) continue;
+                        Arr &Ff = FL(dir, f);
+                        int xf = (lr == Left) ? -1 : n - 1;       // Ifs(lr,ndir)
+                        Item it;
+                        it.cb = nbrGid[6 * b + fc];
+                        it.dir = dir;
+                        it.xc = (lr == Left) ? n - 1 : -1;        // Ics(lr,ndir)
+                        int ta = (dir == MX) ? MY : MX, tb = (dir == MZ) ? MY : MZ;
+                        it.ta0 = octant[3 * b + ta] * h2n;
+                        it.tb0 = octant[3 * b + tb] * h2n;
+                        it.v.resize((size_t)h2n * h2n);
+                        for (int qc = 0; qc < h2n; qc++)
+                            for (int pc = 0; pc < h2n; pc++) {
+                                int pf = 2 * pc, qf = 2 * qc;
+                                auto ff = [&](int p, int q) { int i, j, k; put3(dir, xf, p, q, i, j, k); return Ff.at(b, i, j, k); };
+                                it.v[(size_t)qc * h2n + pc] =
+                                    (ff(pf, qf) + ff(pf, qf + 1) + ff(pf + 1, qf) + ff(pf + 1, qf + 1)) * 0.25;
+                            }
+                        items.push_back(std::move(it));
+                    }
+        for (auto &it : items) {
+            Arr &Fc = FL(it.dir, f);
+            for (int qc = 0; qc < h2n; qc++)
+                for (int pc = 0; pc < h2n; pc++) {
+                    int i, j, k; put3(it.dir, it.xc, pc + it.ta0, qc + it.tb0, i, j, k);
+                    Fc.at(it.cb, i, j, k) = it.v[(size_t)qc * h2n + pc];
+                }
+        }
+    }
+
+    // divergence in Fortran's left-to-right order
+    inline double divF(int b, int f, int i, int j, int k) {
+        Arr &Fx = FL(MX, f), &Fy = FL(MY, f), &Fz = FL(MZ, f);
+        double t = Fx.at(b, i, j, k) - Fx.at(b, i - 1, j, k);
+        t = t + Fy.at(b, i, j, k);
+        t = t - Fy.at(b, i, j - 1, k);
+        t = t + Fz.at(b, i, j, k);
+        t = t - Fz.at(b, i, j, k - 1);
+        return t;
+    }
+
+    // fmg_poisson_relax (:130-213)
+    void relax(int f, int ju, int jrhs, bool bf0) {
+        const double sixth = 1.0 / 6.0;
+        const int n = nF(f);
+        double resmax = 0.0;
+        for (int ipass = 1; ipass <= 2; ipass++) {
+            poisson_flux(f, ju, bf0);
+            Arr &U = F(ju, f), &R = F(jrhs, f);
+            double pm = 0.0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) reduction(max : pm)
+#endif
+            for (int b = 0; b < nb; b++) {
+                if (skip(b)) continue;
+                double hh = h(level[b], f);
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = (j + k + ipass) % 2; i < n; i += 2) {
+                            double resh2 = (divF(b, f, i, j, k) - R.at(b, i, j, k) * hh) * hh;
+                            U.at(b, i, j, k) = U.at(b, i, j, k) + sixth * resh2;
+                            pm = std::max(pm, std::fabs(resh2));
+                        }
+            }
+            resmax = std::max(resmax, pm);
+        }
+        Resh2maxg = resmax;
+    }
+
+    // fmg_poisson_resid (:217-265)
+    void resid(int f, int jres, int ju, int jrhs, bool bf0) {
+        const int n = nF(f);
+        poisson_flux(f, ju, bf0);
+        Arr &Rs = F(jres, f), &R = F(jrhs, f);
+        OMP_FOR
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            double hi = 1.0 / h(level[b], f);
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++)
+                        Rs.at(b, i, j, k) = R.at(b, i, j, k) - divF(b, f, i, j, k) * hi;
+        }
+    }
+
+    // =====================================================================
+    // prolongation (interpolation.F90:40-247; fmg.F90:786-846)
+    // =====================================================================
+    // interp_trilinear for one fine cell: uc is the same block one level coarser
+    static double trilinear_cell(Arr &C, int bc_, int ifn, int jf, int kf, int oi, int oj, int ok) {
+        int ic = fdiv2(ifn) + oi, jc = fdiv2(jf) + oj, kc = fdiv2(kf) + ok;
+        int ic1 = near_(ifn, fdiv2(ifn)) + oi, jc1 = near_(jf, fdiv2(jf)) + oj, kc1 = near_(kf, fdiv2(kf)) + ok;
+        auto uc = [&](int i, int j, int k) { return C.at(bc_, i, j, k); };
+        return (27.0 * uc(ic, jc, kc)
+                + 9.0 * (uc(ic1, jc, kc) + uc(ic, jc1, kc) + uc(ic, jc, kc1))
+                + 3.0 * (uc(ic, jc1, kc1) + uc(ic1, jc, kc1) + uc(ic1, jc1, kc))
+                + uc(ic1, jc1, kc1)) / 64.0;
+    }
+    // interp_tricubic over a whole block (fine interior 0..n-1) from coarse
+    // array uc with buffer bounds [lb, ub] in each dim; falls back to
+    // trilinear when the extent is < 4 (interpolation.F90:87-96)
+    static void tricubic_block(Arr &Fo, int bf, Arr &C, int bcb, int n, int lb, int ub, int oi, int oj, int ok) {
+        // ics..ice as in interpolation.F90:62-84
+        int ics = std::max(fdiv2(0) - 2, lb), ice = std::min(fdiv2(n - 1) + 2, ub);
+        if (ice - ics + 1 < 4) {
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) Fo.at(bf, i, j, k) = trilinear_cell(C, bcb, i, j, k, oi, oj, ok);
+            return;
+        }
+        const int W = ice - ics + 1;
+        std::vector<double> bx((size_t)n * W * W), bxy((size_t)n * n * W);
+        for (int kc = ics; kc <= ice; kc++)
+            for (int jc = ics; jc <= ice; jc++)
+                for (int i = 0; i < n; i++) {
+                    int c[4]; double a[4];
+                    cubic_weights(i, lb, ub, c, a);
+                    bx[((size_t)(kc - ics) * W + (jc - ics)) * n + i] =
+                        a[0] * C.at(bcb, c[0] + oi, jc + oj, kc + ok) + a[1] * C.at(bcb, c[1] + oi, jc + oj, kc + ok)
+                      + a[2] * C.at(bcb, c[2] + oi, jc + oj, kc + ok) + a[3] * C.at(bcb, c[3] + oi, jc + oj, kc + ok);
+                }
+        for (int kc = ics; kc <= ice; kc++)
+            for (int j = 0; j < n; j++) {
+                int c[4]; double a[4];
+                cubic_weights(j, lb, ub, c, a);
+                for (int i = 0; i < n; i++) {
+                    auto X = [&](int jc) { return bx[((size_t)(kc - ics) * W + (jc - ics)) * n + i]; };
+                    bxy[((size_t)(kc - ics) * n + j) * n + i] = a[0] * X(c[0]) + a[1] * X(c[1]) + a[2] * X(c[2]) + a[3] * X(c[3]);
+                }
+            }
+        for (int k = 0; k < n; k++) {
+            int c[4]; double a[4];
+            cubic_weights(k, lb, ub, c, a);
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    auto Y = [&](int kc) { return bxy[((size_t)(kc - ics) * n + j) * n + i]; };
+                    Fo.at(bf, i, j, k) = a[0] * Y(c[0]) + a[1] * Y(c[1]) + a[2] * Y(c[2]) + a[3] * Y(c[3]);
+                }
+        }
+    }
+
+    // fmg_interp (fmg.F90:786-822)
+    void fmg_interp(int f, int iuf, int iuc, bool cubic) {
+        int lc = f + 1;
+        converge_c2p(lc, iuc, cubic);
+        ghostcell_fix(lc, iuc, cubic);
+        boundary_extrap(lc, iuc);
+        Arr &Fo = F(iuf, f), &C = F(iuc, lc);
+        const int n = nF(f), nc = nF(lc);
+        OMP_FOR
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            if (cubic) tricubic_block(Fo, b, C, b, n, -1, nc, 0, 0, 0);
+            else
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) Fo.at(b, i, j, k) = trilinear_cell(C, b, i, j, k, 0, 0, 0);
+        }
+        boundary_fill0(lc, iuc);
+        boundary_fill0(f, iuf);
+    }
+    void fmg_addint(int f, int juf, int juc, int jres) {   // fmg.F90:942-946
+        fmg_interp(f, jres, juc, false);
+        add(f, juf, jres);
+    }
+
+    // =====================================================================
+    // fmg_lin (fmg.F90:270-377)
+    // =====================================================================
+    void fmg_lin() {
+        const int Ncycle = 2, Npre = 2, Npost = 2;
+        for (int f = 1; f <= FMax; f++) fmg_rstrct(f, IRHO, IRHO);
+        fill0(FMax, IU);
+        vmg_fas(IU, IRHO);
+        for (int f = FMax - 1; f >= 0; f--) {
+            fmg_interp(f, IU, IU, true);
+            copy(f, IRHS, IRHO);
+            for (int jc = 1; jc <= Ncycle; jc++) {
+                for (int v = f; v <= FMax - 1; v++) {
+                    for (int jp = 1; jp <= Npre; jp++) relax(v, IU, IRHS, true);
+                    resid(v, IRES, IU, IRHS, true);
+                    fmg_rstrct(v + 1, IRHS, IRES);
+                    fill0(v + 1, IU);
+                    FmgLevel_fill0 = v + 1;
+                }
+                vmg_fas(IU, IRHS);
+                for (int v = FMax - 1; v >= f; v--) {
+                    fmg_addint(v, IU, IU, IRES);
+                    for (int jp = 1; jp <= Npost; jp++) relax(v, IU, IRHS, true);
+                }
+            }
+        }
+        converge_c2p(0, IU);
+    }
+
+    // =====================================================================
+    // vmg: FAS V-cycle over AMR levels at fmg level FMax (vmg.F90)
+    // =====================================================================
+    void vmg_copy(int L, int out, int in) {
+        Arr &O = F(out, FMax), &I = F(in, FMax);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++) std::copy(I.blk(b), I.blk(b) + I.V, O.blk(b));
+    }
+    void vmg_sub(int L, int out, int a, int bb) {
+        Arr &O = F(out, FMax), &A = F(a, FMax), &B = F(bb, FMax);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++)
+            for (size_t q = 0; q < O.V; q++) O.blk(b)[q] = A.blk(b)[q] - B.blk(b)[q];
+    }
+    void vmg_add(int L, int a, int da, bool onov) {
+        Arr &A = F(a, FMax), &D = F(da, FMax);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+            if (onov && child[8 * b] == Undef) continue;
+            for (size_t q = 0; q < A.V; q++) A.blk(b)[q] = A.blk(b)[q] + D.blk(b)[q];
+        }
+    }
+    void vmg_boundary_fill0(int L, int code) {
+        Arr &A = F(code, FMax);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++) fill0_faces_block(A, b, nF(FMax));
+    }
+    void vmg_boundary_extrap(int L, int code) {
+        Arr &A = F(code, FMax);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++) extrap_block(A, b, nF(FMax));
+    }
+    void vmg_ghostcell(int L, int code) {   // vmg.F90:729-743
+        for (int dir = 0; dir < 3; dir++) samelev(L, FMax, dir, code);
+        vmg_boundary_fill0(L, code);
+    }
+    void vmg_gridboundary(int L, int code) {   // vmg.F90:710-725 (CubicInterp = .FALSE. for Ngh = 1)
+        for (int dir = 0; dir < 3; dir++) parentlev(L, FMax, dir, code, false);
+        vmg_boundary_fill0(L, code);
+    }
+    void vmg_poisson_flux(int L, int ju) {   // vmg_poisson.F90:63-94
+        vmg_ghostcell(L, ju);
+        Arr &U = F(ju, FMax);
+        const int n = nF(FMax);
+        double hi = 1.0 / h(L, FMax);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++)
+            for (int k = -1; k <= n - 1; k++)
+                for (int j = -1; j <= n - 1; j++)
+                    for (int i = -1; i <= n - 1; i++) {
+                        double u = U.at(b, i, j, k);
+                        FL(MX, FMax).at(b, i, j, k) = (U.at(b, i + 1, j, k) - u) * hi;
+                        FL(MY, FMax).at(b, i, j, k) = (U.at(b, i, j + 1, k) - u) * hi;
+                        FL(MZ, FMax).at(b, i, j, k) = (U.at(b, i, j, k + 1) - u) * hi;
+                    }
+    }
+    void vmg_relax(int L, int ju, int jrhs) {   // vmg_poisson.F90:98-145
+        const double sixth = 1.0 / 6.0;
+        const int n = nF(FMax);
+        double hh = h(L, FMax), resmax = 0.0;
+        Arr &U = F(ju, FMax), &R = F(jrhs, FMax);
+        for (int ipass = 1; ipass <= 2; ipass++) {
+            vmg_poisson_flux(L, ju);
+            for (int b = lstart[L]; b < lstart[L + 1]; b++)
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = (j + k + ipass) % 2; i < n; i += 2) {
+                            double resh2 = (divF(b, FMax, i, j, k) - R.at(b, i, j, k) * hh) * hh;
+                            U.at(b, i, j, k) = U.at(b, i, j, k) + sixth * resh2;
+                            resmax = std::max(resmax, std::fabs(resh2));
+                        }
+        }
+        vmgResmaxg[L] = resmax / (hh * hh);
+    }
+    void vmg_rstrct(int Lc, int code, bool cubic) {   // vmg.F90:569-585
+        if (cubic)
+            for (int dir = 0; dir < 3; dir++) {
+                parentlev(Lc + 1, FMax, dir, code, true);
+                samelev(Lc + 1, FMax, dir, code);
+            }
+        converge_c2p_lev(Lc, FMax, code, cubic);
+    }
+    // vmg_poisson_tau (vmg_poisson.F90:6-59) + vmg_tau_crop (vmg.F90:463-505)
+    void vmg_tau(int L, int jtau, int ju) {
+        const int n = nF(FMax);
+        int Lf = L + 1;
+        if (Lf <= nlev - 1) {
+            Arr &T = F(jtau, FMax);
+            vmg_poisson_flux(Lf, ju);
+            double hi = 1.0 / h(Lf, FMax);
+            for (int b = lstart[Lf]; b < lstart[Lf + 1]; b++) {
+                std::fill(T.blk(b), T.blk(b) + T.V, 0.0);
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) T.at(b, i, j, k) = -(divF(b, FMax, i, j, k) * hi);
+            }
+            converge_c2p_lev(L, FMax, jtau, false);
+            vmg_poisson_flux(L, ju);
+            hi = 1.0 / h(L, FMax);
+            for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+                if (child[8 * b] == Undef) continue;
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) T.at(b, i, j, k) = T.at(b, i, j, k) + divF(b, FMax, i, j, k) * hi;
+            }
+        }
+        // crop (CubicInterp is .FALSE.): faces in the order Left x,y,z then Right x,y,z
+        if (Lf <= nlev - 1) {
+            Arr &T = F(jtau, FMax);
+            static const int order[6] = {0, 2, 4, 1, 3, 5};
+            for (int cb = lstart[Lf]; cb < lstart[Lf + 1]; cb++)
+                for (int o = 0; o < 6; o++) {
+                    int fc = order[o];
+                    if (!parLev[6 * cb + fc]) continue;
+                    int p = parent[cb], dir = fc / 2, lr = fc % 2;
+                    int x = (lr == Left) ? 0 : n - 1;
+                    for (int q = -1; q <= n; q++)
+                        for (int pp = -1; pp <= n; pp++) {
+                            int i, j, k; put3(dir, x, pp, q, i, j, k);
+                            T.at(p, i, j, k) = 0.0;
+                        }
+                }
+        }
+    }
+    // vmg_interp (vmg.F90:592-601) with vmg_interp_p2c_lev (vmg_interpol.F90:82-164)
+    void vmg_interp(int Lf, int juf, int juc) {
+        int Lc = Lf - 1;
+        vmg_ghostcell(Lc, juc);
+        vmg_boundary_extrap(Lc, juc);
+        Arr &Fo = F(juf, FMax), &C = F(juc, FMax);
+        const int n = nF(FMax), h2n = n / 2;
+        for (int p = lstart[Lc]; p < lstart[Lc + 1]; p++)
+            for (int c = 0; c < 8; c++) {
+                int cb = child[8 * p + c];
+                if (cb == Undef) continue;
+                int oi = (c & 1) * h2n, oj = ((c >> 1) & 1) * h2n, ok = ((c >> 2) & 1) * h2n;
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) Fo.at(cb, i, j, k) = trilinear_cell(C, p, i, j, k, oi, oj, ok);
+            }
+        vmg_boundary_fill0(Lc, juc);
+    }
+    // vmg_zeroAverage (vmg.F90:900-916) through fmg_ave (fmg_data.F90:730-769)
+    void vmg_zeroAverage(int L, int code) {
+        Arr &A = F(code, FMax);
+        const int n = nF(FMax);
+        double ave = 0.0;
+        int ngrid = 0;
+        for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+            ngrid++;
+            double s = 0.0;
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) s = s + A.at(b, i, j, k);
+            ave = ave + s;
+        }
+        ave = (ngrid == 0) ? 0.0 : ave / (double)(n * n * n * ngrid);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) A.at(b, i, j, k) = A.at(b, i, j, k) - ave;
+    }
+    void vmg_slvsml(int ju, int jrhs) {   // vmg.F90:387-432
+        if (!useSerialMg) {
+            for (int q = 0; q < 10; q++) vmg_relax(0, ju, jrhs);
+            return;
+        }
+        mg_dataPrepare(jrhs, ju);
+        mg_cycle();
+        mg_dataRestore(ju);
+    }
+    // vmg_fas (vmg.F90:116-243); IRUF is IPSI at FMax (vmg.F90:115)
+    void vmg_fas(int ju, int jrho) {
+        const int IRUF = IPSI;
+        if (jrho != IRHO)
+            for (int L = 0; L < nlev; L++) vmg_copy(L, IRHO, jrho);
+        converge_c2p(FMax, IU);
+        converge_c2p(FMax, IRHO);
+        boundary_fill0(FMax, IU);
+        for (int L = 0; L < nlev; L++) vmg_copy(L, IRHS, IRHO);
+        for (int v = nlev - 1; v >= 1; v--) {
+            vmg_gridboundary(v, IU);
+            for (int q = 0; q < 2; q++) vmg_relax(v, IU, IRHS);
+            vmg_rstrct(v - 1, IU, true);
+            vmg_copy(v - 1, IRUF, IU);
+            vmg_rstrct(v - 1, IRHS, false);
+            vmg_tau(v - 1, IRES, IU);
+            vmg_add(v - 1, IRHS, IRES, true);
+        }
+        if (zero_mean) vmg_zeroAverage(0, IRHS);
+        vmg_slvsml(IU, IRHS);
+        for (int v = 1; v <= nlev - 1; v++) {
+            vmg_sub(v - 1, IRES, IU, IRUF);
+            vmg_interp(v, IRES, IRES);
+            vmg_add(v, IU, IRES, false);
+            vmg_gridboundary(v, IU);
+            for (int q = 0; q < 2; q++) vmg_relax(v, IU, IRHS);
+        }
+        (void)ju;
+    }
+
+    // =====================================================================
+    // mg: uniform base-grid FMG (mg.F90, mg_poisson.F90, mg_data.F90)
+    // =====================================================================
+    double mg_h(int m) const { return h(0, FMax) * (double)(1 << m); }   // mg_get_h (mg_data.F90:554-559)
+    void mg_dataPrepare(int jrhs, int ju) {   // mg_data.F90:179-253: mg SRC, PSI <- base blocks
+        const int n = nF(FMax);
+        Arr &S = MG(ISRC, 0), &P = MG(IPSI, 0), &R = F(jrhs, FMax), &U = F(ju, FMax);
+        for (int kb = 0; kb < ngb[2]; kb++)
+            for (int jb = 0; jb < ngb[1]; jb++)
+                for (int ib = 0; ib < ngb[0]; ib++) {
+                    int b = baseIdx[((size_t)kb * ngb[1] + jb) * ngb[0] + ib];
+                    for (int k = 0; k < n; k++)
+                        for (int j = 0; j < n; j++)
+                            for (int i = 0; i < n; i++) {
+                                S.at(0, ib * n + i, jb * n + j, kb * n + k) = R.at(b, i, j, k);
+                                P.at(0, ib * n + i, jb * n + j, kb * n + k) = U.at(b, i, j, k);
+                            }
+                }
+    }
+    void mg_dataRestore(int ju) {   // mg_data.F90:257-330
+        const int n = nF(FMax);
+        Arr &P = MG(IPSI, 0), &U = F(ju, FMax);
+        for (int kb = 0; kb < ngb[2]; kb++)
+            for (int jb = 0; jb < ngb[1]; jb++)
+                for (int ib = 0; ib < ngb[0]; ib++) {
+                    int b = baseIdx[((size_t)kb * ngb[1] + jb) * ngb[0] + ib];
+                    for (int k = 0; k < n; k++)
+                        for (int j = 0; j < n; j++)
+                            for (int i = 0; i < n; i++) U.at(b, i, j, k) = P.at(0, ib * n + i, jb * n + j, kb * n + k);
+                }
+    }
+    // periodic wrap of one ghost layer (fmg_boundary_phys_periodic.F90:71-104);
+    // the sphere module's mg_boundary_u is a no-op
+    void mg_boundary_u(int m, int code) {
+        if (bc != SFM_BC_PERIODIC) return;
+        Arr &A = MG(code, m);
+        const int n = A.n;
+        for (int k = -1; k <= n; k++)
+            for (int j = -1; j <= n; j++) { A.at(0, -1, j, k) = A.at(0, n - 1, j, k); A.at(0, n, j, k) = A.at(0, 0, j, k); }
+        for (int k = -1; k <= n; k++)
+            for (int i = -1; i <= n; i++) { A.at(0, i, -1, k) = A.at(0, i, n - 1, k); A.at(0, i, n, k) = A.at(0, i, 0, k); }
+        for (int j = -1; j <= n; j++)
+            for (int i = -1; i <= n; i++) { A.at(0, i, j, -1) = A.at(0, i, j, n - 1); A.at(0, i, j, n) = A.at(0, i, j, 0); }
+    }
+    void mg_boundary_fill0(int m, int code) {   // mg.F90:735-750
+        Arr &A = MG(code, m);
+        const int n = A.n;
+        for (int dir = 0; dir < 3; dir++)
+            for (int lr = 0; lr < 2; lr++) {
+                if (!mgTouch[lr + 2 * dir]) continue;
+                int x = (lr == Left) ? -1 : n;
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) { int i, j, k; put3(dir, x, p, q, i, j, k); A.at(0, i, j, k) = 0.0; }
+            }
+    }
+    void mg_boundary_extrap(int m, int code) {   // mg.F90:754-771
+        Arr &A = MG(code, m);
+        const int n = A.n;
+        for (int dir = 0; dir < 3; dir++)
+            for (int lr = 0; lr < 2; lr++) {
+                if (!mgTouch[lr + 2 * dir]) continue;
+                int x = (lr == Left) ? -1 : n, xi = (lr == Left) ? 0 : n - 1;
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) {
+                        int i, j, k, ii, jj, kk;
+                        put3(dir, x, p, q, i, j, k); put3(dir, xi, p, q, ii, jj, kk);
+                        A.at(0, i, j, k) = -A.at(0, ii, jj, kk);
+                    }
+            }
+    }
+    void mg_resid(int m, int jres, int ju, int jrhs) {   // mg_poisson.F90:5-28
+        Arr &Rs = MG(jres, m), &U = MG(ju, m), &R = MG(jrhs, m);
+        const int n = U.n;
+        double hh = mg_h(m);
+        double h2i = 1.0 / (hh * hh);
+        mg_boundary_u(m, ju);
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) {
+                    double s = U.at(0, i + 1, j, k) + U.at(0, i - 1, j, k);
+                    s = s + U.at(0, i, j + 1, k);
+                    s = s + U.at(0, i, j - 1, k);
+                    s = s + U.at(0, i, j, k + 1);
+                    s = s + U.at(0, i, j, k - 1);
+                    s = s - 6.0 * U.at(0, i, j, k);
+                    Rs.at(0, i, j, k) = -h2i * s + R.at(0, i, j, k);
+                }
+    }
+    void mg_relax(int m, int ju, int jrhs) {   // mg_poisson.F90:32-79
+        const double sixth = 1.0 / 6.0;
+        Arr &U = MG(ju, m), &R = MG(jrhs, m);
+        const int n = U.n;
+        double hh = mg_h(m), h2 = hh * hh, resmax = 0.0;
+        for (int ipass = 1; ipass <= 2; ipass++) {
+            mg_boundary_u(m, ju);
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = (j + k + ipass) % 2; i < n; i += 2) {
+                        double s = U.at(0, i + 1, j, k) + U.at(0, i - 1, j, k);
+                        s = s + U.at(0, i, j + 1, k);
+                        s = s + U.at(0, i, j - 1, k);
+                        s = s + U.at(0, i, j, k + 1);
+                        s = s + U.at(0, i, j, k - 1);
+                        s = s - 6.0 * U.at(0, i, j, k);
+                        double resh2 = s - h2 * R.at(0, i, j, k);
+                        U.at(0, i, j, k) = U.at(0, i, j, k) + sixth * resh2;
+                        resmax = std::max(resmax, std::fabs(resh2));
+                    }
+        }
+        mgResmaxg = resmax / h2;
+    }
+    void mg_rstrct(int m, int iuc, int iuf) {   // mg.F90:581-602 (linear)
+        Arr &C = MG(iuc, m), &Fa = MG(iuf, m - 1);
+        const int n = C.n;
+        for (int k = 0; k < n; k++)
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i < n; i++) rstrct_linear_cell(Fa, 0, 2 * i, 2 * j, 2 * k, C.at(0, i, j, k));
+    }
+    void mg_interp(int m, int iuf, int iuc, bool cubic) {   // mg.F90:608-633
+        int lc = m + 1;
+        mg_boundary_extrap(lc, iuc);
+        mg_boundary_u(lc, iuc);
+        Arr &Fo = MG(iuf, m), &C = MG(iuc, lc);
+        const int n = Fo.n;
+        if (cubic) tricubic_block(Fo, 0, C, 0, n, -1, C.n, 0, 0, 0);
+        else
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) Fo.at(0, i, j, k) = trilinear_cell(C, 0, i, j, k, 0, 0, 0);
+        mg_boundary_fill0(m, iuf);
+        mg_boundary_fill0(lc, iuc);
+        mg_boundary_u(m, iuf);
+        mg_boundary_u(lc, iuc);
+    }
+    void mg_fill0(int m, int code) { std::fill(MG(code, m).d.begin(), MG(code, m).d.end(), 0.0); }
+    void mg_copy(int m, int out, int in) { MG(out, m).d = MG(in, m).d; }
+    void mg_addw(int m, int a, int da) {
+        Arr &A = MG(a, m), &D = MG(da, m);
+        for (size_t q = 0; q < A.d.size(); q++) A.d[q] = A.d[q] + D.d[q];
+    }
+    double mg_absmax(int m, int code) {
+        Arr &A = MG(code, m);
+        double v = 0.0;
+        for (int k = 0; k < A.n; k++)
+            for (int j = 0; j < A.n; j++)
+                for (int i = 0; i < A.n; i++) v = std::max(v, std::fabs(A.at(0, i, j, k)));
+        return v;
+    }
+    void mg_lin() {   // mg.F90:106-218
+        const int Ncycle = 2, Npre = 2, Npost = 2;
+        for (int m = 1; m <= MMax; m++) mg_rstrct(m, IRHO, IRHO);
+        mg_fill0(MMax, IU);
+        for (int q = 0; q < 2; q++) mg_relax(MMax, IU, IRHO);   // mg_slvsml (mg.F90:540-546)
+        for (int m = MMax - 1; m >= 0; m--) {
+            mg_interp(m, IU, IU, true);
+            mg_copy(m, IRHS, IRHO);
+            for (int jc = 1; jc <= Ncycle; jc++) {
+                for (int v = m; v <= MMax - 1; v++) {
+                    for (int q = 0; q < Npre; q++) mg_relax(v, IU, IRHS);
+                    mg_resid(v, IRES, IU, IRHS);
+                    mg_rstrct(v + 1, IRHS, IRES);
+                    mg_fill0(v + 1, IU);
+                }
+                for (int q = 0; q < 2; q++) mg_relax(MMax, IU, IRHS);
+                for (int v = MMax - 1; v >= m; v--) {
+                    mg_interp(v, IRES, IU, false);   // mg_addint (mg.F90:727-731)
+                    mg_addw(v, IU, IRES);
+                    for (int q = 0; q < Npost; q++) mg_relax(v, IU, IRHS);
+                }
+            }
+        }
+    }
+    void mg_cycle() {   // mg.F90:42-94 with ju = IPSI, jrho = ISRC
+        const double errmax = (double)1.e-2f;   // default-real literal (mg.F90:50)
+        mg_boundary_fill0(0, IPSI);
+        mg_boundary_u(0, IPSI);
+        double rhomax = 0.0;
+        for (int it = 1; it <= 10; it++) {
+            mg_resid(0, IRHO, IPSI, ISRC);
+            if (it == 1) rhomax = mg_absmax(0, IRHO);
+            mg_lin();
+            mg_addw(0, IPSI, IU);
+            if (mgResmaxg / rhomax < errmax) break;
+        }
+    }
+
+    // =====================================================================
+    // fmg_psi2g (fmg_poisson.F90:4-49)
+    // =====================================================================
+    void psi2g(int ju, double *g, int gw) {
+        poisson_flux(0, ju, false);
+        Arr &U = F(ju, 0);
+        const int n = NI, Gi = NI + 2 * gw;
+        const size_t V = (size_t)Gi * Gi * Gi;
+        for (int b = 0; b < nb; b++) {
+            double hi = 1.0 / h(level[b], 0);
+            double *gx = g + (size_t)b * 3 * V, *gy = gx + V, *gz = gy + V;
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) {
+                        size_t s = ((size_t)(k + gw) * Gi + (j + gw)) * Gi + (i + gw);
+                        if (skip(b)) {
+                            gx[s] = -((U.at(b, i + 1, j, k) - U.at(b, i - 1, j, k)) * hi * 0.5);
+                            gy[s] = -((U.at(b, i, j + 1, k) - U.at(b, i, j - 1, k)) * hi * 0.5);
+                            gz[s] = -((U.at(b, i, j, k + 1) - U.at(b, i, j, k - 1)) * hi * 0.5);
+                        } else {
+                            gx[s] = -((FL(MX, 0).at(b, i, j, k) + FL(MX, 0).at(b, i - 1, j, k)) * 0.5);
+                            gy[s] = -((FL(MY, 0).at(b, i, j, k) + FL(MY, 0).at(b, i, j - 1, k)) * 0.5);
+                            gz[s] = -((FL(MZ, 0).at(b, i, j, k) + FL(MZ, 0).at(b, i, j, k - 1)) * 0.5);
+                        }
+                    }
+        }
+    }
+
+    // true composite residual max_leaf |h^2 (SRC - L PSI)| (a fresh flux of PSI)
+    double composite_residual(int jpsi) {
+        int save = FmgLevel_fill0;
+        FmgLevel_fill0 = Undef;
+        resid(0, IRES, jpsi, ISRC, false);
+        FmgLevel_fill0 = save;
+        Arr &R = F(IRES, 0);
+        const int n = NI;
+        double m = 0.0;
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            double h2 = h(level[b], 0) * h(level[b], 0);
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) m = std::max(m, std::fabs(R.at(b, i, j, k)) * h2);
+        }
+        return m;
+    }
+
+    // =====================================================================
+    // fmg_cycle (fmg.F90:134-233).  stop_stage > 0 returns early with
+    // `dump` holding a field at fmg level 0 (diagnostics for tests):
+    //   1 SRC after set-up, 2 IRHO after the first fmg_resid,
+    //   3 IU after the first fmg_lin, 4 PSI after the outer loop.
+    // =====================================================================
+    int solve(const double *rho, double *psi, double *g, int gw, sfm_stats *st, int stop_stage, double *dump) {
+        double rhoave = make_physvar(rho, psi, gw);
+        FmgLevel_fill0 = Undef;
+        const int f = 0;
+        copy(f, IPSI, IU);
+        copy(f, ISRC, IRHO);
+        converge_c2p(f, ISRC);
+        converge_c2p(f, IPSI);
+        boundary_physical_grid(IPSI, ISRC);
+        double resh2max = h2absmax(0, ISRC);
+        if (stop_stage == 1) { dumpf(ISRC, dump); return SFM_OK; }
+        double ratio_prev = std::numeric_limits<double>::max();
+        int nmax = nfmgmax;
+        if (std::fabs(resh2max) <= std::numeric_limits<double>::min()) nmax = 0;
+        bool conv = true;
+        int iters = 0;
+        if (st) { std::memset(st, 0, sizeof(*st)); st->resh2max = resh2max; st->rho_mean = rhoave; }
+        bool reached = (nmax == 0);
+        for (int it = 1; it <= nmax; it++) {
+            resid(f, IRHO, IPSI, ISRC, false);
+            if (stop_stage == 2) { dumpf(IRHO, dump); return SFM_OK; }
+            fmg_lin();
+            if (stop_stage == 3) { dumpf(IU, dump); return SFM_OK; }
+            add(f, IPSI, IU);
+            iters = it;
+            double ratio = Resh2maxg / resh2max;
+            if (st && it <= SFM_MAX_HISTORY) st->ratio[it - 1] = ratio;
+            if (ratio < errormax) { reached = true; break; }
+            if (it == nmax) conv = false;
+            if (stagnation_exit && ratio > ratio_prev * 0.5) conv = false;
+            if (!conv) break;
+            ratio_prev = ratio;
+        }
+        if (stop_stage == 4) { dumpf(IPSI, dump); return SFM_OK; }
+        copy(f, IU, IPSI, true);
+        converge_c2p(f, IU);
+        if (g) psi2g(IU, g, gw);
+        else poisson_flux(0, IU, false);
+        // fmg_restore_u: U (with its ghost layer) back into the caller's array
+        if (psi) {
+            const int n = NI, Gi = NI + 2 * gw;
+            Arr &U = F(IU, 0);
+            for (int b = 0; b < nb; b++)
+                for (int k = -1; k <= n; k++)
+                    for (int j = -1; j <= n; j++)
+                        for (int i = -1; i <= n; i++)
+                            psi[(size_t)b * Gi * Gi * Gi + ((size_t)(k + gw) * Gi + (j + gw)) * Gi + (i + gw)] = U.at(b, i, j, k);
+        }
+        if (st) {
+            st->outer_iters = iters;
+            st->converged = (conv && reached) ? 1 : 0;
+            if (resh2max > 0) st->true_rel_residual = composite_residual(IU) / resh2max;
+        }
+        return (conv && reached) ? SFM_OK : SFM_ENOTCONVERGED;
+    }
+    void dumpf(int code, double *dump) {
+        if (!dump) return;
+        Arr &A = F(code, 0);
+        std::copy(A.d.begin(), A.d.end(), dump);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Runs the restated reference solve.  Arrays as in sfm_solve (ghost width
+// p->ngh_io).  Returns SFM_OK / SFM_ENOTCONVERGED / an error code.
+int oracle_solve(const sfm_hier_desc *h, const sfm_params *p, const double *rho, double *psi, double *g,
+                 sfm_stats *st, int stop_stage, double *dump) {
+    if (!h || !p || !rho) return SFM_EINVAL;
+    if (p->ngh_io < 1) return SFM_EINVAL;
+    Oracle *o = new Oracle();
+    int rc = o->setup(h, p);
+    if (rc == SFM_OK) rc = o->solve(rho, psi, g, p->ngh_io, st, stop_stage, dump);
+    delete o;
+    return rc;
+}
+
+// fmg_check_linklist on a hierarchy: SFM_OK or SFM_EHIER.
+int oracle_check_linklist(const sfm_hier_desc *h) {
+    sfm_params p;
+    std::memset(&p, 0, sizeof(p));
+    p.max_outer = 10; p.rel_tol = 1e-3; p.four_pi_G = 4.0 * M_PI; p.ngh_io = 1;
+    Oracle o;
+    return o.setup(h, &p);
+}
+
+// Composite operator applied to a potential: out = L(phi) on leaf interiors,
+// evaluated with the ghost fill and reflux of fmg_poisson_flux at fmg level 0
+// (no boundary fill0; physical ghosts as given in phi).  Layout ghost width 1.
+int oracle_apply_L(const sfm_hier_desc *h, const sfm_params *p, const double *phi, double *out) {
+    Oracle o;
+    int rc = o.setup(h, p);
+    if (rc) return rc;
+    Arr &U = o.F(IU, 0), &R = o.F(IRHS, 0);
+    std::copy(phi, phi + U.d.size(), U.d.begin());
+    std::fill(R.d.begin(), R.d.end(), 0.0);
+    o.FmgLevel_fill0 = Undef;
+    o.resid(0, IRES, IU, IRHS, false);
+    Arr &Rs = o.F(IRES, 0);
+    for (size_t q = 0; q < Rs.d.size(); q++) out[q] = -Rs.d[q];
+    return SFM_OK;
+}
+
+int oracle_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

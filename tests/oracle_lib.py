@@ -1,0 +1,53 @@
+"""ctypes loader of the CPU restatement in oracle/ (the checker)."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from code_only_b200 import abi, workloads
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+
+_lib = None
+
+
+def load_oracle():
+    global _lib
+    if _lib is not None:
+        return _lib
+    src = os.path.join(ORACLE_DIR, "sfmg_oracle.cpp")
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+    lib = C.CDLL(ORACLE_SO)
+    lib.oracle_solve.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.POINTER(abi.SfmStats), C.c_int, C.c_void_p]
+    lib.oracle_solve.restype = C.c_int
+    lib.oracle_check_linklist.argtypes = [C.POINTER(abi.SfmHierDesc)]
+    lib.oracle_check_linklist.restype = C.c_int
+    lib.oracle_apply_L.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p]
+    lib.oracle_apply_L.restype = C.c_int
+    lib.oracle_threads.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def oracle_solve(h, rho, params, psi=None, want_g=True, stage=0):
+    """Runs the oracle; returns (rc, psi, g, stats, dump)."""
+    lib = load_oracle()
+    d = abi.HierDesc(h)
+    psi = np.zeros_like(rho) if psi is None else np.array(psi, dtype=np.float64, copy=True)
+    g = np.zeros((h.nblocks, 3) + rho.shape[1:]) if want_g else None
+    st = abi.SfmStats()
+    G1 = h.ni + 2
+    dump = np.zeros((h.nblocks, G1, G1, G1)) if stage else None
+    rc = lib.oracle_solve(d.ref(), C.byref(params), np.ascontiguousarray(rho).ctypes.data, psi.ctypes.data,
+                          g.ctypes.data if g is not None else None, C.byref(st), stage,
+                          dump.ctypes.data if dump is not None else None)
+    return rc, psi, g, st, dump
+
+
+def make_rho(h, fn, ngh):
+    return workloads.block_field(h, ngh, fn)
