@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--workload", default="jeans6")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--single", choices=["mixed", "fp64"], default=None,
+                    help="run exactly one solve of that precision and exit (for profiler launch lists)")
     return ap.parse_args()
 
 
@@ -173,7 +175,8 @@ def time_device(solver, rho_d, psi_d, g_d, steps, warmup, world):
     """Device-timed solves (CUDA events on the solve's stream).  Returns
     (ms per solve over all ranks' max, last stats, launches, smoother stats)."""
     import torch
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()            # the solve and the events share this stream
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
     st = None
     for _ in range(warmup):
@@ -197,6 +200,26 @@ def time_device(solver, rho_d, psi_d, g_d, steps, warmup, world):
     barrier(world)
     ms = e0.elapsed_time(e1) / steps
     return max_over_ranks(ms, world), st, launches, (sm_ms, sm_n, sm_cells), iters
+
+
+def run_single(args):
+    """One solve (no warm-up) of the chosen precision: the launch list of a
+    profiler run then covers exactly one solve."""
+    import torch
+    from code_only_b200 import abi
+    from code_only_b200.solver import FMGPoisson
+    h, rho, bc = load_workload(args.workload)
+    rho_d = torch.from_numpy(rho).cuda()
+    psi_d = torch.zeros_like(rho_d)
+    G = rho.shape[1]
+    g_d = torch.zeros((h.nblocks, 3, G, G, G), dtype=torch.float64, device="cuda")
+    prec = abi.SFM_PREC_MIXED if args.single == "mixed" else abi.SFM_PREC_FP64
+    with FMGPoisson(h, params=params_for(bc, prec)) as s:
+        st = s.solve_device(rho_d.data_ptr(), psi_d.data_ptr(), g_d.data_ptr())
+        torch.cuda.synchronize()
+    print(json.dumps({"single": args.single, "workload": args.workload, "outer_iters": st.outer_iters,
+                      "true_rel_residual": st.true_rel_residual, "kernel_launches": st.kernel_launches,
+                      "device_ms": st.device_ms}), flush=True)
 
 
 def run_ours(args):
@@ -409,5 +432,7 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.single:
+        run_single(a)
     else:
         run_ours(a)
