@@ -897,6 +897,11 @@ int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out) {
         (p->bc != SFM_BC_PERIODIC && p->bc != SFM_BC_SPHERE) || (p->lmax != 3 && p->lmax != 4) ||
         (p->precision != SFM_PREC_FP64 && p->precision != SFM_PREC_MIXED))
         return SFM_EINVAL;
+    {   // the hierarchy is validated on the host before any device work
+        sfm::HostHier hh;
+        int vr = hh.build(h);
+        if (vr) return vr;
+    }
     int rc = check_device();
     if (rc) return rc;
     sfm_ctx *c = new (std::nothrow) sfm_ctx();

@@ -313,7 +313,7 @@ def gaussian_random_field(n: int, seed: int, kmin: float = 2.0, kmax: float = 64
     band = (kk >= kmin) & (kk <= kmax)
     amp[band] = kk[band] ** (slope / 2.0)
     noise = rng.standard_normal(kk.shape) + 1j * rng.standard_normal(kk.shape)
-    field = np.fft.irfftn(noise * amp, s=(n, n, n))
+    field = np.fft.irfftn(noise * amp, s=(n, n, n), axes=(0, 1, 2))
     field = (field - field.mean()) / field.std() * sigma
     rho = np.exp(field)
     return rho / rho.mean()

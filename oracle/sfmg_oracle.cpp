@@ -1530,6 +1530,22 @@ int oracle_apply_L(const sfm_hier_desc *h, const sfm_params *p, const double *ph
     return SFM_OK;
 }
 
+// Multipole potential of the isolated boundary (fmg_boundary_phys_sphere.F90):
+// moments of `src` (4 pi G rho, fmg level-0 layout, ghost width 1) over the
+// base-level interiors, evaluated at npts points xyz[3*npts] -> out[npts].
+int oracle_multipole(const sfm_hier_desc *h, const sfm_params *p, const double *src, int npts, const double *xyz,
+                     double *out) {
+    Oracle o;
+    int rc = o.setup(h, p);
+    if (rc) return rc;
+    Arr &R = o.F(ISRC, 0);
+    std::copy(src, src + R.d.size(), R.d.begin());
+    double mom[25];
+    o.multipole_moments(R, mom);
+    for (int q = 0; q < npts; q++) out[q] = o.multipole_eval(mom, xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]);
+    return SFM_OK;
+}
+
 int oracle_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

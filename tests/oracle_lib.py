@@ -30,6 +30,9 @@ def load_oracle():
     lib.oracle_apply_L.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p]
     lib.oracle_apply_L.restype = C.c_int
     lib.oracle_threads.restype = C.c_int
+    lib.oracle_multipole.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_int,
+                                     C.c_void_p, C.c_void_p]
+    lib.oracle_multipole.restype = C.c_int
     _lib = lib
     return lib
 

@@ -1,0 +1,69 @@
+"""The C-ABI library builds, loads and exports every entry point declared in
+include/*.h; argument checking works without a GPU (no compute calls)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from code_only_b200 import abi, workloads as w
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for fn in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not fn.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", fn)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?\w[\w\s\*]*?\b(sfm_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_every_declared_symbol_is_exported(sfmg_lib):
+    names = declared_functions()
+    assert set(abi.EXPORTED) <= set(names)
+    for n in names:
+        assert hasattr(sfmg_lib, n), n
+
+
+def test_default_params_match_reference_constants(sfmg_lib):
+    p = abi.SfmParams()
+    sfmg_lib.sfm_default_params(C.byref(p))
+    assert p.max_outer == 10 and p.rel_tol == 1e-3 and p.zero_mean == 1 and p.ngh_io == 2
+    assert p.four_pi_G == 4.0 * np.pi and p.precision == abi.SFM_PREC_FP64
+
+
+def test_strerror(sfmg_lib):
+    for code in range(0, -10, -1):
+        assert sfmg_lib.sfm_strerror(code)
+    assert b"unknown" in sfmg_lib.sfm_strerror(-99)
+
+
+def test_argument_errors(sfmg_lib):
+    h = w.small_periodic(2, 8, 2, 0)
+    ctx = C.c_void_p()
+    p = abi.default_params()
+    assert sfmg_lib.sfm_create(None, C.byref(p), C.byref(ctx)) == abi.SFM_EINVAL
+    bad = abi.default_params(ngh_io=0)
+    assert sfmg_lib.sfm_create(abi.HierDesc(h).ref(), C.byref(bad), C.byref(ctx)) == abi.SFM_EINVAL
+    bad = abi.default_params(lmax=7)
+    assert sfmg_lib.sfm_create(abi.HierDesc(h).ref(), C.byref(bad), C.byref(ctx)) == abi.SFM_EINVAL
+    assert sfmg_lib.sfm_solve(None, None, None, None, None) == abi.SFM_EINVAL
+    sfmg_lib.sfm_destroy(None)
+
+
+def test_without_gpu_create_reports_no_device(sfmg_lib):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    h = w.small_periodic(2, 8, 2, 0)
+    ctx = C.c_void_p()
+    p = abi.default_params()
+    assert sfmg_lib.sfm_create(abi.HierDesc(h).ref(), C.byref(p), C.byref(ctx)) == abi.SFM_EDEVICE
