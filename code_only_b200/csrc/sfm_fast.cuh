@@ -1,0 +1,344 @@
+// sfm_fast.cuh -- block-tiled kernels for the hot operations.
+//
+// These replace the per-element functors for the operations that dominate a
+// solve (ghost passes, red-black colour sweeps, residuals, restriction and
+// prolongation).  Each evaluates exactly the same expressions in the same
+// order as the functors of sfm_device.cuh (and as the reference), so FP64
+// results stay bit-identical; what changes is the work decomposition:
+//   - ghost passes: one warp per block face, compile-time index math;
+//   - smoother / residual: one CTA per block (or several small blocks), the
+//     block with its ghost shell staged in shared memory by coalesced loads,
+//     updated values written back as whole interior rows;
+//   - prolongation: the separable tricubic of interp_tricubic staged in
+//     shared memory per block, as the reference stages bufx/bufxy.
+#pragma once
+#include "sfm_device.cuh"
+
+namespace sfm {
+
+// ---------------------------------------------------------------------------
+// ghost pass: one warp per face item
+// ---------------------------------------------------------------------------
+template <class T, int N>
+__global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const FaceItem *__restrict__ items, int nitems,
+                                                    int dir, int cubic, int sel) {
+    constexpr int G = N + 2, NC = G * G;
+    constexpr int64_t V = (int64_t)G * G * G;
+    const int lane = threadIdx.x & 31;
+    const int it = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (it >= nitems) return;
+    const FaceItem fi = items[it];
+    if (sel >= 0 && fi.type != sel) return;
+    T *ud = u + (int64_t)fi.dst * V;
+    const int xg = fi.lr == 0 ? -1 : N;
+    if (fi.type == 0) {
+        const T *us = u + (int64_t)fi.src * V;
+        const int xs = fi.lr == 0 ? N - 1 : 0;
+#pragma unroll 4
+        for (int c = lane; c < NC; c += 32) {
+            const int p = c % G - 1, q = c / G - 1;
+            int i, j, k, is, js, ks;
+            put3(dir, xg, p, q, i, j, k);
+            put3(dir, xs, p, q, is, js, ks);
+            ud[cidx(G, i, j, k)] = us[cidx(G, is, js, ks)];
+        }
+        return;
+    }
+    const T *uc = u + (int64_t)fi.src * V;
+    constexpr int NB2 = N / 2;
+    const int xc = fi.lr == 0 ? N - 1 : 0;
+    const int oa = fi.oa * NB2, ob = fi.ob * NB2;
+    const int inner = fi.lr == 0 ? 1 : -1;
+    auto B = [&](int pb, int qb) -> T {
+        int ci, cj, ck;
+        put3(dir, xc, pb + oa, qb + ob, ci, cj, ck);
+        return uc[cidx(G, ci, cj, ck)];
+    };
+    for (int c = lane; c < NC; c += 32) {
+        const int p = c % G - 1, q = c / G - 1;
+        T uH;
+        if (cubic && NB2 + 2 >= 4) {
+            int cp[4], cq[4];
+            double wp[4], wq[4];
+            cubic_weights(p, -1, NB2, cp, wp);
+            cubic_weights(q, -1, NB2, cq, wq);
+            T bx[4];
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                bx[m] = (T)wp[0] * B(cp[0], cq[m]) + (T)wp[1] * B(cp[1], cq[m]) + (T)wp[2] * B(cp[2], cq[m])
+                      + (T)wp[3] * B(cp[3], cq[m]);
+            uH = (T)wq[0] * bx[0] + (T)wq[1] * bx[1] + (T)wq[2] * bx[2] + (T)wq[3] * bx[3];
+        } else {
+            const int pc = fdiv2(p), qc = fdiv2(q);
+            const int p1 = near_(p, pc), q1 = near_(q, qc);
+            uH = ((T)9 * B(pc, qc) + B(p1, q1) + (T)3 * B(pc, q1) + (T)3 * B(p1, qc)) / (T)16;
+        }
+        int i, j, k, i0, j0, k0, iN, jN, kN;
+        put3(dir, xg, p, q, i, j, k);
+        put3(dir, xg + inner, p, q, i0, j0, k0);
+        put3(dir, xg + 2 * inner, p, q, iN, jN, kN);
+        const T u0 = ud[cidx(G, i0, j0, k0)], uN = ud[cidx(G, iN, jN, kN)];
+        ud[cidx(G, i, j, k)] = ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// staging of BPC consecutive listed blocks (G^3 each) into shared memory
+// ---------------------------------------------------------------------------
+template <int N>
+struct Tile {
+    static constexpr int G = N + 2;
+    static constexpr int V = G * G * G;
+    static constexpr int CELLS = N * N * N;
+    // blocks per CTA: a CTA covers at least 512 cells
+    static constexpr int BPC = CELLS >= 512 ? 1 : 512 / CELLS;
+};
+
+template <class T, int N>
+__device__ __forceinline__ void stage_blocks(T *sh, const T *__restrict__ u, const int32_t *__restrict__ blocks,
+                                             int first, int nblk) {
+    using Tl = Tile<N>;
+    for (int t = threadIdx.x; t < Tl::BPC * Tl::V; t += blockDim.x) {
+        const int q = t / Tl::V, r = t - q * Tl::V;
+        if (first + q < nblk) sh[t] = u[(int64_t)blocks[first + q] * Tl::V + r];
+    }
+}
+
+// flux / divergence on a staged tile, with the reflux substitution of
+// Flux<T> (sfm_device.cuh) for coarse faces covered by finer blocks
+template <class T, int N>
+struct TileFlux {
+    const T *ub; T hi; const int *slot; const double *rbuf;
+    __device__ __forceinline__ T f(int dir, int i, int j, int k) const {
+        constexpr int G = N + 2;
+        if (slot) {
+            const int x = dir == 0 ? i : (dir == 1 ? j : k);
+            if (x == N - 1 || x == -1) {
+                const int s = slot[(x == -1 ? 0 : 1) + 2 * dir];
+                if (s >= 0) {
+                    const int a = dir == 0 ? j : i, c = dir == 2 ? j : k;
+                    return (T)rbuf[(int64_t)s * N * N + (int64_t)c * N + a];
+                }
+            }
+        }
+        const int i1 = i + (dir == 0), j1 = j + (dir == 1), k1 = k + (dir == 2);
+        return (ub[cidx(G, i1, j1, k1)] - ub[cidx(G, i, j, k)]) * hi;
+    }
+    __device__ __forceinline__ T div(int i, int j, int k) const {
+        T t = f(0, i, j, k) - f(0, i - 1, j, k);
+        t = t + f(1, i, j, k);
+        t = t - f(1, i, j - 1, k);
+        t = t + f(2, i, j, k);
+        t = t - f(2, i, j, k - 1);
+        return t;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// red-black colour sweep on listed blocks (fmg_poisson_relax / vmg_poisson_relax)
+// ---------------------------------------------------------------------------
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T *__restrict__ rhs,
+                                                     const int32_t *__restrict__ blocks, int nblk,
+                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
+                                                     const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
+                                                     int f, int ipass, unsigned long long *out) {
+    using Tl = Tile<N>;
+    constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2;
+    __shared__ T sh[BPC * V];
+    __shared__ int ssl[BPC][6];
+    const int first = blockIdx.x * BPC;
+    stage_blocks<T, N>(sh, u, blocks, first, nblk);
+    if (threadIdx.x < BPC * 6) {
+        const int q = threadIdx.x / 6, fc = threadIdx.x % 6;
+        ssl[q][fc] = (rslot && first + q < nblk) ? rslot[6 * blocks[first + q] + fc] : -1;
+    }
+    __syncthreads();
+    double m = 0.0;
+    for (int t = threadIdx.x; t < BPC * HALF; t += blockDim.x) {
+        const int q = t / HALF, r = t - q * HALF;
+        if (first + q >= nblk) continue;
+        const int b = blocks[first + q];
+        constexpr int HN = N / 2 > 0 ? N / 2 : 1;
+        int i2, j, k, i;
+        if (N == 1) { i2 = 0; j = 0; k = 0; }
+        else { i2 = r % HN; j = (r / HN) % N; k = r / (HN * N); }
+        i = 2 * i2 + ((j + k + ipass) & 1);
+        const double hd = hlev(h0, level[b], f);
+        const T hh = (T)hd, hi = (T)(1.0 / hd);
+        T *ub = sh + q * V;
+        TileFlux<T, N> F{ub, hi, rslot ? ssl[q] : nullptr, rbuf};
+        const int c = (int)cidx(G, i, j, k);
+        const T resh2 = (F.div(i, j, k) - rhs[(int64_t)b * V + c] * hh) * hh;
+        ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
+        const double a = fabs((double)resh2);
+        m = a > m ? a : m;
+    }
+    __syncthreads();
+    // write back the interior rows of every staged block
+    for (int t = threadIdx.x; t < BPC * Tl::CELLS; t += blockDim.x) {
+        const int q = t / Tl::CELLS, r = t - q * Tl::CELLS;
+        if (first + q >= nblk) continue;
+        const int i = r % N, j = (r / N) % N, k = r / (N * N);
+        const int c = (int)cidx(G, i, j, k);
+        u[(int64_t)blocks[first + q] * V + c] = sh[q * V + c];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t2 = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t2 > m ? t2 : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// residual res = rhs - div F / h on listed blocks (fmg_poisson_resid)
+template <class TU, class TR, class TO, int N>
+__global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const TU *__restrict__ u,
+                                                     const TR *__restrict__ rhs, const int32_t *__restrict__ blocks,
+                                                     int nblk, const double *__restrict__ h0,
+                                                     const int32_t *__restrict__ level, const int32_t *__restrict__ rslot,
+                                                     const double *__restrict__ rbuf, int f) {
+    using Tl = Tile<N>;
+    constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC;
+    __shared__ TU sh[BPC * V];
+    __shared__ int ssl[BPC][6];
+    const int first = blockIdx.x * BPC;
+    stage_blocks<TU, N>(sh, u, blocks, first, nblk);
+    if (threadIdx.x < BPC * 6) {
+        const int q = threadIdx.x / 6, fc = threadIdx.x % 6;
+        ssl[q][fc] = (rslot && first + q < nblk) ? rslot[6 * blocks[first + q] + fc] : -1;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < BPC * Tl::CELLS; t += blockDim.x) {
+        const int q = t / Tl::CELLS, r = t - q * Tl::CELLS;
+        if (first + q >= nblk) continue;
+        const int b = blocks[first + q];
+        const int i = r % N, j = (r / N) % N, k = r / (N * N);
+        const double hd = hlev(h0, level[b], f);
+        const TU hi = (TU)(1.0 / hd);
+        TileFlux<TU, N> F{sh + q * V, hi, rslot ? ssl[q] : nullptr, rbuf};
+        const int64_t c = (int64_t)b * V + cidx(G, i, j, k);
+        res[c] = (TO)((TU)rhs[c] - F.div(i, j, k) * hi);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// prolongation of listed blocks: fine level (N) interior from the same block
+// one fmg level coarser (N/2 + 2 cells with ghosts), tricubic staged as
+// interp_tricubic stages bufx / bufxy (interpolation.F90:98-217), or trilinear
+// ---------------------------------------------------------------------------
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const T *__restrict__ uc,
+                                                      const int32_t *__restrict__ blocks, int nblk, int cubic) {
+    constexpr int NC = N / 2, GC = NC + 2, GF = N + 2;
+    constexpr int VC = GC * GC * GC, VF = GF * GF * GF;
+    constexpr int W = GC;                  // coarse extent with ghosts = interp range [-1, NC]
+    __shared__ T sc[VC];
+    __shared__ T bx[N * W * W];            // [kc][jc][i]
+    __shared__ T bxy[N * N * W];           // [kc][j][i]
+    const int b = blocks[blockIdx.x];
+    (void)nblk;
+    for (int t = threadIdx.x; t < VC; t += blockDim.x) sc[t] = uc[(int64_t)b * VC + t];
+    __syncthreads();
+    T *ufb = uf + (int64_t)b * VF;
+    if (!(cubic && NC + 2 >= 4)) {
+        for (int t = threadIdx.x; t < N * N * N; t += blockDim.x) {
+            const int i = t % N, j = (t / N) % N, k = t / (N * N);
+            ufb[cidx(GF, i, j, k)] = trilinear_cell(sc, GC, i, j, k, 0, 0, 0);
+        }
+        return;
+    }
+    // x: bx(i, jc, kc) for kc, jc in [-1, NC]
+    for (int t = threadIdx.x; t < N * W * W; t += blockDim.x) {
+        const int i = t % N, jc = (t / N) % W - 1, kc = t / (N * W) - 1;
+        int c[4];
+        double w[4];
+        cubic_weights(i, -1, NC, c, w);
+        const T *row = sc + cidx(GC, 0, jc, kc);
+        bx[t] = (T)w[0] * row[c[0]] + (T)w[1] * row[c[1]] + (T)w[2] * row[c[2]] + (T)w[3] * row[c[3]];
+    }
+    __syncthreads();
+    // y: bxy(i, j, kc)
+    for (int t = threadIdx.x; t < N * N * W; t += blockDim.x) {
+        const int i = t % N, j = (t / N) % N, kc = t / (N * N) - 1;
+        int c[4];
+        double w[4];
+        cubic_weights(j, -1, NC, c, w);
+        auto X = [&](int jc) { return bx[((kc + 1) * W + (jc + 1)) * N + i]; };
+        bxy[t] = (T)w[0] * X(c[0]) + (T)w[1] * X(c[1]) + (T)w[2] * X(c[2]) + (T)w[3] * X(c[3]);
+    }
+    __syncthreads();
+    // z
+    for (int t = threadIdx.x; t < N * N * N; t += blockDim.x) {
+        const int i = t % N, j = (t / N) % N, k = t / (N * N);
+        int c[4];
+        double w[4];
+        cubic_weights(k, -1, NC, c, w);
+        auto Y = [&](int kc) { return bxy[((kc + 1) * N + j) * N + i]; };
+        ufb[cidx(GF, i, j, k)] = (T)w[0] * Y(c[0]) + (T)w[1] * Y(c[1]) + (T)w[2] * Y(c[2]) + (T)w[3] * Y(c[3]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// child -> parent restriction of one level: one CTA per BPC children
+// ---------------------------------------------------------------------------
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_converge_tiled(T *__restrict__ u, const int32_t *__restrict__ parent,
+                                                        const int8_t *__restrict__ oct, int first, int nchild,
+                                                        int cubic) {
+    using Tl = Tile<N>;
+    constexpr int G = Tl::G, V = Tl::V, H = N / 2 > 0 ? N / 2 : 1, PER = H * H * H;
+    constexpr int BPC = Tl::BPC;
+    const int c0 = blockIdx.x * BPC;
+    for (int t = threadIdx.x; t < BPC * PER; t += blockDim.x) {
+        const int q = t / PER, r = t - q * PER;
+        if (c0 + q >= nchild) continue;
+        const int b = first + c0 + q;
+        const int ic = r % H, jc = (r / H) % H, kc = r / (H * H);
+        const T *uf = u + (int64_t)b * V;
+        const T v = cubic ? rstrct_cubic(uf, G, 2 * ic, 2 * jc, 2 * kc) : rstrct_linear(uf, G, 2 * ic, 2 * jc, 2 * kc);
+        u[(int64_t)parent[b] * V + cidx(G, ic + oct[3 * b] * H, jc + oct[3 * b + 1] * H, kc + oct[3 * b + 2] * H)] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ordered FP64 sums: a warp stages 32 partial sums at a time in registers and
+// lane 0 adds them in list order -- the same sequence of roundings as a
+// single-thread loop, without its load latency
+// ---------------------------------------------------------------------------
+__global__ void k_mean_combine_w(const double *__restrict__ psum, const int32_t *__restrict__ blocks, int nblk,
+                                 const int32_t *__restrict__ level, const double *__restrict__ h0, int n,
+                                 double *out) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x >= 32 || blockIdx.x != 0) return;
+    double mass = 0.0, vol = 0.0;
+    const double ncell = (double)(n * n * n);
+    for (int base = 0; base < nblk; base += 32) {
+        double s = 0.0, dv = 0.0;
+        if (base + lane < nblk) {
+            s = psum[base + lane];
+            const double hd = h0[level[blocks[base + lane]]];
+            dv = hd * hd * hd;
+        }
+        const int cnt = nblk - base < 32 ? nblk - base : 32;
+        for (int l = 0; l < cnt; l++) {
+            const double sl = __shfl_sync(0xffffffffu, s, l), dl = __shfl_sync(0xffffffffu, dv, l);
+            mass = mass + sl * dl;
+            vol = vol + ncell * dl;
+        }
+    }
+    if (lane == 0) *out = mass / vol;
+}
+
+__global__ void k_ave_combine_w(const double *__restrict__ psum, int nblk, int n, double *out) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x >= 32 || blockIdx.x != 0) return;
+    double ave = 0.0;
+    for (int base = 0; base < nblk; base += 32) {
+        const double s = base + lane < nblk ? psum[base + lane] : 0.0;
+        const int cnt = nblk - base < 32 ? nblk - base : 32;
+        for (int l = 0; l < cnt; l++) ave = ave + __shfl_sync(0xffffffffu, s, l);
+    }
+    if (lane == 0) *out = nblk == 0 ? 0.0 : ave / (double)(n * n * n * nblk);
+}
+
+}  // namespace sfm

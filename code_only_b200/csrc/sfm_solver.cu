@@ -28,10 +28,22 @@
 #include "sfm_device.cuh"
 #include "sfm_kernels_misc.cuh"
 #include "sfm_mg.cuh"
+#include "sfm_fast.cuh"
 
 namespace sfm {
 
 constexpr int Undef = -1;
+
+// Runs BODY with a compile-time block edge N for the tiled kernels
+// (N = 2, 4, 8, 16); other sizes take the per-element functors.
+#define SFM_WITH_N(n, BODY, FALLBACK)                      \
+    switch (n) {                                           \
+        case 2: { constexpr int N = 2; BODY; } break;      \
+        case 4: { constexpr int N = 4; BODY; } break;      \
+        case 8: { constexpr int N = 8; BODY; } break;      \
+        case 16: { constexpr int N = 16; BODY; } break;    \
+        default: { FALLBACK; } break;                      \
+    }
 
 // ---------------------------------------------------------------------------
 // host copy of the hierarchy, links and invariants
@@ -234,7 +246,52 @@ public:
 
     int FmgLevel_fill0 = Undef;
 
+    // One defect-correction iteration of fmg_cycle (fmg.F90:183-185): the
+    // FP64 composite residual, fmg_lin, and phi += u.  The launch sequence is
+    // the same every iteration, so it is captured once as a CUDA graph and
+    // replayed; without stream capture it runs eagerly.
+    cudaGraphExec_t iterExec = nullptr;
+    int64_t iterLaunches = 0;
+    bool graphsOff = false;
+    void outer_iteration_body() {
+        resid<double, double, T>(0, RHO[0], PSI0, SRC0, false);
+        fmg_lin();
+        add(0, PSI0, U[0]);
+    }
+    void outer_iteration() {
+        if (graphsOff || P.profile) { outer_iteration_body(); return; }
+        if (!iterExec) {
+            int64_t l0 = launches;
+            int save = FmgLevel_fill0;
+            if (cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                cudaGetLastError();
+                graphsOff = true;
+                outer_iteration_body();
+                return;
+            }
+            outer_iteration_body();
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st_, &g);
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&iterExec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            iterLaunches = launches - l0;
+            launches = l0;
+            FmgLevel_fill0 = save;
+            if (e != cudaSuccess) {   // capture refused: run eagerly from now on
+                cudaGetLastError();
+                iterExec = nullptr;
+                graphsOff = true;
+                outer_iteration_body();
+                return;
+            }
+        }
+        cudaGraphLaunch(iterExec, st_);
+        launches += iterLaunches;
+        FmgLevel_fill0 = Undef;   // every iteration ends with a fresh flux at level 0
+    }
+
     ~Solver() override {
+        if (iterExec) cudaGraphExecDestroy(iterExec);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (own_) cudaStreamDestroy(own_);
@@ -429,17 +486,25 @@ public:
             for (int dir = 0; dir < 3; dir++) ghost_pass(L, f, dir, u, cubic);
     }
     template <class TT>
-    void ghost_pass(int L, int f, int dir, TT *u, bool cubic) {   // parentlev + samelev of (L, dir)
+    void ghost_pass(int L, int f, int dir, TT *u, bool cubic, int sel = -1) {   // parentlev/samelev of (L, dir)
         int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
         if (c <= 0) return;
         int GT = nf[f] + 2;
-        run(OpGhostPass<TT>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, -1}, c * GT * GT);
+        SFM_WITH_N(nf[f],
+                   (k_ghost_pass<TT, N><<<(unsigned)((c + 3) / 4), 128, 0, st_>>>(u, d_faces + o, (int)c, dir,
+                                                                                 cubic ? 1 : 0, sel),
+                    ++launches),
+                   run(OpGhostPass<TT>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, sel}, c * GT * GT))
     }
     template <class TT>
     void converge_c2p_lev(int Lc, int f, TT *u, bool cubic) {
         int Lf = Lc + 1, h = nf[f] / 2;
-        run(OpConverge<TT>{u, d_parent, d_oct, H.lstart[Lf], nf[f], Gf[f], Vf[f], cubic ? 1 : 0},
-            (int64_t)cnt(Lf) * h * h * h);
+        SFM_WITH_N(nf[f],
+                   (k_converge_tiled<TT, N><<<(unsigned)((cnt(Lf) + Tile<N>::BPC - 1) / Tile<N>::BPC), 256, 0, st_>>>(
+                        u, d_parent, d_oct, H.lstart[Lf], cnt(Lf), cubic ? 1 : 0),
+                    ++launches),
+                   run(OpConverge<TT>{u, d_parent, d_oct, H.lstart[Lf], nf[f], Gf[f], Vf[f], cubic ? 1 : 0},
+                       (int64_t)cnt(Lf) * h * h * h))
     }
     template <class TT>
     void converge_c2p(int f, TT *u, bool cubic = false) {
@@ -499,10 +564,19 @@ public:
             poisson_flux(f, u, bf0);
             bool prof = P.profile && f == 0 && profEv.size() < 2 * kMaxProf;
             if (prof) { profEv.push_back(nullptr); cudaEventCreate(&profEv.back()); cudaEventRecord(profEv.back(), st_); }
-            runMax(OpRelax<T, T>{u, rhs, d_leaves, d_h0, d_level, d_rslot, rbuf[f], f, n, Gf[f], Vf[f], ipass},
-                   (int64_t)nLeaves * n * n * n / 2, d_max + slot);
+            relax_launch(u, rhs, d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max + slot);
             if (prof) { profEv.push_back(nullptr); cudaEventCreate(&profEv.back()); cudaEventRecord(profEv.back(), st_); }
         }
+    }
+    void relax_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
+                      int f, int ipass, unsigned long long *out) {
+        const int n = nf[f];
+        SFM_WITH_N(n,
+                   (k_relax_tiled<T, N><<<(unsigned)((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC), 256, 0, st_>>>(
+                        u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
+                    ++launches),
+                   runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
+                          (int64_t)nblk * n * n * n / 2, out))
     }
     static constexpr size_t kMaxProf = 4096;
     std::vector<cudaEvent_t> profEv;
@@ -525,8 +599,13 @@ public:
     void resid(int f, TO *res, TU *u, const TR *rhs, bool bf0) {   // fmg_poisson_resid
         poisson_flux(f, u, bf0);
         const int n = nf[f];
-        run(OpResid<TU, TR, TO>{res, u, rhs, d_leaves, d_h0, d_level, d_rslot, rbuf[f], f, n, Gf[f], Vf[f]},
-            (int64_t)nLeaves * n * n * n);
+        SFM_WITH_N(n,
+                   (k_resid_tiled<TU, TR, TO, N><<<(unsigned)((nLeaves + Tile<N>::BPC - 1) / Tile<N>::BPC), 256, 0,
+                                                   st_>>>(res, u, rhs, d_leaves, nLeaves, d_h0, d_level, d_rslot,
+                                                          rbuf[f], f),
+                    ++launches),
+                   run(OpResid<TU, TR, TO>{res, u, rhs, d_leaves, d_h0, d_level, d_rslot, rbuf[f], f, n, Gf[f], Vf[f]},
+                       (int64_t)nLeaves * n * n * n))
     }
     void fmg_rstrct(int f, T *uc, const T *uf) {
         int nc = nf[f];
@@ -547,7 +626,11 @@ public:
         ghostcell_fix(lc, uc, cubic);
         boundary_extrap(lc, uc);
         const int n = nf[f];
-        run(OpInterp<T>{uf, uc, d_leaves, n, Gf[f], Gf[lc], Vf[f], Vf[lc], cubic ? 1 : 0}, (int64_t)nLeaves * n * n * n);
+        SFM_WITH_N(n,
+                   (k_interp_tiled<T, N><<<(unsigned)nLeaves, 256, 0, st_>>>(uf, uc, d_leaves, nLeaves, cubic ? 1 : 0),
+                    ++launches),
+                   run(OpInterp<T>{uf, uc, d_leaves, n, Gf[f], Gf[lc], Vf[f], Vf[lc], cubic ? 1 : 0},
+                       (int64_t)nLeaves * n * n * n))
         boundary_fill0(lc, uc);
         boundary_fill0(f, uf);
     }
@@ -588,19 +671,11 @@ public:
         boundary_fill0_level(L, F, u);
     }
     // same-level face copies of (L, dir) only (fmg_ghfix_samelev)
-    void ghost_pass_same(int L, int f, int dir, T *u) {
-        int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
-        if (c <= 0) return;
-        int GT = nf[f] + 2;
-        run(OpGhostPass<T>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, 0, 0}, c * GT * GT);
-    }
+    void ghost_pass_same(int L, int f, int dir, T *u) { ghost_pass(L, f, dir, u, false, 0); }
     // coarse-fine faces of (L, dir) only (fmg_ghfix_parentlev)
     void ghost_pass_parent(int L, int f, int dir, T *u, bool cubic) {
         if (L <= 0) return;
-        int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
-        if (c <= 0) return;
-        int GT = nf[f] + 2;
-        run(OpGhostPass<T>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, 1}, c * GT * GT);
+        ghost_pass(L, f, dir, u, cubic, 1);
     }
     void vmg_gridboundary(int L, T *u) {
         const int F = H.FMax;
@@ -611,8 +686,8 @@ public:
         const int F = H.FMax, n = nf[F];
         for (int ipass = 1; ipass <= 2; ipass++) {
             vmg_ghostcell(L, u);
-            runMax(OpRelax<T, T>{u, rhs, d_all + H.lstart[L], d_h0, d_level, nullptr, nullptr, F, n, Gf[F], Vf[F], ipass},
-                   (int64_t)cnt(L) * n * n * n / 2, d_max + 1);
+            (void)n;
+            relax_launch(u, rhs, d_all + H.lstart[L], cnt(L), nullptr, nullptr, F, ipass, d_max + 1);
         }
     }
     void vmg_rstrct(int Lc, T *u, bool cubic) {
@@ -655,7 +730,7 @@ public:
     void vmg_zeroAverage(T *a) {
         const int F = H.FMax, n = nf[F];
         run(OpBlockSum<T>{a, d_all, d_psum, n, Gf[F], Vf[F]}, (int64_t)cnt(0));
-        k_ave_combine<<<1, 1, 0, st_>>>(d_psum, cnt(0), n, d_scal + 1);
+        k_ave_combine_w<<<1, 32, 0, st_>>>(d_psum, cnt(0), n, d_scal + 1);
         ++launches;
         run(OpSubScalarInterior<T>{a, d_scal + 1, 0, n, Gf[F], Vf[F]}, (int64_t)cnt(0) * n * n * n);
     }
@@ -759,7 +834,7 @@ public:
         run(OpPhysvar<double>{PHI0, RES0d, rho, psi, H.NI, Gf[0], gw, Vf[0], P.four_pi_G, d_bad}, (int64_t)nb * Vf[0]);
         if (P.zero_mean) {
             run(OpBlockSum<double>{RES0d, d_leaves, d_psum, H.NI, Gf[0], Vf[0]}, (int64_t)nLeaves);
-            k_mean_combine<<<1, 1, 0, st_>>>(d_psum, d_leaves, nLeaves, d_level, d_h0, H.NI, d_scal);
+            k_mean_combine_w<<<1, 32, 0, st_>>>(d_psum, d_leaves, nLeaves, d_level, d_h0, H.NI, d_scal);
             ++launches;
             run(OpSubScalarAll<double>{RES0d, d_scal}, (int64_t)nb * Vf[0]);
         } else {
@@ -788,11 +863,14 @@ public:
         bool conv = true, reached = (nmax == 0);
         int iters = 0;
         for (int it = 1; it <= nmax; it++) {
-            resid<double, double, T>(0, RHO[0], PSI0, SRC0, false);
-            if (stop_stage == 2) { rc = check("resid"); return rc ? rc : dumpT(RHO[0], dump); }
-            fmg_lin();
-            if (stop_stage == 3) { rc = check("fmg_lin"); return rc ? rc : dumpT(U[0], dump); }
-            add(0, PSI0, U[0]);
+            if (stop_stage == 2 || stop_stage == 3) {
+                resid<double, double, T>(0, RHO[0], PSI0, SRC0, false);
+                if (stop_stage == 2) { rc = check("resid"); return rc ? rc : dumpT(RHO[0], dump); }
+                fmg_lin();
+                rc = check("fmg_lin");
+                return rc ? rc : dumpT(U[0], dump);
+            }
+            outer_iteration();
             rc = check("outer");
             if (rc) return rc;
             iters = it;
