@@ -4,8 +4,9 @@
 // The reference gathers the base level to rank 0 and runs mg_cycle there
 // serially (vmg.F90:407-428, mg_data.F90:179-330).  Here the whole cycle
 // (<= 10 defect corrections of an FMG with Ncycle 2, 2/2 smoothing) runs in
-// one CTA of 1024 threads on a base grid of at most 64^3 cells, its levels
-// resident in global memory (L2), every operation separated by
+// one CTA of 1024 threads on a base grid of at most 64^3 cells: the coarse
+// levels' working arrays in shared memory, level 0 and the data exchanged
+// with the AMR levels in global memory (L2), every operation separated by
 // __syncthreads; nothing returns to the host.  FP64 throughout (the
 // coarsest-level solve stays in FP64 in the mixed-precision path).
 #pragma once
@@ -195,9 +196,46 @@ __device__ double mg_lin(const MgData &d, double *sh) {
     return res;
 }
 
+// dynamic shared memory of the base-grid CTA
+__device__ __forceinline__ double *mg_dyn_smem() {
+    extern __shared__ double mg_smem[];
+    return mg_smem;
+}
+
+// Shared-memory plan: U, RES and RHS of the coarse levels m >= smem_from
+// live in shared memory (their values never carry over between calls:
+// mg_lin rewrites every cell it reads, mg.F90:142-215); level 0's arrays,
+// PSI, SRC and RHO stay in global memory.
+__host__ __device__ inline int mg_smem_from(int N, int MMax, size_t budget_doubles, size_t *used) {
+    size_t tot = 0;
+    int from = MMax + 1;
+    for (int m = MMax; m >= 0; m--) {
+        size_t G = (size_t)(N >> m) + 2, V = G * G * G;
+        if (tot + 3 * V > budget_doubles) break;
+        tot += 3 * V;
+        from = m;
+    }
+    if (used) *used = tot;
+    return from;
+}
+
 // mg_cycle (mg.F90:42-94) with ju = PSI, jrho = SRC; one CTA
-__global__ void __launch_bounds__(1024) k_mg_cycle(MgData d, int *iters_out) {
+__global__ void __launch_bounds__(1024) k_mg_cycle(MgData dg, int smem_from, int *iters_out) {
     __shared__ double sh[32];
+    MgData d = dg;
+    {
+        double *p = mg_dyn_smem();
+        for (int m = d.MMax; m >= smem_from; m--) {
+            size_t G = (size_t)(d.N >> m) + 2, V = G * G * G;
+            d.U[m] = p; p += V;
+            d.RES[m] = p; p += V;
+            d.RHS[m] = p; p += V;
+        }
+        const int64_t tot = p - mg_dyn_smem();
+        double *z = mg_dyn_smem();
+        for (int64_t t = threadIdx.x; t < tot; t += blockDim.x) z[t] = 0.0;
+        __syncthreads();
+    }
     const double errmax = (double)1.e-2f;   // default-real literal (mg.F90:50)
     mg_boundary_fill0(d, 0, d.PSI);
     mg_boundary_u(d, 0, d.PSI);

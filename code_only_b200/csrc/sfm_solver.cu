@@ -239,6 +239,8 @@ public:
     int *d_mgit = nullptr;
     // base grid
     MgData mg;
+    int mgSmemFrom = 0;
+    size_t mgSmemBytes = 0;
     bool useSerialMg = false;
     int NBc = 0;
     std::vector<std::pair<void *, size_t>> zeroList;   // re-zeroed at every solve
@@ -445,6 +447,16 @@ public:
                 mg.U[m] = mem.alloc<double>(V); mg.RES[m] = mem.alloc<double>(V);
                 mg.RHS[m] = mem.alloc<double>(V); mg.RHO[m] = mem.alloc<double>(V);
                 for (double *q : {mg.U[m], mg.RES[m], mg.RHS[m], mg.RHO[m]}) zeroList.push_back({q, V * sizeof(double)});
+            }
+            size_t used = 0;
+            mgSmemFrom = mg_smem_from(NBc, MMax, (size_t)200 * 1024 / sizeof(double), &used);
+            mgSmemBytes = used * sizeof(double);
+            if (mgSmemBytes > 48 * 1024 &&
+                cudaFuncSetAttribute(k_mg_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mgSmemBytes) !=
+                    cudaSuccess) {
+                cudaGetLastError();
+                mgSmemFrom = MMax + 1;   // no opt-in: all levels in global memory
+                mgSmemBytes = 0;
             }
             size_t G0 = (size_t)NBc + 2, V0 = G0 * G0 * G0;
             mg.SRC = mem.alloc<double>(V0); mg.PSI = mem.alloc<double>(V0);
@@ -742,7 +754,7 @@ public:
         const int F = H.FMax;
         int64_t N3 = (int64_t)NBc * NBc * NBc;
         run(OpMgGather<T>{mg.SRC, mg.PSI, rhs, u, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
-        k_mg_cycle<<<1, 1024, 0, st_>>>(mg, d_mgit);
+        k_mg_cycle<<<1, 1024, mgSmemBytes, st_>>>(mg, mgSmemFrom, d_mgit);
         ++launches;
         run(OpMgScatter<T>{u, mg.PSI, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
     }
