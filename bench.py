@@ -140,38 +140,22 @@ class ClockSampler:
 
 
 def dist_setup(n):
-    if n <= 1 and "RANK" not in os.environ:
-        return 0, 1, 0
-    import datetime
-    import torch.distributed as dist
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-    import torch
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                            device_id=torch.device("cuda", local))
-    return rank, world, local
+    from code_only_b200 import replicas
+    info = replicas.setup()
+    return info
 
 
-def max_over_ranks(x, world):
-    if world <= 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+def max_over_ranks(x, info):
+    from code_only_b200 import replicas
+    return replicas.max_over_ranks(info, x)
 
 
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+def barrier(info):
+    from code_only_b200 import replicas
+    replicas.barrier(info)
 
 
-def time_device(solver, rho_d, psi_d, g_d, steps, warmup, world):
+def time_device(solver, rho_d, psi_d, g_d, steps, warmup, info):
     """Device-timed solves (CUDA events on the solve's stream).  Returns
     (ms per solve over all ranks' max, last stats, launches, smoother stats)."""
     import torch
@@ -182,7 +166,7 @@ def time_device(solver, rho_d, psi_d, g_d, steps, warmup, world):
     for _ in range(warmup):
         psi_d.zero_()
         st = solver.solve_device(rho_d.data_ptr(), psi_d.data_ptr(), g_d.data_ptr(), sptr)
-    barrier(world)
+    barrier(info)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches, sm_ms, sm_n, sm_cells, iters = 0, 0.0, 0, 0, []
@@ -197,9 +181,9 @@ def time_device(solver, rho_d, psi_d, g_d, steps, warmup, world):
         iters.append(st.outer_iters)
     e1.record(stream)
     torch.cuda.synchronize()
-    barrier(world)
+    barrier(info)
     ms = e0.elapsed_time(e1) / steps
-    return max_over_ranks(ms, world), st, launches, (sm_ms, sm_n, sm_cells), iters
+    return max_over_ranks(ms, info), st, launches, (sm_ms, sm_n, sm_cells), iters
 
 
 def run_single(args):
@@ -228,10 +212,11 @@ def run_ours(args):
     from code_only_b200 import abi, build as b
     from code_only_b200.solver import FMGPoisson
 
-    rank, world, local = dist_setup(args.gpus)
+    info = dist_setup(args.gpus)
+    rank, world, local = info.rank, info.world, info.local
     if rank == 0:
         b.build(verbose=False)
-    barrier(world)
+    barrier(info)
     h, rho, bc = load_workload(args.workload)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -247,7 +232,7 @@ def run_ours(args):
         with FMGPoisson(h, params=params_for(bc, prec, profile=1)) as s:
             if key == "mixed" and sampler:
                 sampler.start()
-            ms, st, launches, smo, iters = time_device(s, rho_d, psi_d, g_d, args.steps, args.warmup, world)
+            ms, st, launches, smo, iters = time_device(s, rho_d, psi_d, g_d, args.steps, args.warmup, info)
             if key == "mixed" and sampler:
                 clocks = sampler.stop()
             results[key] = dict(ms=ms, st=st, launches=launches, smo=smo, iters=iters,
@@ -262,7 +247,7 @@ def run_ours(args):
             for _ in range(max(1, args.warmup // 2)):
                 psi_h[...] = 0.0
                 s.solve(rho_h, psi_h)
-            barrier(world)
+            barrier(info)
             t0 = time.perf_counter()
             for _ in range(args.steps):
                 psi_h[...] = 0.0
@@ -270,17 +255,16 @@ def run_ours(args):
                 if out not in (abi.SFM_OK, abi.SFM_ENOTCONVERGED):
                     raise RuntimeError(f"sfm_solve failed {out}")
             t1 = time.perf_counter()
-            barrier(world)
-            ms_e2e = max_over_ranks((t1 - t0) * 1e3 / args.steps, world)
+            barrier(info)
+            ms_e2e = max_over_ranks((t1 - t0) * 1e3 / args.steps, info)
             nbytes = rho.nbytes
             e2e = {"value": world * 1e3 / ms_e2e, "unit": "solves/s",
                    "h2d_bytes_per_step": 5 * nbytes,   # rho, psi (warm start), g (kept outside interiors)
                    "d2h_bytes_per_step": 4 * nbytes,   # psi, g
                    "timing": "host wall clock around blocking sfm_solve calls"}
     if rank != 0:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        from code_only_b200 import replicas
+        replicas.teardown(info)
         return
     mx, fp = results["mixed"], results["fp64"]
     value = world * 1e3 / mx["ms"]
@@ -348,9 +332,8 @@ def run_ours(args):
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(h, rho, bc, fp["iters"][-1], sample_iters=1)
     print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from code_only_b200 import replicas
+    replicas.teardown(info)
 
 
 def cpu_baseline(h, rho, bc, n_outer, sample_iters=1):
