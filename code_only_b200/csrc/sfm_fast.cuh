@@ -137,6 +137,23 @@ struct TileFlux {
 // ---------------------------------------------------------------------------
 // red-black colour sweep on listed blocks (fmg_poisson_relax / vmg_poisson_relax)
 // ---------------------------------------------------------------------------
+// CTA-wide max of non-negative doubles, folded into *out with one atomic
+__device__ __forceinline__ void cta_max_atomic(double m, unsigned long long *out) {
+    __shared__ double wm[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t2 = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t2 > m ? t2 : m;
+    }
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = wm[w] > r ? wm[w] : r;
+        if (r > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(r));
+    }
+}
+
+// persistent: each CTA walks tiles of BPC consecutive listed blocks
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T *__restrict__ rhs,
                                                      const int32_t *__restrict__ blocks, int nblk,
@@ -147,47 +164,50 @@ __global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T 
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2;
     __shared__ T sh[BPC * V];
     __shared__ int ssl[BPC][6];
-    const int first = blockIdx.x * BPC;
-    stage_blocks<T, N>(sh, u, blocks, first, nblk);
-    if (threadIdx.x < BPC * 6) {
-        const int q = threadIdx.x / 6, fc = threadIdx.x % 6;
-        ssl[q][fc] = (rslot && first + q < nblk) ? rslot[6 * blocks[first + q] + fc] : -1;
-    }
-    __syncthreads();
+    __shared__ T shh[BPC], shi[BPC];
+    const int ntiles = (nblk + BPC - 1) / BPC;
     double m = 0.0;
-    for (int t = threadIdx.x; t < BPC * HALF; t += blockDim.x) {
-        const int q = t / HALF, r = t - q * HALF;
-        if (first + q >= nblk) continue;
-        const int b = blocks[first + q];
-        constexpr int HN = N / 2 > 0 ? N / 2 : 1;
-        int i2, j, k, i;
-        if (N == 1) { i2 = 0; j = 0; k = 0; }
-        else { i2 = r % HN; j = (r / HN) % N; k = r / (HN * N); }
-        i = 2 * i2 + ((j + k + ipass) & 1);
-        const double hd = hlev(h0, level[b], f);
-        const T hh = (T)hd, hi = (T)(1.0 / hd);
-        T *ub = sh + q * V;
-        TileFlux<T, N> F{ub, hi, rslot ? ssl[q] : nullptr, rbuf};
-        const int c = (int)cidx(G, i, j, k);
-        const T resh2 = (F.div(i, j, k) - rhs[(int64_t)b * V + c] * hh) * hh;
-        ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
-        const double a = fabs((double)resh2);
-        m = a > m ? a : m;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int first = tile * BPC;
+        stage_blocks<T, N>(sh, u, blocks, first, nblk);
+        if (threadIdx.x < BPC * 6) {
+            const int q = threadIdx.x / 6, fc = threadIdx.x % 6;
+            ssl[q][fc] = (rslot && first + q < nblk) ? rslot[6 * blocks[first + q] + fc] : -1;
+        }
+        if (threadIdx.x < BPC && first + (int)threadIdx.x < nblk) {
+            const double hd = hlev(h0, level[blocks[first + threadIdx.x]], f);
+            shh[threadIdx.x] = (T)hd;
+            shi[threadIdx.x] = (T)(1.0 / hd);
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < BPC * HALF; t += blockDim.x) {
+            const int q = t / HALF, r = t - q * HALF;
+            if (first + q >= nblk) continue;
+            const int b = blocks[first + q];
+            constexpr int HN = N / 2;
+            const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
+            const int i = 2 * i2 + ((j + k + ipass) & 1);
+            const T hh = shh[q], hi = shi[q];
+            T *ub = sh + q * V;
+            TileFlux<T, N> F{ub, hi, rslot ? ssl[q] : nullptr, rbuf};
+            const int c = (int)cidx(G, i, j, k);
+            const T resh2 = (F.div(i, j, k) - rhs[(int64_t)b * V + c] * hh) * hh;
+            ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
+            const double a = fabs((double)resh2);
+            m = a > m ? a : m;
+        }
+        __syncthreads();
+        // write back the interior rows of every staged block
+        for (int t = threadIdx.x; t < BPC * Tl::CELLS; t += blockDim.x) {
+            const int q = t / Tl::CELLS, r = t - q * Tl::CELLS;
+            if (first + q >= nblk) continue;
+            const int i = r % N, j = (r / N) % N, k = r / (N * N);
+            const int c = (int)cidx(G, i, j, k);
+            u[(int64_t)blocks[first + q] * V + c] = sh[q * V + c];
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    // write back the interior rows of every staged block
-    for (int t = threadIdx.x; t < BPC * Tl::CELLS; t += blockDim.x) {
-        const int q = t / Tl::CELLS, r = t - q * Tl::CELLS;
-        if (first + q >= nblk) continue;
-        const int i = r % N, j = (r / N) % N, k = r / (N * N);
-        const int c = (int)cidx(G, i, j, k);
-        u[(int64_t)blocks[first + q] * V + c] = sh[q * V + c];
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        const double t2 = __shfl_xor_sync(0xffffffffu, m, o);
-        m = t2 > m ? t2 : m;
-    }
-    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    cta_max_atomic(m, out);
 }
 
 // residual res = rhs - div F / h on listed blocks (fmg_poisson_resid)

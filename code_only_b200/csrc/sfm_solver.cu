@@ -211,6 +211,7 @@ public:
     cudaStream_t st_ = nullptr;    // stream of the current call (caller's or own_)
     int64_t launches = 0;
     int maxBlocks = 148 * 16;
+    int persistGrid = 148 * 8;   // CTAs of a persistent tiled sweep (set from the SM count in init)
 
     // device tables
     int32_t *d_level = nullptr, *d_parent = nullptr, *d_rslot = nullptr, *d_all = nullptr, *d_leaves = nullptr;
@@ -309,6 +310,13 @@ public:
         P = *p;
         if (cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking) != cudaSuccess) return SFM_ECUDA;
         st_ = own_;
+        {
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+            persistGrid = sms * 8;
+            maxBlocks = sms * 16;
+        }
         cudaEventCreate(&ev0);
         cudaEventCreate(&ev1);
         const int nb = H.nb, nlev = H.nlev, FMax = H.FMax;
@@ -584,8 +592,8 @@ public:
                       int f, int ipass, unsigned long long *out) {
         const int n = nf[f];
         SFM_WITH_N(n,
-                   (k_relax_tiled<T, N><<<(unsigned)((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC), 256, 0, st_>>>(
-                        u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
+                   (k_relax_tiled<T, N><<<(unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
+                                          256, 0, st_>>>(u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
                     ++launches),
                    runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
                           (int64_t)nblk * n * n * n / 2, out))
