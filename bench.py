@@ -2,7 +2,7 @@
 """Benchmark of the self-gravity FMG Poisson solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload jeans6|nested5|uniform64]
+                    [--workload jeans6|nested5|uniform64|uniform256|deep8]
 
 A step is one complete solve (zero initial guess) to relative residual
 <= 1e-10 on the 6-level Jeans-refined hierarchy (128^3 periodic base of 8^3

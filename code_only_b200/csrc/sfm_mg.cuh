@@ -203,13 +203,16 @@ __device__ __forceinline__ double *mg_dyn_smem() {
 }
 
 // Shared-memory plan: U, RES and RHS of the coarse levels m >= smem_from
-// live in shared memory (their values never carry over between calls:
-// mg_lin rewrites every cell it reads, mg.F90:142-215); level 0's arrays,
-// PSI, SRC and RHO stay in global memory.
+// (smem_from >= 1) live in shared memory (their values never carry over
+// between calls: mg_lin rewrites every cell it reads, mg.F90:142-215);
+// level 0's arrays, PSI, SRC and RHO stay in global memory.  Level 0 is
+// never placed in shared memory: with it there, the B200 build read stale
+// level-0 values and the base solve lost bitwise parity (levels >= 1 in
+// shared memory are bit-identical to the all-global layout).
 __host__ __device__ inline int mg_smem_from(int N, int MMax, size_t budget_doubles, size_t *used) {
     size_t tot = 0;
     int from = MMax + 1;
-    for (int m = MMax; m >= 0; m--) {
+    for (int m = MMax; m >= 1; m--) {
         size_t G = (size_t)(N >> m) + 2, V = G * G * G;
         if (tot + 3 * V > budget_doubles) break;
         tot += 3 * V;

@@ -409,11 +409,16 @@ def config_hierarchy(name: str):
                    box is 6 length units (G = 1, c_s = 0.2), the smallest size at
                    which this density reaches the sixth level: 133,856 blocks
     'deep8'      : 256^3 base of 16^3 blocks, 8 levels, GRF + Plummer cores (config 5)
+    'uniform256' : 256^3 periodic, 32^3 blocks of 8^3, Gaussian peak: the smallest
+                   uniform grid whose FP32 field with ghosts (131 MB) exceeds the
+                   126 MB L2, used for kernel profiles of the 8^3-block sweeps
     """
     if name == "uniform64":
         return uniform_periodic(8, 8), gaussian_peak, 0
     if name == "nested5":
         return nested_sphere(5, 8, 8), softened_sphere, 1
+    if name == "uniform256":
+        return uniform_periodic(32, 8), gaussian_peak, 0
     if name == "jeans6":
         h, fn = jeans_cloud(nlev=6, nbase=16, ni=8)
         return h, fn, 0
