@@ -34,7 +34,8 @@ SFM_MAX_HISTORY = 64
 
 # every exported symbol of include/sfmg.h
 EXPORTED = ("sfm_default_params", "sfm_create", "sfm_solve", "sfm_solve_device",
-            "sfm_adjoint", "sfm_destroy", "sfm_strerror", "sfm_info")
+            "sfm_adjoint", "sfm_destroy", "sfm_strerror", "sfm_info", "sfm_uniform_solve_noalloc")
+SFM_NOALLOC_MAX_N = 32
 
 
 class SfmHierDesc(C.Structure):

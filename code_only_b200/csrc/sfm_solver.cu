@@ -16,10 +16,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -29,6 +31,7 @@
 #include "sfm_kernels_misc.cuh"
 #include "sfm_mg.cuh"
 #include "sfm_fast.cuh"
+#include "sfm_noalloc.cuh"
 
 namespace sfm {
 
@@ -1121,3 +1124,73 @@ int sfm_debug_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_s
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// sfm_uniform_solve_noalloc: device address of the fixed scratch array,
+// looked up once per device with that device current
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+int noalloc_scratch(int dev, double **out) {
+    if (dev < 0 || dev >= kNoallocMaxDevices) return SFM_EDEVICE;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, sfm::g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return SFM_ECUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return SFM_OK;
+}
+
+bool device_accessible(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+}  // namespace
+
+extern "C" int sfm_uniform_solve_noalloc(const double *d_rho, double *d_psi, int n, double h, double four_pi_G,
+                                         double rel_tol, int max_cycles, int *cycles, double *rel_residual,
+                                         void *stream) {
+    if (!d_rho || !d_psi) return SFM_EINVAL;
+    if (n < 2 || n > sfm::NOALLOC_MAX_N || (n & (n - 1)) != 0) return SFM_ESIZE;
+    if (!(h > 0.0) || !std::isfinite(h) || !std::isfinite(four_pi_G) || !(rel_tol >= 0.0) || max_cycles < 0 ||
+        max_cycles > 1000)
+        return SFM_EINVAL;
+    if ((reinterpret_cast<uintptr_t>(d_rho) | reinterpret_cast<uintptr_t>(d_psi)) % alignof(double) != 0)
+        return SFM_EINVAL;
+    int rc = check_device();
+    if (rc != SFM_OK) return rc;
+    if (!device_accessible(d_rho) || !device_accessible(d_psi)) return SFM_EINVAL;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return SFM_EDEVICE;
+    double *s = nullptr;
+    rc = noalloc_scratch(dev, &s);
+    if (rc != SFM_OK) return rc;
+    const sfm::MgData d = sfm::noalloc_layout(s, n, h);
+    double *out = s + sfm::noalloc_level_doubles(sfm::NOALLOC_MAX_N);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    sfm::k_mg_uniform_noalloc<<<1, 1024, 0, st>>>(d, d_rho, d_psi, four_pi_G, rel_tol, max_cycles, out,
+                                                  (int64_t)sfm::noalloc_level_doubles(n));
+    if (cudaGetLastError() != cudaSuccess) return SFM_ECUDA;
+    if (!cycles && !rel_residual) return SFM_OK;
+    double hv[2] = {0.0, 0.0};
+    if (cudaMemcpyAsync(hv, out, sizeof hv, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return SFM_ECUDA;
+    }
+    if (cycles) *cycles = (int)hv[1];
+    if (rel_residual) *rel_residual = hv[0];
+    return hv[0] <= rel_tol ? SFM_OK : SFM_ENOTCONVERGED;
+}

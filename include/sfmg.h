@@ -158,6 +158,37 @@ const char *sfm_strerror(int code);
  * bytes of device memory held by the context. */
 int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes);
 
+/* Uniform periodic base-grid solve that allocates nothing.  No counterpart
+ * in the reference: it runs the reference's base-grid multigrid (mg_cycle's
+ * residual / mg_lin / correction loop, mg.F90:42-94, with mg_lin of
+ * mg.F90:106-218) for callers that cannot allocate device memory when they
+ * need a solve: code inside a fixed memory pool or a start-up arena, a
+ * real-time step in which an allocator call would synchronise the device,
+ * a host library that promises a fixed device footprint.
+ *   d_rho, d_psi  device arrays of n^3 doubles, x fastest; psi is written
+ *                 (it starts from zero: no warm start)
+ *   n             cells per edge, a power of two, 2 <= n <= SFM_NOALLOC_MAX_N;
+ *                 larger n returns SFM_ESIZE
+ *   h, four_pi_G  cell width and the source factor: lap(psi) = four_pi_G (rho - mean rho)
+ *   rel_tol, max_cycles  stop when max|residual| <= rel_tol * max|four_pi_G (rho - mean)|,
+ *                 or after max_cycles mg_lin cycles (0 <= max_cycles <= 1000)
+ *   cycles, rel_residual  host outputs, may be NULL; when either is given the
+ *                 call waits for `stream` and returns SFM_ENOTCONVERGED if
+ *                 rel_tol was not reached; when both are NULL it returns
+ *                 after queueing the work
+ *   stream        a cudaStream_t, or NULL for the legacy default stream
+ * Working arrays live in one fixed device array of the library (about
+ * 2 MiB, enough for n = 32), cleared by the kernel itself before use, so
+ * nothing needs zeroing and nothing carries over between calls.  There is
+ * one such array per device: calls on one device whose executions overlap
+ * (unordered streams, concurrent host threads) race and give wrong results.
+ * The first call on each device looks up the array's address; make it
+ * before any stream capture on that device.  Uses the current device. */
+#define SFM_NOALLOC_MAX_N 32
+int sfm_uniform_solve_noalloc(const double *d_rho, double *d_psi, int n, double h, double four_pi_G,
+                              double rel_tol, int max_cycles, int *cycles, double *rel_residual,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

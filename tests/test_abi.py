@@ -67,3 +67,29 @@ def test_without_gpu_create_reports_no_device(sfmg_lib):
     ctx = C.c_void_p()
     p = abi.default_params()
     assert sfmg_lib.sfm_create(abi.HierDesc(h).ref(), C.byref(p), C.byref(ctx)) == abi.SFM_EDEVICE
+
+
+def test_noalloc_argument_checks_precede_device_work(sfmg_lib):
+    """sizes and arguments are refused before any CUDA call; valid arguments
+    without a GPU report SFM_EDEVICE (no kernel is launched on either path)"""
+    f = sfmg_lib.sfm_uniform_solve_noalloc
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                  C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_void_p]
+    f.restype = C.c_int
+    fake = 1 << 20                              # never dereferenced: every call below returns early
+    ok = (1.0 / 32, 1.0, 1e-10, 10, None, None, None)
+    assert f(fake, fake, abi.SFM_NOALLOC_MAX_N * 2, *ok) == abi.SFM_ESIZE
+    assert f(fake, fake, 24, *ok) == abi.SFM_ESIZE
+    assert f(fake, fake, 0, *ok) == abi.SFM_ESIZE
+    assert f(None, fake, 32, *ok) == abi.SFM_EINVAL
+    assert f(fake, fake, 32, 0.0, 1.0, 1e-10, 10, None, None, None) == abi.SFM_EINVAL
+    assert f(fake, fake, 32, 1.0, 1.0, -1.0, 10, None, None, None) == abi.SFM_EINVAL
+    assert f(fake, fake, 32, 1.0, 1.0, 1e-10, -1, None, None, None) == abi.SFM_EINVAL
+    assert f(fake + 4, fake, 32, *ok) == abi.SFM_EINVAL
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return
+    except ImportError:
+        pass
+    assert f(fake, fake, 32, *ok) == abi.SFM_EDEVICE
