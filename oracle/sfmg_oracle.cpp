@@ -1480,6 +1480,446 @@ struct Oracle {
         }
         return (conv && reached) ? SFM_OK : SFM_ENOTCONVERGED;
     }
+    // =====================================================================
+    // Adjoint of the converged solve (no counterpart in the reference).
+    //
+    // The outer loop of solve() stops at the fixed point of its FP64
+    // residual: on leaf interiors, A x + A_bc phi_bc = SRC, where A x is the
+    // fmg-level-0 operator of resid() (converge_c2p, bilinear ghostcell_fix,
+    // fluxes, fluxcorrection, divergence) with zero physical ghosts, and
+    // phi_bc the physical-ghost values of boundary_physical_grid.  SRC is the
+    // masked 4 pi G (rho - mean) and phi_bc the multipole expansion of the
+    // masked, converged SRC on the base level.  For a functional J(phi):
+    //   lambda = A^-T dJ/dphi,  dJ/dSRC(leaf) = lambda,
+    //   dJ/dphi_bc = -A_bc^T lambda  (moments chain to base-level SRC),
+    //   dJ/drho = 4 pi G (P^T (mask * dJ/dSRC)) with the mean removal P.
+    // apply_AT transposes the residual pipeline operation by operation in
+    // reverse order; A^-T comes from FGMRES, right-preconditioned with the
+    // volume-weighted forward fmg_lin.
+    // =====================================================================
+    Arr ub, fb[3];   // adjoints of u (every cell, ghosts included) and of the fluxes
+
+    void leaf_interior_only(Arr &A) {
+        const int n = NI;
+        for (int b = 0; b < nb; b++)
+            for (int k = -1; k <= n; k++)
+                for (int j = -1; j <= n; j++)
+                    for (int i = -1; i <= n; i++) {
+                        bool in = !skip(b) && i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n;
+                        if (!in) A.at(b, i, j, k) = 0.0;
+                    }
+    }
+    // transpose of converge_c2p (linear 8-mean into the parent octant), coarsest level first
+    void converge_c2p_T(Arr &A) {
+        const int n = NI, h2n = n / 2;
+        for (int Lc = 0; Lc <= nlev - 2; Lc++)
+            for (int b = lstart[Lc + 1]; b < lstart[Lc + 2]; b++) {
+                int p = parent[b];
+                int oi = octant[3 * b] * h2n, oj = octant[3 * b + 1] * h2n, ok = octant[3 * b + 2] * h2n;
+                for (int kc = 0; kc < h2n; kc++)
+                    for (int jc = 0; jc < h2n; jc++)
+                        for (int ic = 0; ic < h2n; ic++) {
+                            double v = A.at(p, ic + oi, jc + oj, kc + ok) * (1.0 / 8.0);
+                            A.at(p, ic + oi, jc + oj, kc + ok) = 0.0;
+                            for (int c = 0; c < 8; c++)
+                                A.at(b, 2 * ic + (c & 1), 2 * jc + ((c >> 1) & 1), 2 * kc + (c >> 2)) += v;
+                        }
+            }
+    }
+    void samelev_T(int L, int dir, Arr &A) {
+        const int n = NI;
+        for (int b = lstart[L]; b < lstart[L + 1]; b++)
+            for (int lr = 0; lr < 2; lr++) {
+                int fc = lr + 2 * dir;
+                if (!sameLev[6 * b + fc]) continue;
+                int s = nbrGid[6 * b + fc];
+                int xr = (lr == Left) ? -1 : n, xs = (lr == Left) ? n - 1 : 0;
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) {
+                        int i, j, k, is, js, ks;
+                        put3(dir, xr, p, q, i, j, k);
+                        put3(dir, xs, p, q, is, js, ks);
+                        double v = A.at(b, i, j, k);
+                        A.at(b, i, j, k) = 0.0;
+                        A.at(s, is, js, ks) += v;
+                    }
+            }
+    }
+    // transpose of the bilinear coarse-fine ghost (the outer operator uses no bicubic)
+    void parentlev_T(int L, int dir, Arr &A) {
+        if (L <= 0) return;
+        const int n = NI, nb2 = n / 2, W = nb2 + 2;
+        for (int b = lstart[L]; b < lstart[L + 1]; b++)
+            for (int lr = 0; lr < 2; lr++) {
+                int fc = lr + 2 * dir;
+                if (!parLev[6 * b + fc]) continue;
+                int cb = nbrGid[6 * b + fc];
+                int xc = (lr == Left) ? n - 1 : 0;
+                int ta = (dir == MX) ? MY : MX, tb = (dir == MZ) ? MY : MZ;
+                int oa = octant[3 * b + ta] * nb2, ob = octant[3 * b + tb] * nb2;
+                std::vector<double> Bb((size_t)W * W, 0.0);
+                auto B = [&](int a, int bb) -> double & { return Bb[(size_t)(bb + 1) * W + (a + 1)]; };
+                int xg = (lr == Left) ? -1 : n, inner = (lr == Left) ? 1 : -1;
+                for (int q = -1; q <= n; q++)
+                    for (int p = -1; p <= n; p++) {
+                        int i, j, k, i0, j0, k0, iN, jN, kN;
+                        put3(dir, xg, p, q, i, j, k);
+                        put3(dir, xg + inner, p, q, i0, j0, k0);
+                        put3(dir, xg + 2 * inner, p, q, iN, jN, kN);
+                        double gv = A.at(b, i, j, k);
+                        A.at(b, i, j, k) = 0.0;
+                        A.at(b, i0, j0, k0) += (10.0 / 15.0) * gv;
+                        A.at(b, iN, jN, kN) += (-3.0 / 15.0) * gv;
+                        double hv = (8.0 / 15.0) * gv;
+                        int pc = fdiv2(p), qc = fdiv2(q), p1 = near_(p, pc), q1 = near_(q, qc);
+                        B(pc, qc) += (9.0 / 16.0) * hv;
+                        B(p1, q1) += (1.0 / 16.0) * hv;
+                        B(pc, q1) += (3.0 / 16.0) * hv;
+                        B(p1, qc) += (3.0 / 16.0) * hv;
+                    }
+                for (int q = -1; q <= nb2; q++)
+                    for (int p = -1; p <= nb2; p++) {
+                        int i, j, k;
+                        put3(dir, xc, p + oa, q + ob, i, j, k);
+                        A.at(cb, i, j, k) += B(p, q);
+                    }
+            }
+    }
+    // ub = (residual pipeline)^T g, g on leaf interiors: A^T g on leaf
+    // interiors, A_bc^T g on the physical ghosts, zero elsewhere
+    void apply_AT(Arr &g) {
+        const int n = NI;
+        ub.init(nb, n);
+        for (auto &a : fb) a.init(nb, n);
+        // divergence / h on leaf blocks (resid, divF)
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            double hi = 1.0 / h(level[b], 0);
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) {
+                        double v = g.at(b, i, j, k) * hi;
+                        fb[MX].at(b, i, j, k) += v; fb[MX].at(b, i - 1, j, k) -= v;
+                        fb[MY].at(b, i, j, k) += v; fb[MY].at(b, i, j - 1, k) -= v;
+                        fb[MZ].at(b, i, j, k) += v; fb[MZ].at(b, i, j, k - 1) -= v;
+                    }
+        }
+        // fluxcorrection: the coarse quarter face took the mean of 4 fine fluxes
+        const int h2n = n / 2;
+        struct Item { int b, cb, dir, xf, xc, ta0, tb0; std::vector<double> v; };
+        std::vector<Item> items;
+        for (int L = 1; L < nlev; L++)
+            for (int b = lstart[L]; b < lstart[L + 1]; b++)
+                for (int dir = 0; dir < 3; dir++)
+                    for (int lr = 0; lr < 2; lr++) {
+                        int fc = lr + 2 * dir;
+                        if (!parLev[6 * b + fc]) continue;
+                        Item it;
+                        it.b = b; it.cb = nbrGid[6 * b + fc]; it.dir = dir;
+                        it.xf = (lr == Left) ? -1 : n - 1;
+                        it.xc = (lr == Left) ? n - 1 : -1;
+                        int ta = (dir == MX) ? MY : MX, tb = (dir == MZ) ? MY : MZ;
+                        it.ta0 = octant[3 * b + ta] * h2n; it.tb0 = octant[3 * b + tb] * h2n;
+                        it.v.assign((size_t)h2n * h2n, 0.0);
+                        items.push_back(std::move(it));
+                    }
+        for (auto &it : items)
+            for (int qc = 0; qc < h2n; qc++)
+                for (int pc = 0; pc < h2n; pc++) {
+                    int i, j, k; put3(it.dir, it.xc, pc + it.ta0, qc + it.tb0, i, j, k);
+                    it.v[(size_t)qc * h2n + pc] = fb[it.dir].at(it.cb, i, j, k);
+                    fb[it.dir].at(it.cb, i, j, k) = 0.0;
+                }
+        for (auto &it : items)
+            for (int qc = 0; qc < h2n; qc++)
+                for (int pc = 0; pc < h2n; pc++) {
+                    double v = it.v[(size_t)qc * h2n + pc] * 0.25;
+                    for (int c = 0; c < 4; c++) {
+                        int i, j, k; put3(it.dir, it.xf, 2 * pc + (c & 1), 2 * qc + (c >> 1), i, j, k);
+                        fb[it.dir].at(it.b, i, j, k) += v;
+                    }
+                }
+        // fluxes F_d(i) = (u(i + e_d) - u(i)) / h on leaf blocks, i in [-1, n-1]^3
+        for (int b = 0; b < nb; b++) {
+            if (skip(b)) continue;
+            double hi = 1.0 / h(level[b], 0);
+            for (int k = -1; k <= n - 1; k++)
+                for (int j = -1; j <= n - 1; j++)
+                    for (int i = -1; i <= n - 1; i++) {
+                        double vx = fb[MX].at(b, i, j, k) * hi, vy = fb[MY].at(b, i, j, k) * hi,
+                               vz = fb[MZ].at(b, i, j, k) * hi;
+                        ub.at(b, i + 1, j, k) += vx; ub.at(b, i, j + 1, k) += vy; ub.at(b, i, j, k + 1) += vz;
+                        ub.at(b, i, j, k) -= vx + vy + vz;
+                    }
+        }
+        // ghostcell_fix in reverse: levels down, z y x, samelev then parentlev
+        for (int L = nlev - 1; L >= 0; L--)
+            for (int dir = 2; dir >= 0; dir--) {
+                samelev_T(L, dir, ub);
+                parentlev_T(L, dir, ub);
+            }
+        converge_c2p_T(ub);
+    }
+
+    // per-cell moment terms T_k (the factors of rhodv in multipole_moments)
+    // and the normalisations: mom_k = -nrm_k sum T_k rho dv
+    void moment_terms(double x, double y, double z, double t[25]) const {
+        double r2 = x * x + y * y + z * z, r = std::sqrt(r2), r3 = r2 * r, rc = std::sqrt(x * x + y * y);
+        double cost = z / r, sint = rc / r, cosp = x / rc, sinp = y / rc;
+        double c2 = cost * cost, s2 = sint * sint, cp2 = cosp * cosp, sp2 = sinp * sinp;
+        t[0] = 1.0; t[1] = r * cost; t[2] = r * sint * cosp; t[3] = r * sint * sinp;
+        t[4] = r2 * (3 * c2 - 1); t[5] = r2 * sint * cost * cosp; t[6] = r2 * sint * cost * sinp;
+        t[7] = r2 * s2 * (cp2 - sp2); t[8] = r2 * s2 * 2 * sinp * cosp;
+        t[9] = r3 * cost * (5 * c2 - 3); t[10] = r3 * sint * (5 * c2 - 1) * cosp; t[11] = r3 * sint * (5 * c2 - 1) * sinp;
+        t[12] = r3 * cost * s2 * (cp2 - sp2); t[13] = r3 * cost * s2 * 2 * sinp * cosp;
+        t[14] = r3 * s2 * sint * cosp * (cp2 - 3 * sp2); t[15] = r3 * s2 * sint * sinp * (3 * cp2 - sp2);
+        double r4 = r2 * r2, cos2p = cp2 - sp2, sin2p = 2 * sinp * cosp;
+        double cos3p = cosp * (cp2 - 3 * sp2), sin3p = sinp * (3 * cp2 - sp2);
+        double cos4p = cos2p * cos2p - sin2p * sin2p, sin4p = 2 * sin2p * cos2p;
+        t[16] = r4 * (35 * c2 * c2 - 30 * c2 + 3); t[17] = r4 * sint * cost * (7 * c2 - 3) * cosp;
+        t[18] = r4 * sint * cost * (7 * c2 - 3) * sinp; t[19] = r4 * s2 * (7 * c2 - 1) * cos2p;
+        t[20] = r4 * s2 * (7 * c2 - 1) * sin2p; t[21] = r4 * s2 * sint * cost * cos3p;
+        t[22] = r4 * s2 * sint * cost * sin3p; t[23] = r4 * s2 * s2 * cos4p; t[24] = r4 * s2 * s2 * sin4p;
+    }
+    static void moment_norms(double nrm[25]) {
+        const double pi = M_PI;
+        const double v[25] = {1 / (4 * pi), 1 / (4 * pi), 1 / (8 * pi), 1 / (8 * pi), 1 / (16 * pi),
+                              3 / (8 * pi), 3 / (8 * pi), 3 / (32 * pi), 3 / (32 * pi), 1 / (16 * pi),
+                              3 / (64 * pi), 3 / (64 * pi), 15 / (32 * pi), 15 / (32 * pi), 5 / (64 * pi),
+                              5 / (64 * pi), 1 / (4 * pi * 64), 5 / (4 * pi * 8), 5 / (4 * pi * 8), 5 / (4 * pi * 16),
+                              5 / (4 * pi * 16), 35 / (4 * pi * 8), 35 / (4 * pi * 8), 35 / (4 * pi * 64),
+                              35 / (4 * pi * 64)};
+        for (int k = 0; k < 25; k++) nrm[k] = v[k];
+    }
+    double sphere_rad2() {
+        const int n = NI;
+        auto X = [&](int b, int d, int i) { return x0[3 * b + d] + (double)i * h0[level[b]]; };
+        int bmin = baseIdx[0], bmax = baseIdx.back();
+        double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
+        double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
+        double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        return rr * rr;
+    }
+    // Preconditioner for A^T: W M W^-1 with M one forward fmg_lin and W the
+    // cell volumes.  The flux form with conservative reflux makes W A nearly
+    // symmetric (exactly so away from coarse-fine faces), so A^T ~ W A W^-1
+    // and W M W^-1 ~ A^-T; plain M stalls FGMRES on refined hierarchies.
+    void precond(Arr &v, Arr &z) {
+        Arr &R = F(IRHO, 0);
+        std::copy(v.d.begin(), v.d.end(), R.d.begin());
+        leaf_interior_only(R);
+        for (int b = 0; b < nb; b++) {
+            double dv = h(level[b], 0) * h(level[b], 0) * h(level[b], 0);
+            for (size_t q = 0; q < R.V; q++) R.blk(b)[q] = R.blk(b)[q] / dv;
+        }
+        FmgLevel_fill0 = Undef;
+        fmg_lin();
+        z.d = F(IU, 0).d;
+        for (int b = 0; b < nb; b++) {
+            double dv = h(level[b], 0) * h(level[b], 0) * h(level[b], 0);
+            for (size_t q = 0; q < z.V; q++) z.blk(b)[q] = z.blk(b)[q] * dv;
+        }
+        leaf_interior_only(z);
+    }
+    static double dot(const Arr &a, const Arr &b) {
+        double s = 0.0;
+        for (size_t q = 0; q < a.d.size(); q++) s += a.d[q] * b.d[q];
+        return s;
+    }
+
+    // dJdphi, dJdrho: [nb][(NI+2gw)^3]; interiors used / written
+    int adjoint(const double *dJdphi, double *dJdrho, int gw, sfm_stats *st) {
+        const int n = NI, Gi = NI + 2 * gw;
+        for (auto &a : fld) std::fill(a.d.begin(), a.d.end(), 0.0);
+        for (auto &a : flx) std::fill(a.d.begin(), a.d.end(), 0.0);
+        Arr g;
+        g.init(nb, n);
+        for (int b = 0; b < nb; b++)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++)
+                        g.at(b, i, j, k) = dJdphi[(size_t)b * Gi * Gi * Gi + ((size_t)(k + gw) * Gi + (j + gw)) * Gi + (i + gw)];
+        converge_c2p_T(g);   // phi on covered blocks is the restriction of the leaves
+        leaf_interior_only(g);
+        if (bc == SFM_BC_PERIODIC) {   // A is singular (constants): keep g orthogonal to them
+            double s = 0.0, c = 0.0;
+            for (int b = 0; b < nb; b++)
+                if (!skip(b))
+                    for (int k = 0; k < n; k++)
+                        for (int j = 0; j < n; j++)
+                            for (int i = 0; i < n; i++) { s += g.at(b, i, j, k); c += 1.0; }
+            double m = s / c;
+            for (int b = 0; b < nb; b++)
+                if (!skip(b))
+                    for (int k = 0; k < n; k++)
+                        for (int j = 0; j < n; j++)
+                            for (int i = 0; i < n; i++) g.at(b, i, j, k) -= m;
+        }
+        if (st) std::memset(st, 0, sizeof(*st));
+        // FGMRES(m) on A^T lambda = g
+        const int m = 30, maxit = std::max(1, nfmgmax);
+        const double gnorm = std::sqrt(dot(g, g));
+        Arr lam;
+        lam.init(nb, n);
+        int iters = 0;
+        bool reached = gnorm == 0.0;
+        Arr r = g;
+        double beta = gnorm;
+        while (!reached && iters < maxit) {
+            std::vector<Arr> Vv(m + 1), Zv(m);
+            std::vector<double> Hm((size_t)(m + 1) * m, 0.0), cs(m, 0.0), sn(m, 0.0), s(m + 1, 0.0);
+            auto Hij = [&](int i, int j) -> double & { return Hm[(size_t)i * m + j]; };
+            Vv[0] = r;
+            for (double &x : Vv[0].d) x /= beta;
+            s[0] = beta;
+            int jlast = -1;
+            for (int j = 0; j < m && iters < maxit; j++) {
+                Zv[j].init(nb, n);
+                precond(Vv[j], Zv[j]);
+                apply_AT(Zv[j]);
+                Arr w = ub;
+                leaf_interior_only(w);
+                for (int i = 0; i <= j; i++) {
+                    Hij(i, j) = dot(w, Vv[i]);
+                    for (size_t q = 0; q < w.d.size(); q++) w.d[q] -= Hij(i, j) * Vv[i].d[q];
+                }
+                Hij(j + 1, j) = std::sqrt(dot(w, w));
+                Vv[j + 1] = w;
+                if (Hij(j + 1, j) > 0.0)
+                    for (double &x : Vv[j + 1].d) x /= Hij(j + 1, j);
+                for (int i = 0; i < j; i++) {
+                    double t = cs[i] * Hij(i, j) + sn[i] * Hij(i + 1, j);
+                    Hij(i + 1, j) = -sn[i] * Hij(i, j) + cs[i] * Hij(i + 1, j);
+                    Hij(i, j) = t;
+                }
+                double den = std::hypot(Hij(j, j), Hij(j + 1, j));
+                cs[j] = den > 0 ? Hij(j, j) / den : 1.0;
+                sn[j] = den > 0 ? Hij(j + 1, j) / den : 0.0;
+                Hij(j, j) = den;
+                Hij(j + 1, j) = 0.0;
+                s[j + 1] = -sn[j] * s[j];
+                s[j] = cs[j] * s[j];
+                iters++;
+                jlast = j;
+                double rel = std::fabs(s[j + 1]) / gnorm;
+                if (st && iters <= SFM_MAX_HISTORY) st->ratio[iters - 1] = rel;
+                if (rel < errormax) { reached = true; break; }
+            }
+            // lambda += Z y, H y = s
+            std::vector<double> y(jlast + 1, 0.0);
+            for (int i = jlast; i >= 0; i--) {
+                double t = s[i];
+                for (int k = i + 1; k <= jlast; k++) t -= Hij(i, k) * y[k];
+                y[i] = t / Hij(i, i);
+            }
+            for (int i = 0; i <= jlast; i++)
+                for (size_t q = 0; q < lam.d.size(); q++) lam.d[q] += y[i] * Zv[i].d[q];
+            apply_AT(lam);
+            r = g;
+            for (size_t q = 0; q < r.d.size(); q++) r.d[q] -= (ub.d[q]);
+            leaf_interior_only(r);
+            beta = std::sqrt(dot(r, r));
+            reached = beta / gnorm < errormax;
+        }
+        apply_AT(lam);   // ub: A^T lambda on leaves, A_bc^T lambda on the physical ghosts
+        // dJ/dSRC: lambda on leaf interiors, plus the multipole path to the base level
+        Arr sbar;
+        sbar.init(nb, n);
+        if (bc == SFM_BC_SPHERE) {
+            const double rad2 = sphere_rad2();
+            auto X = [&](int b, int d, int i) { return x0[3 * b + d] + (double)i * h0[level[b]]; };
+            Arr mark;
+            mark.init(nb, n);
+            for (int b = 0; b < nb; b++)
+                for (int dir = 0; dir < 3; dir++)
+                    for (int lr = 0; lr < 2; lr++) {
+                        if (!touch[6 * b + lr + 2 * dir]) continue;
+                        int xg = (lr == Left) ? -1 : n;
+                        for (int q = -1; q <= n; q++)
+                            for (int p = -1; p <= n; p++) {
+                                int i, j, k; put3(dir, xg, p, q, i, j, k);
+                                mark.at(b, i, j, k) = 1.0;
+                            }
+                    }
+            // beta_k = sum_c E_k(x_c) dJ/dphi_bc(c), dJ/dphi_bc = -ub
+            double betak[25] = {0.0};
+            for (int b = 0; b < nb; b++)
+                for (int k = -1; k <= n; k++)
+                    for (int j = -1; j <= n; j++)
+                        for (int i = -1; i <= n; i++) {
+                            if (mark.at(b, i, j, k) == 0.0) continue;
+                            double w = -ub.at(b, i, j, k);
+                            if (w == 0.0) continue;
+                            for (int q = 0; q < 25; q++) {
+                                double e[25] = {0.0};
+                                e[q] = 1.0;
+                                betak[q] += w * multipole_eval(e, X(b, 0, i), X(b, 1, j), X(b, 2, k));
+                            }
+                        }
+            double nrm[25];
+            moment_norms(nrm);
+            const int kmax = lmax >= 4 ? 25 : 16;
+            const double dv = h0[0] * h0[0] * h0[0];
+            for (int b = lstart[0]; b < lstart[1]; b++)
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) {
+                            double x = X(b, 0, i), y2 = X(b, 1, j), z = X(b, 2, k);
+                            if (x * x + y2 * y2 + z * z >= rad2) continue;
+                            double t[25];
+                            moment_terms(x, y2, z, t);
+                            double v = 0.0;
+                            for (int q = 0; q < kmax; q++) v += betak[q] * (-nrm[q]) * t[q] * dv;
+                            sbar.at(b, i, j, k) = v;
+                        }
+            converge_c2p_T(sbar);
+            for (int b = 0; b < nb; b++)
+                if (!skip(b))
+                    for (int k = 0; k < n; k++)
+                        for (int j = 0; j < n; j++)
+                            for (int i = 0; i < n; i++) {
+                                double x = X(b, 0, i), y2 = X(b, 1, j), z = X(b, 2, k);
+                                bool masked = x * x + y2 * y2 + z * z >= rad2;
+                                sbar.at(b, i, j, k) += masked ? 0.0 : lam.at(b, i, j, k);
+                            }
+        } else {
+            sbar.d = lam.d;
+        }
+        leaf_interior_only(sbar);
+        // mean removal: S = 4 pi G rho - sum(4 pi G rho dv)/vol over leaf cells
+        double corr = 0.0;
+        if (zero_mean) {
+            double ssum = 0.0, vol = 0.0;
+            for (int b = 0; b < nb; b++) {
+                if (skip(b)) continue;
+                double dv = h(level[b], 0) * h(level[b], 0) * h(level[b], 0);
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) ssum += sbar.at(b, i, j, k);
+                vol += (double)(n * n * n) * dv;
+            }
+            corr = ssum / vol;
+        }
+        for (int b = 0; b < nb; b++) {
+            double dv = h(level[b], 0) * h(level[b], 0) * h(level[b], 0);
+            for (int k = -gw; k < n + gw; k++)
+                for (int j = -gw; j < n + gw; j++)
+                    for (int i = -gw; i < n + gw; i++) {
+                        size_t o = (size_t)b * Gi * Gi * Gi + ((size_t)(k + gw) * Gi + (j + gw)) * Gi + (i + gw);
+                        bool in = !skip(b) && i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n;
+                        dJdrho[o] = in ? four_pi_G * (sbar.at(b, i, j, k) - dv * corr) : 0.0;
+                    }
+        }
+        if (st) {
+            st->outer_iters = iters;
+            st->converged = reached ? 1 : 0;
+            Arr rr = g;
+            for (size_t q = 0; q < rr.d.size(); q++) rr.d[q] -= ub.d[q];
+            leaf_interior_only(rr);
+            st->true_rel_residual = gnorm > 0 ? std::sqrt(dot(rr, rr)) / gnorm : 0.0;
+        }
+        return reached ? SFM_OK : SFM_ENOTCONVERGED;
+    }
     void dumpf(int code, double *dump) {
         if (!dump) return;
         Arr &A = F(code, 0);
@@ -1543,6 +1983,35 @@ int oracle_multipole(const sfm_hier_desc *h, const sfm_params *p, const double *
     double mom[25];
     o.multipole_moments(R, mom);
     for (int q = 0; q < npts; q++) out[q] = o.multipole_eval(mom, xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]);
+    return SFM_OK;
+}
+
+// Adjoint of the converged solve: dJ/drho from dJ/dphi (interiors of the
+// [nb][(ni+2g)^3] layout, g = p->ngh_io).  p->rel_tol is the FGMRES
+// tolerance on ||g - A^T lambda||_2 / ||g||_2, p->max_outer its iteration cap.
+int oracle_adjoint(const sfm_hier_desc *h, const sfm_params *p, const double *dJdphi, double *dJdrho,
+                   sfm_stats *st) {
+    if (!h || !p || !dJdphi || !dJdrho || p->ngh_io < 1) return SFM_EINVAL;
+    Oracle *o = new Oracle();
+    int rc = o->setup(h, p);
+    if (rc == SFM_OK) rc = o->adjoint(dJdphi, dJdrho, p->ngh_io, st);
+    delete o;
+    return rc;
+}
+
+// Transposed residual pipeline: out = (ghost width 1 layout, every cell) the
+// adjoint of oracle_apply_L's input phi for output weights y on leaf interiors,
+// so that <L(phi), y>_leaf = <phi, out>_all for every phi.
+int oracle_apply_LT(const sfm_hier_desc *h, const sfm_params *p, const double *y, double *out) {
+    Oracle o;
+    int rc = o.setup(h, p);
+    if (rc) return rc;
+    Arr g;
+    g.init(o.nb, o.NI);
+    std::copy(y, y + g.d.size(), g.d.begin());
+    o.leaf_interior_only(g);
+    o.apply_AT(g);
+    std::copy(o.ub.d.begin(), o.ub.d.end(), out);
     return SFM_OK;
 }
 

@@ -33,6 +33,11 @@ def load_oracle():
     lib.oracle_multipole.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_int,
                                      C.c_void_p, C.c_void_p]
     lib.oracle_multipole.restype = C.c_int
+    lib.oracle_apply_LT.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p]
+    lib.oracle_apply_LT.restype = C.c_int
+    lib.oracle_adjoint.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p,
+                                   C.POINTER(abi.SfmStats)]
+    lib.oracle_adjoint.restype = C.c_int
     _lib = lib
     return lib
 
@@ -50,6 +55,25 @@ def oracle_solve(h, rho, params, psi=None, want_g=True, stage=0):
                           g.ctypes.data if g is not None else None, C.byref(st), stage,
                           dump.ctypes.data if dump is not None else None)
     return rc, psi, g, st, dump
+
+
+def oracle_adjoint(h, dJ_dphi, params):
+    """Runs the oracle's adjoint; returns (rc, dJ_drho, stats)."""
+    lib = load_oracle()
+    out = np.zeros_like(dJ_dphi)
+    st = abi.SfmStats()
+    rc = lib.oracle_adjoint(abi.HierDesc(h).ref(), C.byref(params), np.ascontiguousarray(dJ_dphi).ctypes.data,
+                            out.ctypes.data, C.byref(st))
+    return rc, out, st
+
+
+def leaf_mask(h, n_ghost):
+    """bool [nb, G, G, G]: interior cells of leaf blocks (blocks whose fields the solve determines)"""
+    G = h.ni + 2 * n_ghost
+    m = np.zeros((h.nblocks, G, G, G), bool)
+    leaf = (h.level == h.nlev - 1) | (h.child[:, 0] < 0)
+    m[leaf, n_ghost:n_ghost + h.ni, n_ghost:n_ghost + h.ni, n_ghost:n_ghost + h.ni] = True
+    return m
 
 
 def make_rho(h, fn, ngh):
