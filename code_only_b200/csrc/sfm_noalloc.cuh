@@ -46,7 +46,7 @@ __host__ __device__ constexpr size_t noalloc_level_doubles(int n) {
 constexpr size_t NOALLOC_OUT_DOUBLES = 2;
 constexpr size_t NOALLOC_SCRATCH_DOUBLES = noalloc_level_doubles(NOALLOC_MAX_N) + NOALLOC_OUT_DOUBLES;
 
-__device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
 
 // level arrays of an n^3 base grid laid out from the start of the scratch
 __host__ __device__ inline MgData noalloc_layout(double *s, int n, double h) {
