@@ -32,6 +32,7 @@
 #include "sfm_mg.cuh"
 #include "sfm_fast.cuh"
 #include "sfm_noalloc.cuh"
+#include "sfm_adjoint.cuh"
 
 namespace sfm {
 
@@ -199,6 +200,7 @@ public:
     virtual ~SolverBase() {}
     virtual int solve(const double *rho, double *psi, double *g, sfm_stats *st, cudaStream_t s, int stop_stage,
                       double *dump) = 0;
+    virtual int adjoint(const double *dJdphi, double *dJdrho, sfm_stats *st, cudaStream_t s) = 0;
     virtual int64_t device_bytes() const = 0;
     virtual int fmg_levels() const = 0;
     std::string last_error;
@@ -934,6 +936,241 @@ public:
         prof_collect(stats);
         return (conv && reached) ? SFM_OK : SFM_ENOTCONVERGED;
     }
+    // -----------------------------------------------------------------
+    // adjoint of the converged solve (sfm_adjoint; device side in
+    // sfm_adjoint.cuh).  FGMRES(m) on A^T lambda = dJ/dphi, right-
+    // preconditioned with W M W^-1 (M one fmg_lin of this solver, W the cell
+    // volumes: the conservative flux form makes W A nearly symmetric, so
+    // A^T ~ W A W^-1), then the chain rule through the multipole boundary,
+    // the mask and the mean removal back to rho.
+    // -----------------------------------------------------------------
+    bool adjReady = false;
+    int adjM = 0, nAdjRefl = 0;
+    AdjReflux *d_adjRefl = nullptr;
+    int8_t *d_touch = nullptr;
+    double *aG = nullptr, *aLam = nullptr, *aR = nullptr, *aW = nullptr, *aUB = nullptr, *aS = nullptr,
+           *aIO = nullptr, *aPart = nullptr, *aBeta = nullptr, *aDot = nullptr;
+    double *aF[3] = {nullptr, nullptr, nullptr};
+    std::vector<double *> aV, aZ;
+
+    int adj_init() {
+        if (adjReady) return SFM_OK;
+        std::vector<AdjReflux> ar;
+        for (int L = 1; L < H.nlev; L++)
+            for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                for (int dir = 0; dir < 3; dir++)
+                    for (int lr = 0; lr < 2; lr++) {
+                        const int f = lr + 2 * dir;
+                        if (!H.parLev[6 * b + f]) continue;
+                        AdjReflux it;
+                        it.fine = b; it.coarse = H.nbrGid[6 * b + f]; it.dir = (int8_t)dir; it.lr = (int8_t)lr;
+                        it.oa = H.oct[3 * b + tra(dir)]; it.ob = H.oct[3 * b + trb(dir)];
+                        ar.push_back(it);
+                    }
+        nAdjRefl = (int)ar.size();
+        d_adjRefl = mem.upload(ar);
+        d_touch = mem.upload(H.touch);
+        const size_t NV = (size_t)H.nb * Vf[0];
+        const int gw = P.ngh_io;
+        const size_t NIO = (size_t)H.nb * (size_t)(H.NI + 2 * gw) * (H.NI + 2 * gw) * (H.NI + 2 * gw);
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        const size_t per = NV * sizeof(double);
+        const double avail = 0.8 * (double)fr - (double)NIO * sizeof(double);
+        const long vecs = (long)(avail / (double)per) - 9;   // G, lambda, R, W, UB, 3 fluxes, S
+        const long m = (vecs - 1) / 2;
+        if (m < 2) return SFM_ENOMEM;
+        adjM = (int)std::min<long>(m, 30);
+        aG = mem.alloc<double>(NV); aLam = mem.alloc<double>(NV); aR = mem.alloc<double>(NV);
+        aW = mem.alloc<double>(NV); aUB = mem.alloc<double>(NV); aS = mem.alloc<double>(NV);
+        for (auto &f : aF) f = mem.alloc<double>(NV);
+        for (int j = 0; j <= adjM; j++) aV.push_back(mem.alloc<double>(NV));
+        for (int j = 0; j < adjM; j++) aZ.push_back(mem.alloc<double>(NV));
+        aIO = mem.alloc<double>(NIO);
+        aPart = mem.alloc<double>((size_t)std::max<int64_t>(tfLOff[H.nlev], 1) * 25);
+        aBeta = mem.alloc<double>(32);
+        aDot = mem.alloc<double>(8);
+        if (mem.err != cudaSuccess) {
+            last_error = cudaGetErrorString(mem.err);
+            return mem.err == cudaErrorMemoryAllocation ? SFM_ENOMEM : SFM_ECUDA;
+        }
+        adjReady = true;
+        return SFM_OK;
+    }
+    int64_t adj_nv() const { return (int64_t)H.nb * Vf[0]; }
+    void adj_leaf_only(double *a) { run(OpLeafInterior{a, d_skip, nf[0], Gf[0], Vf[0]}, adj_nv()); }
+    void adj_converge_T(double *a) {
+        const int n = nf[0], h = n / 2;
+        for (int Lc = 0; Lc <= H.nlev - 2; Lc++)
+            run(OpConvergeT{a, d_parent, d_oct, H.lstart[Lc + 1], n, Gf[0], Vf[0]}, (int64_t)cnt(Lc + 1) * h * h * h);
+    }
+    // ordered sum over leaf interiors of a*b (of a when b is null)
+    double adj_dot(const double *a, const double *b) {
+        run(OpBlockDot{a, b, d_leaves, d_psum, nf[0], Gf[0], Vf[0]}, (int64_t)nLeaves);
+        k_sum_ordered<<<1, 32, 0, st_>>>(d_psum, nLeaves, aDot);
+        ++launches;
+        double v = 0.0;
+        cudaMemcpyAsync(&v, aDot, sizeof(double), cudaMemcpyDeviceToHost, st_);
+        cudaStreamSynchronize(st_);
+        return v;
+    }
+    // aUB = (residual pipeline)^T g: A^T g on leaf interiors, A_bc^T g on
+    // the physical ghosts
+    void adj_apply_AT(const double *g) {
+        const int n = nf[0], G = Gf[0], GT = n + 2, h = n / 2;
+        const int64_t V = Vf[0], NV = adj_nv();
+        run(OpDivT{aF[0], aF[1], aF[2], g, d_skip, d_h0, d_level, n, G, V}, NV);
+        run(OpRefluxT{aF[0], aF[1], aF[2], d_adjRefl, n, G, V}, (int64_t)nAdjRefl * h * h);
+        run(OpFluxT{aUB, aF[0], aF[1], aF[2], d_skip, d_h0, d_level, n, G, V}, NV);
+        for (int L = H.nlev - 1; L >= 0; L--)
+            for (int dir = 2; dir >= 0; dir--) {
+                const int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
+                run(OpGhostT{aUB, d_faces + o, n, G, V, dir}, c * GT * GT);
+            }
+        adj_converge_T(aUB);
+    }
+    void adj_precond(const double *v, double *z) {
+        const int64_t NV = adj_nv();
+        run(OpPrecIn<T>{RHO[0], v, d_skip, d_h0, d_level, nf[0], Gf[0], Vf[0]}, NV);
+        FmgLevel_fill0 = Undef;
+        fmg_lin();
+        run(OpPrecOut<T>{z, U[0], d_skip, d_h0, d_level, nf[0], Gf[0], Vf[0]}, NV);
+    }
+    void adj_copy(double *o, const double *a) {
+        cudaMemcpyAsync(o, a, (size_t)adj_nv() * sizeof(double), cudaMemcpyDeviceToDevice, st_);
+    }
+    double sphere_rad2() const {
+        const int n = H.NI;
+        int bmin = H.baseIdx.front(), bmax = H.baseIdx.back();
+        auto X = [&](int b, int d, int i) { return H.x0[3 * b + d] + (double)i * H.h0[H.level[b]]; };
+        double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
+        double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
+        double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        return rr * rr;
+    }
+
+    int adjoint(const double *dJdphi, double *dJdrho, sfm_stats *stats, cudaStream_t s) override {
+        st_ = s ? s : own_;
+        launches = 0;
+        int rc = adj_init();
+        if (rc) return rc;
+        cudaEventRecord(ev0, st_);
+        const int n = nf[0], G = Gf[0], gw = P.ngh_io;
+        const int64_t V = Vf[0], NV = adj_nv();
+        const int64_t NIO = (int64_t)H.nb * (n + 2 * gw) * (n + 2 * gw) * (n + 2 * gw);
+        for (auto &z : zeroList) cudaMemsetAsync(z.first, 0, z.second, st_);   // fresh inner arrays
+        cudaMemcpyAsync(aIO, dJdphi, (size_t)NIO * sizeof(double), cudaMemcpyHostToDevice, st_);
+        run(OpAdjIn{aG, aIO, n, G, gw, V}, NV);
+        adj_converge_T(aG);   // phi on covered blocks is the restriction of the leaves
+        adj_leaf_only(aG);
+        const double ncell = (double)nLeaves * n * n * n;
+        if (P.bc == SFM_BC_PERIODIC) {   // A is singular (constants): keep g orthogonal to them
+            const double mean = adj_dot(aG, nullptr) / ncell;
+            run(OpAxpyLeafConst{aG, -mean, d_skip, n, G, V}, NV);
+        }
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        const int m = adjM, maxit = std::max(1, P.max_outer);
+        const double tol = P.rel_tol;
+        const double gnorm = std::sqrt(adj_dot(aG, aG));
+        cudaMemsetAsync(aLam, 0, (size_t)NV * sizeof(double), st_);
+        adj_copy(aR, aG);
+        double beta = gnorm, trr = 0.0;
+        int iters = 0;
+        bool reached = gnorm == 0.0;
+        std::vector<double> Hm((size_t)(m + 1) * m), cs(m), sn(m), sv(m + 1), y;
+        auto Hij = [&](int i, int j) -> double & { return Hm[(size_t)i * m + j]; };
+        while (!reached && iters < maxit) {
+            std::fill(Hm.begin(), Hm.end(), 0.0);
+            std::fill(sv.begin(), sv.end(), 0.0);
+            adj_copy(aV[0], aR);
+            run(OpScale{aV[0], 1.0 / beta}, NV);
+            sv[0] = beta;
+            int jlast = -1;
+            for (int j = 0; j < m && iters < maxit; j++) {
+                adj_precond(aV[j], aZ[j]);
+                adj_apply_AT(aZ[j]);
+                adj_copy(aW, aUB);
+                adj_leaf_only(aW);
+                for (int i = 0; i <= j; i++) {
+                    Hij(i, j) = adj_dot(aW, aV[i]);
+                    run(OpAxpy{aW, aV[i], -Hij(i, j)}, NV);
+                }
+                Hij(j + 1, j) = std::sqrt(adj_dot(aW, aW));
+                adj_copy(aV[j + 1], aW);
+                if (Hij(j + 1, j) > 0.0) run(OpScale{aV[j + 1], 1.0 / Hij(j + 1, j)}, NV);
+                for (int i = 0; i < j; i++) {
+                    const double t = cs[i] * Hij(i, j) + sn[i] * Hij(i + 1, j);
+                    Hij(i + 1, j) = -sn[i] * Hij(i, j) + cs[i] * Hij(i + 1, j);
+                    Hij(i, j) = t;
+                }
+                const double den = std::hypot(Hij(j, j), Hij(j + 1, j));
+                cs[j] = den > 0 ? Hij(j, j) / den : 1.0;
+                sn[j] = den > 0 ? Hij(j + 1, j) / den : 0.0;
+                Hij(j, j) = den;
+                Hij(j + 1, j) = 0.0;
+                sv[j + 1] = -sn[j] * sv[j];
+                sv[j] = cs[j] * sv[j];
+                iters++;
+                jlast = j;
+                const double rel = std::fabs(sv[j + 1]) / gnorm;
+                if (stats && iters <= SFM_MAX_HISTORY) stats->ratio[iters - 1] = rel;
+                if (rel < tol) break;
+            }
+            y.assign(jlast + 1, 0.0);
+            for (int i = jlast; i >= 0; i--) {
+                double t = sv[i];
+                for (int k = i + 1; k <= jlast; k++) t -= Hij(i, k) * y[k];
+                y[i] = t / Hij(i, i);
+            }
+            for (int i = 0; i <= jlast; i++) run(OpAxpy{aLam, aZ[i], y[i]}, NV);
+            adj_apply_AT(aLam);
+            run(OpSubArr{aR, aG, aUB}, NV);
+            adj_leaf_only(aR);
+            beta = std::sqrt(adj_dot(aR, aR));
+            trr = gnorm > 0 ? beta / gnorm : 0.0;
+            reached = trr < tol;
+        }
+        if (gnorm == 0.0) cudaMemsetAsync(aUB, 0, (size_t)NV * sizeof(double), st_);
+        // aUB holds the transposed pipeline applied to lambda
+        cudaMemsetAsync(aS, 0, (size_t)NV * sizeof(double), st_);
+        double rad2 = -1.0;
+        if (P.bc == SFM_BC_SPHERE) {
+            rad2 = sphere_rad2();
+            const int64_t nfaces = tfLOff[H.nlev];
+            run(OpBcBeta{aUB, d_tfL, d_touch, d_x0, d_h0, d_level, aPart, n, G, V, P.lmax}, nfaces);
+            k_bc_beta_combine<<<1, 32, 0, st_>>>(aPart, (int)nfaces, aBeta);
+            ++launches;
+            run(OpMomentT{aS, aBeta, d_x0, d_h0, H.lstart[0], n, G, V, rad2, P.lmax}, (int64_t)cnt(0) * n * n * n);
+            adj_converge_T(aS);
+        }
+        run(OpAddMaskedLambda{aS, aLam, d_skip, d_x0, d_h0, d_level, n, G, V, rad2}, NV);
+        double corr = 0.0;
+        if (P.zero_mean) {
+            double vol = 0.0;
+            for (int b : leafList) {
+                const double h = H.h0[H.level[b]];
+                vol += (double)(n * n * n) * (h * h * h);
+            }
+            corr = adj_dot(aS, nullptr) / vol;
+        }
+        run(OpAdjOut{aIO, aS, d_skip, d_h0, d_level, n, G, gw, V, P.four_pi_G, corr}, NIO);
+        cudaMemcpyAsync(dJdrho, aIO, (size_t)NIO * sizeof(double), cudaMemcpyDeviceToHost, st_);
+        cudaEventRecord(ev1, st_);
+        rc = check("adjoint");
+        if (rc) return rc;
+        if (stats) {
+            stats->outer_iters = iters;
+            stats->converged = reached ? 1 : 0;
+            stats->true_rel_residual = trr;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            stats->device_ms = ms;
+            stats->kernel_launches = launches;
+            stats->elem_bytes = (int32_t)sizeof(T);
+        }
+        return reached ? SFM_OK : SFM_ENOTCONVERGED;
+    }
+
     int dumpd(const double *a, double *dump) {
         int rc = check("dump");
         if (rc) return rc;
@@ -1059,9 +1296,9 @@ int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *
 }
 
 int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st) {
-    (void)st;
-    if (!c || !dJ_dphi || !dJ_drho) return SFM_EINVAL;
-    return SFM_EINVAL;
+    if (!c || !c->s || !dJ_dphi || !dJ_drho) return SFM_EINVAL;
+    cudaSetDevice(c->device);
+    return c->s->adjoint(dJ_dphi, dJ_drho, st, nullptr);
 }
 
 void sfm_destroy(sfm_ctx *c) {

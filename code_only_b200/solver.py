@@ -8,6 +8,7 @@ explicitly:
 
     ctx = FMGPoisson(hierarchy, bc=SFM_BC_SPHERE)        # fmg_data_init + fmg_alloc_LoL
     psi, g, stats = ctx.solve(rho, psi0)                 # fmg_cycle
+    dJ_drho, astats = ctx.adjoint(dJ_dphi)               # adjoint (no reference counterpart)
     ctx.close()
 
 ``rho``/``psi0`` are float64 arrays [nblocks, G, G, G] (G = ni + 2*ngh_io,
@@ -72,6 +73,25 @@ class FMGPoisson:
         if rc not in (abi.SFM_OK, abi.SFM_ENOTCONVERGED):
             raise SFMError(rc, "sfm_solve_device")
         return st
+
+    def adjoint(self, dJ_dphi: np.ndarray, allow_unconverged=False):
+        """Gradient of a functional of the converged potential (sfm_adjoint).
+
+        dJ_dphi: [nblocks, G, G, G], dJ/dphi on block interiors (ghost entries
+        ignored; entries on covered blocks act through the restriction that
+        defines phi there).  Returns (dJ_drho, stats): dJ/drho on leaf
+        interiors, zero elsewhere.  params.rel_tol is the tolerance on
+        ||dJ/dphi - A^T lambda||_2 relative to ||dJ/dphi||_2 and
+        params.max_outer the iteration cap of the Krylov solve."""
+        dJ = np.ascontiguousarray(dJ_dphi, dtype=np.float64)
+        if dJ.shape != self.shape:
+            raise ValueError(f"dJ_dphi has shape {dJ.shape}, expected {self.shape}")
+        out = np.zeros(self.shape)
+        st = abi.SfmStats()
+        rc = self.lib.sfm_adjoint(self.ctx, dJ.ctypes.data, out.ctypes.data, C.byref(st))
+        if rc not in (abi.SFM_OK, abi.SFM_ENOTCONVERGED) or (rc != abi.SFM_OK and not allow_unconverged):
+            raise SFMError(rc, "sfm_adjoint")
+        return out, st
 
     def info(self):
         lv = C.c_int32()

@@ -145,10 +145,28 @@ int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g
                      sfm_stats *st, void *stream);
 
 /* Adjoint of the solve: given dJ/dphi on the interior of every block
- * (layout as psi; ghost entries ignored), returns dJ/drho on the interior of
- * every block (layout as rho) for the linear map rho -> phi that sfm_solve
- * converges to (the transposed composite operator).  No counterpart in the
- * reference. */
+ * (layout as psi; ghost entries ignored; entries on covered blocks act
+ * through the restriction that defines phi there), returns dJ/drho on the
+ * interior of every block (layout as rho) for the linear map rho -> phi that
+ * sfm_solve converges to.  No counterpart in the reference.
+ *   - The map is the fixed point of the solve's FP64 outer residual
+ *     (fmg_poisson_resid at fmg level 0, fmg_poisson.F90:217-265, with the
+ *     bilinear ghost fill and reflux); its transpose is applied exactly,
+ *     operation by operation, and A^T lambda = dJ/dphi is solved by FGMRES
+ *     preconditioned with this context's fmg_lin (FP32 inside when
+ *     precision is SFM_PREC_MIXED).  The isolated-sphere boundary
+ *     (multipoles of the masked source), the mask and the mean removal are
+ *     chained back to rho.
+ *   - params.rel_tol is the tolerance on ||dJ/dphi - A^T lambda||_2 relative
+ *     to ||dJ/dphi||_2; params.max_outer caps the Krylov iterations.
+ *   - dJ/drho is zero on covered blocks (the solve overwrites rho there by
+ *     restriction) and on ghost entries.  With periodic boundaries phi's
+ *     constant is free: dJ/dphi is taken orthogonal to constants.
+ *   - The first call allocates the Krylov vectors (as many as fit, up to 30
+ *     restarts' worth, in 80% of the free device memory).
+ *   - Results are reproducible to roundoff, not bitwise (FP64 atomics).
+ * st: outer_iters = Krylov iterations, ratio[] = their residual history,
+ * true_rel_residual = the final true relative residual. */
 int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st);
 
 void sfm_destroy(sfm_ctx *c);
