@@ -29,18 +29,34 @@ __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const Fac
     if (it >= nitems) return;
     const FaceItem fi = items[it];
     if (sel >= 0 && fi.type != sel) return;
+    // A pass never reads a ghost cell of its own direction (sources are
+    // planes interior along `dir`), so each lane issues all of its loads
+    // before any of its stores: IT independent DRAM round trips in flight
+    // instead of IT dependent ones.
+    constexpr int IT = (NC + 31) / 32;
     T *ud = u + (int64_t)fi.dst * V;
     const int xg = fi.lr == 0 ? -1 : N;
+    T val[IT];
     if (fi.type == 0) {
         const T *us = u + (int64_t)fi.src * V;
         const int xs = fi.lr == 0 ? N - 1 : 0;
-#pragma unroll 4
-        for (int c = lane; c < NC; c += 32) {
+#pragma unroll
+        for (int t = 0; t < IT; t++) {
+            const int c = lane + 32 * t;
+            if (c >= NC) break;
             const int p = c % G - 1, q = c / G - 1;
-            int i, j, k, is, js, ks;
-            put3(dir, xg, p, q, i, j, k);
+            int is, js, ks;
             put3(dir, xs, p, q, is, js, ks);
-            ud[cidx(G, i, j, k)] = us[cidx(G, is, js, ks)];
+            val[t] = us[cidx(G, is, js, ks)];
+        }
+#pragma unroll
+        for (int t = 0; t < IT; t++) {
+            const int c = lane + 32 * t;
+            if (c >= NC) break;
+            const int p = c % G - 1, q = c / G - 1;
+            int i, j, k;
+            put3(dir, xg, p, q, i, j, k);
+            ud[cidx(G, i, j, k)] = val[t];
         }
         return;
     }
@@ -54,7 +70,10 @@ __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const Fac
         put3(dir, xc, pb + oa, qb + ob, ci, cj, ck);
         return uc[cidx(G, ci, cj, ck)];
     };
-    for (int c = lane; c < NC; c += 32) {
+#pragma unroll
+    for (int t = 0; t < IT; t++) {
+        const int c = lane + 32 * t;
+        if (c >= NC) break;
         const int p = c % G - 1, q = c / G - 1;
         T uH;
         if (cubic && NB2 + 2 >= 4) {
@@ -73,12 +92,20 @@ __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const Fac
             const int p1 = near_(p, pc), q1 = near_(q, qc);
             uH = ((T)9 * B(pc, qc) + B(p1, q1) + (T)3 * B(pc, q1) + (T)3 * B(p1, qc)) / (T)16;
         }
-        int i, j, k, i0, j0, k0, iN, jN, kN;
-        put3(dir, xg, p, q, i, j, k);
+        int i0, j0, k0, iN, jN, kN;
         put3(dir, xg + inner, p, q, i0, j0, k0);
         put3(dir, xg + 2 * inner, p, q, iN, jN, kN);
         const T u0 = ud[cidx(G, i0, j0, k0)], uN = ud[cidx(G, iN, jN, kN)];
-        ud[cidx(G, i, j, k)] = ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
+        val[t] = ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
+    }
+#pragma unroll
+    for (int t = 0; t < IT; t++) {
+        const int c = lane + 32 * t;
+        if (c >= NC) break;
+        const int p = c % G - 1, q = c / G - 1;
+        int i, j, k;
+        put3(dir, xg, p, q, i, j, k);
+        ud[cidx(G, i, j, k)] = val[t];
     }
 }
 
@@ -206,6 +233,190 @@ __global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T 
             u[(int64_t)blocks[first + q] * V + c] = sh[q * V + c];
         }
         __syncthreads();
+    }
+    cta_max_atomic(m, out);
+}
+
+// ---------------------------------------------------------------------------
+// bulk-copy pipeline (1D cp.async.bulk, no multicast) for the block sweeps
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: false after `limit` unsuccessful polls
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t t = 0; t < limit; t++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+constexpr uint32_t kWaitPolls = 1u << 20;   // bound on every mbarrier wait of a sweep
+
+// stages of the bulk pipeline: up to 4, within 48 KB of u + rhs tiles.
+// [LO, LO + SPAN) is the 16-byte-aligned element range of a block that
+// holds every interior cell (cidx of (0,0,0) to (N-1,N-1,N-1)).
+template <class T, int N>
+struct BulkPlan {
+    static constexpr int G = N + 2, V = G * G * G;
+    static constexpr int STAGE_BYTES = 2 * Tile<N>::BPC * V * (int)sizeof(T);
+    static constexpr int S0 = 49152 / STAGE_BYTES;
+    static constexpr int S = S0 >= 4 ? 4 : (S0 >= 2 ? S0 : 2);
+    static constexpr int SMEM = S * STAGE_BYTES;
+    static constexpr int EPB = 16 / (int)sizeof(T);
+    static constexpr int LO = (1 + G + G * G) / EPB * EPB;
+    static constexpr int HI = ((N + N * G + N * G * G) + 1 + EPB - 1) / EPB * EPB;
+    static constexpr int SPAN = HI - LO;
+    static_assert(HI <= V && (V * (int)sizeof(T)) % 16 == 0, "span within the block, blocks 16-byte aligned");
+};
+
+// Red-black colour sweep with whole blocks of u (ghost shell included) and
+// the interior span of rhs brought in by bulk async copies, and the interior
+// span of each updated block written back by one bulk store (the ghost cells
+// inside the span go back unchanged).  Same arithmetic as k_relax_tiled.
+// Warp 0 fills the stages: with a tile's copies it also loads that tile's
+// per-block data (reflux slots, cell widths), so a sweep step waits only on
+// its stage's mbarrier.  After storing the stage of step `it` it refills the
+// stage of step it-1, whose store has had a whole step to read it.  A wait
+// that exceeds kWaitPolls sets *err, drains this CTA's copies (again
+// bounded) and returns.
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
+                                                    const int32_t *__restrict__ blocks, int nblk,
+                                                    const double *__restrict__ h0, const int32_t *__restrict__ level,
+                                                    const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
+                                                    int f, int ipass, unsigned long long *out, int *err) {
+    using Tl = Tile<N>;
+    using Pl = BulkPlan<T, N>;
+    constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2, S = Pl::S;
+    constexpr uint32_t BB = (uint32_t)(V * sizeof(T));
+    constexpr int LO = Pl::LO;
+    constexpr uint32_t SB = (uint32_t)(Pl::SPAN * sizeof(T));
+    static_assert(BB % 16 == 0 && SB % 16 == 0 && (LO * sizeof(T)) % 16 == 0, "bulk copies move 16-byte units");
+    extern __shared__ __align__(128) unsigned char bulk_smem[];
+    T *ust = reinterpret_cast<T *>(bulk_smem);   // [S][BPC][V]
+    T *rst = ust + S * BPC * V;                  // [S][BPC][V]
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ int pend[S], ph[S], abort_flag;
+    __shared__ int ssl[S][BPC][6];
+    __shared__ T shh[S][BPC], shi[S][BPC];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int ntiles = (nblk + BPC - 1) / BPC;
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) { mbar_init(&bar[s], 1); pend[s] = 0; ph[s] = 0; }
+        abort_flag = 0;
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // warp 0 fills stage s with tile `tile` and its per-block data
+    auto issue = [&](int s, int tile) {
+        const int first = tile * BPC;
+        const int cnt = nblk - first < BPC ? nblk - first : BPC;
+        if (lane == 0) { pend[s] = 1; mbar_expect_tx(&bar[s], (uint32_t)cnt * (BB + SB)); }
+        __syncwarp();
+        for (int q = lane; q < BPC; q += 32) {
+            if (q >= cnt) {
+                for (int fc = 0; fc < 6; fc++) ssl[s][q][fc] = -1;
+                continue;
+            }
+            const int64_t b = blocks[first + q];
+            bulk_load(ust + (s * BPC + q) * V, u + b * V, BB, &bar[s]);
+            bulk_load(rst + (s * BPC + q) * V + LO, rhs + b * V + LO, SB, &bar[s]);
+            for (int fc = 0; fc < 6; fc++) ssl[s][q][fc] = rslot ? rslot[6 * b + fc] : -1;
+            const double hd = hlev(h0, level[b], f);
+            shh[s][q] = (T)hd;
+            shi[s][q] = (T)(1.0 / hd);
+        }
+    };
+    if (tid < 32)
+        for (int s = 0; s < S; s++) {
+            const int tile = blockIdx.x + s * (int)gridDim.x;
+            if (tile < ntiles) issue(s, tile);
+        }
+    double m = 0.0;
+    int it = 0, sprev = -1, tprev = -1;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int s = it % S;
+        const int first = tile * BPC;
+        if (!mbar_wait_bounded(&bar[s], (uint32_t)(ph[s] & 1), kWaitPolls)) atomicExch(&abort_flag, 1);
+        __syncthreads();
+        if (abort_flag) break;
+        T *ut = ust + s * BPC * V;
+        const T *rt = rst + s * BPC * V;
+        for (int t = tid; t < BPC * HALF; t += blockDim.x) {
+            const int q = t / HALF, r = t - q * HALF;
+            if (first + q >= nblk) continue;
+            constexpr int HN = N / 2;
+            const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
+            const int i = 2 * i2 + ((j + k + ipass) & 1);
+            const T hh = shh[s][q], hi = shi[s][q];
+            T *ub = ut + q * V;
+            TileFlux<T, N> F{ub, hi, rslot ? ssl[s][q] : nullptr, rbuf};
+            const int c = (int)cidx(G, i, j, k);
+            const T resh2 = (F.div(i, j, k) - rt[q * V + c] * hh) * hh;
+            ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
+            const double a = fabs((double)resh2);
+            m = a > m ? a : m;
+        }
+        fence_async_shared();
+        __syncthreads();
+        if (tid < 32) {
+            const int cnt = nblk - first < BPC ? nblk - first : BPC;
+            if (lane == 0) {
+                ph[s]++;
+                pend[s] = 0;
+                for (int q = 0; q < cnt; q++)
+                    bulk_store(u + (int64_t)blocks[first + q] * V + LO, ut + q * V + LO, SB);
+                bulk_commit();
+            }
+            // refill the previous step's stage; its store group is the older one
+            const int nt = tprev >= 0 ? tprev + S * (int)gridDim.x : ntiles;
+            if (nt < ntiles) {
+                if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                __syncwarp();
+                issue(sprev, nt);
+            }
+        }
+        sprev = s;
+        tprev = tile;
+    }
+    if (tid == 0) {
+        if (abort_flag) {   // drain this CTA's loads in flight, bounded, then report
+            for (int s = 0; s < S; s++)
+                if (pend[s]) mbar_wait_bounded(&bar[s], (uint32_t)(ph[s] & 1), kWaitPolls);
+            atomicExch(err, 1);
+        }
+        bulk_wait_all();
     }
     cta_max_atomic(m, out);
 }

@@ -241,6 +241,9 @@ public:
     unsigned long long *d_max = nullptr;   // [8]
     double *d_scal = nullptr;              // [8]
     int *d_bad = nullptr;
+    int *d_err = nullptr;                  // set by a device wait that gave up
+    int nSM = 148;
+    int bulkGrid[5] = {0, 0, 0, 0, 0};     // persistent CTAs of k_relax_bulk<T, N>, by log2(N)
     double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
     int *d_mgit = nullptr;
     // base grid
@@ -320,6 +323,7 @@ public:
             cudaGetDevice(&dev);
             if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
             persistGrid = sms * 8;
+            nSM = sms;
             maxBlocks = sms * 16;
         }
         cudaEventCreate(&ev0);
@@ -435,6 +439,9 @@ public:
         d_max = mem.alloc<unsigned long long>(8);
         d_scal = mem.alloc<double>(8);
         d_bad = mem.alloc<int>(1);
+        d_err = mem.alloc<int>(1);
+        zeroList.push_back({d_err, sizeof(int)});
+        for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], (void)bulk_grid<N>(), (void)0);
         d_mom = mem.alloc<double>(32);
         d_part = mem.alloc<double>((size_t)(H.lstart[1]) * 25);
         d_psum = mem.alloc<double>((size_t)nb);
@@ -593,15 +600,51 @@ public:
             if (prof) { profEv.push_back(nullptr); cudaEventCreate(&profEv.back()); cudaEventRecord(profEv.back(), st_); }
         }
     }
+    // persistent grid of k_relax_bulk<T, N> (N >= 4): every SM filled to the
+    // kernel's occupancy; computed once, at set-up, outside stream capture
+    // the bulk pipeline serves blocks of 4^3 and up whose stages fit in 220 KB
+    template <int N>
+    static constexpr bool bulk_ok() { return N >= 4 && BulkPlan<T, N>::SMEM <= 220 * 1024; }
+    template <int N>
+    int bulk_grid() {
+        if (!bulk_ok<N>()) return 0;
+        constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : 2);
+        if (!bulkGrid[li]) {
+            const int smem = BulkPlan<T, N>::SMEM;
+            if (smem > 48 * 1024)
+                cudaFuncSetAttribute(k_relax_bulk<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            int per = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N>, 256, smem) != cudaSuccess ||
+                per < 1) {
+                cudaGetLastError();
+                per = 1;
+            }
+            bulkGrid[li] = nSM * per;
+        }
+        return bulkGrid[li];
+    }
     void relax_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
                       int f, int ipass, unsigned long long *out) {
         const int n = nf[f];
+        if (nblk <= 0) return;
         SFM_WITH_N(n,
-                   (k_relax_tiled<T, N><<<(unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
-                                          256, 0, st_>>>(u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
+                   (bulk_ok<N>() ? (k_relax_bulk<T, N><<<(unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC,
+                                                                      bulk_grid<N>()),
+                                                    256, BulkPlan<T, N>::SMEM, st_>>>(
+                                  u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out, d_err))
+                            : (k_relax_tiled<T, N><<<(unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC,
+                                                                        persistGrid),
+                                                     256, 0, st_>>>(u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f,
+                                                                    ipass, out)),
                     ++launches),
                    runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
                           (int64_t)nblk * n * n * n / 2, out))
+    }
+    int check_err() {
+        int e = 0;
+        if (cudaMemcpy(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SFM_ECUDA;
+        if (e) { last_error = "a bulk-copy wait in the smoother gave up"; return SFM_ETIMEOUT; }
+        return SFM_OK;
     }
     static constexpr size_t kMaxProf = 4096;
     std::vector<cudaEvent_t> profEv;
@@ -922,6 +965,7 @@ public:
             trr = read_max(3) / resh2max;
         }
         rc = check("finish");
+        if (rc == SFM_OK) rc = check_err();
         if (rc) return rc;
         if (stats) {
             stats->outer_iters = iters;
@@ -1157,6 +1201,7 @@ public:
         cudaMemcpyAsync(dJdrho, aIO, (size_t)NIO * sizeof(double), cudaMemcpyDeviceToHost, st_);
         cudaEventRecord(ev1, st_);
         rc = check("adjoint");
+        if (rc == SFM_OK) rc = check_err();
         if (rc) return rc;
         if (stats) {
             stats->outer_iters = iters;
