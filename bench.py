@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--workload", default="jeans6")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="also time one adjoint solve (gradient of W = 1/2 sum rho phi dV), mixed precision")
     ap.add_argument("--single", choices=["mixed", "fp64"], default=None,
                     help="run exactly one solve of that precision and exit (for profiler launch lists)")
     return ap.parse_args()
@@ -237,6 +239,18 @@ def run_ours(args):
                 clocks = sampler.stop()
             results[key] = dict(ms=ms, st=st, launches=launches, smo=smo, iters=iters,
                                 resid=st.true_rel_residual, info=s.info())
+            if key == "mixed":
+                psi_mixed = psi_d.clone()
+    # phi of the mixed path against the plain FP64 path (block interiors;
+    # each potential's mean removed first: a periodic box fixes phi up to a constant)
+    ng = (G - h.ni) // 2
+    a = psi_mixed[:, ng:ng + h.ni, ng:ng + h.ni, ng:ng + h.ni]
+    bfp = psi_d[:, ng:ng + h.ni, ng:ng + h.ni, ng:ng + h.ni]
+    if bc == abi.SFM_BC_PERIODIC:
+        a = a - a.mean()
+        bfp = bfp - bfp.mean()
+    phi_err = float((a - bfp).abs().max() / bfp.abs().max())
+    del psi_mixed, a, bfp
     # end to end through the host-buffer ABI (pinned host memory)
     e2e = None
     if not args.no_e2e:
@@ -315,6 +329,7 @@ def run_ours(args):
         "true_rel_residual": {"mixed": mx["resid"], "fp64": fp["resid"]},
         "fp64": {"value": round(world * 1e3 / fp["ms"], 4), "unit": "solves/s", "ms_per_step": round(fp["ms"], 4)},
         "mixed_over_fp64": round(fp["ms"] / mx["ms"], 3),
+        "phi_rel_err_mixed_vs_fp64": phi_err,
         "roofline": {
             "kernel": "red-black colour sweep, fmg level 0 (OpRelax<float>)",
             "bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
@@ -329,11 +344,39 @@ def run_ours(args):
     }
     if e2e:
         line["e2e"] = e2e
+    if args.adjoint:
+        line["adjoint"] = time_adjoint(h, rho, bc)
     if not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(h, rho, bc, fp["iters"][-1], sample_iters=1)
     print(json.dumps(line), flush=True)
     from code_only_b200 import replicas
     replicas.teardown(info)
+
+
+def time_adjoint(h, rho, bc):
+    """One adjoint solve (sfm_adjoint, host arrays, mixed precision) of
+    W = 1/2 sum rho phi dV over leaf cells, to a Krylov residual of 1e-10;
+    wall time around the call (host<->device copies of two fields included)."""
+    import numpy as np
+    from code_only_b200 import abi
+    from code_only_b200.solver import FMGPoisson
+    kw = dict(rel_tol=1e-10, max_outer=60, precision=abi.SFM_PREC_MIXED)
+    if bc == abi.SFM_BC_SPHERE:
+        kw.update(zero_mean=0, lmax=4)
+    G = rho.shape[1]
+    ng = (G - h.ni) // 2
+    leaf = (h.level == h.nlev - 1) | (h.child[:, 0] < 0)
+    dv = np.asarray(h.cellwidth)[np.asarray(h.level)] ** 3
+    dJ = np.zeros_like(rho)
+    sl = slice(ng, ng + h.ni)
+    dJ[leaf, sl, sl, sl] = 0.5 * rho[leaf, sl, sl, sl] * dv[leaf, None, None, None]
+    with FMGPoisson(h, params=abi.default_params(bc, **kw)) as s:
+        s.adjoint(dJ, allow_unconverged=True)          # first call allocates the Krylov vectors
+        t0 = time.perf_counter()
+        _, st = s.adjoint(dJ, allow_unconverged=True)
+        ms = (time.perf_counter() - t0) * 1e3
+    return {"ms": round(ms, 2), "krylov_iterations": st.outer_iters, "true_rel_residual": st.true_rel_residual,
+            "device_ms": round(st.device_ms, 2), "functional": "W = 1/2 sum(rho phi dV), leaf cells"}
 
 
 def cpu_baseline(h, rho, bc, n_outer, sample_iters=1):

@@ -241,13 +241,10 @@ __device__ __forceinline__ T trilinear_cell(const T *uc, int G, int ifn, int jf,
 }
 // interp_tricubic for one fine cell of an n^3 block from the coarse array
 // (buffer bounds [lb,ub] = [-1, nc]); the caller guarantees nc + 2 >= 4
+// (nodes c* and weights w* of cubic_weights along each axis given)
 template <class T>
-__device__ __forceinline__ T tricubic_cell(const T *uc, int Gc, int i, int j, int k, int lb, int ub) {
-    int ci[4], cj[4], ck[4];
-    double wi[4], wj[4], wk[4];
-    cubic_weights(i, lb, ub, ci, wi);
-    cubic_weights(j, lb, ub, cj, wj);
-    cubic_weights(k, lb, ub, ck, wk);
+__device__ __forceinline__ T tricubic_cell_w(const T *uc, int Gc, const int *ci, const double *wi, const int *cj,
+                                             const double *wj, const int *ck, const double *wk) {
     T bxy[4];
 #pragma unroll
     for (int mk = 0; mk < 4; mk++) {
@@ -260,6 +257,15 @@ __device__ __forceinline__ T tricubic_cell(const T *uc, int Gc, int i, int j, in
         bxy[mk] = (T)wj[0] * bx[0] + (T)wj[1] * bx[1] + (T)wj[2] * bx[2] + (T)wj[3] * bx[3];
     }
     return (T)wk[0] * bxy[0] + (T)wk[1] * bxy[1] + (T)wk[2] * bxy[2] + (T)wk[3] * bxy[3];
+}
+template <class T>
+__device__ __forceinline__ T tricubic_cell(const T *uc, int Gc, int i, int j, int k, int lb, int ub) {
+    int ci[4], cj[4], ck[4];
+    double wi[4], wj[4], wk[4];
+    cubic_weights(i, lb, ub, ci, wi);
+    cubic_weights(j, lb, ub, cj, wj);
+    cubic_weights(k, lb, ub, ck, wk);
+    return tricubic_cell_w(uc, Gc, ci, wi, cj, wj, ck, wk);
 }
 
 // fmg_interp_cubic / fmg_interp_linear over the listed blocks (fmg.F90:826-843,

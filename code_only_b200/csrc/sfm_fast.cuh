@@ -22,10 +22,19 @@ namespace sfm {
 template <class T, int N>
 __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const FaceItem *__restrict__ items, int nitems,
                                                     int dir, int cubic, int sel) {
-    constexpr int G = N + 2, NC = G * G;
+    constexpr int G = N + 2, NC = G * G, NB2 = N / 2;
     constexpr int64_t V = (int64_t)G * G * G;
     const int lane = threadIdx.x & 31;
     const int it = blockIdx.x * 4 + (threadIdx.x >> 5);
+    // transverse Lagrange nodes and weights of the bicubic coarse-fine ghost,
+    // for p in [-1, N] (entry p + 1): evaluated once per CTA
+    __shared__ int gwc[G][4];
+    __shared__ double gww[G][4];
+    const bool bicubic = cubic && NB2 + 2 >= 4;
+    if (bicubic) {
+        if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, gwc[threadIdx.x], gww[threadIdx.x]);
+        __syncthreads();
+    }
     if (it >= nitems) return;
     const FaceItem fi = items[it];
     if (sel >= 0 && fi.type != sel) return;
@@ -61,7 +70,6 @@ __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const Fac
         return;
     }
     const T *uc = u + (int64_t)fi.src * V;
-    constexpr int NB2 = N / 2;
     const int xc = fi.lr == 0 ? N - 1 : 0;
     const int oa = fi.oa * NB2, ob = fi.ob * NB2;
     const int inner = fi.lr == 0 ? 1 : -1;
@@ -76,11 +84,9 @@ __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const Fac
         if (c >= NC) break;
         const int p = c % G - 1, q = c / G - 1;
         T uH;
-        if (cubic && NB2 + 2 >= 4) {
-            int cp[4], cq[4];
-            double wp[4], wq[4];
-            cubic_weights(p, -1, NB2, cp, wp);
-            cubic_weights(q, -1, NB2, cq, wq);
+        if (bicubic) {
+            const int *cp = gwc[p + 1], *cq = gwc[q + 1];
+            const double *wp = gww[p + 1], *wq = gww[q + 1];
             T bx[4];
 #pragma unroll
             for (int m = 0; m < 4; m++)
@@ -466,9 +472,14 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
     __shared__ T sc[VC];
     __shared__ T bx[N * W * W];            // [kc][jc][i]
     __shared__ T bxy[N * N * W];           // [kc][j][i]
+    // Lagrange nodes and weights of fine index p (the same for x, y and z):
+    // cubic_weights evaluated once per CTA instead of once per staged value
+    __shared__ int cwc[N][4];
+    __shared__ double cww[N][4];
     const int b = blocks[blockIdx.x];
     (void)nblk;
     for (int t = threadIdx.x; t < VC; t += blockDim.x) sc[t] = uc[(int64_t)b * VC + t];
+    if (threadIdx.x < N) cubic_weights((int)threadIdx.x, -1, NC, cwc[threadIdx.x], cww[threadIdx.x]);
     __syncthreads();
     T *ufb = uf + (int64_t)b * VF;
     if (!(cubic && NC + 2 >= 4)) {
@@ -481,9 +492,8 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
     // x: bx(i, jc, kc) for kc, jc in [-1, NC]
     for (int t = threadIdx.x; t < N * W * W; t += blockDim.x) {
         const int i = t % N, jc = (t / N) % W - 1, kc = t / (N * W) - 1;
-        int c[4];
-        double w[4];
-        cubic_weights(i, -1, NC, c, w);
+        const int *c = cwc[i];
+        const double *w = cww[i];
         const T *row = sc + cidx(GC, 0, jc, kc);
         bx[t] = (T)w[0] * row[c[0]] + (T)w[1] * row[c[1]] + (T)w[2] * row[c[2]] + (T)w[3] * row[c[3]];
     }
@@ -491,9 +501,8 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
     // y: bxy(i, j, kc)
     for (int t = threadIdx.x; t < N * N * W; t += blockDim.x) {
         const int i = t % N, j = (t / N) % N, kc = t / (N * N) - 1;
-        int c[4];
-        double w[4];
-        cubic_weights(j, -1, NC, c, w);
+        const int *c = cwc[j];
+        const double *w = cww[j];
         auto X = [&](int jc) { return bx[((kc + 1) * W + (jc + 1)) * N + i]; };
         bxy[t] = (T)w[0] * X(c[0]) + (T)w[1] * X(c[1]) + (T)w[2] * X(c[2]) + (T)w[3] * X(c[3]);
     }
@@ -501,9 +510,8 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
     // z
     for (int t = threadIdx.x; t < N * N * N; t += blockDim.x) {
         const int i = t % N, j = (t / N) % N, k = t / (N * N);
-        int c[4];
-        double w[4];
-        cubic_weights(k, -1, NC, c, w);
+        const int *c = cwc[k];
+        const double *w = cww[k];
         auto Y = [&](int kc) { return bxy[((kc + 1) * N + j) * N + i]; };
         ufb[cidx(GF, i, j, k)] = (T)w[0] * Y(c[0]) + (T)w[1] * Y(c[1]) + (T)w[2] * Y(c[2]) + (T)w[3] * Y(c[3]);
     }
@@ -532,44 +540,76 @@ __global__ void __launch_bounds__(256) k_converge_tiled(T *__restrict__ u, const
 }
 
 // ---------------------------------------------------------------------------
-// ordered FP64 sums: a warp stages 32 partial sums at a time in registers and
-// lane 0 adds them in list order -- the same sequence of roundings as a
-// single-thread loop, without its load latency
+// ordered FP64 sums: warps 1..31 stage the terms of the next chunk into shared
+// memory (double-buffered) while thread 0 adds the current chunk in list
+// order -- the same sequence of roundings as a single-thread loop, with the
+// loads off its critical path.  One CTA of 1024 threads.
 // ---------------------------------------------------------------------------
-__global__ void k_mean_combine_w(const double *__restrict__ psum, const int32_t *__restrict__ blocks, int nblk,
-                                 const int32_t *__restrict__ level, const double *__restrict__ h0, int n,
-                                 double *out) {
-    const int lane = threadIdx.x & 31;
-    if (threadIdx.x >= 32 || blockIdx.x != 0) return;
-    double mass = 0.0, vol = 0.0;
+constexpr int kSumChunk = 1024;
+
+// leaf mean: sum_b psum_b dv_b / sum_b n^3 dv_b over the listed blocks
+__global__ void __launch_bounds__(1024) k_mean_combine_w(const double *__restrict__ psum,
+                                                         const int32_t *__restrict__ blocks, int nblk,
+                                                         const int32_t *__restrict__ level,
+                                                         const double *__restrict__ h0, int n, double *out) {
+    __shared__ double tm[2][kSumChunk], tv[2][kSumChunk];
+    const int tid = threadIdx.x;
     const double ncell = (double)(n * n * n);
-    for (int base = 0; base < nblk; base += 32) {
-        double s = 0.0, dv = 0.0;
-        if (base + lane < nblk) {
-            s = psum[base + lane];
-            const double hd = h0[level[blocks[base + lane]]];
-            dv = hd * hd * hd;
+    const int nch = (nblk + kSumChunk - 1) / kSumChunk;
+    auto stage = [&](int c) {
+        for (int t = tid - 32; t < kSumChunk; t += (int)blockDim.x - 32) {
+            const int b = c * kSumChunk + t;
+            if (b >= nblk) break;
+            const double hd = h0[level[blocks[b]]];
+            const double dv = hd * hd * hd;
+            tm[c & 1][t] = psum[b] * dv;
+            tv[c & 1][t] = ncell * dv;
         }
-        const int cnt = nblk - base < 32 ? nblk - base : 32;
-        for (int l = 0; l < cnt; l++) {
-            const double sl = __shfl_sync(0xffffffffu, s, l), dl = __shfl_sync(0xffffffffu, dv, l);
-            mass = mass + sl * dl;
-            vol = vol + ncell * dl;
+    };
+    double mass = 0.0, vol = 0.0;
+    if (tid >= 32 && nch > 0) stage(0);
+    __syncthreads();
+    for (int c = 0; c < nch; c++) {
+        if (tid >= 32) {
+            if (c + 1 < nch) stage(c + 1);
+        } else if (tid == 0) {
+            const int cnt = nblk - c * kSumChunk < kSumChunk ? nblk - c * kSumChunk : kSumChunk;
+            for (int q = 0; q < cnt; q++) {
+                mass = mass + tm[c & 1][q];
+                vol = vol + tv[c & 1][q];
+            }
         }
+        __syncthreads();
     }
-    if (lane == 0) *out = mass / vol;
+    if (tid == 0) *out = mass / vol;
 }
 
-__global__ void k_ave_combine_w(const double *__restrict__ psum, int nblk, int n, double *out) {
-    const int lane = threadIdx.x & 31;
-    if (threadIdx.x >= 32 || blockIdx.x != 0) return;
+// base-level average: sum_b psum_b / (n^3 nblk)
+__global__ void __launch_bounds__(1024) k_ave_combine_w(const double *__restrict__ psum, int nblk, int n,
+                                                        double *out) {
+    __shared__ double ts[2][kSumChunk];
+    const int tid = threadIdx.x;
+    const int nch = (nblk + kSumChunk - 1) / kSumChunk;
+    auto stage = [&](int c) {
+        for (int t = tid - 32; t < kSumChunk; t += (int)blockDim.x - 32) {
+            const int b = c * kSumChunk + t;
+            if (b >= nblk) break;
+            ts[c & 1][t] = psum[b];
+        }
+    };
     double ave = 0.0;
-    for (int base = 0; base < nblk; base += 32) {
-        const double s = base + lane < nblk ? psum[base + lane] : 0.0;
-        const int cnt = nblk - base < 32 ? nblk - base : 32;
-        for (int l = 0; l < cnt; l++) ave = ave + __shfl_sync(0xffffffffu, s, l);
+    if (tid >= 32 && nch > 0) stage(0);
+    __syncthreads();
+    for (int c = 0; c < nch; c++) {
+        if (tid >= 32) {
+            if (c + 1 < nch) stage(c + 1);
+        } else if (tid == 0) {
+            const int cnt = nblk - c * kSumChunk < kSumChunk ? nblk - c * kSumChunk : kSumChunk;
+            for (int q = 0; q < cnt; q++) ave = ave + ts[c & 1][q];
+        }
+        __syncthreads();
     }
-    if (lane == 0) *out = nblk == 0 ? 0.0 : ave / (double)(n * n * n * nblk);
+    if (tid == 0) *out = nblk == 0 ? 0.0 : ave / (double)(n * n * n * nblk);
 }
 
 }  // namespace sfm

@@ -15,6 +15,7 @@
 namespace sfm {
 
 constexpr int MG_MAXLEV = 8;
+constexpr int MG_NMAX = 128;   // base-grid cells per edge (the mg CTA handles at most 64)
 
 struct MgData {
     double *U[MG_MAXLEV], *RES[MG_MAXLEV], *RHS[MG_MAXLEV], *RHO[MG_MAXLEV];
@@ -140,12 +141,17 @@ __device__ void mg_rstrct(const MgData &d, int m, double *uc, const double *uf) 
 }
 __device__ void mg_interp(const MgData &d, int m, double *uf, double *uc, bool cubic) {   // mg.F90:608-633
     const int lc = m + 1, n = mgN(d, m), G = n + 2, nc = mgN(d, lc), Gc = nc + 2;
-    mg_boundary_extrap(d, lc, uc);
+    // Lagrange nodes and weights per fine index, evaluated once per call
+    __shared__ int tcw[MG_NMAX][4];
+    __shared__ double tww[MG_NMAX][4];
+    const bool tri = cubic && nc + 2 >= 4;
+    if (tri && (int)threadIdx.x < n) cubic_weights((int)threadIdx.x, -1, nc, tcw[threadIdx.x], tww[threadIdx.x]);
+    mg_boundary_extrap(d, lc, uc);   // ends with __syncthreads
     mg_boundary_u(d, lc, uc);
     for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
         int i = c % n, j = (c / n) % n, k = c / (n * n);
-        uf[cidx(G, i, j, k)] = (cubic && nc + 2 >= 4) ? tricubic_cell(uc, Gc, i, j, k, -1, nc)
-                                                      : trilinear_cell(uc, Gc, i, j, k, 0, 0, 0);
+        uf[cidx(G, i, j, k)] = tri ? tricubic_cell_w(uc, Gc, tcw[i], tww[i], tcw[j], tww[j], tcw[k], tww[k])
+                                   : trilinear_cell(uc, Gc, i, j, k, 0, 0, 0);
     }
     __syncthreads();
     mg_boundary_fill0(d, m, uf);

@@ -798,7 +798,7 @@ public:
     void vmg_zeroAverage(T *a) {
         const int F = H.FMax, n = nf[F];
         run(OpBlockSum<T>{a, d_all, d_psum, n, Gf[F], Vf[F]}, (int64_t)cnt(0));
-        k_ave_combine_w<<<1, 32, 0, st_>>>(d_psum, cnt(0), n, d_scal + 1);
+        k_ave_combine_w<<<1, 1024, 0, st_>>>(d_psum, cnt(0), n, d_scal + 1);
         ++launches;
         run(OpSubScalarInterior<T>{a, d_scal + 1, 0, n, Gf[F], Vf[F]}, (int64_t)cnt(0) * n * n * n);
     }
@@ -902,7 +902,7 @@ public:
         run(OpPhysvar<double>{PHI0, RES0d, rho, psi, H.NI, Gf[0], gw, Vf[0], P.four_pi_G, d_bad}, (int64_t)nb * Vf[0]);
         if (P.zero_mean) {
             run(OpBlockSum<double>{RES0d, d_leaves, d_psum, H.NI, Gf[0], Vf[0]}, (int64_t)nLeaves);
-            k_mean_combine_w<<<1, 32, 0, st_>>>(d_psum, d_leaves, nLeaves, d_level, d_h0, H.NI, d_scal);
+            k_mean_combine_w<<<1, 1024, 0, st_>>>(d_psum, d_leaves, nLeaves, d_level, d_h0, H.NI, d_scal);
             ++launches;
             run(OpSubScalarAll<double>{RES0d, d_scal}, (int64_t)nb * Vf[0]);
         } else {
