@@ -23,6 +23,8 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from typing import Callable, Optional, Sequence
 
 import numpy as np
@@ -238,13 +240,27 @@ def cell_centres(h: Hierarchy, ngh: int):
     return xs, ys, zs
 
 
+def _threads() -> int:
+    return max(1, min(32, os.cpu_count() or 1))
+
+
 def block_field(h: Hierarchy, ngh: int, fn: Callable) -> np.ndarray:
     """Evaluates fn(x,y,z) at every cell centre (ghosts included), returning
-    [nb, G, G, G] with axes (k, j, i) -- i fastest in memory."""
+    [nb, G, G, G] with axes (k, j, i) -- i fastest in memory.  Chunks of
+    blocks are evaluated on a thread pool (elementwise: same values)."""
     xs, ys, zs = cell_centres(h, ngh)
-    out = fn(xs[:, None, None, :], ys[:, None, :, None], zs[:, :, None, None])
     G = h.ni + 2 * ngh
-    return np.array(np.broadcast_to(out, (h.nblocks, G, G, G)), dtype=np.float64, order="C", copy=True)
+    out = np.empty((h.nblocks, G, G, G), dtype=np.float64)
+    chunk = 2048
+
+    def part(s):
+        e = min(s + chunk, h.nblocks)
+        v = fn(xs[s:e, None, None, :], ys[s:e, None, :, None], zs[s:e, :, None, None])
+        out[s:e] = np.broadcast_to(v, (e - s, G, G, G))
+
+    with ThreadPoolExecutor(_threads()) as ex:
+        list(ex.map(part, range(0, h.nblocks, chunk)))
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -373,8 +389,9 @@ def jeans_cloud(nlev: int = 6, nbase: int = 16, ni: int = 8, seed: int = 12345,
         idx = (np.arange(ni) + 0.5) * h
         lo = q.astype(np.float64) * ni * h
         out = np.zeros(q.shape[0], dtype=bool)
-        chunk = 4096
-        for s in range(0, q.shape[0], chunk):
+        chunk = 512
+
+        def part(s):
             qs = lo[s:s + chunk]
             xs = qs[:, 0:1] + idx[None, :]
             ys = qs[:, 1:2] + idx[None, :]
@@ -383,6 +400,9 @@ def jeans_cloud(nlev: int = 6, nbase: int = 16, ni: int = 8, seed: int = 12345,
             rmax = r.reshape(r.shape[0], -1).max(axis=1)
             jlen = cs * np.sqrt(math.pi / rmax)
             out[s:s + chunk] = jlen < jeans_const * h
+
+        with ThreadPoolExecutor(_threads()) as ex:   # elementwise per block: same decisions
+            list(ex.map(part, range(0, q.shape[0], chunk)))
         return out
 
     h = build_hierarchy((nbase,) * 3, ni, nlev, refine, True, box_lo=(0.0, 0.0, 0.0), box_size=box_size)
