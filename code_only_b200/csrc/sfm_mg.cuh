@@ -28,6 +28,13 @@ struct MgData {
 };
 
 __device__ __forceinline__ int mgN(const MgData &d, int m) { return d.N >> m; }
+// cell (i, j, k) of flat index c in an n^3 level, n a power of two (ln = log2 n):
+// shifts and masks instead of integer division
+__device__ __forceinline__ void mg_ijk(int c, int n, int ln, int &i, int &j, int &k) {
+    i = c & (n - 1);
+    j = (c >> ln) & (n - 1);
+    k = c >> (2 * ln);
+}
 __device__ __forceinline__ double mgH(const MgData &d, int m) { return d.hbase * (double)(1 << m); }
 
 __device__ double mg_block_max(double v, double *sh) {
@@ -97,12 +104,13 @@ __device__ __forceinline__ double mg_lap_sum(const double *u, int G, int i, int 
     return s;
 }
 __device__ void mg_resid(const MgData &d, int m, double *res, double *u, const double *rhs) {   // mg_poisson.F90:5-28
-    const int n = mgN(d, m), G = n + 2;
+    const int n = mgN(d, m), G = n + 2, ln = __ffs(n) - 1;
     double hh = mgH(d, m);
     double h2i = 1.0 / (hh * hh);
     mg_boundary_u(d, m, u);
     for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-        int i = c % n, j = (c / n) % n, k = c / (n * n);
+        int i, j, k;
+        mg_ijk(c, n, ln, i, j, k);
         res[cidx(G, i, j, k)] = -h2i * mg_lap_sum(u, G, i, j, k) + rhs[cidx(G, i, j, k)];
     }
     __syncthreads();
@@ -119,7 +127,8 @@ __device__ double mg_relax(const MgData &d, int m, double *u, const double *rhs,
             if (n == 1) { if (((ipass) & 1) != 0) continue; i = 0; j = 0; k = 0; }
             else {
                 int hn = n / 2;
-                i2 = c % hn; j = (c / hn) % n; k = c / (hn * n);
+                const int lhn = __ffs(hn) - 1;
+                i2 = c & (hn - 1); j = (c >> lhn) & (n - 1); k = c >> (lhn + __ffs(n) - 1);
                 i = 2 * i2 + ((j + k + ipass) & 1);
             }
             double resh2 = mg_lap_sum(u, G, i, j, k) - h2 * rhs[cidx(G, i, j, k)];
@@ -132,15 +141,16 @@ __device__ double mg_relax(const MgData &d, int m, double *u, const double *rhs,
     return mg_block_max(rm, sh) / h2;
 }
 __device__ void mg_rstrct(const MgData &d, int m, double *uc, const double *uf) {   // linear (mg.F90:581-602)
-    const int n = mgN(d, m), G = n + 2, Gf = 2 * n + 2;
+    const int n = mgN(d, m), G = n + 2, Gf = 2 * n + 2, ln = __ffs(n) - 1;
     for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-        int i = c % n, j = (c / n) % n, k = c / (n * n);
+        int i, j, k;
+        mg_ijk(c, n, ln, i, j, k);
         uc[cidx(G, i, j, k)] = rstrct_linear(uf, Gf, 2 * i, 2 * j, 2 * k);
     }
     __syncthreads();
 }
 __device__ void mg_interp(const MgData &d, int m, double *uf, double *uc, bool cubic) {   // mg.F90:608-633
-    const int lc = m + 1, n = mgN(d, m), G = n + 2, nc = mgN(d, lc), Gc = nc + 2;
+    const int lc = m + 1, n = mgN(d, m), G = n + 2, nc = mgN(d, lc), Gc = nc + 2, ln = __ffs(n) - 1;
     // Lagrange nodes and weights per fine index, evaluated once per call
     __shared__ int tcw[MG_NMAX][4];
     __shared__ double tww[MG_NMAX][4];
@@ -149,7 +159,8 @@ __device__ void mg_interp(const MgData &d, int m, double *uf, double *uc, bool c
     mg_boundary_extrap(d, lc, uc);   // ends with __syncthreads
     mg_boundary_u(d, lc, uc);
     for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-        int i = c % n, j = (c / n) % n, k = c / (n * n);
+        int i, j, k;
+        mg_ijk(c, n, ln, i, j, k);
         uf[cidx(G, i, j, k)] = tri ? tricubic_cell_w(uc, Gc, tcw[i], tww[i], tcw[j], tww[j], tcw[k], tww[k])
                                    : trilinear_cell(uc, Gc, i, j, k, 0, 0, 0);
     }
@@ -256,7 +267,9 @@ __global__ void __launch_bounds__(1024) k_mg_cycle(MgData dg, int smem_from, int
             const int n = d.N, G = n + 2;
             double v = 0.0;
             for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-                double a = fabs(d.RHO[0][cidx(G, c % n, (c / n) % n, c / (n * n))]);
+                int i, j, k;
+                mg_ijk(c, n, __ffs(n) - 1, i, j, k);
+                double a = fabs(d.RHO[0][cidx(G, i, j, k)]);
                 v = a > v ? a : v;
             }
             rhomax = mg_block_max(v, sh);

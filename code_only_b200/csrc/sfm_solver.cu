@@ -357,6 +357,17 @@ public:
                         it.oa = H.oct[3 * b + tra(dir)]; it.ob = H.oct[3 * b + trb(dir)];
                         faces.push_back(it);
                     }
+                // Items of one pass are independent (a pass writes only ghost
+                // cells of its direction and reads none), so their order is
+                // free: put the two faces of a same-level pair, and the fine
+                // faces under one coarse face, next to each other, so the
+                // 32-byte sectors they share are fetched from DRAM once.
+                auto key = [](const FaceItem &x) {
+                    const int64_t lo = std::min(x.dst, x.src), hi = std::max(x.dst, x.src);
+                    return x.type == 0 ? (lo << 32) | hi : ((int64_t)x.src << 32) | (int64_t)(1u << 31);
+                };
+                std::stable_sort(faces.begin() + faceOff[L * 3 + dir], faces.end(),
+                                 [&](const FaceItem &a, const FaceItem &c) { return key(a) < key(c); });
             }
         faceOff[nlev * 3] = (int64_t)faces.size();
         // reflux: coarse faces covered by finer blocks get a slot

@@ -432,6 +432,8 @@ def config_hierarchy(name: str):
     'uniform256' : 256^3 periodic, 32^3 blocks of 8^3, Gaussian peak: the smallest
                    uniform grid whose FP32 field with ghosts (131 MB) exceeds the
                    126 MB L2, used for kernel profiles of the 8^3-block sweeps
+    'uniform128' : 128^3 periodic, 16^3 blocks of 8^3: the smallest uniform grid
+                   with jeans6's 32^3 base grid, used to profile the base-grid CTA
     """
     if name == "uniform64":
         return uniform_periodic(8, 8), gaussian_peak, 0
@@ -439,6 +441,8 @@ def config_hierarchy(name: str):
         return nested_sphere(5, 8, 8), softened_sphere, 1
     if name == "uniform256":
         return uniform_periodic(32, 8), gaussian_peak, 0
+    if name == "uniform128":
+        return uniform_periodic(16, 8), gaussian_peak, 0
     if name == "jeans6":
         h, fn = jeans_cloud(nlev=6, nbase=16, ni=8)
         return h, fn, 0
