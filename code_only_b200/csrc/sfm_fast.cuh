@@ -19,25 +19,20 @@ namespace sfm {
 // ---------------------------------------------------------------------------
 // ghost pass: one warp per face item
 // ---------------------------------------------------------------------------
+// transverse Lagrange nodes and weights of the bicubic coarse-fine ghost for
+// p in [-1, N] (entry p + 1), built once per CTA by its first G threads
+template <int N>
+struct GhostCubicTable {
+    int c[N + 2][4];
+    double w[N + 2][4];
+};
+
+// one face item, by one warp (lane = 0..31)
 template <class T, int N>
-__global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const FaceItem *__restrict__ items, int nitems,
-                                                    int dir, int cubic, int sel) {
+__device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bool bicubic,
+                                           const GhostCubicTable<N> &tab, int lane) {
     constexpr int G = N + 2, NC = G * G, NB2 = N / 2;
     constexpr int64_t V = (int64_t)G * G * G;
-    const int lane = threadIdx.x & 31;
-    const int it = blockIdx.x * 4 + (threadIdx.x >> 5);
-    // transverse Lagrange nodes and weights of the bicubic coarse-fine ghost,
-    // for p in [-1, N] (entry p + 1): evaluated once per CTA
-    __shared__ int gwc[G][4];
-    __shared__ double gww[G][4];
-    const bool bicubic = cubic && NB2 + 2 >= 4;
-    if (bicubic) {
-        if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, gwc[threadIdx.x], gww[threadIdx.x]);
-        __syncthreads();
-    }
-    if (it >= nitems) return;
-    const FaceItem fi = items[it];
-    if (sel >= 0 && fi.type != sel) return;
     // A pass never reads a ghost cell of its own direction (sources are
     // planes interior along `dir`), so each lane issues all of its loads
     // before any of its stores: IT independent DRAM round trips in flight
@@ -85,8 +80,8 @@ __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const Fac
         const int p = c % G - 1, q = c / G - 1;
         T uH;
         if (bicubic) {
-            const int *cp = gwc[p + 1], *cq = gwc[q + 1];
-            const double *wp = gww[p + 1], *wq = gww[q + 1];
+            const int *cp = tab.c[p + 1], *cq = tab.c[q + 1];
+            const double *wp = tab.w[p + 1], *wq = tab.w[q + 1];
             T bx[4];
 #pragma unroll
             for (int m = 0; m < 4; m++)
@@ -115,6 +110,24 @@ __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const Fac
     }
 }
 
+template <class T, int N>
+__global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const FaceItem *__restrict__ items, int nitems,
+                                                    int dir, int cubic, int sel) {
+    constexpr int G = N + 2, NB2 = N / 2;
+    const int lane = threadIdx.x & 31;
+    const int it = blockIdx.x * 4 + (threadIdx.x >> 5);
+    __shared__ GhostCubicTable<N> tab;
+    const bool bicubic = cubic && NB2 + 2 >= 4;
+    if (bicubic) {
+        if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, tab.c[threadIdx.x], tab.w[threadIdx.x]);
+        __syncthreads();
+    }
+    if (it >= nitems) return;
+    const FaceItem fi = items[it];
+    if (sel >= 0 && fi.type != sel) return;
+    ghost_face<T, N>(u, fi, dir, bicubic, tab, lane);
+}
+
 // ---------------------------------------------------------------------------
 // staging of BPC consecutive listed blocks (G^3 each) into shared memory
 // ---------------------------------------------------------------------------
@@ -128,7 +141,7 @@ struct Tile {
 };
 
 template <class T, int N>
-__device__ __forceinline__ void stage_blocks(T *sh, const T *__restrict__ u, const int32_t *__restrict__ blocks,
+__device__ __forceinline__ void stage_blocks(T *sh, const T *u, const int32_t *__restrict__ blocks,
                                              int first, int nblk) {
     using Tl = Tile<N>;
     for (int t = threadIdx.x; t < Tl::BPC * Tl::V; t += blockDim.x) {
@@ -186,31 +199,38 @@ __device__ __forceinline__ void cta_max_atomic(double m, unsigned long long *out
     }
 }
 
-// persistent: each CTA walks tiles of BPC consecutive listed blocks
+// shared buffers of one CTA's tiled colour sweep
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T *__restrict__ rhs,
-                                                     const int32_t *__restrict__ blocks, int nblk,
-                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
-                                                     const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
-                                                     int f, int ipass, unsigned long long *out) {
+struct RelaxTileSmem {
+    T sh[Tile<N>::BPC * Tile<N>::V];
+    int ssl[Tile<N>::BPC][6];
+    T shh[Tile<N>::BPC], shi[Tile<N>::BPC];
+};
+
+// one colour over tiles tile0, tile0 + tstride, ... of BPC consecutive listed
+// blocks: each block with its ghost shell staged in shared memory, updated,
+// interior rows written back; |resh2| folded into m.  u and rbuf are plain
+// pointers: inside k_exec earlier phases of the same launch write them.
+template <class T, int N>
+__device__ __forceinline__ void relax_tiles(RelaxTileSmem<T, N> &sm, T *u, const T *__restrict__ rhs,
+                                            const int32_t *__restrict__ blocks, int nblk,
+                                            const double *__restrict__ h0, const int32_t *__restrict__ level,
+                                            const int32_t *__restrict__ rslot, const double *rbuf,
+                                            int f, int ipass, int tile0, int tstride, double &m) {
     using Tl = Tile<N>;
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2;
-    __shared__ T sh[BPC * V];
-    __shared__ int ssl[BPC][6];
-    __shared__ T shh[BPC], shi[BPC];
     const int ntiles = (nblk + BPC - 1) / BPC;
-    double m = 0.0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    for (int tile = tile0; tile < ntiles; tile += tstride) {
         const int first = tile * BPC;
-        stage_blocks<T, N>(sh, u, blocks, first, nblk);
+        stage_blocks<T, N>(sm.sh, u, blocks, first, nblk);
         if (threadIdx.x < BPC * 6) {
             const int q = threadIdx.x / 6, fc = threadIdx.x % 6;
-            ssl[q][fc] = (rslot && first + q < nblk) ? rslot[6 * blocks[first + q] + fc] : -1;
+            sm.ssl[q][fc] = (rslot && first + q < nblk) ? rslot[6 * blocks[first + q] + fc] : -1;
         }
         if (threadIdx.x < BPC && first + (int)threadIdx.x < nblk) {
             const double hd = hlev(h0, level[blocks[first + threadIdx.x]], f);
-            shh[threadIdx.x] = (T)hd;
-            shi[threadIdx.x] = (T)(1.0 / hd);
+            sm.shh[threadIdx.x] = (T)hd;
+            sm.shi[threadIdx.x] = (T)(1.0 / hd);
         }
         __syncthreads();
         for (int t = threadIdx.x; t < BPC * HALF; t += blockDim.x) {
@@ -220,9 +240,9 @@ __global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T 
             constexpr int HN = N / 2;
             const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
             const int i = 2 * i2 + ((j + k + ipass) & 1);
-            const T hh = shh[q], hi = shi[q];
-            T *ub = sh + q * V;
-            TileFlux<T, N> F{ub, hi, rslot ? ssl[q] : nullptr, rbuf};
+            const T hh = sm.shh[q], hi = sm.shi[q];
+            T *ub = sm.sh + q * V;
+            TileFlux<T, N> F{ub, hi, rslot ? sm.ssl[q] : nullptr, rbuf};
             const int c = (int)cidx(G, i, j, k);
             const T resh2 = (F.div(i, j, k) - rhs[(int64_t)b * V + c] * hh) * hh;
             ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
@@ -236,10 +256,22 @@ __global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T 
             if (first + q >= nblk) continue;
             const int i = r % N, j = (r / N) % N, k = r / (N * N);
             const int c = (int)cidx(G, i, j, k);
-            u[(int64_t)blocks[first + q] * V + c] = sh[q * V + c];
+            u[(int64_t)blocks[first + q] * V + c] = sm.sh[q * V + c];
         }
         __syncthreads();
     }
+}
+
+// persistent: each CTA walks tiles of BPC consecutive listed blocks
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T *__restrict__ rhs,
+                                                     const int32_t *__restrict__ blocks, int nblk,
+                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
+                                                     const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
+                                                     int f, int ipass, unsigned long long *out) {
+    __shared__ RelaxTileSmem<T, N> sm;
+    double m = 0.0;
+    relax_tiles<T, N>(sm, u, rhs, blocks, nblk, h0, level, rslot, rbuf, f, ipass, blockIdx.x, gridDim.x, m);
     cta_max_atomic(m, out);
 }
 
@@ -306,16 +338,21 @@ struct BulkPlan {
     static_assert(HI <= V && (V * (int)sizeof(T)) % 16 == 0, "span within the block, blocks 16-byte aligned");
 };
 
-// Red-black colour sweep with whole blocks of u (ghost shell included) and
-// the interior span of rhs brought in by bulk async copies, and the interior
-// span of each updated block written back by one bulk store (the ghost cells
-// inside the span go back unchanged).  Same arithmetic as k_relax_tiled.
-// Warp 0 fills the stages: with a tile's copies it also loads that tile's
-// per-block data (reflux slots, cell widths), so a sweep step waits only on
-// its stage's mbarrier.  After storing the stage of step `it` it refills the
-// stage of step it-1, whose store has had a whole step to read it.  A wait
-// that exceeds kWaitPolls sets *err, drains this CTA's copies (again
-// bounded) and returns.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Red-black colour sweep, warp-specialised.  Warp 0 produces: for each tile
+// it waits until the consumers have released a stage (mbarrier `empty`),
+// loads the tile's per-block data (block ids, reflux slots, cell widths) into
+// that stage and brings the whole u blocks (ghost shell included) and the
+// interior span of rhs with 1D bulk async copies (mbarrier `full`).  Warps
+// 1..7 consume: each warp computes its cells of one colour from the staged
+// block (the arithmetic of k_relax_tiled), stores the new values straight to
+// u and releases the stage -- so a stage can be refilled as soon as it has
+// been read, and the producer's latencies stay off the consumers' path.
+// Every mbarrier wait is bounded (kWaitPolls): a wait that gives up sets
+// *err, the warp leaves, and the producer stops issuing.
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
                                                     const int32_t *__restrict__ blocks, int nblk,
@@ -325,6 +362,7 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
     using Tl = Tile<N>;
     using Pl = BulkPlan<T, N>;
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2, S = Pl::S;
+    constexpr int NCW = 7, NCT = 32 * NCW;   // consumer warps / threads
     constexpr uint32_t BB = (uint32_t)(V * sizeof(T));
     constexpr int LO = Pl::LO;
     constexpr uint32_t SB = (uint32_t)(Pl::SPAN * sizeof(T));
@@ -332,97 +370,119 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
     extern __shared__ __align__(128) unsigned char bulk_smem[];
     T *ust = reinterpret_cast<T *>(bulk_smem);   // [S][BPC][V]
     T *rst = ust + S * BPC * V;                  // [S][BPC][V]
-    __shared__ __align__(8) uint64_t bar[S];
-    __shared__ int pend[S], ph[S], abort_flag;
-    __shared__ int ssl[S][BPC][6];
-    __shared__ T shh[S][BPC], shi[S][BPC];
-    const int tid = threadIdx.x, lane = tid & 31;
+    __shared__ __align__(8) uint64_t full[S], empty[S];
+    // pab: the producer gave up; cab: a consumer warp gave up
+    __shared__ int issued[S], consumed[S], pab, cab;
+    // per-block data of the tiles, by this CTA's step index: a ring of two
+    // windows of R steps; the producer fills a whole window at once (one
+    // latency for R tiles) S steps into the previous window, when every
+    // consumer (at most S steps behind) has left the window it overwrites
+    constexpr int R = (32 / BPC) > 2 * S ? 32 / BPC : 2 * S;
+    __shared__ int bid[2 * R][BPC];
+    __shared__ int ssl[2 * R][BPC][6];
+    __shared__ T shh[2 * R][BPC], shi[2 * R][BPC];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (nblk + BPC - 1) / BPC;
     if (tid == 0) {
-        for (int s = 0; s < S; s++) { mbar_init(&bar[s], 1); pend[s] = 0; ph[s] = 0; }
-        abort_flag = 0;
+        for (int s = 0; s < S; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NCW);
+            issued[s] = 0;
+            consumed[s] = 0;
+        }
+        pab = 0;
+        cab = 0;
         mbar_init_fence();
     }
     __syncthreads();
-    // warp 0 fills stage s with tile `tile` and its per-block data
-    auto issue = [&](int s, int tile) {
-        const int first = tile * BPC;
-        const int cnt = nblk - first < BPC ? nblk - first : BPC;
-        if (lane == 0) { pend[s] = 1; mbar_expect_tx(&bar[s], (uint32_t)cnt * (BB + SB)); }
-        __syncwarp();
-        for (int q = lane; q < BPC; q += 32) {
-            if (q >= cnt) {
-                for (int fc = 0; fc < 6; fc++) ssl[s][q][fc] = -1;
-                continue;
-            }
-            const int64_t b = blocks[first + q];
-            bulk_load(ust + (s * BPC + q) * V, u + b * V, BB, &bar[s]);
-            bulk_load(rst + (s * BPC + q) * V + LO, rhs + b * V + LO, SB, &bar[s]);
-            for (int fc = 0; fc < 6; fc++) ssl[s][q][fc] = rslot ? rslot[6 * b + fc] : -1;
-            const double hd = hlev(h0, level[b], f);
-            shh[s][q] = (T)hd;
-            shi[s][q] = (T)(1.0 / hd);
-        }
-    };
-    if (tid < 32)
-        for (int s = 0; s < S; s++) {
-            const int tile = blockIdx.x + s * (int)gridDim.x;
-            if (tile < ntiles) issue(s, tile);
-        }
     double m = 0.0;
-    int it = 0, sprev = -1, tprev = -1;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
-        const int s = it % S;
-        const int first = tile * BPC;
-        if (!mbar_wait_bounded(&bar[s], (uint32_t)(ph[s] & 1), kWaitPolls)) atomicExch(&abort_flag, 1);
-        __syncthreads();
-        if (abort_flag) break;
-        T *ut = ust + s * BPC * V;
-        const T *rt = rst + s * BPC * V;
-        for (int t = tid; t < BPC * HALF; t += blockDim.x) {
-            const int q = t / HALF, r = t - q * HALF;
-            if (first + q >= nblk) continue;
-            constexpr int HN = N / 2;
-            const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
-            const int i = 2 * i2 + ((j + k + ipass) & 1);
-            const T hh = shh[s][q], hi = shi[s][q];
-            T *ub = ut + q * V;
-            TileFlux<T, N> F{ub, hi, rslot ? ssl[s][q] : nullptr, rbuf};
-            const int c = (int)cidx(G, i, j, k);
-            const T resh2 = (F.div(i, j, k) - rt[q * V + c] * hh) * hh;
-            ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
-            const double a = fabs((double)resh2);
-            m = a > m ? a : m;
+    const int nsteps = ntiles > (int)blockIdx.x ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    auto fill_window = [&](int w) {   // warp 0
+        for (int e = lane; e < R * BPC; e += 32) {
+            const int step = w * R + e / BPC, q = e % BPC, slot = step % (2 * R);
+            const int first = ((int)blockIdx.x + step * (int)gridDim.x) * BPC;
+            if (step < nsteps && first + q < nblk) {
+                const int b = blocks[first + q];
+                bid[slot][q] = b;
+                for (int fc = 0; fc < 6; fc++) ssl[slot][q][fc] = rslot ? rslot[6 * b + fc] : -1;
+                const double hd = hlev(h0, level[b], f);
+                shh[slot][q] = (T)hd;
+                shi[slot][q] = (T)(1.0 / hd);
+            } else {
+                for (int fc = 0; fc < 6; fc++) ssl[slot][q][fc] = -1;
+            }
         }
-        fence_async_shared();
-        __syncthreads();
-        if (tid < 32) {
+        __syncwarp();
+    };
+    if (warp == 0) {
+        fill_window(0);
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+            const int s = it % S;
+            if (it >= S && !mbar_wait_bounded(&empty[s], (uint32_t)((it / S - 1) & 1), kWaitPolls)) {
+                if (lane == 0) pab = 1;
+                break;
+            }
+            if (*(volatile int *)&cab) break;
+            if (it % R == S && (it / R + 1) * R < nsteps) fill_window(it / R + 1);
+            const int first = tile * BPC;
             const int cnt = nblk - first < BPC ? nblk - first : BPC;
+            const int slot = it % (2 * R);
             if (lane == 0) {
-                ph[s]++;
-                pend[s] = 0;
-                for (int q = 0; q < cnt; q++)
-                    bulk_store(u + (int64_t)blocks[first + q] * V + LO, ut + q * V + LO, SB);
-                bulk_commit();
+                issued[s]++;
+                mbar_expect_tx(&full[s], (uint32_t)cnt * (BB + SB));   // releases the per-block data
             }
-            // refill the previous step's stage; its store group is the older one
-            const int nt = tprev >= 0 ? tprev + S * (int)gridDim.x : ntiles;
-            if (nt < ntiles) {
-                if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-                __syncwarp();
-                issue(sprev, nt);
+            __syncwarp();
+            for (int q = lane; q < cnt; q += 32) {
+                const int64_t b = bid[slot][q];
+                bulk_load(ust + (s * BPC + q) * V, u + b * V, BB, &full[s]);
+                bulk_load(rst + (s * BPC + q) * V + LO, rhs + b * V + LO, SB, &full[s]);
             }
         }
-        sprev = s;
-        tprev = tile;
+    } else {
+        // Cells of one colour depend only on cells of the other colour, so
+        // each consumer thread stores its updated cells straight to u and no
+        // consumer waits for another: a warp waits for the stage, updates,
+        // stores and releases the stage on its own.
+        const int ct = tid - 32;   // consumer thread 0..NCT-1
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+            const int s = it % S;
+            if (!mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), kWaitPolls)) {
+                atomicExch(&cab, 1);
+                break;
+            }
+            const int first = tile * BPC;
+            const int slot = it % (2 * R);
+            const T *ut = ust + s * BPC * V;
+            const T *rt = rst + s * BPC * V;
+            for (int t = ct; t < BPC * HALF; t += NCT) {
+                const int q = t / HALF, r = t - q * HALF;
+                if (first + q >= nblk) continue;
+                constexpr int HN = N / 2;
+                const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
+                const int i = 2 * i2 + ((j + k + ipass) & 1);
+                const T hh = shh[slot][q], hi = shi[slot][q];
+                const T *ub = ut + q * V;
+                TileFlux<T, N> F{ub, hi, rslot ? ssl[slot][q] : nullptr, rbuf};
+                const int c = (int)cidx(G, i, j, k);
+                const T resh2 = (F.div(i, j, k) - rt[q * V + c] * hh) * hh;
+                u[(int64_t)bid[slot][q] * V + c] = ub[c] + (T)(1.0 / 6.0) * resh2;
+                const double a = fabs((double)resh2);
+                m = a > m ? a : m;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                if (warp == 1) consumed[s]++;
+                mbar_arrive(&empty[s]);   // this warp is done with stage s
+            }
+        }
     }
-    if (tid == 0) {
-        if (abort_flag) {   // drain this CTA's loads in flight, bounded, then report
-            for (int s = 0; s < S; s++)
-                if (pend[s]) mbar_wait_bounded(&bar[s], (uint32_t)(ph[s] & 1), kWaitPolls);
-            atomicExch(err, 1);
-        }
-        bulk_wait_all();
+    __syncthreads();
+    if (tid == 0 && (pab || cab)) {   // loads still in flight: wait for them (bounded), then report
+        for (int s = 0; s < S; s++)
+            for (int ph = consumed[s]; ph < issued[s]; ph++) mbar_wait_bounded(&full[s], (uint32_t)(ph & 1), kWaitPolls);
+        atomicExch(err, 1);
     }
     cta_max_atomic(m, out);
 }
