@@ -321,7 +321,8 @@ __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy
 
 constexpr uint32_t kWaitPolls = 1u << 20;   // bound on every mbarrier wait of a sweep
 
-// stages of the bulk pipeline: up to 4, within 48 KB of u + rhs tiles.
+// stages of the bulk pipeline: up to 3 within 48 KB of u + rhs tiles (3
+// stages keep 8 CTAs per SM; deeper rings measured slower: 4 -> 11%, 6 -> 36%).
 // [LO, LO + SPAN) is the 16-byte-aligned element range of a block that
 // holds every interior cell (cidx of (0,0,0) to (N-1,N-1,N-1)).
 template <class T, int N>
@@ -329,7 +330,7 @@ struct BulkPlan {
     static constexpr int G = N + 2, V = G * G * G;
     static constexpr int STAGE_BYTES = 2 * Tile<N>::BPC * V * (int)sizeof(T);
     static constexpr int S0 = 49152 / STAGE_BYTES;
-    static constexpr int S = S0 >= 4 ? 4 : (S0 >= 2 ? S0 : 2);
+    static constexpr int S = S0 >= 3 ? 3 : (S0 >= 2 ? S0 : 2);
     static constexpr int SMEM = S * STAGE_BYTES;
     static constexpr int EPB = 16 / (int)sizeof(T);
     static constexpr int LO = (1 + G + G * G) / EPB * EPB;

@@ -56,7 +56,7 @@ constexpr int Undef = -1;
 // ---------------------------------------------------------------------------
 struct HostHier {
     int nb = 0, nlev = 0, NI = 0, FMax = 0, ngb[3] = {0, 0, 0};
-    std::vector<int> lstart, level, parent, child, nbr, nbrGid, baseIdx;
+    std::vector<int> lstart, level, parent, child, nbr, nbrGid, baseIdx, ijk;
     std::vector<int8_t> oct, touch, sameLev, parLev, skip;
     std::vector<double> h0, x0;
 
@@ -72,6 +72,7 @@ struct HostHier {
         parent.assign(hd->parent, hd->parent + nb);
         child.assign(hd->child, hd->child + 8 * (size_t)nb);
         nbr.assign(hd->nbr, hd->nbr + 6 * (size_t)nb);
+        ijk.assign(hd->ijk, hd->ijk + 3 * (size_t)nb);
         touch.resize(6 * (size_t)nb);
         for (size_t i = 0; i < touch.size(); i++) touch[i] = hd->touch[i] ? 1 : 0;
         h0.assign(hd->cellwidth, hd->cellwidth + nlev);
@@ -360,12 +361,17 @@ public:
                     }
                 // Items of one pass are independent (a pass writes only ghost
                 // cells of its direction and reads none), so their order is
-                // free: put the two faces of a same-level pair, and the fine
-                // faces under one coarse face, next to each other, so the
-                // 32-byte sectors they share are fetched from DRAM once.
-                auto key = [](const FaceItem &x) {
-                    const int64_t lo = std::min(x.dst, x.src), hi = std::max(x.dst, x.src);
-                    return x.type == 0 ? (lo << 32) | hi : ((int64_t)x.src << 32) | (int64_t)(1u << 31);
+                // free.  A block's row-boundary sectors hold its ghosts and its
+                // boundary planes on both sides, touched by the two faces it
+                // shares with each neighbour: same-level pairs are ordered
+                // along each line of blocks in the pass direction, so
+                // consecutive pairs meet those sectors while they are in L2;
+                // the fine faces under one coarse face follow each other.
+                auto key = [&](const FaceItem &x) -> int64_t {
+                    if (x.type != 0) return ((int64_t)1 << 62) | ((int64_t)x.src << 8);
+                    const int lo = H.ijk[3 * x.dst + dir] <= H.ijk[3 * x.src + dir] ? x.dst : x.src;
+                    const int64_t ta = H.ijk[3 * lo + tra(dir)], tb = H.ijk[3 * lo + trb(dir)];
+                    return (ta << 42) | (tb << 21) | (int64_t)H.ijk[3 * lo + dir];
                 };
                 std::stable_sort(faces.begin() + faceOff[L * 3 + dir], faces.end(),
                                  [&](const FaceItem &a, const FaceItem &c) { return key(a) < key(c); });
