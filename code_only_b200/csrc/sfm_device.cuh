@@ -93,6 +93,19 @@ __global__ void k_apply(Op op, int64_t n) {
         op(i);
 }
 
+// element-wise op over whole listed blocks (functors with blocks, V and
+// cell(c)): CTAs step over groups of bpc blocks, threads over their cells --
+// no 64-bit division per element
+template <class Op>
+__global__ void __launch_bounds__(256) k_blocks(Op op, int nblk, int bpc) {
+    const int V = (int)op.V;
+    for (int b0 = blockIdx.x * bpc; b0 < nblk; b0 += gridDim.x * bpc)
+        for (int e = threadIdx.x; e < bpc * V; e += blockDim.x) {
+            const int q = e / V, c = e - q * V;
+            if (b0 + q < nblk) op.cell((int64_t)op.blocks[b0 + q] * V + c);
+        }
+}
+
 // max over items of op(i) >= 0, folded into *out by atomicMax on the IEEE
 // bit pattern (order-preserving for non-negative doubles)
 template <class Op>
@@ -308,9 +321,10 @@ template <class T>
 struct OpFill0Faces {      // zero the listed ghost planes (whole transverse range)
     T *u; const BFace *faces; int n, G; int64_t V;
     __device__ void operator()(int64_t idx) const {
-        const int GT = n + 2;
-        int64_t it = idx / (GT * GT);
-        int r = (int)(idx - it * GT * GT);
+        // boundary faces x (n+2)^2 elements: far below 2^32
+        const uint32_t GT = (uint32_t)n + 2, ui = (uint32_t)idx;
+        const uint32_t it = ui / (GT * GT);
+        int r = (int)(ui - it * GT * GT);
         BFace bf = faces[it];
         int dir = bf.face >> 1, lr = bf.face & 1, i, j, k;
         put3(dir, lr == 0 ? -1 : n, r % GT - 1, r / GT - 1, i, j, k);
@@ -321,9 +335,10 @@ template <class T>
 struct OpExtrapFaces {     // u_ghost = -u_inner for the listed faces of one direction
     T *u; const BFace *faces; int n, G; int64_t V;
     __device__ void operator()(int64_t idx) const {
-        const int GT = n + 2;
-        int64_t it = idx / (GT * GT);
-        int r = (int)(idx - it * GT * GT);
+        // boundary faces x (n+2)^2 elements: far below 2^32
+        const uint32_t GT = (uint32_t)n + 2, ui = (uint32_t)idx;
+        const uint32_t it = ui / (GT * GT);
+        int r = (int)(ui - it * GT * GT);
         BFace bf = faces[it];
         int dir = bf.face >> 1, lr = bf.face & 1, i, j, k, ii, jj, kk;
         put3(dir, lr == 0 ? -1 : n, r % GT - 1, r / GT - 1, i, j, k);
@@ -374,9 +389,10 @@ template <class T>
 struct OpReflux {
     const T *u; const RefluxItem *items; double *rbuf; const double *h0; const int32_t *level; int f, n, G; int64_t V;
     __device__ void operator()(int64_t idx) const {
-        const int h = n / 2, per = h * h;
-        RefluxItem it = items[idx / per];
-        int r = (int)(idx % per);
+        // items x (n/2)^2 elements: far below 2^32 (6 faces per block, n <= 16)
+        const uint32_t h = (uint32_t)n / 2, per = h * h, ui = (uint32_t)idx;
+        RefluxItem it = items[ui / per];
+        int r = (int)(ui % per);
         int pc = r % h, qc = r / h;
         const T *ub = u + (int64_t)it.fine * V;
         double hd = hlev(h0, level[it.fine], f);
@@ -456,31 +472,26 @@ struct OpH2Abs {
 template <class TO, class TI>
 struct OpCopy {
     TO *o; const TI *a; const int32_t *blocks; int64_t V;
-    __device__ void operator()(int64_t idx) const {
-        int64_t c = (int64_t)blocks[idx / V] * V + idx % V;
-        o[c] = (TO)a[c];
-    }
+    __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
+    __device__ void cell(int64_t c) const { o[c] = (TO)a[c]; }
 };
 template <class TA, class TD>
 struct OpAdd {
     TA *a; const TD *d; const int32_t *blocks; int64_t V;
-    __device__ void operator()(int64_t idx) const {
-        int64_t c = (int64_t)blocks[idx / V] * V + idx % V;
-        a[c] = a[c] + (TA)d[c];
-    }
+    __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
+    __device__ void cell(int64_t c) const { a[c] = a[c] + (TA)d[c]; }
 };
 template <class T>
 struct OpSub {
     T *o; const T *a; const T *b_; const int32_t *blocks; int64_t V;
-    __device__ void operator()(int64_t idx) const {
-        int64_t c = (int64_t)blocks[idx / V] * V + idx % V;
-        o[c] = a[c] - b_[c];
-    }
+    __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
+    __device__ void cell(int64_t c) const { o[c] = a[c] - b_[c]; }
 };
 template <class T>
 struct OpZero {
     T *o; const int32_t *blocks; int64_t V;
-    __device__ void operator()(int64_t idx) const { o[(int64_t)blocks[idx / V] * V + idx % V] = (T)0; }
+    __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
+    __device__ void cell(int64_t c) const { o[c] = (T)0; }
 };
 
 }  // namespace sfm

@@ -678,7 +678,7 @@ public:
                 cudaGetLastError();
                 per = 1;
             }
-            execGrid[li] = nSM * std::min(per, 2);
+            execGrid[li] = nSM * std::min(per, 2);   // more CTAs measured slower: barrier cost
         }
         return execGrid[li];
     }
@@ -706,7 +706,7 @@ public:
         a.rslot = rslot; a.f = f; a.out = out; a.err = d_err; a.gb = d_gb; a.nphase = 0;
         return a;
     }
-    // A cooperative launch holds ~2 CTAs per SM, so a phase walks its items
+    // A cooperative launch holds only its co-resident CTAs, so a phase walks its items
     // with far fewer warps than a launch of its own would: worth it only
     // while every phase is small enough to be latency-bound.
     static constexpr int64_t kExecMaxItems = 8192;
@@ -809,13 +809,22 @@ public:
         int nc = nf[f];
         run(OpRstrct<T, T>{uc, uf, d_leaves, nc, Gf[f], Gf[f - 1], Vf[f], Vf[f - 1]}, (int64_t)nLeaves * nc * nc * nc);
     }
-    void fill0(int f, T *u) { run(OpZero<T>{u, d_leaves, Vf[f]}, (int64_t)nLeaves * Vf[f]); }
+    // element-wise over nblk whole listed blocks (k_blocks)
+    template <class Op>
+    void runB(const Op &op, int64_t nblk) {
+        if (nblk <= 0) return;
+        const int bpc = std::max(1, 256 / (int)op.V);
+        const int64_t g = std::min<int64_t>((nblk + bpc - 1) / bpc, (int64_t)nSM * 16);
+        k_blocks<Op><<<(unsigned)g, 256, 0, st_>>>(op, (int)nblk, bpc);
+        ++launches;
+    }
+    void fill0(int f, T *u) { runB(OpZero<T>{u, d_leaves, Vf[f]}, nLeaves); }
     template <class TO, class TI>
     void copy(int f, TO *o, const TI *a, bool noskip) {
-        run(OpCopy<TO, TI>{o, a, noskip ? d_all : d_leaves, Vf[f]}, (int64_t)(noskip ? H.nb : nLeaves) * Vf[f]);
+        runB(OpCopy<TO, TI>{o, a, noskip ? d_all : d_leaves, Vf[f]}, noskip ? H.nb : nLeaves);
     }
     template <class TA, class TD>
-    void add(int f, TA *a, const TD *d) { run(OpAdd<TA, TD>{a, d, d_leaves, Vf[f]}, (int64_t)nLeaves * Vf[f]); }
+    void add(int f, TA *a, const TD *d) { runB(OpAdd<TA, TD>{a, d, d_leaves, Vf[f]}, nLeaves); }
 
     // fmg_interp (fmg.F90:786-822)
     void fmg_interp(int f, T *uf, T *uc, bool cubic) {
@@ -900,7 +909,7 @@ public:
     }
     void vmg_copy_level(int L, T *o, const T *a) {
         const int F = H.FMax;
-        run(OpCopy<T, T>{o, a, d_all + H.lstart[L], Vf[F]}, (int64_t)cnt(L) * Vf[F]);
+        runB(OpCopy<T, T>{o, a, d_all + H.lstart[L], Vf[F]}, cnt(L));
     }
     void vmg_tau(int L) {   // vmg_poisson_tau + vmg_tau_crop, tau in RES
         const int F = H.FMax, n = nf[F];
@@ -962,14 +971,14 @@ public:
             vmg_rstrct(v - 1, RHS[F], false);
             vmg_tau(v - 1);
             int64_t wc = wcOff[v] - wcOff[v - 1];
-            run(OpAdd<T, T>{RHS[F], RES[F], d_withChild + wcOff[v - 1], Vf[F]}, wc * Vf[F]);
+            runB(OpAdd<T, T>{RHS[F], RES[F], d_withChild + wcOff[v - 1], Vf[F]}, wc);
         }
         if (P.zero_mean) vmg_zeroAverage(RHS[F]);
         vmg_slvsml(U[F], RHS[F]);
         for (int v = 1; v <= nlev - 1; v++) {
-            run(OpSub<T>{RES[F], U[F], RUF, d_all + H.lstart[v - 1], Vf[F]}, (int64_t)cnt(v - 1) * Vf[F]);
+            runB(OpSub<T>{RES[F], U[F], RUF, d_all + H.lstart[v - 1], Vf[F]}, cnt(v - 1));
             vmg_interp(v, RES[F], RES[F]);
-            run(OpAdd<T, T>{U[F], RES[F], d_all + H.lstart[v], Vf[F]}, (int64_t)cnt(v) * Vf[F]);
+            runB(OpAdd<T, T>{U[F], RES[F], d_all + H.lstart[v], Vf[F]}, cnt(v));
             vmg_gridboundary(v, U[F]);
             for (int q = 0; q < 2; q++) vmg_relax(v, U[F], RHS[F]);
         }
