@@ -108,9 +108,10 @@ __global__ void __launch_bounds__(256) k_exec(const __grid_constant__ ExecArgs<T
     if (kBicubicOk && threadIdx.x < G)
         cubic_weights((int)threadIdx.x - 1, -1, NB2, tab.c[threadIdx.x], tab.w[threadIdx.x]);
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    constexpr int LN = ghost_lanes<N>();   // lanes per face item
+    const int lane = threadIdx.x % LN;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) / LN);
+    const int nwarps = (int)((gridDim.x * blockDim.x) / LN);
     double m = 0.0;
     for (int p = 0; p < a.nphase; p++) {
         const ExecPhase ph = a.ph[p];

@@ -27,17 +27,22 @@ struct GhostCubicTable {
     double w[N + 2][4];
 };
 
-// one face item, by one warp (lane = 0..31)
+// lanes serving one face: a 2^3 block's face has 16 ghost cells, so a warp
+// serves two of them
+template <int N>
+__host__ __device__ constexpr int ghost_lanes() { return (N + 2) * (N + 2) <= 16 ? 16 : 32; }
+
+// one face item, by ghost_lanes<N>() lanes (lane = 0..ghost_lanes-1)
 template <class T, int N>
 __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bool bicubic,
                                            const GhostCubicTable<N> &tab, int lane) {
-    constexpr int G = N + 2, NC = G * G, NB2 = N / 2;
+    constexpr int G = N + 2, NC = G * G, NB2 = N / 2, LN = ghost_lanes<N>();
     constexpr int64_t V = (int64_t)G * G * G;
     // A pass never reads a ghost cell of its own direction (sources are
     // planes interior along `dir`), so each lane issues all of its loads
     // before any of its stores: IT independent DRAM round trips in flight
     // instead of IT dependent ones.
-    constexpr int IT = (NC + 31) / 32;
+    constexpr int IT = (NC + LN - 1) / LN;
     T *ud = u + (int64_t)fi.dst * V;
     const int xg = fi.lr == 0 ? -1 : N;
     T val[IT];
@@ -46,7 +51,7 @@ __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bo
         const int xs = fi.lr == 0 ? N - 1 : 0;
 #pragma unroll
         for (int t = 0; t < IT; t++) {
-            const int c = lane + 32 * t;
+            const int c = lane + LN * t;
             if (c >= NC) break;
             const int p = c % G - 1, q = c / G - 1;
             int is, js, ks;
@@ -55,7 +60,7 @@ __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bo
         }
 #pragma unroll
         for (int t = 0; t < IT; t++) {
-            const int c = lane + 32 * t;
+            const int c = lane + LN * t;
             if (c >= NC) break;
             const int p = c % G - 1, q = c / G - 1;
             int i, j, k;
@@ -75,7 +80,7 @@ __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bo
     };
 #pragma unroll
     for (int t = 0; t < IT; t++) {
-        const int c = lane + 32 * t;
+        const int c = lane + LN * t;
         if (c >= NC) break;
         const int p = c % G - 1, q = c / G - 1;
         T uH;
@@ -101,7 +106,7 @@ __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bo
     }
 #pragma unroll
     for (int t = 0; t < IT; t++) {
-        const int c = lane + 32 * t;
+        const int c = lane + LN * t;
         if (c >= NC) break;
         const int p = c % G - 1, q = c / G - 1;
         int i, j, k;
@@ -113,9 +118,9 @@ __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bo
 template <class T, int N>
 __global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const FaceItem *__restrict__ items, int nitems,
                                                     int dir, int cubic, int sel) {
-    constexpr int G = N + 2, NB2 = N / 2;
-    const int lane = threadIdx.x & 31;
-    const int it = blockIdx.x * 4 + (threadIdx.x >> 5);
+    constexpr int G = N + 2, NB2 = N / 2, LN = ghost_lanes<N>();
+    const int lane = threadIdx.x % LN;
+    const int it = blockIdx.x * (128 / LN) + (int)threadIdx.x / LN;
     __shared__ GhostCubicTable<N> tab;
     const bool bicubic = cubic && NB2 + 2 >= 4;
     if (bicubic) {

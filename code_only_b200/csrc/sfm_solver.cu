@@ -545,7 +545,7 @@ public:
         if (c <= 0) return;
         int GT = nf[f] + 2;
         SFM_WITH_N(nf[f],
-                   (k_ghost_pass<TT, N><<<(unsigned)((c + 3) / 4), 128, 0, st_>>>(u, d_faces + o, (int)c, dir,
+                   (k_ghost_pass<TT, N><<<(unsigned)((c + 128 / ghost_lanes<N>() - 1) / (128 / ghost_lanes<N>())), 128, 0, st_>>>(u, d_faces + o, (int)c, dir,
                                                                                  cubic ? 1 : 0, sel),
                     ++launches),
                    run(OpGhostPass<TT>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, sel}, c * GT * GT))
