@@ -67,6 +67,7 @@ struct ExecPhase {
     int32_t first, count;           // converge: first child block, children; ghost: face items;
                                     // fill0: boundary faces; reflux: reflux items
     int32_t ipass;                  // relax colour
+    int32_t count0;                 // ghost: the first count0 items are same-level copies
 };
 
 template <class T>
@@ -120,13 +121,17 @@ __global__ void __launch_bounds__(256) k_exec(const __grid_constant__ ExecArgs<T
                 exec_elements(OpConverge<T>{a.u, a.parent, a.oct, ph.first, N, G, V, ph.cubic},
                               (int64_t)ph.count * NB2 * NB2 * NB2);
                 break;
-            case PH_GHOST:
-                for (int it = warp; it < ph.count; it += nwarps) {
-                    const FaceItem fi = a.faces[ph.first + it];
-                    if (ph.sel >= 0 && fi.type != ph.sel) continue;
-                    ghost_face<T, N>(a.u, fi, ph.dir, ph.cubic && kBicubicOk, tab, lane);
-                }
+            case PH_GHOST: {
+                // cells spread over the whole grid: a phase is small
+                const int nc0 = ph.count0 * G * G, nthr = (int)(gridDim.x * blockDim.x);
+                const int gt = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+                for (int b0 = 0; b0 < nc0; b0 += nthr * kGhostK)
+                    ghost_copy<T, N>(a.u, a.faces + ph.first, nc0, ph.dir, b0 + gt, nthr);
+                const FaceItem *f1 = a.faces + ph.first + ph.count0;
+                for (int it = warp; it < ph.count - ph.count0; it += nwarps)
+                    ghost_face<T, N>(a.u, f1[it], ph.dir, ph.cubic && kBicubicOk, tab, lane);
                 break;
+            }
             case PH_FILL0:
                 exec_elements(OpFill0Faces<T>{a.u, a.bfaces + ph.first, N, G, V}, (int64_t)ph.count * GT * GT);
                 break;

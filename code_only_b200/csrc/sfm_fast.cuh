@@ -115,22 +115,74 @@ __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bo
     }
 }
 
+// Same-level faces (type 0, fmg_ghfix_samelev) as a flat copy: cell g of a
+// list of type-0 items is ghost cell g % NC of face g / NC, at in-block
+// offset (x+1) sd + (p+1) sa + (q+1) sb with the pass direction's strides.
+// A thread serves K cells `stride` apart and issues its K item loads, then
+// its K value loads, then its K stores: the gather is latency-bound, and
+// HBM only fills with several round trips in flight per thread (K = 4
+// measured faster than 8, and than fewer cells per thread on small passes;
+// K is a compile-time constant -- a run-time count measured slower).
+constexpr int kGhostK = 4;
 template <class T, int N>
-__global__ void __launch_bounds__(128) k_ghost_pass(T *__restrict__ u, const FaceItem *__restrict__ items, int nitems,
-                                                    int dir, int cubic, int sel) {
+__device__ __forceinline__ void ghost_copy(T *u, const FaceItem *items, int ncell, int dir, int g0, int stride) {
+    constexpr int G = N + 2, NC = G * G, K = kGhostK;
+    constexpr int64_t V = (int64_t)G * G * G;
+    const int sd = dir == 0 ? 1 : (dir == 1 ? G : G * G);
+    const int sa = dir == 0 ? G : 1;
+    const int sb = dir == 2 ? G : G * G;
+    int64_t src[K], dst[K];
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+        const int g = g0 + t * stride;
+        src[t] = -1;
+        dst[t] = 0;
+        if (g < ncell) {
+            const int fidx = g / NC, c = g - fidx * NC;
+            const FaceItem fi = items[fidx];
+            const int base = (c % G) * sa + (c / G) * sb;
+            const bool lo = fi.lr == 0;   // ghost plane x = -1 fed by the source's x = N-1, or N by 0
+            dst[t] = (int64_t)fi.dst * V + base + (lo ? 0 : N + 1) * sd;
+            src[t] = (int64_t)fi.src * V + base + (lo ? N : 1) * sd;
+        }
+    }
+    T val[K];
+#pragma unroll
+    for (int t = 0; t < K; t++)
+        if (src[t] >= 0) val[t] = u[src[t]];
+#pragma unroll
+    for (int t = 0; t < K; t++)
+        if (src[t] >= 0) u[dst[t]] = val[t];
+}
+
+// One ghost pass of (level, direction): the n0 same-level items0 by flat
+// copy in the first CTAs, the n1 coarse-fine items1
+// (fmg_ghfix_parentlev) by ghost_face in the rest.  The two sets write
+// disjoint ghost cells and read none of the pass direction, so they run
+// side by side.
+template <int N>
+__host__ __device__ constexpr int ghost_copy_ctas(int n0) {
+    return (int)(((int64_t)n0 * (N + 2) * (N + 2) + 256 * kGhostK - 1) / (256 * kGhostK));
+}
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_ghost_faces(T *u, const FaceItem *__restrict__ items0, int n0,
+                                                     const FaceItem *__restrict__ items1, int n1, int dir,
+                                                     int cubic) {
     constexpr int G = N + 2, NB2 = N / 2, LN = ghost_lanes<N>();
-    const int lane = threadIdx.x % LN;
-    const int it = blockIdx.x * (128 / LN) + (int)threadIdx.x / LN;
+    const int nb0 = ghost_copy_ctas<N>(n0);
+    if ((int)blockIdx.x < nb0) {
+        ghost_copy<T, N>(u, items0, n0 * G * G, dir, (int)blockIdx.x * 256 * kGhostK + (int)threadIdx.x, 256);
+        return;
+    }
     __shared__ GhostCubicTable<N> tab;
     const bool bicubic = cubic && NB2 + 2 >= 4;
     if (bicubic) {
         if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, tab.c[threadIdx.x], tab.w[threadIdx.x]);
         __syncthreads();
     }
-    if (it >= nitems) return;
-    const FaceItem fi = items[it];
-    if (sel >= 0 && fi.type != sel) return;
-    ghost_face<T, N>(u, fi, dir, bicubic, tab, lane);
+    const int it = ((int)blockIdx.x - nb0) * (256 / LN) + (int)threadIdx.x / LN;
+    if (it >= n1) return;
+    ghost_face<T, N>(u, items1[it], dir, bicubic, tab, threadIdx.x % LN);
 }
 
 // ---------------------------------------------------------------------------

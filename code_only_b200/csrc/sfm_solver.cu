@@ -228,7 +228,7 @@ public:
     FaceItem *d_faces = nullptr;
     RefluxItem *d_reflux = nullptr;
     BFace *d_tfL = nullptr, *d_tfDL = nullptr, *d_crop = nullptr;
-    std::vector<int64_t> faceOff, tfLOff, tfDLOff, cropOff, wcOff;
+    std::vector<int64_t> faceOff, faceSplit, tfLOff, tfDLOff, cropOff, wcOff;
     int nLeaves = 0, nReflux = 0, nSlots = 0;
     std::vector<int> leafList;
 
@@ -377,6 +377,14 @@ public:
                                  [&](const FaceItem &a, const FaceItem &c) { return key(a) < key(c); });
             }
         faceOff[nlev * 3] = (int64_t)faces.size();
+        // each list holds its same-level items first (key bit 62 marks
+        // coarse-fine ones): faceSplit is where the coarse-fine ones start
+        faceSplit.assign(nlev * 3, 0);
+        for (int k = 0; k < nlev * 3; k++) {
+            int64_t i = faceOff[k];
+            while (i < faceOff[k + 1] && faces[i].type == 0) i++;
+            faceSplit[k] = i;
+        }
         // reflux: coarse faces covered by finer blocks get a slot
         std::vector<int32_t> rslot(6 * (size_t)nb, -1);
         std::vector<RefluxItem> refl;
@@ -541,14 +549,23 @@ public:
     }
     template <class TT>
     void ghost_pass(int L, int f, int dir, TT *u, bool cubic, int sel = -1) {   // parentlev/samelev of (L, dir)
-        int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
-        if (c <= 0) return;
+        const int k = L * 3 + dir;
+        const int64_t o = faceOff[k], sp = faceSplit[k], c = faceOff[k + 1] - o;
+        const int64_t n0 = sel != 1 ? sp - o : 0, n1 = sel != 0 ? faceOff[k + 1] - sp : 0;
+        if (n0 + n1 <= 0) return;
         int GT = nf[f] + 2;
-        SFM_WITH_N(nf[f],
-                   (k_ghost_pass<TT, N><<<(unsigned)((c + 128 / ghost_lanes<N>() - 1) / (128 / ghost_lanes<N>())), 128, 0, st_>>>(u, d_faces + o, (int)c, dir,
-                                                                                 cubic ? 1 : 0, sel),
-                    ++launches),
-                   run(OpGhostPass<TT>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, sel}, c * GT * GT))
+        const int n = nf[f];
+        if ((n == 2 || n == 4 || n == 8 || n == 16) && n0 * GT * GT <= INT32_MAX) {
+            SFM_WITH_N(n,
+                       (k_ghost_faces<TT, N><<<(unsigned)(ghost_copy_ctas<N>((int)n0) +
+                                                          (n1 + 256 / ghost_lanes<N>() - 1) / (256 / ghost_lanes<N>())),
+                                               256, 0, st_>>>(u, d_faces + o, (int)n0, d_faces + sp, (int)n1, dir,
+                                                              cubic ? 1 : 0),
+                        ++launches),
+                       (void)0)
+            return;
+        }
+        run(OpGhostPass<TT>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, sel}, c * GT * GT);
     }
     template <class TT>
     void converge_c2p_lev(int Lc, int f, TT *u, bool cubic) {
@@ -710,12 +727,22 @@ public:
     // with far fewer warps than a launch of its own would: worth it only
     // while every phase is small enough to be latency-bound.
     static constexpr int64_t kExecMaxItems = 8192;
-    static bool exec_add(ExecArgs<T> &a, int8_t kind, int dir, int sel, int cubic, int64_t first, int64_t count,
-                         int ipass = 0) {
-        if (a.nphase >= kMaxPhases || count > kExecMaxItems) return false;
+    int64_t execMaxItems = kExecMaxItems;
+    bool exec_add(ExecArgs<T> &a, int8_t kind, int dir, int sel, int cubic, int64_t first, int64_t count,
+                  int ipass = 0) {
+        if (a.nphase >= kMaxPhases || count > execMaxItems) return false;
         ExecPhase &p = a.ph[a.nphase++];
         p.kind = kind; p.dir = (int8_t)dir; p.sel = (int8_t)sel; p.cubic = (int8_t)cubic;
-        p.first = (int32_t)first; p.count = (int32_t)count; p.ipass = ipass;
+        p.first = (int32_t)first; p.count = (int32_t)count; p.ipass = ipass; p.count0 = 0;
+        return true;
+    }
+    // ghost pass of (L, dir): same-level items, then coarse-fine ones unless same_only
+    bool exec_ghost(ExecArgs<T> &a, int L, int dir, bool same_only) {
+        const int k = L * 3 + dir;
+        const int64_t o = faceOff[k], n0 = faceSplit[k] - o, c = same_only ? n0 : faceOff[k + 1] - o;
+        if (!c) return true;
+        if (!exec_add(a, PH_GHOST, dir, -1, 0, o, c)) return false;
+        a.ph[a.nphase - 1].count0 = (int32_t)n0;
         return true;
     }
     // fmg_poisson_relax on level f (blocks of 2^3 or 4^3): the phases of
@@ -733,10 +760,7 @@ public:
                 for (int Lc = H.nlev - 2; Lc >= 0; Lc--)
                     if (cnt(Lc + 1)) ok = ok && exec_add(a, PH_CONVERGE, 0, -1, 0, H.lstart[Lc + 1], cnt(Lc + 1));
                 for (int L = 0; L < H.nlev; L++)
-                    for (int dir = 0; dir < 3; dir++) {
-                        const int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
-                        if (c) ok = ok && exec_add(a, PH_GHOST, dir, -1, 0, o, c);
-                    }
+                    for (int dir = 0; dir < 3; dir++) ok = ok && exec_ghost(a, L, dir, false);
                 if (bf0 && tfLOff[H.nlev] > 0) ok = ok && exec_add(a, PH_FILL0, 0, -1, 0, 0, tfLOff[H.nlev]);
             }
             fill0 = Undef;
@@ -757,10 +781,7 @@ public:
         ExecArgs<T> a = exec_args(u, rhs, F, d_all + H.lstart[L], cnt(L), nullptr, d_max + 1);
         bool ok = true;
         for (int ipass = 1; ipass <= 2; ipass++) {
-            for (int dir = 0; dir < 3; dir++) {
-                const int64_t o = faceOff[L * 3 + dir], c = faceOff[L * 3 + dir + 1] - o;
-                if (c) ok = ok && exec_add(a, PH_GHOST, dir, 0, 0, o, c);
-            }
+            for (int dir = 0; dir < 3; dir++) ok = ok && exec_ghost(a, L, dir, true);
             const int64_t o = tfLOff[L], c = tfLOff[L + 1] - o;
             if (c) ok = ok && exec_add(a, PH_FILL0, 0, -1, 0, o, c);
             ok = ok && exec_add(a, PH_RELAX, 0, -1, 0, 0, cnt(L), ipass);
