@@ -21,7 +21,9 @@ namespace sfm {
 
 #define SFM_HD __host__ __device__ __forceinline__
 
-SFM_HD int64_t cidx(int G, int i, int j, int k) { return ((int64_t)(k + 1) * G + (j + 1)) * G + (i + 1); }
+// offset inside one block or the base grid (G <= 130: G^3 < 2^31); callers
+// add it to a 64-bit block base
+SFM_HD int cidx(int G, int i, int j, int k) { return ((k + 1) * G + (j + 1)) * G + (i + 1); }
 // IJKC(i,0) = floor(i/2) (config.h:249)
 SFM_HD int fdiv2(int i) { return i >= 0 ? i / 2 : -((-i + 1) / 2); }
 // Fortran MODULO(i,2)

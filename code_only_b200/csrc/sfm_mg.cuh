@@ -51,29 +51,44 @@ __device__ double mg_block_max(double v, double *sh) {
     return m;
 }
 
-// periodic wrap of one ghost layer, x then y then z
-// (fmg_boundary_phys_periodic.F90:71-104)
+// (p, q) = (t mod G, t div G) for t < G^2 <= 130^2 without an integer
+// division: (t + 1/2) / G lies at least 1/(2G) from an integer, far above
+// the float rounding of (t + 1/2) * (1/G)
+__device__ __forceinline__ void mg_pq(int t, int G, float rG, int &p, int &q) {
+    q = (int)(((float)t + 0.5f) * rG);
+    p = t - q * G;
+}
+// periodic wrap of one ghost layer (fmg_boundary_phys_periodic.F90:71-104).
+// The reference copies x, then y, then z faces, each face including the
+// ghost rows of the other directions; after the three passes every ghost
+// cell holds the interior cell at its periodic image (wrap each coordinate
+// -1 -> n-1, n -> 0).  That final state is written here in one pass:
+// cells on several faces are written with the same value more than once.
 __device__ void mg_boundary_u(const MgData &d, int m, double *a) {
     if (!d.periodic) return;
     const int n = mgN(d, m), G = n + 2;
-    for (int dir = 0; dir < 3; dir++) {
-        for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
-            int p = t % G - 1, q = t / G - 1, i, j, k, is, js, ks;
-            put3(dir, -1, p, q, i, j, k); put3(dir, n - 1, p, q, is, js, ks);
-            a[cidx(G, i, j, k)] = a[cidx(G, is, js, ks)];
-            put3(dir, n, p, q, i, j, k); put3(dir, 0, p, q, is, js, ks);
-            a[cidx(G, i, j, k)] = a[cidx(G, is, js, ks)];
-        }
-        __syncthreads();
+    const float rG = 1.0f / (float)G;
+    auto wrap = [n](int x) { return x < 0 ? n - 1 : (x >= n ? 0 : x); };
+    for (int t = threadIdx.x; t < 3 * G * G; t += blockDim.x) {
+        const int dir = t >= 2 * G * G ? 2 : (t >= G * G ? 1 : 0);
+        int p, q, i, j, k;
+        mg_pq(t - dir * G * G, G, rG, p, q);
+        put3(dir, -1, p - 1, q - 1, i, j, k);
+        a[cidx(G, i, j, k)] = a[cidx(G, wrap(i), wrap(j), wrap(k))];
+        put3(dir, n, p - 1, q - 1, i, j, k);
+        a[cidx(G, i, j, k)] = a[cidx(G, wrap(i), wrap(j), wrap(k))];
     }
+    __syncthreads();
 }
 __device__ void mg_boundary_fill0(const MgData &d, int m, double *a) {   // mg.F90:735-750
     const int n = mgN(d, m), G = n + 2;
+    const float rG = 1.0f / (float)G;
     for (int f = 0; f < 6; f++) {
         if (!d.touch[f]) continue;
         for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
-            int i, j, k;
-            put3(f >> 1, (f & 1) ? n : -1, t % G - 1, t / G - 1, i, j, k);
+            int i, j, k, p, q;
+            mg_pq(t, G, rG, p, q);
+            put3(f >> 1, (f & 1) ? n : -1, p - 1, q - 1, i, j, k);
             a[cidx(G, i, j, k)] = 0.0;
         }
     }
@@ -81,13 +96,15 @@ __device__ void mg_boundary_fill0(const MgData &d, int m, double *a) {   // mg.F
 }
 __device__ void mg_boundary_extrap(const MgData &d, int m, double *a) {  // mg.F90:754-771
     const int n = mgN(d, m), G = n + 2;
+    const float rG = 1.0f / (float)G;
     for (int dir = 0; dir < 3; dir++) {
         for (int lr = 0; lr < 2; lr++) {
             if (!d.touch[lr + 2 * dir]) continue;
             for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
-                int i, j, k, ii, jj, kk;
-                put3(dir, lr ? n : -1, t % G - 1, t / G - 1, i, j, k);
-                put3(dir, lr ? n - 1 : 0, t % G - 1, t / G - 1, ii, jj, kk);
+                int i, j, k, ii, jj, kk, p, q;
+                mg_pq(t, G, rG, p, q);
+                put3(dir, lr ? n : -1, p - 1, q - 1, i, j, k);
+                put3(dir, lr ? n - 1 : 0, p - 1, q - 1, ii, jj, kk);
                 a[cidx(G, i, j, k)] = -a[cidx(G, ii, jj, kk)];
             }
         }
@@ -115,11 +132,14 @@ __device__ void mg_resid(const MgData &d, int m, double *res, double *u, const d
     }
     __syncthreads();
 }
-// returns Resmaxg = max|resh2| / h^2 over both colours (mg_poisson.F90:32-79)
-__device__ double mg_relax(const MgData &d, int m, double *u, const double *rhs, double *sh) {
+// both colours (mg_poisson.F90:32-79); returns this thread's max|resh2|:
+// Resmaxg = (max over the CTA) / h^2 is formed by the caller where it is
+// used (the max is exact, so where it is reduced does not change it)
+__device__ double mg_relax(const MgData &d, int m, double *u, const double *rhs) {
     const int n = mgN(d, m), G = n + 2;
     double hh = mgH(d, m), h2 = hh * hh, rm = 0.0;
     const int half = (n * n * n + 1) / 2;
+    (void)G;
     for (int ipass = 1; ipass <= 2; ipass++) {
         mg_boundary_u(d, m, u);
         for (int c = threadIdx.x; c < half; c += blockDim.x) {
@@ -138,7 +158,7 @@ __device__ double mg_relax(const MgData &d, int m, double *u, const double *rhs,
         }
         __syncthreads();
     }
-    return mg_block_max(rm, sh) / h2;
+    return rm;
 }
 __device__ void mg_rstrct(const MgData &d, int m, double *uc, const double *uf) {   // linear (mg.F90:581-602)
     const int n = mgN(d, m), G = n + 2, Gf = 2 * n + 2, ln = __ffs(n) - 1;
@@ -186,31 +206,37 @@ __device__ void mg_addw(const MgData &d, int m, double *a, const double *da) {
     __syncthreads();
 }
 
-// mg_lin (mg.F90:106-218); returns the last Resmaxg
+// mg_lin (mg.F90:106-218); returns the last Resmaxg (the Resmaxg of every
+// earlier mg_relax is overwritten unread, so only the last one is reduced)
 __device__ double mg_lin(const MgData &d, double *sh) {
-    double res = 0.0;
+    double rm = 0.0;   // this thread's max|resh2| of the last mg_relax
+    int mr = d.MMax;   // its level
     for (int m = 1; m <= d.MMax; m++) mg_rstrct(d, m, d.RHO[m], d.RHO[m - 1]);
     mg_fill0(d, d.MMax, d.U[d.MMax]);
-    for (int q = 0; q < 2; q++) res = mg_relax(d, d.MMax, d.U[d.MMax], d.RHO[d.MMax], sh);
+    for (int q = 0; q < 2; q++) rm = mg_relax(d, d.MMax, d.U[d.MMax], d.RHO[d.MMax]);
     for (int m = d.MMax - 1; m >= 0; m--) {
         mg_interp(d, m, d.U[m], d.U[m + 1], true);
         mg_copy(d, m, d.RHS[m], d.RHO[m]);
         for (int jc = 1; jc <= 2; jc++) {
             for (int v = m; v <= d.MMax - 1; v++) {
-                for (int q = 0; q < 2; q++) res = mg_relax(d, v, d.U[v], d.RHS[v], sh);
+                for (int q = 0; q < 2; q++) rm = mg_relax(d, v, d.U[v], d.RHS[v]);
+                mr = v;
                 mg_resid(d, v, d.RES[v], d.U[v], d.RHS[v]);
                 mg_rstrct(d, v + 1, d.RHS[v + 1], d.RES[v]);
                 mg_fill0(d, v + 1, d.U[v + 1]);
             }
-            for (int q = 0; q < 2; q++) res = mg_relax(d, d.MMax, d.U[d.MMax], d.RHS[d.MMax], sh);
+            for (int q = 0; q < 2; q++) rm = mg_relax(d, d.MMax, d.U[d.MMax], d.RHS[d.MMax]);
+            mr = d.MMax;
             for (int v = d.MMax - 1; v >= m; v--) {
                 mg_interp(d, v, d.RES[v], d.U[v + 1], false);
                 mg_addw(d, v, d.U[v], d.RES[v]);
-                for (int q = 0; q < 2; q++) res = mg_relax(d, v, d.U[v], d.RHS[v], sh);
+                for (int q = 0; q < 2; q++) rm = mg_relax(d, v, d.U[v], d.RHS[v]);
+                mr = v;
             }
         }
     }
-    return res;
+    const double hh = mgH(d, mr);
+    return mg_block_max(rm, sh) / (hh * hh);
 }
 
 // dynamic shared memory of the base-grid CTA
