@@ -267,12 +267,14 @@ public:
     int64_t iterLaunches = 0;
     bool graphsOff = false;
     void outer_iteration_body() {
+        profNext = 0;
         resid<double, double, T>(0, RHO[0], PSI0, SRC0, false);
         fmg_lin();
         add(0, PSI0, U[0]);
+        profPairs = profNext;
     }
     void outer_iteration() {
-        if (graphsOff || P.profile) { outer_iteration_body(); return; }
+        if (graphsOff) { outer_iteration_body(); return; }
         if (!iterExec) {
             int64_t l0 = launches;
             int save = FmgLevel_fill0;
@@ -305,6 +307,7 @@ public:
 
     ~Solver() override {
         if (iterExec) cudaGraphExecDestroy(iterExec);
+        prof_release();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (own_) cudaStreamDestroy(own_);
@@ -634,10 +637,10 @@ public:
         const int n = nf[f];
         for (int ipass = 1; ipass <= 2; ipass++) {
             poisson_flux(f, u, bf0);
-            bool prof = P.profile && f == 0 && profEv.size() < 2 * kMaxProf;
-            if (prof) { profEv.push_back(nullptr); cudaEventCreate(&profEv.back()); cudaEventRecord(profEv.back(), st_); }
+            const bool prof = f == 0 && profNext < (int)profEv.size() / 2;
+            if (prof) prof_mark(2 * profNext);
             relax_launch(u, rhs, d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max + slot);
-            if (prof) { profEv.push_back(nullptr); cudaEventCreate(&profEv.back()); cudaEventRecord(profEv.back(), st_); }
+            if (prof) prof_mark(2 * profNext++ + 1);
         }
     }
     // persistent grid of k_relax_bulk<T, N> (N >= 4): every SM filled to the
@@ -797,22 +800,63 @@ public:
         if (e) { last_error = "a bulk-copy wait in the smoother gave up"; return SFM_ETIMEOUT; }
         return SFM_OK;
     }
-    static constexpr size_t kMaxProf = 4096;
-    std::vector<cudaEvent_t> profEv;
-    void prof_collect(sfm_stats *stats) {
-        double ms = 0.0;
-        for (size_t q = 0; q + 1 < profEv.size(); q += 2) {
-            float t = 0.f;
-            cudaEventElapsedTime(&t, profEv[q], profEv[q + 1]);
-            ms += t;
-        }
-        if (stats) {
-            stats->smoother_ms = ms;
-            stats->smoother_launches = (int64_t)(profEv.size() / 2);
-            stats->smoother_cells = (int64_t)(profEv.size() / 2) * nLeaves * H.NI * H.NI * H.NI;
-        }
-        for (auto e : profEv) cudaEventDestroy(e);
+    // Smoother timing (P.profile): an event pair around every level-0 colour
+    // sweep of an outer iteration.  Inside stream capture the records become
+    // event nodes of the iteration's graph (cudaEventRecordExternal), so the
+    // timed solve keeps its graphs; the pairs are read after every iteration
+    // (its residual read-back has synchronised the stream).
+    static constexpr int kProfPairs = 64;
+    std::vector<cudaEvent_t> profEv;   // 2 kProfPairs events, created at the first profiled solve
+    int profNext = 0;                  // next pair while an iteration's launches are issued
+    int profPairs = 0;                 // pairs one outer iteration records (kept with its graph)
+    double profMs = 0.0;
+    int64_t profN = 0;
+    void prof_init() {
+        profMs = 0.0;
+        profN = 0;
+        if (!P.profile || !profEv.empty()) return;
+        profEv.assign(2 * kProfPairs, nullptr);
+        for (auto &e : profEv)
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                cudaGetLastError();
+                e = nullptr;
+            }
+        for (auto e : profEv)
+            if (!e) {   // no timing rather than a partial pool
+                prof_release();
+                break;
+            }
+    }
+    void prof_release() {
+        for (auto e : profEv)
+            if (e) cudaEventDestroy(e);
         profEv.clear();
+    }
+    void prof_mark(int q) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(st_, &cs);
+        cudaEventRecordWithFlags(profEv[q], st_,
+                                 cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault);
+    }
+    void prof_iteration() {   // after an outer iteration's stream work has completed
+        for (int q = 0; q < profPairs; q++) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, profEv[2 * q], profEv[2 * q + 1]) == cudaSuccess) {
+                profMs += t;
+                profN++;
+            } else {
+                cudaGetLastError();
+            }
+        }
+    }
+    void prof_collect(sfm_stats *stats) {
+        if (stats) {
+            stats->smoother_ms = profMs;
+            stats->smoother_launches = profN;
+            stats->smoother_cells = profN * nLeaves * H.NI * H.NI * H.NI;
+        }
+        profMs = 0.0;
+        profN = 0;
     }
     template <class TU, class TR, class TO>
     void resid(int f, TO *res, TU *u, const TR *rhs, bool bf0) {   // fmg_poisson_resid
@@ -1053,6 +1097,7 @@ public:
               double *dump) override {
         st_ = s ? s : own_;   // all work of this call is ordered on the caller's stream
         launches = 0;
+        prof_init();
         const int nb = H.nb, gw = P.ngh_io;
         cudaEventRecord(ev0, st_);
         // fresh, zero-filled arrays as fmg_alloc_arr gives (fmg_data.F90:393)
@@ -1104,6 +1149,7 @@ public:
             if (rc) return rc;
             iters = it;
             double ratio = read_max(0) / resh2max;
+            prof_iteration();
             if (stats && it <= SFM_MAX_HISTORY) stats->ratio[it - 1] = ratio;
             if (ratio < P.rel_tol) { reached = true; break; }
             if (it == nmax) conv = false;
