@@ -331,7 +331,7 @@ def run_ours(args):
         "mixed_over_fp64": round(fp["ms"] / mx["ms"], 3),
         "phi_rel_err_mixed_vs_fp64": phi_err,
         "roofline": {
-            "kernel": "red-black colour sweep, fmg level 0 (OpRelax<float>)",
+            "kernel": f"k_relax_bulk<float, {h.ni}>: one red-black colour over the leaf cells, fmg level 0",
             "bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4) if achieved else None,
             "traffic": traffic,

@@ -251,6 +251,7 @@ struct OpBlockDot {
 };
 // ordered sum of cnt partials into *out: one warp, contiguous chunks per lane
 __global__ void __launch_bounds__(32) k_sum_ordered(const double *psum, int cnt, double *out) {
+    pdl_enter();
     __shared__ double part[32];
     const int lane = threadIdx.x;
     const int chunk = (cnt + 31) / 32;
@@ -346,6 +347,7 @@ struct OpBcBeta {
 };
 // beta_q = ordered sum of the face partials (one thread per q)
 __global__ void k_bc_beta_combine(const double *part, int nfaces, double *beta) {
+    pdl_enter();
     const int q = threadIdx.x;
     if (q >= 25) return;
     double s = 0.0;

@@ -168,6 +168,7 @@ template <class T, int N>
 __global__ void __launch_bounds__(256) k_ghost_faces(T *u, const FaceItem *__restrict__ items0, int n0,
                                                      const FaceItem *__restrict__ items1, int n1, int dir,
                                                      int cubic) {
+    pdl_enter();
     constexpr int G = N + 2, NB2 = N / 2, LN = ghost_lanes<N>();
     const int nb0 = ghost_copy_ctas<N>(n0);
     if ((int)blockIdx.x < nb0) {
@@ -326,6 +327,7 @@ __global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T 
                                                      const double *__restrict__ h0, const int32_t *__restrict__ level,
                                                      const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
                                                      int f, int ipass, unsigned long long *out) {
+    pdl_enter();
     __shared__ RelaxTileSmem<T, N> sm;
     double m = 0.0;
     relax_tiles<T, N>(sm, u, rhs, blocks, nblk, h0, level, rslot, rbuf, f, ipass, blockIdx.x, gridDim.x, m);
@@ -417,6 +419,7 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
                                                     const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
                                                     int f, int ipass, unsigned long long *out, int *err) {
+    pdl_enter();
     using Tl = Tile<N>;
     using Pl = BulkPlan<T, N>;
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2, S = Pl::S;
@@ -552,6 +555,7 @@ __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const
                                                      int nblk, const double *__restrict__ h0,
                                                      const int32_t *__restrict__ level, const int32_t *__restrict__ rslot,
                                                      const double *__restrict__ rbuf, int f) {
+    pdl_enter();
     using Tl = Tile<N>;
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC;
     __shared__ TU sh[BPC * V];
@@ -584,6 +588,7 @@ __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const T *__restrict__ uc,
                                                       const int32_t *__restrict__ blocks, int nblk, int cubic) {
+    pdl_enter();
     constexpr int NC = N / 2, GC = NC + 2, GF = N + 2;
     constexpr int VC = GC * GC * GC, VF = GF * GF * GF;
     constexpr int W = GC;                  // coarse extent with ghosts = interp range [-1, NC]
@@ -642,6 +647,7 @@ template <class T, int N>
 __global__ void __launch_bounds__(256) k_converge_tiled(T *__restrict__ u, const int32_t *__restrict__ parent,
                                                         const int8_t *__restrict__ oct, int first, int nchild,
                                                         int cubic) {
+    pdl_enter();
     using Tl = Tile<N>;
     constexpr int G = Tl::G, V = Tl::V, H = N / 2 > 0 ? N / 2 : 1, PER = H * H * H;
     constexpr int BPC = Tl::BPC;
@@ -670,6 +676,7 @@ __global__ void __launch_bounds__(1024) k_mean_combine_w(const double *__restric
                                                          const int32_t *__restrict__ blocks, int nblk,
                                                          const int32_t *__restrict__ level,
                                                          const double *__restrict__ h0, int n, double *out) {
+    pdl_enter();
     __shared__ double tm[2][kSumChunk], tv[2][kSumChunk];
     const int tid = threadIdx.x;
     const double ncell = (double)(n * n * n);
@@ -705,6 +712,7 @@ __global__ void __launch_bounds__(1024) k_mean_combine_w(const double *__restric
 // base-level average: sum_b psum_b / (n^3 nblk)
 __global__ void __launch_bounds__(1024) k_ave_combine_w(const double *__restrict__ psum, int nblk, int n,
                                                         double *out) {
+    pdl_enter();
     __shared__ double ts[2][kSumChunk];
     const int tid = threadIdx.x;
     const int nch = (nblk + kSumChunk - 1) / kSumChunk;

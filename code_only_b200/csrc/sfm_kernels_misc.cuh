@@ -43,6 +43,7 @@ struct OpBlockSum {
 // block after block in level order, then rho_ave -> *out
 __global__ void k_mean_combine(const double *psum, const int32_t *blocks, int nblk, const int32_t *level,
                                const double *h0, int n, double *out) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double mass = 0.0, vol = 0.0;
     for (int q = 0; q < nblk; q++) {
@@ -56,6 +57,7 @@ __global__ void k_mean_combine(const double *psum, const int32_t *blocks, int nb
 
 // vmg_zeroAverage (vmg.F90:900-916) via fmg_ave (fmg_data.F90:730-769)
 __global__ void k_ave_combine(const double *psum, int nblk, int n, double *out) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double ave = 0.0;
     for (int q = 0; q < nblk; q++) ave = ave + psum[q];
@@ -97,6 +99,7 @@ struct OpSphereMask {        // rho := 0 where x^2+y^2+z^2 >= rad2, all cells of
 // moments of one base block: one CTA per block, fixed-order tree reduction
 __global__ void k_moments_block(const double *R, const double *x0, const double *h0, int n, int G, int64_t V,
                                 int lmax, double *part /* [nbase][25] */) {
+    pdl_enter();
     __shared__ double red[25][128];   // blockDim.x == 128
     const int b = blockIdx.x;
     const double h = h0[0], dv = h * h * h;
@@ -158,6 +161,7 @@ __global__ void k_moments_block(const double *R, const double *x0, const double 
 // sum of the per-block moments in block order, then the normalisations of
 // sphere.F90:227-242 (and of the l = 4 extension)
 __global__ void k_moments_combine(const double *part, int nbase, double *mom) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double a[25];
     for (int m = 0; m < 25; m++) a[m] = 0.0;

@@ -267,6 +267,7 @@ __host__ __device__ inline int mg_smem_from(int N, int MMax, size_t budget_doubl
 
 // mg_cycle (mg.F90:42-94) with ju = PSI, jrho = SRC; one CTA
 __global__ void __launch_bounds__(1024) k_mg_cycle(MgData dg, int smem_from, int *iters_out) {
+    pdl_enter();
     __shared__ double sh[32];
     MgData d = dg;
     {

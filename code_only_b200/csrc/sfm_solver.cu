@@ -525,12 +525,30 @@ public:
 
     // -----------------------------------------------------------------
     // launch helpers
+    // Every kernel of the solve starts with pdl_enter(), so each launch may
+    // carry a programmatic dependency on the previous kernel of the stream:
+    // it is scheduled while that one drains.  (The cooperative k_exec never
+    // does: it needs all of its CTAs co-resident.)
+    template <class... KArgs, class... Args>
+    void launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, Args... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st_;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k, args...);
+    }
     template <class Op>
     void run(const Op &op, int64_t n) {
         if (n <= 0) return;
         int64_t blocks = (n + 255) / 256;
         if (blocks > maxBlocks) blocks = maxBlocks;
-        k_apply<Op><<<(unsigned)blocks, 256, 0, st_>>>(op, n);
+        launch_pdl(k_apply<Op>, (unsigned)blocks, 256, 0, op, n);
         ++launches;
     }
     template <class Op>
@@ -538,7 +556,7 @@ public:
         if (n <= 0) return;
         int64_t blocks = (n + 255) / 256;
         if (blocks > maxBlocks) blocks = maxBlocks;
-        k_apply_max<Op><<<(unsigned)blocks, 256, 0, st_>>>(op, n, out);
+        launch_pdl(k_apply_max<Op>, (unsigned)blocks, 256, 0, op, n, out);
         ++launches;
     }
     int cnt(int L) const { return H.lstart[L + 1] - H.lstart[L]; }
@@ -560,10 +578,10 @@ public:
         const int n = nf[f];
         if ((n == 2 || n == 4 || n == 8 || n == 16) && n0 * GT * GT <= INT32_MAX) {
             SFM_WITH_N(n,
-                       (k_ghost_faces<TT, N><<<(unsigned)(ghost_copy_ctas<N>((int)n0) +
-                                                          (n1 + 256 / ghost_lanes<N>() - 1) / (256 / ghost_lanes<N>())),
-                                               256, 0, st_>>>(u, d_faces + o, (int)n0, d_faces + sp, (int)n1, dir,
-                                                              cubic ? 1 : 0),
+                       (launch_pdl(k_ghost_faces<TT, N>,
+                                   (unsigned)(ghost_copy_ctas<N>((int)n0) +
+                                              (n1 + 256 / ghost_lanes<N>() - 1) / (256 / ghost_lanes<N>())),
+                                   256, 0, u, d_faces + o, (int)n0, d_faces + sp, (int)n1, dir, cubic ? 1 : 0),
                         ++launches),
                        (void)0)
             return;
@@ -574,8 +592,8 @@ public:
     void converge_c2p_lev(int Lc, int f, TT *u, bool cubic) {
         int Lf = Lc + 1, h = nf[f] / 2;
         SFM_WITH_N(nf[f],
-                   (k_converge_tiled<TT, N><<<(unsigned)((cnt(Lf) + Tile<N>::BPC - 1) / Tile<N>::BPC), 256, 0, st_>>>(
-                        u, d_parent, d_oct, H.lstart[Lf], cnt(Lf), cubic ? 1 : 0),
+                   (launch_pdl(k_converge_tiled<TT, N>, (unsigned)((cnt(Lf) + Tile<N>::BPC - 1) / Tile<N>::BPC), 256,
+                               0, u, d_parent, d_oct, H.lstart[Lf], cnt(Lf), cubic ? 1 : 0),
                     ++launches),
                    run(OpConverge<TT>{u, d_parent, d_oct, H.lstart[Lf], nf[f], Gf[f], Vf[f], cubic ? 1 : 0},
                        (int64_t)cnt(Lf) * h * h * h))
@@ -671,14 +689,13 @@ public:
         const int n = nf[f];
         if (nblk <= 0) return;
         SFM_WITH_N(n,
-                   (bulk_ok<N>() ? (k_relax_bulk<T, N><<<(unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC,
-                                                                      bulk_grid<N>()),
-                                                    256, BulkPlan<T, N>::SMEM, st_>>>(
-                                  u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out, d_err))
-                            : (k_relax_tiled<T, N><<<(unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC,
-                                                                        persistGrid),
-                                                     256, 0, st_>>>(u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f,
-                                                                    ipass, out)),
+                   (bulk_ok<N>() ? launch_pdl(k_relax_bulk<T, N>,
+                                              (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N>()),
+                                              256, BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0, d_level, rslot,
+                                              rb, f, ipass, out, d_err)
+                                 : launch_pdl(k_relax_tiled<T, N>,
+                                              (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
+                                              256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
                     ++launches),
                    runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
                           (int64_t)nblk * n * n * n / 2, out))
@@ -863,9 +880,8 @@ public:
         poisson_flux(f, u, bf0);
         const int n = nf[f];
         SFM_WITH_N(n,
-                   (k_resid_tiled<TU, TR, TO, N><<<(unsigned)((nLeaves + Tile<N>::BPC - 1) / Tile<N>::BPC), 256, 0,
-                                                   st_>>>(res, u, rhs, d_leaves, nLeaves, d_h0, d_level, d_rslot,
-                                                          rbuf[f], f),
+                   (launch_pdl(k_resid_tiled<TU, TR, TO, N>, (unsigned)((nLeaves + Tile<N>::BPC - 1) / Tile<N>::BPC),
+                               256, 0, res, u, rhs, d_leaves, nLeaves, d_h0, d_level, d_rslot, rbuf[f], f),
                     ++launches),
                    run(OpResid<TU, TR, TO>{res, u, rhs, d_leaves, d_h0, d_level, d_rslot, rbuf[f], f, n, Gf[f], Vf[f]},
                        (int64_t)nLeaves * n * n * n))
@@ -880,7 +896,7 @@ public:
         if (nblk <= 0) return;
         const int bpc = std::max(1, 256 / (int)op.V);
         const int64_t g = std::min<int64_t>((nblk + bpc - 1) / bpc, (int64_t)nSM * 16);
-        k_blocks<Op><<<(unsigned)g, 256, 0, st_>>>(op, (int)nblk, bpc);
+        launch_pdl(k_blocks<Op>, (unsigned)g, 256, 0, op, (int)nblk, bpc);
         ++launches;
     }
     void fill0(int f, T *u) { runB(OpZero<T>{u, d_leaves, Vf[f]}, nLeaves); }
@@ -899,7 +915,7 @@ public:
         boundary_extrap(lc, uc);
         const int n = nf[f];
         SFM_WITH_N(n,
-                   (k_interp_tiled<T, N><<<(unsigned)nLeaves, 256, 0, st_>>>(uf, uc, d_leaves, nLeaves, cubic ? 1 : 0),
+                   (launch_pdl(k_interp_tiled<T, N>, (unsigned)nLeaves, 256, 0, uf, uc, d_leaves, nLeaves, cubic ? 1 : 0),
                     ++launches),
                    run(OpInterp<T>{uf, uc, d_leaves, n, Gf[f], Gf[lc], Vf[f], Vf[lc], cubic ? 1 : 0},
                        (int64_t)nLeaves * n * n * n))
@@ -1003,7 +1019,7 @@ public:
     void vmg_zeroAverage(T *a) {
         const int F = H.FMax, n = nf[F];
         run(OpBlockSum<T>{a, d_all, d_psum, n, Gf[F], Vf[F]}, (int64_t)cnt(0));
-        k_ave_combine_w<<<1, 1024, 0, st_>>>(d_psum, cnt(0), n, d_scal + 1);
+        launch_pdl(k_ave_combine_w, 1, 1024, 0, d_psum, cnt(0), n, d_scal + 1);
         ++launches;
         run(OpSubScalarInterior<T>{a, d_scal + 1, 0, n, Gf[F], Vf[F]}, (int64_t)cnt(0) * n * n * n);
     }
@@ -1015,7 +1031,7 @@ public:
         const int F = H.FMax;
         int64_t N3 = (int64_t)NBc * NBc * NBc;
         run(OpMgGather<T>{mg.SRC, mg.PSI, rhs, u, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
-        k_mg_cycle<<<1, 1024, mgSmemBytes, st_>>>(mg, mgSmemFrom, d_mgit);
+        launch_pdl(k_mg_cycle, 1, 1024, mgSmemBytes, mg, mgSmemFrom, d_mgit);
         ++launches;
         run(OpMgScatter<T>{u, mg.PSI, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
     }
@@ -1061,8 +1077,8 @@ public:
         double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
         double rad2 = rr * rr;
         run(OpSphereMask{SRC0, d_x0, d_h0, d_level, n, Gf[0], Vf[0], rad2}, (int64_t)H.nb * Vf[0]);
-        k_moments_block<<<cnt(0), 128, 0, st_>>>(SRC0, d_x0, d_h0, n, Gf[0], Vf[0], P.lmax, d_part);
-        k_moments_combine<<<1, 1, 0, st_>>>(d_part, cnt(0), d_mom);
+        launch_pdl(k_moments_block, (unsigned)cnt(0), 128, 0, SRC0, d_x0, d_h0, n, Gf[0], Vf[0], P.lmax, d_part);
+        launch_pdl(k_moments_combine, 1, 1, 0, d_part, cnt(0), d_mom);
         launches += 2;
         int GT = n + 2;
         run(OpSphereGhost{PSI0, d_tfL, d_mom, d_x0, d_h0, d_level, n, Gf[0], Vf[0], P.lmax}, tfLOff[H.nlev] * GT * GT);
@@ -1108,7 +1124,7 @@ public:
         run(OpPhysvar<double>{PHI0, RES0d, rho, psi, H.NI, Gf[0], gw, Vf[0], P.four_pi_G, d_bad}, (int64_t)nb * Vf[0]);
         if (P.zero_mean) {
             run(OpBlockSum<double>{RES0d, d_leaves, d_psum, H.NI, Gf[0], Vf[0]}, (int64_t)nLeaves);
-            k_mean_combine_w<<<1, 1024, 0, st_>>>(d_psum, d_leaves, nLeaves, d_level, d_h0, H.NI, d_scal);
+            launch_pdl(k_mean_combine_w, 1, 1024, 0, d_psum, d_leaves, nLeaves, d_level, d_h0, H.NI, d_scal);
             ++launches;
             run(OpSubScalarAll<double>{RES0d, d_scal}, (int64_t)nb * Vf[0]);
         } else {
@@ -1258,7 +1274,7 @@ public:
     // ordered sum over leaf interiors of a*b (of a when b is null)
     double adj_dot(const double *a, const double *b) {
         run(OpBlockDot{a, b, d_leaves, d_psum, nf[0], Gf[0], Vf[0]}, (int64_t)nLeaves);
-        k_sum_ordered<<<1, 32, 0, st_>>>(d_psum, nLeaves, aDot);
+        launch_pdl(k_sum_ordered, 1, 32, 0, d_psum, nLeaves, aDot);
         ++launches;
         double v = 0.0;
         cudaMemcpyAsync(&v, aDot, sizeof(double), cudaMemcpyDeviceToHost, st_);
@@ -1389,7 +1405,7 @@ public:
             rad2 = sphere_rad2();
             const int64_t nfaces = tfLOff[H.nlev];
             run(OpBcBeta{aUB, d_tfL, d_touch, d_x0, d_h0, d_level, aPart, n, G, V, P.lmax}, nfaces);
-            k_bc_beta_combine<<<1, 32, 0, st_>>>(aPart, (int)nfaces, aBeta);
+            launch_pdl(k_bc_beta_combine, 1, 32, 0, aPart, (int)nfaces, aBeta);
             ++launches;
             run(OpMomentT{aS, aBeta, d_x0, d_h0, H.lstart[0], n, G, V, rad2, P.lmax}, (int64_t)cnt(0) * n * n * n);
             adj_converge_T(aS);
