@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
     constexpr int R = (32 / BPC) > 2 * S ? 32 / BPC : 2 * S;
     __shared__ int bid[2 * R][BPC];
     __shared__ int ssl[2 * R][BPC][6];
+    __shared__ int8_t hasr[2 * R][BPC];   // a face of the block takes a reflux flux
     __shared__ T shh[2 * R][BPC], shi[2 * R][BPC];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (nblk + BPC - 1) / BPC;
@@ -465,12 +466,19 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
             if (step < nsteps && first + q < nblk) {
                 const int b = blocks[first + q];
                 bid[slot][q] = b;
-                for (int fc = 0; fc < 6; fc++) ssl[slot][q][fc] = rslot ? rslot[6 * b + fc] : -1;
+                int any = 0;
+                for (int fc = 0; fc < 6; fc++) {
+                    const int v = rslot ? rslot[6 * b + fc] : -1;
+                    ssl[slot][q][fc] = v;
+                    any |= v >= 0;
+                }
+                hasr[slot][q] = (int8_t)any;
                 const double hd = hlev(h0, level[b], f);
                 shh[slot][q] = (T)hd;
                 shi[slot][q] = (T)(1.0 / hd);
             } else {
                 for (int fc = 0; fc < 6; fc++) ssl[slot][q][fc] = -1;
+                hasr[slot][q] = 0;
             }
         }
         __syncwarp();
@@ -506,6 +514,7 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
         // consumer waits for another: a warp waits for the stage, updates,
         // stores and releases the stage on its own.
         const int ct = tid - 32;   // consumer thread 0..NCT-1
+        T mt = (T)0;               // max |resh2| (exact in T; widened once)
         int it = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
@@ -525,12 +534,14 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
                 const int i = 2 * i2 + ((j + k + ipass) & 1);
                 const T hh = shh[slot][q], hi = shi[slot][q];
                 const T *ub = ut + q * V;
-                TileFlux<T, N> F{ub, hi, rslot ? ssl[slot][q] : nullptr, rbuf};
-                const int c = (int)cidx(G, i, j, k);
+                // blocks without a reflux face (a warp's cells share a block)
+                // skip the per-face slot tests: same fluxes, fewer instructions
+                TileFlux<T, N> F{ub, hi, hasr[slot][q] ? ssl[slot][q] : nullptr, rbuf};
+                const int c = cidx(G, i, j, k);
                 const T resh2 = (F.div(i, j, k) - rt[q * V + c] * hh) * hh;
                 u[(int64_t)bid[slot][q] * V + c] = ub[c] + (T)(1.0 / 6.0) * resh2;
-                const double a = fabs((double)resh2);
-                m = a > m ? a : m;
+                const T a = resh2 < (T)0 ? -resh2 : resh2;
+                mt = a > mt ? a : mt;
             }
             __syncwarp();
             if (lane == 0) {
@@ -538,6 +549,7 @@ __global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *
                 mbar_arrive(&empty[s]);   // this warp is done with stage s
             }
         }
+        m = (double)mt;
     }
     __syncthreads();
     if (tid == 0 && (pab || cab)) {   // loads still in flight: wait for them (bounded), then report
@@ -560,22 +572,31 @@ __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC;
     __shared__ TU sh[BPC * V];
     __shared__ int ssl[BPC][6];
+    __shared__ int sbid[BPC];
+    __shared__ TU shi[BPC];
+    __shared__ int8_t hasr[BPC];   // a face of the block takes a reflux flux
     const int first = blockIdx.x * BPC;
     stage_blocks<TU, N>(sh, u, blocks, first, nblk);
-    if (threadIdx.x < BPC * 6) {
-        const int q = threadIdx.x / 6, fc = threadIdx.x % 6;
-        ssl[q][fc] = (rslot && first + q < nblk) ? rslot[6 * blocks[first + q] + fc] : -1;
+    if (threadIdx.x < BPC && first + (int)threadIdx.x < nblk) {   // per-block data, once per block
+        const int q = threadIdx.x, b = blocks[first + q];
+        int any = 0;
+        for (int fc = 0; fc < 6; fc++) {
+            const int v = rslot ? rslot[6 * b + fc] : -1;
+            ssl[q][fc] = v;
+            any |= v >= 0;
+        }
+        sbid[q] = b;
+        hasr[q] = (int8_t)any;
+        shi[q] = (TU)(1.0 / hlev(h0, level[b], f));
     }
     __syncthreads();
     for (int t = threadIdx.x; t < BPC * Tl::CELLS; t += blockDim.x) {
         const int q = t / Tl::CELLS, r = t - q * Tl::CELLS;
         if (first + q >= nblk) continue;
-        const int b = blocks[first + q];
         const int i = r % N, j = (r / N) % N, k = r / (N * N);
-        const double hd = hlev(h0, level[b], f);
-        const TU hi = (TU)(1.0 / hd);
-        TileFlux<TU, N> F{sh + q * V, hi, rslot ? ssl[q] : nullptr, rbuf};
-        const int64_t c = (int64_t)b * V + cidx(G, i, j, k);
+        const TU hi = shi[q];
+        TileFlux<TU, N> F{sh + q * V, hi, hasr[q] ? ssl[q] : nullptr, rbuf};
+        const int64_t c = (int64_t)sbid[q] * V + cidx(G, i, j, k);
         res[c] = (TO)((TU)rhs[c] - F.div(i, j, k) * hi);
     }
 }
