@@ -4,7 +4,7 @@
 // The reference gathers the base level to rank 0 and runs mg_cycle there
 // serially (vmg.F90:407-428, mg_data.F90:179-330).  Here the whole cycle
 // (<= 10 defect corrections of an FMG with Ncycle 2, 2/2 smoothing) runs in
-// one CTA of 1024 threads on a base grid of at most 64^3 cells: the coarse
+// one CTA of 512 threads on a base grid of at most 64^3 cells: the coarse
 // levels' working arrays in shared memory, level 0 and the data exchanged
 // with the AMR levels in global memory (L2), every operation separated by
 // __syncthreads; nothing returns to the host.  FP64 throughout (the
@@ -266,7 +266,7 @@ __host__ __device__ inline int mg_smem_from(int N, int MMax, size_t budget_doubl
 }
 
 // mg_cycle (mg.F90:42-94) with ju = PSI, jrho = SRC; one CTA
-__global__ void __launch_bounds__(1024) k_mg_cycle(MgData dg, int smem_from, int *iters_out) {
+__global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, int *iters_out) {
     pdl_enter();
     __shared__ double sh[32];
     MgData d = dg;

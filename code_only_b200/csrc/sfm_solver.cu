@@ -1031,7 +1031,7 @@ public:
         const int F = H.FMax;
         int64_t N3 = (int64_t)NBc * NBc * NBc;
         run(OpMgGather<T>{mg.SRC, mg.PSI, rhs, u, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
-        launch_pdl(k_mg_cycle, 1, 1024, mgSmemBytes, mg, mgSmemFrom, d_mgit);
+        launch_pdl(k_mg_cycle, 1, 512, mgSmemBytes, mg, mgSmemFrom, d_mgit);
         ++launches;
         run(OpMgScatter<T>{u, mg.PSI, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
     }
