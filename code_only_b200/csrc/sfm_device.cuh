@@ -210,15 +210,17 @@ __device__ __forceinline__ T rstrct_linear(const T *uf, int G, int i0, int j0, i
           + uf[cidx(G, i0 + 1, j0 + 1, k0)] + uf[cidx(G, i0 + 1, j0, k0 + 1)]
           + uf[cidx(G, i0, j0 + 1, k0 + 1)] + uf[cidx(G, i0 + 1, j0 + 1, k0 + 1)]) * rdv;
 }
+// 1D weights {-1, 9, 9, -1} / 16 of the cubic restriction (exact in binary)
+__device__ __forceinline__ double rstrct_w(int i) { return (i == 0 || i == 3) ? -1.0 / 16.0 : 9.0 / 16.0; }
 template <class T>
 __device__ __forceinline__ T rstrct_cubic(const T *uf, int G, int i1, int j1, int k1) {
-    const double s1d[4] = {-1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0};
     T s = (T)0;
 #pragma unroll 1
     for (int kk = 0; kk < 4; kk++)
         for (int jj = 0; jj < 4; jj++)
             for (int ii = 0; ii < 4; ii++) {
-                T t = uf[cidx(G, i1 - 1 + ii, j1 - 1 + jj, k1 - 1 + kk)] * (T)((s1d[ii] * s1d[jj]) * s1d[kk]);
+                T t = uf[cidx(G, i1 - 1 + ii, j1 - 1 + jj, k1 - 1 + kk)] *
+                      (T)((rstrct_w(ii) * rstrct_w(jj)) * rstrct_w(kk));
                 s = (ii | jj | kk) ? s + t : t;
             }
     return s;

@@ -413,8 +413,15 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // been read, and the producer's latencies stay off the consumers' path.
 // Every mbarrier wait is bounded (kWaitPolls): a wait that gives up sets
 // *err, the warp leaves, and the producer stops issuing.
+// resident CTAs per SM the bulk ring's shared memory allows: the register
+// budget that leaves (at 4^3 blocks ptxas otherwise settles on 32 registers
+// and spills)
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
+__host__ __device__ constexpr int relax_bulk_min_ctas() {
+    return (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024) < 8 ? (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024) : 8;
+}
+template <class T, int N>
+__global__ void __launch_bounds__(256, relax_bulk_min_ctas<T, N>()) k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
                                                     const int32_t *__restrict__ blocks, int nblk,
                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
                                                     const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
