@@ -24,6 +24,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/sfmg.h"
@@ -206,6 +207,10 @@ public:
     virtual int64_t device_bytes() const = 0;
     virtual int fmg_levels() const = 0;
     std::string last_error;
+    // g written as [nblocks][3][ni^3] (block interiors only, no io ghost
+    // layers) instead of the caller's layout: the host-array entry point
+    // stages g this way
+    bool gCompact = false;
 };
 
 template <class T>
@@ -1177,7 +1182,9 @@ public:
         copy(0, PHI0, PSI0, true);
         converge_c2p(0, PHI0);
         poisson_flux(0, PHI0, false);
-        if (g) run(OpPsi2g{g, PHI0, d_skip, d_level, d_h0, d_rslot, rbuf[0], H.NI, Gf[0], gw, Vf[0]}, (int64_t)nb * H.NI * H.NI * H.NI);
+        if (g)
+            run(OpPsi2g{g, PHI0, d_skip, d_level, d_h0, d_rslot, rbuf[0], H.NI, Gf[0], gCompact ? 0 : gw, Vf[0]},
+                (int64_t)nb * H.NI * H.NI * H.NI);
         if (psi) run(OpRestore{psi, PHI0, H.NI, Gf[0], gw, Vf[0]}, (int64_t)nb * Vf[0]);
         cudaEventRecord(ev1, st_);
         double trr = 0.0;
@@ -1463,7 +1470,11 @@ struct sfm_ctx {
     sfm::SolverBase *s = nullptr;
     sfm_params p;
     int device = 0, nb = 0, ni = 0, ngh = 0;
-    double *d_rho = nullptr, *d_psi = nullptr, *d_g = nullptr;   // staging for host calls
+    double *d_rho = nullptr, *d_psi = nullptr;   // staging for host calls
+    double *d_gc = nullptr, *h_gc = nullptr;     // g interiors, device and pinned host staging
+    cudaStream_t cs = nullptr;                   // device-to-host copies of the outputs
+    static constexpr int kGChunks = 8;           // g leaves in chunks, each scattered as it lands
+    cudaEvent_t gev[kGChunks] = {};
     std::string err;
 };
 
@@ -1542,24 +1553,79 @@ int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g
     return c->s->solve(d_rho, d_psi, d_g, st, (cudaStream_t)stream, 0, nullptr);
 }
 
+// rows [row0, row1) of the g interiors [nblocks][3][ni^3] (a row = ni
+// values) into the caller's [nblocks][3][(ni+2g)^3], on up to 16 host
+// threads; the io ghost layers of the caller's array are not touched
+static void scatter_g_interiors(const double *src, double *g, int64_t row0, int64_t row1, int n, int gw) {
+    const int Gi = n + 2 * gw;
+    const int64_t Vi = (int64_t)Gi * Gi * Gi, rows = row1 - row0;
+    auto work = [=](int64_t r0, int64_t r1) {
+        r0 += row0;
+        r1 += row0;
+        for (int64_t r = r0; r < r1; r++) {
+            const int64_t bc = r / ((int64_t)n * n);
+            const int kj = (int)(r - bc * n * n), k = kj / n, j = kj - k * n;
+            std::memcpy(g + bc * Vi + ((int64_t)(k + gw) * Gi + (j + gw)) * Gi + gw, src + r * n,
+                        (size_t)n * sizeof(double));
+        }
+    };
+    const int64_t per = (int64_t)1 << 16;   // rows per thread at least
+    const int nt = (int)std::max<int64_t>(1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(),
+                                                                  rows / per}));
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(work, rows * t / nt, rows * (t + 1) / nt);
+    work(0, rows / nt);
+    for (auto &x : th) x.join();
+}
+
 int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
     if (!c || !c->s || !rho) return SFM_EINVAL;
     cudaSetDevice(c->device);
     int64_t n = io_elems(c);
     size_t bytes = (size_t)n * sizeof(double);
+    const size_t gbytes = (size_t)c->nb * 3 * c->ni * c->ni * c->ni * sizeof(double);
     if (!c->d_rho) {
-        if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess ||
-            cudaMalloc(&c->d_g, 3 * bytes) != cudaSuccess)
+        if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess)
             return SFM_ENOMEM;
+    }
+    if (g && !c->d_gc) {
+        if (cudaMalloc(&c->d_gc, gbytes) != cudaSuccess) return SFM_ENOMEM;
+        if (cudaMallocHost(&c->h_gc, gbytes) != cudaSuccess) {
+            c->h_gc = nullptr;
+            return SFM_ENOMEM;
+        }
     }
     if (cudaMemcpy(c->d_rho, rho, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA;
     if (psi) { if (cudaMemcpy(c->d_psi, psi, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA; }
-    // the solve writes g on block interiors only; the rest of the caller's array is kept
-    if (g) { if (cudaMemcpy(c->d_g, g, 3 * bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA; }
-    int rc = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, g ? c->d_g : nullptr, st, nullptr, 0, nullptr);
+    // g: the solve writes block interiors only, staged compact on the device
+    // and scattered into the caller's array on the host -- its io ghost
+    // layers keep the caller's values without a copy in
+    c->s->gCompact = true;
+    int rc = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, g ? c->d_gc : nullptr, st, nullptr, 0, nullptr);
+    c->s->gCompact = false;
     if (rc != SFM_OK && rc != SFM_ENOTCONVERGED) return rc;
     if (psi && cudaMemcpy(psi, c->d_psi, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return SFM_ECUDA;
-    if (g && cudaMemcpy(g, c->d_g, 3 * bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return SFM_ECUDA;
+    if (g) {
+        // chunk q is scattered on the host while chunks q+1.. are in flight
+        if (!c->cs) {
+            if (cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking) != cudaSuccess) return SFM_ECUDA;
+            for (auto &e : c->gev)
+                if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return SFM_ECUDA;
+        }
+        const int64_t rows = (int64_t)c->nb * 3 * c->ni * c->ni;
+        for (int q = 0; q < sfm_ctx::kGChunks; q++) {
+            const int64_t r0 = rows * q / sfm_ctx::kGChunks, r1 = rows * (q + 1) / sfm_ctx::kGChunks;
+            if (cudaMemcpyAsync(c->h_gc + r0 * c->ni, c->d_gc + r0 * c->ni, (size_t)(r1 - r0) * c->ni * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->cs) != cudaSuccess ||
+                cudaEventRecord(c->gev[q], c->cs) != cudaSuccess)
+                return SFM_ECUDA;
+        }
+        for (int q = 0; q < sfm_ctx::kGChunks; q++) {
+            const int64_t r0 = rows * q / sfm_ctx::kGChunks, r1 = rows * (q + 1) / sfm_ctx::kGChunks;
+            if (cudaEventSynchronize(c->gev[q]) != cudaSuccess) return SFM_ECUDA;
+            scatter_g_interiors(c->h_gc, g, r0, r1, c->ni, c->ngh);
+        }
+    }
     return rc;
 }
 
@@ -1574,7 +1640,11 @@ void sfm_destroy(sfm_ctx *c) {
     cudaSetDevice(c->device);
     if (c->d_rho) cudaFree(c->d_rho);
     if (c->d_psi) cudaFree(c->d_psi);
-    if (c->d_g) cudaFree(c->d_g);
+    if (c->d_gc) cudaFree(c->d_gc);
+    if (c->h_gc) cudaFreeHost(c->h_gc);
+    for (auto e : c->gev)
+        if (e) cudaEventDestroy(e);
+    if (c->cs) cudaStreamDestroy(c->cs);
     delete c->s;
     delete c;
 }
@@ -1612,20 +1682,15 @@ int sfm_debug_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_s
     cudaSetDevice(c->device);
     int64_t n = io_elems(c);
     size_t bytes = (size_t)n * sizeof(double);
+    if (stop_stage == 0) return sfm_solve(c, rho, psi, g, st);
     if (!c->d_rho) {
-        if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess ||
-            cudaMalloc(&c->d_g, 3 * bytes) != cudaSuccess)
+        if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess)
             return SFM_ENOMEM;
     }
     cudaMemcpy(c->d_rho, rho, bytes, cudaMemcpyHostToDevice);
     if (psi) cudaMemcpy(c->d_psi, psi, bytes, cudaMemcpyHostToDevice);
-    if (g) cudaMemcpy(c->d_g, g, 3 * bytes, cudaMemcpyHostToDevice);
-    int rc = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, g ? c->d_g : nullptr, st, nullptr, stop_stage, dump);
-    if (stop_stage == 0 && (rc == SFM_OK || rc == SFM_ENOTCONVERGED)) {
-        if (psi) cudaMemcpy(psi, c->d_psi, bytes, cudaMemcpyDeviceToHost);
-        if (g) cudaMemcpy(g, c->d_g, 3 * bytes, cudaMemcpyDeviceToHost);
-    }
-    return rc;
+    (void)g;   // an early stop writes no g
+    return c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, nullptr, st, nullptr, stop_stage, dump);
 }
 
 }  // extern "C"

@@ -133,6 +133,7 @@ int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out);
  *   psi [nblocks][(ni+2g)^3]   in: warm start U(MPSI) (fmg_data_if.F90:46), read on (-1:ni)^3
  *                              out: potential on (-1:ni)^3 (fmg_restore_u, fmg_data_if.F90:275-294)
  *   g   [nblocks][3][(ni+2g)^3] out: -grad phi on the interior (fmg_psi2g, fmg_poisson.F90:4-49);
+ *                              entries outside the interiors are left as they are;
  *                              may be NULL
  *   st  may be NULL.
  * Returns SFM_OK, or SFM_ENOTCONVERGED when the outer loop stopped early

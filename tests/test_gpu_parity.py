@@ -121,3 +121,32 @@ def test_nonfinite_density_is_an_error():
         psi = np.zeros_like(rho)
         rc = s.lib.sfm_solve(s.ctx, rho.ctypes.data, psi.ctypes.data, None, C.byref(st))
     assert rc == abi.SFM_ENONFINITE
+
+
+def test_host_g_writes_interiors_only():
+    """sfm_solve stages g compact on the device and scatters the interiors into
+    the caller's array: every io ghost entry keeps the caller's value, and the
+    interiors equal those of the device-array entry point (full layout)."""
+    import torch
+    h = w.small_periodic(2, 8, 3, 1)
+    p = abi.default_params(abi.SFM_BC_PERIODIC)
+    rho = w.block_field(h, p.ngh_io, w.gaussian_peak)
+    with FMGPoisson(h, params=p) as s:
+        G = s.G
+        sentinel = 12345.0
+        g_host = np.full((h.nblocks, 3, G, G, G), sentinel)
+        psi = np.zeros_like(rho)
+        rc = s.lib.sfm_solve(s.ctx, rho.ctypes.data, psi.ctypes.data, g_host.ctypes.data, None)
+        assert rc == abi.SFM_OK
+        rho_d = torch.from_numpy(rho).cuda()
+        psi_d = torch.zeros_like(rho_d)
+        g_d = torch.full((h.nblocks, 3, G, G, G), -1.0, dtype=torch.float64, device="cuda")
+        s.solve_device(rho_d.data_ptr(), psi_d.data_ptr(), g_d.data_ptr())
+        torch.cuda.synchronize()
+        g_dev = g_d.cpu().numpy()
+    n, gw = h.ni, p.ngh_io
+    inner = np.zeros((G, G, G), dtype=bool)
+    inner[gw:gw + n, gw:gw + n, gw:gw + n] = True
+    assert np.all(g_host[:, :, ~inner] == sentinel)
+    assert np.array_equal(g_host[:, :, inner], g_dev[:, :, inner])
+    assert np.array_equal(psi, psi_d.cpu().numpy())
