@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(256) k_exec(const __grid_constant__ ExecArgs<T
                 // cells spread over the whole grid: a phase is small
                 const int nc0 = ph.count0 * G * G, nthr = (int)(gridDim.x * blockDim.x);
                 const int gt = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-                for (int b0 = 0; b0 < nc0; b0 += nthr * kGhostK)
+                for (int b0 = 0; b0 < nc0; b0 += nthr * ghost_k<N>())
                     ghost_copy<T, N>(a.u, a.faces + ph.first, nc0, ph.dir, b0 + gt, nthr);
                 const FaceItem *f1 = a.faces + ph.first + ph.count0;
                 for (int it = warp; it < ph.count - ph.count0; it += nwarps)

@@ -120,13 +120,18 @@ __device__ __forceinline__ void ghost_face(T *u, const FaceItem &fi, int dir, bo
 // offset (x+1) sd + (p+1) sa + (q+1) sb with the pass direction's strides.
 // A thread serves K cells `stride` apart and issues its K item loads, then
 // its K value loads, then its K stores: the gather is latency-bound, and
-// HBM only fills with several round trips in flight per thread (K = 4
-// measured faster than 8, and than fewer cells per thread on small passes;
-// K is a compile-time constant -- a run-time count measured slower).
+// HBM only fills with several round trips in flight per thread (K =
+// ghost_k<N>(); fewer cells per thread measured slower, also on small
+// passes, and K is a compile-time constant -- a run-time count measured
+// slower).
 constexpr int kGhostK = 4;
+// from 8^3 blocks on (faces of >= 100 cells, passes of megabytes) eight
+// cells per thread measured faster; below, four
+template <int N>
+__host__ __device__ constexpr int ghost_k() { return N >= 8 ? 8 : kGhostK; }
 template <class T, int N>
 __device__ __forceinline__ void ghost_copy(T *u, const FaceItem *items, int ncell, int dir, int g0, int stride) {
-    constexpr int G = N + 2, NC = G * G, K = kGhostK;
+    constexpr int G = N + 2, NC = G * G, K = ghost_k<N>();
     constexpr int64_t V = (int64_t)G * G * G;
     const int sd = dir == 0 ? 1 : (dir == 1 ? G : G * G);
     const int sa = dir == 0 ? G : 1;
@@ -162,7 +167,7 @@ __device__ __forceinline__ void ghost_copy(T *u, const FaceItem *items, int ncel
 // side by side.
 template <int N>
 __host__ __device__ constexpr int ghost_copy_ctas(int n0) {
-    return (int)(((int64_t)n0 * (N + 2) * (N + 2) + 256 * kGhostK - 1) / (256 * kGhostK));
+    return (int)(((int64_t)n0 * (N + 2) * (N + 2) + 256 * ghost_k<N>() - 1) / (256 * ghost_k<N>()));
 }
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_ghost_faces(T *u, const FaceItem *__restrict__ items0, int n0,
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(256) k_ghost_faces(T *u, const FaceItem *__res
     constexpr int G = N + 2, NB2 = N / 2, LN = ghost_lanes<N>();
     const int nb0 = ghost_copy_ctas<N>(n0);
     if ((int)blockIdx.x < nb0) {
-        ghost_copy<T, N>(u, items0, n0 * G * G, dir, (int)blockIdx.x * 256 * kGhostK + (int)threadIdx.x, 256);
+        ghost_copy<T, N>(u, items0, n0 * G * G, dir, (int)blockIdx.x * 256 * ghost_k<N>() + (int)threadIdx.x, 256);
         return;
     }
     __shared__ GhostCubicTable<N> tab;
