@@ -618,6 +618,9 @@ __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const
 // one fmg level coarser (N/2 + 2 cells with ghosts), tricubic staged as
 // interp_tricubic stages bufx / bufxy (interpolation.F90:98-217), or trilinear
 // ---------------------------------------------------------------------------
+// blocks per CTA of k_interp_tiled: at least 512 fine cells per CTA
+template <int N>
+__host__ __device__ constexpr int interp_bpc() { return N * N * N >= 512 ? 1 : 512 / (N * N * N); }
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const T *__restrict__ uc,
                                                       const int32_t *__restrict__ blocks, int nblk, int cubic) {
@@ -625,51 +628,64 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
     constexpr int NC = N / 2, GC = NC + 2, GF = N + 2;
     constexpr int VC = GC * GC * GC, VF = GF * GF * GF;
     constexpr int W = GC;                  // coarse extent with ghosts = interp range [-1, NC]
-    __shared__ T sc[VC];
-    __shared__ T bx[N * W * W];            // [kc][jc][i]
-    __shared__ T bxy[N * N * W];           // [kc][j][i]
+    constexpr int IB = interp_bpc<N>(), BX = N * W * W, BXY = N * N * W, NF = N * N * N;
+    __shared__ T sc[IB * VC];
+    __shared__ T bx[IB * BX];              // per block [kc][jc][i]
+    __shared__ T bxy[IB * BXY];            // per block [kc][j][i]
+    __shared__ int sb[IB];
     // Lagrange nodes and weights of fine index p (the same for x, y and z):
     // cubic_weights evaluated once per CTA instead of once per staged value
     __shared__ int cwc[N][4];
     __shared__ double cww[N][4];
-    const int b = blocks[blockIdx.x];
-    (void)nblk;
-    for (int t = threadIdx.x; t < VC; t += blockDim.x) sc[t] = uc[(int64_t)b * VC + t];
+    const int q0 = blockIdx.x * IB;
+    const int nq = nblk - q0 < IB ? nblk - q0 : IB;
+    if ((int)threadIdx.x < nq) sb[threadIdx.x] = blocks[q0 + threadIdx.x];
     if (threadIdx.x < N) cubic_weights((int)threadIdx.x, -1, NC, cwc[threadIdx.x], cww[threadIdx.x]);
     __syncthreads();
-    T *ufb = uf + (int64_t)b * VF;
+    for (int t = threadIdx.x; t < nq * VC; t += blockDim.x) {
+        const int q = t / VC;
+        sc[t] = uc[(int64_t)sb[q] * VC + (t - q * VC)];
+    }
+    __syncthreads();
     if (!(cubic && NC + 2 >= 4)) {
-        for (int t = threadIdx.x; t < N * N * N; t += blockDim.x) {
-            const int i = t % N, j = (t / N) % N, k = t / (N * N);
-            ufb[cidx(GF, i, j, k)] = trilinear_cell(sc, GC, i, j, k, 0, 0, 0);
+        for (int t = threadIdx.x; t < nq * NF; t += blockDim.x) {
+            const int q = t / NF, r = t - q * NF;
+            const int i = r % N, j = (r / N) % N, k = r / (N * N);
+            uf[(int64_t)sb[q] * VF + cidx(GF, i, j, k)] = trilinear_cell(sc + q * VC, GC, i, j, k, 0, 0, 0);
         }
         return;
     }
     // x: bx(i, jc, kc) for kc, jc in [-1, NC]
-    for (int t = threadIdx.x; t < N * W * W; t += blockDim.x) {
-        const int i = t % N, jc = (t / N) % W - 1, kc = t / (N * W) - 1;
+    for (int t = threadIdx.x; t < nq * BX; t += blockDim.x) {
+        const int q = t / BX, r = t - q * BX;
+        const int i = r % N, jc = (r / N) % W - 1, kc = r / (N * W) - 1;
         const int *c = cwc[i];
         const double *w = cww[i];
-        const T *row = sc + cidx(GC, 0, jc, kc);
+        const T *row = sc + q * VC + cidx(GC, 0, jc, kc);
         bx[t] = (T)w[0] * row[c[0]] + (T)w[1] * row[c[1]] + (T)w[2] * row[c[2]] + (T)w[3] * row[c[3]];
     }
     __syncthreads();
     // y: bxy(i, j, kc)
-    for (int t = threadIdx.x; t < N * N * W; t += blockDim.x) {
-        const int i = t % N, j = (t / N) % N, kc = t / (N * N) - 1;
+    for (int t = threadIdx.x; t < nq * BXY; t += blockDim.x) {
+        const int q = t / BXY, r = t - q * BXY;
+        const int i = r % N, j = (r / N) % N, kc = r / (N * N) - 1;
         const int *c = cwc[j];
         const double *w = cww[j];
-        auto X = [&](int jc) { return bx[((kc + 1) * W + (jc + 1)) * N + i]; };
+        const T *bq = bx + q * BX;
+        auto X = [&](int jc) { return bq[((kc + 1) * W + (jc + 1)) * N + i]; };
         bxy[t] = (T)w[0] * X(c[0]) + (T)w[1] * X(c[1]) + (T)w[2] * X(c[2]) + (T)w[3] * X(c[3]);
     }
     __syncthreads();
     // z
-    for (int t = threadIdx.x; t < N * N * N; t += blockDim.x) {
-        const int i = t % N, j = (t / N) % N, k = t / (N * N);
+    for (int t = threadIdx.x; t < nq * NF; t += blockDim.x) {
+        const int q = t / NF, r = t - q * NF;
+        const int i = r % N, j = (r / N) % N, k = r / (N * N);
         const int *c = cwc[k];
         const double *w = cww[k];
-        auto Y = [&](int kc) { return bxy[((kc + 1) * N + j) * N + i]; };
-        ufb[cidx(GF, i, j, k)] = (T)w[0] * Y(c[0]) + (T)w[1] * Y(c[1]) + (T)w[2] * Y(c[2]) + (T)w[3] * Y(c[3]);
+        const T *bq = bxy + q * BXY;
+        auto Y = [&](int kc) { return bq[((kc + 1) * N + j) * N + i]; };
+        uf[(int64_t)sb[q] * VF + cidx(GF, i, j, k)] =
+            (T)w[0] * Y(c[0]) + (T)w[1] * Y(c[1]) + (T)w[2] * Y(c[2]) + (T)w[3] * Y(c[3]);
     }
 }
 

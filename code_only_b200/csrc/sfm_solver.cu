@@ -920,7 +920,8 @@ public:
         boundary_extrap(lc, uc);
         const int n = nf[f];
         SFM_WITH_N(n,
-                   (launch_pdl(k_interp_tiled<T, N>, (unsigned)nLeaves, 256, 0, uf, uc, d_leaves, nLeaves, cubic ? 1 : 0),
+                   (launch_pdl(k_interp_tiled<T, N>, (unsigned)((nLeaves + interp_bpc<N>() - 1) / interp_bpc<N>()), 256, 0, uf,
+                               uc, d_leaves, nLeaves, cubic ? 1 : 0),
                     ++launches),
                    run(OpInterp<T>{uf, uc, d_leaves, n, Gf[f], Gf[lc], Vf[f], Vf[lc], cubic ? 1 : 0},
                        (int64_t)nLeaves * n * n * n))
