@@ -272,8 +272,7 @@ struct RelaxTileSmem {
 
 // one colour over tiles tile0, tile0 + tstride, ... of BPC consecutive listed
 // blocks: each block with its ghost shell staged in shared memory, updated,
-// interior rows written back; |resh2| folded into m.  u and rbuf are plain
-// pointers: inside k_exec earlier phases of the same launch write them.
+// interior rows written back; |resh2| folded into m.
 template <class T, int N>
 __device__ __forceinline__ void relax_tiles(RelaxTileSmem<T, N> &sm, T *u, const T *__restrict__ rhs,
                                             const int32_t *__restrict__ blocks, int nblk,

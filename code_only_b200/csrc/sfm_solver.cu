@@ -34,7 +34,6 @@
 #include "sfm_fast.cuh"
 #include "sfm_noalloc.cuh"
 #include "sfm_adjoint.cuh"
-#include "sfm_exec.cuh"
 
 namespace sfm {
 
@@ -475,11 +474,7 @@ public:
         d_bad = mem.alloc<int>(1);
         d_err = mem.alloc<int>(1);
         zeroList.push_back({d_err, sizeof(int)});
-        d_gb = mem.alloc<GridBarrier>(1);
-        zeroList.push_back({d_gb, sizeof(GridBarrier)});
         for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], (void)bulk_grid<N>(), (void)0);
-        (void)exec_grid<2>();
-        (void)exec_grid<4>();
         d_mom = mem.alloc<double>(32);
         d_part = mem.alloc<double>((size_t)(H.lstart[1]) * 25);
         d_psum = mem.alloc<double>((size_t)nb);
@@ -530,10 +525,12 @@ public:
 
     // -----------------------------------------------------------------
     // launch helpers
-    // Every kernel of the solve starts with pdl_enter(), so each launch may
-    // carry a programmatic dependency on the previous kernel of the stream:
-    // it is scheduled while that one drains.  (The cooperative k_exec never
-    // does: it needs all of its CTAs co-resident.)
+    // Every kernel of the solve starts with pdl_enter(), so each launch
+    // carries a programmatic dependency on the previous kernel of the
+    // stream: it is scheduled while that one drains.  (Chained this way,
+    // separate launches measured faster than one cooperative launch per
+    // small-level relax with grid barriers between its phases: nested5 89
+    // -> 67 ms.)
     template <class... KArgs, class... Args>
     void launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, Args... args) {
         cudaLaunchConfig_t cfg = {};
@@ -655,7 +652,6 @@ public:
     // -----------------------------------------------------------------
     // fmg level operations on the inner fields
     void relax(int f, T *u, T *rhs, bool bf0, int slot) {   // fmg_poisson_relax
-        if (relax_exec(f, u, rhs, bf0, slot)) return;
         cudaMemsetAsync(d_max + slot, 0, sizeof(unsigned long long), st_);
         const int n = nf[f];
         for (int ipass = 1; ipass <= 2; ipass++) {
@@ -704,117 +700,6 @@ public:
                     ++launches),
                    runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
                           (int64_t)nblk * n * n * n / 2, out))
-    }
-    // -----------------------------------------------------------------
-    // small fmg levels: a whole relax (both colours with their converge,
-    // ghost passes, boundary fill and reflux) as one cooperative k_exec launch
-    // -----------------------------------------------------------------
-    GridBarrier *d_gb = nullptr;
-    int execGrid[3] = {0, 0, 0};   // CTAs of k_exec<T, N>: N = 2 -> [1], N = 4 -> [2]
-    template <int N>
-    int exec_grid() {
-        constexpr int li = N == 2 ? 1 : 2;
-        if (!execGrid[li]) {
-            int per = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_exec<T, N>, 256, 0) != cudaSuccess || per < 1) {
-                cudaGetLastError();
-                per = 1;
-            }
-            execGrid[li] = nSM * std::min(per, 2);   // more CTAs measured slower: barrier cost
-        }
-        return execGrid[li];
-    }
-    template <int N>
-    void exec_launch(const ExecArgs<T> &a) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)exec_grid<N>());
-        cfg.blockDim = dim3(256);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = st_;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, k_exec<T, N>, a);
-        ++launches;
-    }
-    ExecArgs<T> exec_args(T *u, const T *rhs, int f, const int32_t *blocks, int nblk, const int32_t *rslot,
-                          unsigned long long *out) {
-        ExecArgs<T> a;
-        std::memset(&a, 0, sizeof(a));
-        a.u = u; a.rhs = rhs; a.parent = d_parent; a.oct = d_oct; a.faces = d_faces; a.bfaces = d_tfL;
-        a.reflux = d_reflux; a.rbuf = rbuf[f]; a.h0 = d_h0; a.level = d_level; a.blocks = blocks; a.nblk = nblk;
-        a.rslot = rslot; a.f = f; a.out = out; a.err = d_err; a.gb = d_gb; a.nphase = 0;
-        return a;
-    }
-    // A cooperative launch holds only its co-resident CTAs, so a phase walks its items
-    // with far fewer warps than a launch of its own would: worth it only
-    // while every phase is small enough to be latency-bound.
-    static constexpr int64_t kExecMaxItems = 8192;
-    int64_t execMaxItems = kExecMaxItems;
-    bool exec_add(ExecArgs<T> &a, int8_t kind, int dir, int sel, int cubic, int64_t first, int64_t count,
-                  int ipass = 0) {
-        if (a.nphase >= kMaxPhases || count > execMaxItems) return false;
-        ExecPhase &p = a.ph[a.nphase++];
-        p.kind = kind; p.dir = (int8_t)dir; p.sel = (int8_t)sel; p.cubic = (int8_t)cubic;
-        p.first = (int32_t)first; p.count = (int32_t)count; p.ipass = ipass; p.count0 = 0;
-        return true;
-    }
-    // ghost pass of (L, dir): same-level items, then coarse-fine ones unless same_only
-    bool exec_ghost(ExecArgs<T> &a, int L, int dir, bool same_only) {
-        const int k = L * 3 + dir;
-        const int64_t o = faceOff[k], n0 = faceSplit[k] - o, c = same_only ? n0 : faceOff[k + 1] - o;
-        if (!c) return true;
-        if (!exec_add(a, PH_GHOST, dir, -1, 0, o, c)) return false;
-        a.ph[a.nphase - 1].count0 = (int32_t)n0;
-        return true;
-    }
-    // fmg_poisson_relax on level f (blocks of 2^3 or 4^3): the phases of
-    // poisson_flux (converge finest -> coarsest, ghost passes per level and
-    // direction, boundary fill, reflux) and the colour sweep, twice.  False
-    // (nothing launched, FmgLevel_fill0 untouched) when the program does not fit.
-    bool relax_exec(int f, T *u, T *rhs, bool bf0, int slot) {
-        const int n = nf[f];
-        if (n != 2 && n != 4) return false;
-        ExecArgs<T> a = exec_args(u, rhs, f, d_leaves, nLeaves, d_rslot, d_max + slot);
-        int fill0 = FmgLevel_fill0;
-        bool ok = true;
-        for (int ipass = 1; ipass <= 2; ipass++) {
-            if (fill0 != f) {
-                for (int Lc = H.nlev - 2; Lc >= 0; Lc--)
-                    if (cnt(Lc + 1)) ok = ok && exec_add(a, PH_CONVERGE, 0, -1, 0, H.lstart[Lc + 1], cnt(Lc + 1));
-                for (int L = 0; L < H.nlev; L++)
-                    for (int dir = 0; dir < 3; dir++) ok = ok && exec_ghost(a, L, dir, false);
-                if (bf0 && tfLOff[H.nlev] > 0) ok = ok && exec_add(a, PH_FILL0, 0, -1, 0, 0, tfLOff[H.nlev]);
-            }
-            fill0 = Undef;
-            if (nReflux) ok = ok && exec_add(a, PH_REFLUX, 0, -1, 0, 0, nReflux);
-            ok = ok && exec_add(a, PH_RELAX, 0, -1, 0, 0, nLeaves, ipass);
-        }
-        if (!ok) return false;
-        FmgLevel_fill0 = Undef;
-        cudaMemsetAsync(d_max + slot, 0, sizeof(unsigned long long), st_);
-        if (n == 2) exec_launch<2>(a);
-        else exec_launch<4>(a);
-        return true;
-    }
-    // vmg_poisson_relax on AMR level L (vmg_ghostcell then a colour, twice)
-    bool vmg_relax_exec(int L, T *u, const T *rhs) {
-        const int F = H.FMax, n = nf[F];
-        if (n != 2 && n != 4) return false;
-        ExecArgs<T> a = exec_args(u, rhs, F, d_all + H.lstart[L], cnt(L), nullptr, d_max + 1);
-        bool ok = true;
-        for (int ipass = 1; ipass <= 2; ipass++) {
-            for (int dir = 0; dir < 3; dir++) ok = ok && exec_ghost(a, L, dir, true);
-            const int64_t o = tfLOff[L], c = tfLOff[L + 1] - o;
-            if (c) ok = ok && exec_add(a, PH_FILL0, 0, -1, 0, o, c);
-            ok = ok && exec_add(a, PH_RELAX, 0, -1, 0, 0, cnt(L), ipass);
-        }
-        if (!ok) return false;
-        if (n == 2) exec_launch<2>(a);
-        else exec_launch<4>(a);
-        return true;
     }
     int check_err() {
         int e = 0;
@@ -977,7 +862,6 @@ public:
         boundary_fill0_level(L, F, u);
     }
     void vmg_relax(int L, T *u, const T *rhs) {
-        if (vmg_relax_exec(L, u, rhs)) return;
         const int F = H.FMax, n = nf[F];
         for (int ipass = 1; ipass <= 2; ipass++) {
             vmg_ghostcell(L, u);
