@@ -928,12 +928,13 @@ public:
     // vmg_fas (vmg.F90:116-243); jrho = IRHS when copy_rhs (second and later calls)
     void vmg_fas(bool copy_rhs) {
         const int F = H.FMax, nlev = H.nlev;
-        if (copy_rhs)
-            for (int L = 0; L < nlev; L++) vmg_copy_level(L, RHO[F], RHS[F]);
+        // the level lists are consecutive ranges of d_all: the per-level
+        // copies of vmg_fas are one launch over all blocks
+        if (copy_rhs) runB(OpCopy<T, T>{RHO[F], RHS[F], d_all, Vf[F]}, H.nb);
         converge_c2p(F, U[F]);
         converge_c2p(F, RHO[F]);
         boundary_fill0(F, U[F]);
-        for (int L = 0; L < nlev; L++) vmg_copy_level(L, RHS[F], RHO[F]);
+        runB(OpCopy<T, T>{RHS[F], RHO[F], d_all, Vf[F]}, H.nb);
         for (int v = nlev - 1; v >= 1; v--) {
             vmg_gridboundary(v, U[F]);
             for (int q = 0; q < 2; q++) vmg_relax(v, U[F], RHS[F]);
