@@ -1393,7 +1393,23 @@ void sfm_default_params(sfm_params *p) {
     p->profile = 0;
 }
 
-int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out) {
+// No C++ exception may cross the C ABI: every entry point below runs its
+// body under sfm_guard, which turns an exception into an error code
+// (SFM_ENOMEM for a failed host allocation).
+extern "C++" {
+template <class F>
+static int sfm_guard(F &&body) {
+    try {
+        return body();
+    } catch (const std::bad_alloc &) {
+        return SFM_ENOMEM;
+    } catch (...) {
+        return SFM_ECUDA;
+    }
+}
+}
+
+static int create_impl(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out) {
     if (!h || !p || !out) return SFM_EINVAL;
     *out = nullptr;
     if (p->ngh_io < 1 || p->max_outer < 0 || p->max_outer > 1000 || !(p->rel_tol >= 0) ||
@@ -1407,25 +1423,28 @@ int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out) {
     }
     int rc = check_device();
     if (rc) return rc;
-    sfm_ctx *c = new (std::nothrow) sfm_ctx();
-    if (!c) return SFM_ENOMEM;
+    std::unique_ptr<sfm_ctx> c(new sfm_ctx());
     c->p = *p;
     cudaGetDevice(&c->device);
+    std::unique_ptr<sfm::SolverBase> s;
     if (p->precision == SFM_PREC_FP64) {
-        auto *s = new (std::nothrow) sfm::Solver<double>();
-        if (!s) { delete c; return SFM_ENOMEM; }
-        rc = s->init(h, p);
-        c->s = s;
+        auto *sd = new sfm::Solver<double>();
+        s.reset(sd);
+        rc = sd->init(h, p);
     } else {
-        auto *s = new (std::nothrow) sfm::Solver<float>();
-        if (!s) { delete c; return SFM_ENOMEM; }
-        rc = s->init(h, p);
-        c->s = s;
+        auto *sf = new sfm::Solver<float>();
+        s.reset(sf);
+        rc = sf->init(h, p);
     }
-    if (rc) { delete c->s; delete c; return rc; }
+    if (rc) return rc;
+    c->s = s.release();
     c->nb = h->nblocks; c->ni = h->ni; c->ngh = p->ngh_io;
-    *out = c;
+    *out = c.release();
     return SFM_OK;
+}
+
+int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out) {
+    return sfm_guard([&] { return create_impl(h, p, out); });
 }
 
 static int64_t io_elems(const sfm_ctx *c) {
@@ -1436,7 +1455,7 @@ static int64_t io_elems(const sfm_ctx *c) {
 int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g, sfm_stats *st, void *stream) {
     if (!c || !c->s || !d_rho) return SFM_EINVAL;
     cudaSetDevice(c->device);
-    return c->s->solve(d_rho, d_psi, d_g, st, (cudaStream_t)stream, 0, nullptr);
+    return sfm_guard([&] { return c->s->solve(d_rho, d_psi, d_g, st, (cudaStream_t)stream, 0, nullptr); });
 }
 
 // rows [row0, row1) of the g interiors [nblocks][3][ni^3] (a row = ni
@@ -1459,12 +1478,17 @@ static void scatter_g_interiors(const double *src, double *g, int64_t row0, int6
     const int nt = (int)std::max<int64_t>(1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(),
                                                                   rows / per}));
     std::vector<std::thread> th;
-    for (int t = 1; t < nt; t++) th.emplace_back(work, rows * t / nt, rows * (t + 1) / nt);
+    int t = 1;
+    try {
+        for (; t < nt; t++) th.emplace_back(work, rows * t / nt, rows * (t + 1) / nt);
+    } catch (...) {   // no thread to be had: the rest on this one (nothing may leave the C ABI)
+        work(rows * t / nt, rows);
+    }
     work(0, rows / nt);
     for (auto &x : th) x.join();
 }
 
-int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
+static int solve_impl(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
     if (!c || !c->s || !rho) return SFM_EINVAL;
     cudaSetDevice(c->device);
     int64_t n = io_elems(c);
@@ -1515,10 +1539,14 @@ int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *
     return rc;
 }
 
+int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
+    return sfm_guard([&] { return solve_impl(c, rho, psi, g, st); });
+}
+
 int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st) {
     if (!c || !c->s || !dJ_dphi || !dJ_drho) return SFM_EINVAL;
     cudaSetDevice(c->device);
-    return c->s->adjoint(dJ_dphi, dJ_drho, st, nullptr);
+    return sfm_guard([&] { return c->s->adjoint(dJ_dphi, dJ_drho, st, nullptr); });
 }
 
 void sfm_destroy(sfm_ctx *c) {
@@ -1576,7 +1604,8 @@ int sfm_debug_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_s
     cudaMemcpy(c->d_rho, rho, bytes, cudaMemcpyHostToDevice);
     if (psi) cudaMemcpy(c->d_psi, psi, bytes, cudaMemcpyHostToDevice);
     (void)g;   // an early stop writes no g
-    return c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, nullptr, st, nullptr, stop_stage, dump);
+    return sfm_guard(
+        [&] { return c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, nullptr, st, nullptr, stop_stage, dump); });
 }
 
 }  // extern "C"
