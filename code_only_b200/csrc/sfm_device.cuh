@@ -215,9 +215,11 @@ __device__ __forceinline__ double rstrct_w(int i) { return (i == 0 || i == 3) ? 
 template <class T>
 __device__ __forceinline__ T rstrct_cubic(const T *uf, int G, int i1, int j1, int k1) {
     T s = (T)0;
-#pragma unroll 1
+#pragma unroll
     for (int kk = 0; kk < 4; kk++)
+#pragma unroll
         for (int jj = 0; jj < 4; jj++)
+#pragma unroll
             for (int ii = 0; ii < 4; ii++) {
                 T t = uf[cidx(G, i1 - 1 + ii, j1 - 1 + jj, k1 - 1 + kk)] *
                       (T)((rstrct_w(ii) * rstrct_w(jj)) * rstrct_w(kk));

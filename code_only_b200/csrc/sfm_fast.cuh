@@ -617,9 +617,11 @@ __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const
 // one fmg level coarser (N/2 + 2 cells with ghosts), tricubic staged as
 // interp_tricubic stages bufx / bufxy (interpolation.F90:98-217), or trilinear
 // ---------------------------------------------------------------------------
-// blocks per CTA of k_interp_tiled: at least 512 fine cells per CTA
+// blocks per CTA of k_interp_tiled: at least 512 fine cells per CTA, and
+// four 8^3 blocks (the per-CTA weights, load and three barriers amortised
+// over more cells measured faster)
 template <int N>
-__host__ __device__ constexpr int interp_bpc() { return N * N * N >= 512 ? 1 : 512 / (N * N * N); }
+__host__ __device__ constexpr int interp_bpc() { return N == 8 ? 4 : (N * N * N >= 512 ? 1 : 512 / (N * N * N)); }
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const T *__restrict__ uc,
                                                       const int32_t *__restrict__ blocks, int nblk, int cubic) {
