@@ -424,8 +424,14 @@ template <class T, int N>
 __host__ __device__ constexpr int relax_bulk_min_ctas() {
     return (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024) < 8 ? (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024) : 8;
 }
+// threads of k_relax_bulk: warp 0 produces, the others consume.  A 16^3
+// block's stages allow only one or two CTAs per SM, so those CTAs get 15
+// consumer warps instead of 7.
+template <int N>
+__host__ __device__ constexpr int relax_bulk_threads() { return N >= 16 ? 512 : 256; }
 template <class T, int N>
-__global__ void __launch_bounds__(256, relax_bulk_min_ctas<T, N>()) k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
+__global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T, N>())
+    k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
                                                     const int32_t *__restrict__ blocks, int nblk,
                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
                                                     const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
@@ -434,7 +440,7 @@ __global__ void __launch_bounds__(256, relax_bulk_min_ctas<T, N>()) k_relax_bulk
     using Tl = Tile<N>;
     using Pl = BulkPlan<T, N>;
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2, S = Pl::S;
-    constexpr int NCW = 7, NCT = 32 * NCW;   // consumer warps / threads
+    constexpr int NCW = relax_bulk_threads<N>() / 32 - 1, NCT = 32 * NCW;   // consumer warps / threads
     constexpr uint32_t BB = (uint32_t)(V * sizeof(T));
     constexpr int LO = Pl::LO;
     constexpr uint32_t SB = (uint32_t)(Pl::SPAN * sizeof(T));

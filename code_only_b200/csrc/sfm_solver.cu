@@ -676,7 +676,8 @@ public:
             // opt in whatever the size: static and dynamic shared memory together may pass 48 KB
             cudaFuncSetAttribute(k_relax_bulk<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             int per = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N>, 256, smem) != cudaSuccess ||
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N>, relax_bulk_threads<N>(), smem) !=
+                    cudaSuccess ||
                 per < 1) {
                 cudaGetLastError();
                 per = 1;
@@ -692,7 +693,8 @@ public:
         SFM_WITH_N(n,
                    (bulk_ok<N>() ? launch_pdl(k_relax_bulk<T, N>,
                                               (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N>()),
-                                              256, BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0, d_level, rslot,
+                                              relax_bulk_threads<N>(), BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0,
+                                              d_level, rslot,
                                               rb, f, ipass, out, d_err)
                                  : launch_pdl(k_relax_tiled<T, N>,
                                               (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
