@@ -665,12 +665,13 @@ public:
     // persistent grid of k_relax_bulk<T, N> (N >= 4): every SM filled to the
     // kernel's occupancy; computed once, at set-up, outside stream capture
     // the bulk pipeline serves blocks of 4^3 and up whose stages fit in 220 KB
+    // (on 2^3 blocks it measured slower than k_relax_tiled)
     template <int N>
     static constexpr bool bulk_ok() { return N >= 4 && BulkPlan<T, N>::SMEM <= 220 * 1024; }
     template <int N>
     int bulk_grid() {
         if (!bulk_ok<N>()) return 0;
-        constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : 2);
+        constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : (N >= 4 ? 2 : 1));   // log2(N), capped
         if (!bulkGrid[li]) {
             const int smem = BulkPlan<T, N>::SMEM;
             // opt in whatever the size: static and dynamic shared memory together may pass 48 KB
