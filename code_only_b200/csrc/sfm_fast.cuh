@@ -203,11 +203,11 @@ struct Tile {
     static constexpr int BPC = CELLS >= 512 ? 1 : 512 / CELLS;
 };
 
-template <class T, int N>
+template <class T, int N, int BPCX = Tile<N>::BPC>
 __device__ __forceinline__ void stage_blocks(T *sh, const T *u, const int32_t *__restrict__ blocks,
                                              int first, int nblk) {
     using Tl = Tile<N>;
-    for (int t = threadIdx.x; t < Tl::BPC * Tl::V; t += blockDim.x) {
+    for (int t = threadIdx.x; t < BPCX * Tl::V; t += blockDim.x) {
         const int q = t / Tl::V, r = t - q * Tl::V;
         if (first + q < nblk) sh[t] = u[(int64_t)blocks[first + q] * Tl::V + r];
     }
@@ -578,6 +578,10 @@ __global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T
 }
 
 // residual res = rhs - div F / h on listed blocks (fmg_poisson_resid)
+// blocks per CTA of k_resid_tiled: two 8^3 blocks (1024 cells) measured
+// faster than one
+template <int N>
+__host__ __device__ constexpr int resid_bpc() { return N == 8 ? 2 : Tile<N>::BPC; }
 template <class TU, class TR, class TO, int N>
 __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const TU *__restrict__ u,
                                                      const TR *__restrict__ rhs, const int32_t *__restrict__ blocks,
@@ -586,14 +590,14 @@ __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const
                                                      const double *__restrict__ rbuf, int f) {
     pdl_enter();
     using Tl = Tile<N>;
-    constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC;
+    constexpr int G = Tl::G, V = Tl::V, BPC = resid_bpc<N>();
     __shared__ TU sh[BPC * V];
     __shared__ int ssl[BPC][6];
     __shared__ int sbid[BPC];
     __shared__ TU shi[BPC];
     __shared__ int8_t hasr[BPC];   // a face of the block takes a reflux flux
     const int first = blockIdx.x * BPC;
-    stage_blocks<TU, N>(sh, u, blocks, first, nblk);
+    stage_blocks<TU, N, BPC>(sh, u, blocks, first, nblk);
     if (threadIdx.x < BPC && first + (int)threadIdx.x < nblk) {   // per-block data, once per block
         const int q = threadIdx.x, b = blocks[first + q];
         int any = 0;

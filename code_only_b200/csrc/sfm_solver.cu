@@ -773,7 +773,7 @@ public:
         poisson_flux(f, u, bf0);
         const int n = nf[f];
         SFM_WITH_N(n,
-                   (launch_pdl(k_resid_tiled<TU, TR, TO, N>, (unsigned)((nLeaves + Tile<N>::BPC - 1) / Tile<N>::BPC),
+                   (launch_pdl(k_resid_tiled<TU, TR, TO, N>, (unsigned)((nLeaves + resid_bpc<N>() - 1) / resid_bpc<N>()),
                                256, 0, res, u, rhs, d_leaves, nLeaves, d_h0, d_level, d_rslot, rbuf[f], f),
                     ++launches),
                    run(OpResid<TU, TR, TO>{res, u, rhs, d_leaves, d_h0, d_level, d_rslot, rbuf[f], f, n, Gf[f], Vf[f]},
