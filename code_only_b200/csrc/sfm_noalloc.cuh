@@ -86,6 +86,21 @@ __global__ void __launch_bounds__(1024) k_mg_uniform_noalloc(MgData d, const dou
     const int n = d.N, G = n + 2, n3 = n * n * n;
     // every array read below starts at zero (U, RES, RHS, RHO of all levels, SRC, PSI)
     for (int64_t t = threadIdx.x; t < clear_doubles; t += blockDim.x) d.U[0][t] = 0.0;
+    // A NaN or Inf density would make the mean and every source value NaN;
+    // max|source| would then stay 0 (NaN fails every comparison) and the
+    // loop would stop at once with psi = 0 reported as converged.  Refuse
+    // it instead: psi is set to NaN everywhere and the result words carry a
+    // cycle count of -1, which the host turns into SFM_ENONFINITE.
+    int bad = 0;
+    for (int c = threadIdx.x; c < n3; c += blockDim.x) bad |= !isfinite(rho[c]);
+    if (__syncthreads_or(bad)) {
+        for (int c = threadIdx.x; c < n3; c += blockDim.x) psi[c] = __longlong_as_double(0x7ff8000000000000LL);
+        if (threadIdx.x == 0) {
+            out[0] = __longlong_as_double(0x7ff8000000000000LL);
+            out[1] = -1.0;
+        }
+        return;
+    }
     // mean of rho: per-thread sums in cell order, then a fixed tree (deterministic)
     double s = 0.0;
     for (int c = threadIdx.x; c < n3; c += blockDim.x) s = s + rho[c];

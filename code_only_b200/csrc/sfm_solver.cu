@@ -67,6 +67,16 @@ struct HostHier {
         if (!hd->level || !hd->ijk || !hd->parent || !hd->child || !hd->nbr || !hd->touch || !hd->cellwidth || !hd->x0)
             return SFM_EINVAL;
         for (int d = 0; d < 3; d++) { ngb[d] = hd->ngb[d]; if (ngb[d] <= 0) return SFM_EINVAL; }
+        // The reference runs its serial base-grid multigrid whenever NGI/NGJ/
+        // NGK_BASE are powers of two (vmg.F90:85-91), on boxes of any shape
+        // (mg_data.F90:57-75, levels following min(boxsize)).  The base-grid
+        // CTA here handles cubic boxes only, so a power-of-two box that is not
+        // cubic is refused rather than solved by another method.
+        {
+            auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
+            if (pow2(ngb[0]) && pow2(ngb[1]) && pow2(ngb[2]) && (ngb[0] != ngb[1] || ngb[1] != ngb[2]))
+                return SFM_EHIER;
+        }
         FMax = 0; while ((2 << FMax) < NI) FMax++;
         level.assign(hd->level, hd->level + nb);
         parent.assign(hd->parent, hd->parent + nb);
@@ -482,6 +492,7 @@ public:
         // ---- base grid (mg_data_init, mg_data.F90:45-90)
         auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
         int NBx = (H.ngb[0] * H.NI) >> FMax, NBy = (H.ngb[1] * H.NI) >> FMax, NBz = (H.ngb[2] * H.NI) >> FMax;
+        // UseSerialMg (vmg.F90:85-91); non-cubic power-of-two boxes were refused in HostHier::build
         useSerialMg = pow2(H.ngb[0]) && pow2(H.ngb[1]) && pow2(H.ngb[2]) && NBx == NBy && NBy == NBz;
         std::memset(&mg, 0, sizeof(mg));
         if (useSerialMg) {
@@ -1378,6 +1389,37 @@ static int check_device(void) {
     return SFM_OK;
 }
 
+// Makes `dev` current for the lifetime of the guard and gives the caller's
+// current device back on every return path: a host program that drives
+// other GPUs finds its current device unchanged after a call.
+struct DeviceGuard {
+    int saved = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            cudaGetLastError();
+            saved = -1;
+        }
+        if (saved != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (saved >= 0 && cudaGetDevice(&now) == cudaSuccess && now != saved) cudaSetDevice(saved);
+    }
+};
+
+// true when p is device memory of device `dev` or managed memory: a host
+// pointer or another GPU's memory handed to a kernel on `dev` would fault
+// (or, where the GPU can reach host memory, silently use the wrong data)
+static bool device_pointer_on(const void *p, int dev) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 extern "C" {
 
 void sfm_default_params(sfm_params *p) {
@@ -1457,7 +1499,10 @@ static int64_t io_elems(const sfm_ctx *c) {
 
 int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g, sfm_stats *st, void *stream) {
     if (!c || !c->s || !d_rho) return SFM_EINVAL;
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
+    if (!device_pointer_on(d_rho, c->device) || (d_psi && !device_pointer_on(d_psi, c->device)) ||
+        (d_g && !device_pointer_on(d_g, c->device)))
+        return SFM_EINVAL;
     return sfm_guard([&] { return c->s->solve(d_rho, d_psi, d_g, st, (cudaStream_t)stream, 0, nullptr); });
 }
 
@@ -1493,7 +1538,7 @@ static void scatter_g_interiors(const double *src, double *g, int64_t row0, int6
 
 static int solve_impl(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
     if (!c || !c->s || !rho) return SFM_EINVAL;
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int64_t n = io_elems(c);
     size_t bytes = (size_t)n * sizeof(double);
     const size_t gbytes = (size_t)c->nb * 3 * c->ni * c->ni * c->ni * sizeof(double);
@@ -1548,13 +1593,13 @@ int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *
 
 int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st) {
     if (!c || !c->s || !dJ_dphi || !dJ_drho) return SFM_EINVAL;
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     return sfm_guard([&] { return c->s->adjoint(dJ_dphi, dJ_drho, st, nullptr); });
 }
 
 void sfm_destroy(sfm_ctx *c) {
     if (!c) return;
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if (c->d_rho) cudaFree(c->d_rho);
     if (c->d_psi) cudaFree(c->d_psi);
     if (c->d_gc) cudaFree(c->d_gc);
@@ -1596,7 +1641,7 @@ int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes) {
 int sfm_debug_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st, int stop_stage,
                     double *dump) {
     if (!c || !c->s || !rho) return SFM_EINVAL;
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int64_t n = io_elems(c);
     size_t bytes = (size_t)n * sizeof(double);
     if (stop_stage == 0) return sfm_solve(c, rho, psi, g, st);
@@ -1637,14 +1682,6 @@ int noalloc_scratch(int dev, double **out) {
     return SFM_OK;
 }
 
-bool device_accessible(const void *p) {
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
 }  // namespace
 
 extern "C" int sfm_uniform_solve_noalloc(const double *d_rho, double *d_psi, int n, double h, double four_pi_G,
@@ -1657,17 +1694,27 @@ extern "C" int sfm_uniform_solve_noalloc(const double *d_rho, double *d_psi, int
         return SFM_EINVAL;
     if ((reinterpret_cast<uintptr_t>(d_rho) | reinterpret_cast<uintptr_t>(d_psi)) % alignof(double) != 0)
         return SFM_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cycles || rel_residual) {
+        // the host outputs need a copy and a wait, which a stream under capture
+        // forbids: refuse before any other runtime call (the capture stays valid)
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+            cudaGetLastError();
+            return SFM_EINVAL;
+        }
+        if (cs != cudaStreamCaptureStatusNone) return SFM_EINVAL;
+    }
     int rc = check_device();
     if (rc != SFM_OK) return rc;
-    if (!device_accessible(d_rho) || !device_accessible(d_psi)) return SFM_EINVAL;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return SFM_EDEVICE;
+    if (!device_pointer_on(d_rho, dev) || !device_pointer_on(d_psi, dev)) return SFM_EINVAL;
     double *s = nullptr;
     rc = noalloc_scratch(dev, &s);
     if (rc != SFM_OK) return rc;
     const sfm::MgData d = sfm::noalloc_layout(s, n, h);
     double *out = s + sfm::noalloc_level_doubles(sfm::NOALLOC_MAX_N);
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     sfm::k_mg_uniform_noalloc<<<1, 1024, 0, st>>>(d, d_rho, d_psi, four_pi_G, rel_tol, max_cycles, out,
                                                   (int64_t)sfm::noalloc_level_doubles(n));
     if (cudaGetLastError() != cudaSuccess) return SFM_ECUDA;
@@ -1680,5 +1727,6 @@ extern "C" int sfm_uniform_solve_noalloc(const double *d_rho, double *d_psi, int
     }
     if (cycles) *cycles = (int)hv[1];
     if (rel_residual) *rel_residual = hv[0];
+    if (hv[1] < 0.0) return SFM_ENONFINITE;   // the kernel found a non-finite density
     return hv[0] <= rel_tol ? SFM_OK : SFM_ENOTCONVERGED;
 }

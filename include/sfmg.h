@@ -9,8 +9,9 @@
  * replacement receives the same information explicitly: a hierarchy
  * descriptor (the link tables of grid.F90:44-52 in fmg-local numbering) and
  * per-block arrays laid out like BlockMem(gid)%u(:,:,:,m) (Fortran order,
- * i fastest, `ngh_io` ghost layers).  A Fortran ISO_C_BINDING shim that keeps
- * the name `fmg_poisson` is shown in INTEGRATION.md.
+ * i fastest, `ngh_io` ghost layers).  A Fortran host keeps the name
+ * `fmg_poisson` through an ISO_C_BINDING shim that gathers these arrays and
+ * calls sfm_solve.
  *
  * Conventions shared by every entry point:
  *   - blocks are numbered 0..nblocks-1 and must be sorted by AMR level
@@ -26,7 +27,9 @@
  *
  * Threading: a context is used by one host thread at a time and owns all of
  * its device memory; it lives on the CUDA device that was current when it
- * was created.
+ * was created.  Every call that takes a context makes that device current
+ * for its duration and gives the caller's current device back before it
+ * returns.
  */
 #ifndef SFMG_H
 #define SFMG_H
@@ -141,7 +144,9 @@ int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out);
 int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st);
 
 /* Same with DEVICE pointers on the context's device (no host copies).
- * `stream` is a cudaStream_t or NULL for the context's own stream. */
+ * `stream` is a cudaStream_t or NULL for the context's own stream.  Each
+ * pointer must be device memory of the context's device (or managed
+ * memory); a host pointer or another GPU's memory returns SFM_EINVAL. */
 int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g,
                      sfm_stats *st, void *stream);
 
@@ -194,8 +199,15 @@ int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes);
  *   cycles, rel_residual  host outputs, may be NULL; when either is given the
  *                 call waits for `stream` and returns SFM_ENOTCONVERGED if
  *                 rel_tol was not reached; when both are NULL it returns
- *                 after queueing the work
+ *                 after queueing the work.  A stream under capture cannot be
+ *                 waited for: with either output given on such a stream the
+ *                 call returns SFM_EINVAL without touching the stream, so
+ *                 pass NULL for both there
  *   stream        a cudaStream_t, or NULL for the legacy default stream
+ * A NaN or Inf anywhere in rho sets psi to NaN everywhere; with host
+ * outputs the call then returns SFM_ENONFINITE (*cycles = -1).
+ * d_rho and d_psi must be device memory of the current device (or managed
+ * memory): anything else returns SFM_EINVAL.
  * Working arrays live in one fixed device array of the library (about
  * 2 MiB, enough for n = 32), cleared by the kernel itself before use, so
  * nothing needs zeroing and nothing carries over between calls.  There is

@@ -176,12 +176,14 @@ struct Oracle {
         for (int d = 0; d < 3; d++) NBc[d] = (ngb[d] * NI) >> FMax;
         int boxsize = std::min(NBc[0], std::min(NBc[1], NBc[2]));
         MMax = 0; while ((1 << MMax) < boxsize) MMax++;   // log2(boxsize)
-        if ((1 << MMax) != boxsize || NBc[0] != NBc[1] || NBc[1] != NBc[2]) {
-            // non-cubic or non-power-of-two base: UseSerialMg = .FALSE. (vmg.F90:85-91)
-            useSerialMg = false;
-        }
+        // UseSerialMg when NGI/NGJ/NGK_BASE are powers of two (vmg.F90:85-91).
+        // The reference's mg_data_init also serves non-cubic boxes (levels
+        // follow min(boxsize), mg_data.F90:57-75); this restatement, like the
+        // device solver, covers cubic ones and refuses a non-cubic
+        // power-of-two box.
         auto pow2 = [](int v) { return v > 0 && (v & (v - 1)) == 0; };
-        useSerialMg = pow2(ngb[0]) && pow2(ngb[1]) && pow2(ngb[2]) && NBc[0] == NBc[1] && NBc[1] == NBc[2];
+        useSerialMg = pow2(ngb[0]) && pow2(ngb[1]) && pow2(ngb[2]);
+        if (useSerialMg && (ngb[0] != ngb[1] || ngb[1] != ngb[2])) return SFM_EHIER;
         if (useSerialMg) {
             mgf.resize(NCODE * (MMax + 1));
             for (int c = 0; c < NCODE; c++)

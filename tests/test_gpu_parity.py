@@ -150,3 +150,27 @@ def test_host_g_writes_interiors_only():
     assert np.all(g_host[:, :, ~inner] == sentinel)
     assert np.array_equal(g_host[:, :, inner], g_dev[:, :, inner])
     assert np.array_equal(psi, psi_d.cpu().numpy())
+
+
+def test_solve_device_rejects_host_pointers():
+    """sfm_solve_device checks that every array is device memory of the
+    context's device before it launches anything, and leaves the caller's
+    current device as it found it."""
+    import torch
+    h = w.small_periodic(2, 8, 2, 0)
+    p = abi.default_params(abi.SFM_BC_PERIODIC)
+    rho = w.block_field(h, p.ngh_io, w.gaussian_peak)
+    with FMGPoisson(h, params=p) as s:
+        rho_d = torch.from_numpy(rho).cuda()
+        psi_d = torch.zeros_like(rho_d)
+        psi_h = np.zeros_like(rho)
+        dev = torch.cuda.current_device()
+        rc = s.lib.sfm_solve_device(s.ctx, C.c_void_p(rho.ctypes.data), C.c_void_p(psi_d.data_ptr()), None, None,
+                                    None)
+        assert rc == abi.SFM_EINVAL
+        rc = s.lib.sfm_solve_device(s.ctx, C.c_void_p(rho_d.data_ptr()), C.c_void_p(psi_h.ctypes.data), None,
+                                    None, None)
+        assert rc == abi.SFM_EINVAL
+        st = s.solve_device(rho_d.data_ptr(), psi_d.data_ptr())
+        torch.cuda.synchronize()
+        assert st.outer_iters > 0 and torch.cuda.current_device() == dev

@@ -112,3 +112,47 @@ def test_noalloc_rejects_bad_arguments():
     assert f(host.ctypes.data, b.data_ptr(), 32, *args) == abi.SFM_EINVAL  # not device memory
     assert f(a.data_ptr() + 4, b.data_ptr(), 32, *args) == abi.SFM_EINVAL  # misaligned
     assert f(a.data_ptr(), b.data_ptr(), 32, -1.0, 1.0, 1e-10, 10, None, None, None) == abi.SFM_EINVAL
+
+
+def test_noalloc_nonfinite_density_is_reported():
+    """A NaN in rho must not come back as a converged zero potential: psi is
+    all NaN and the call returns SFM_ENONFINITE with a cycle count of -1."""
+    import torch
+    f = _entry(abi.load_library())
+    n = 16
+    rho = torch.ones((n, n, n), dtype=torch.float64, device="cuda")
+    rho[3, 5, 7] = float("nan")
+    psi = torch.zeros_like(rho)
+    cycles, rr = C.c_int(0), C.c_double(0.0)
+    rc = f(rho.data_ptr(), psi.data_ptr(), n, 1.0 / n, 1.0, 1e-10, 100, C.byref(cycles), C.byref(rr),
+           C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == abi.SFM_ENONFINITE
+    assert cycles.value == -1 and np.isnan(rr.value)
+    assert torch.isnan(psi).all()
+    # the next call on clean data is unaffected
+    rho[3, 5, 7] = 2.0
+    rc = f(rho.data_ptr(), psi.data_ptr(), n, 1.0 / n, 1.0, 1e-10, 100, C.byref(cycles), C.byref(rr),
+           C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == abi.SFM_OK and torch.isfinite(psi).all()
+
+
+def test_noalloc_refuses_host_outputs_under_capture():
+    """Host outputs need a wait, which stream capture forbids: the call
+    returns SFM_EINVAL and leaves the capture intact."""
+    import torch
+    f = _entry(abi.load_library())
+    n = 8
+    rho = torch.ones((n, n, n), dtype=torch.float64, device="cuda")
+    psi = torch.zeros_like(rho)
+    s = torch.cuda.Stream()
+    # a first call outside capture looks up the scratch array
+    assert f(rho.data_ptr(), psi.data_ptr(), n, 1.0 / n, 1.0, 1e-10, 10, None, None,
+             C.c_void_p(s.cuda_stream)) == abi.SFM_OK
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    cycles = C.c_int(0)
+    with torch.cuda.graph(g, stream=s, capture_error_mode="thread_local"):
+        rc = f(rho.data_ptr(), psi.data_ptr(), n, 1.0 / n, 1.0, 1e-10, 10, C.byref(cycles), None,
+               C.c_void_p(s.cuda_stream))
+        psi.add_(1.0)   # the capture is still usable after the refusal
+    assert rc == abi.SFM_EINVAL and cycles.value == 0
