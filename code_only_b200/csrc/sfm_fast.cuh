@@ -192,6 +192,185 @@ __global__ void __launch_bounds__(256) k_ghost_faces(T *u, const FaceItem *__res
 }
 
 // ---------------------------------------------------------------------------
+// one ghost fill of a whole AMR level in one launch
+// ---------------------------------------------------------------------------
+// fmg_ghostcell_fix fills a level by three passes, x then y then z
+// (fmg_ghostcell.F90:49-54); pass d writes the d-ghost planes (whole
+// transverse range) of the level's linked faces and reads no d-ghost plane.
+// So the value a ghost cell ends with comes from the pass of its highest
+// ghost dimension D whose face is filled, and that pass reads (a) cells
+// interior along D of the same level -- which hold either interior values or
+// ghost values of dimensions below D, themselves final after passes < D --
+// and (b) coarse cells of the level above, complete before this level
+// starts.  k_ghost_level evaluates that composition for every shell cell of
+// the level's blocks (depth <= 3: gval<D> calls gval<D-1>), reading only
+// interior cells, coarse cells and ghost cells no pass of this fill writes,
+// and writing only ghost cells of the level: no read meets a write of the
+// same launch.  The same expressions as ghost_face / ghost_copy give
+// bit-identical values.  A ghost cell that no pass writes is left alone; a
+// composition that would read a ghost cell some later pass of the same fill
+// rewrites (possible next to the physical boundary or when one kind of face
+// is filled alone) is detected on the host, and such a level keeps the three
+// passes (Solver::ghost_merge_ok).
+struct GFace {             // one face of one block for the level fills
+    int32_t src;           // same-level neighbour, parent-level neighbour, or -1
+    int8_t type;           // 0 same level, 1 coarse-fine, 2 physical boundary
+    int8_t pad[3];
+};
+// true when a fill of kind `sel` (-1 both kinds, 0 same level only, 1
+// coarse-fine only) writes the ghost plane of a face of this type
+__host__ __device__ __forceinline__ bool gface_filled(int type, int sel) {
+    return (type == 0 && sel != 1) || (type == 1 && sel != 0);
+}
+
+template <class T, int N>
+struct GhostLevelArgs {
+    const T *u; const GFace *gf; const int8_t *oct; int sel; bool bicubic;
+    const GhostCubicTable<N> *tab;
+};
+
+template <class T, int N, int D>
+__device__ __forceinline__ T ghost_pass_value(const GhostLevelArgs<T, N> &a, const GFace &f, int lr, int X, int i, int j,
+                                              int k);
+
+// state of cell (i,j,k) of block X after passes 0..DL of the fill; the
+// coordinates of dimensions above DL are interior
+template <class T, int N, int DL>
+__device__ __forceinline__ T ghost_value(const GhostLevelArgs<T, N> &a, int X, int i, int j, int k) {
+    constexpr int G = N + 2;
+    constexpr int64_t V = (int64_t)G * G * G;
+    if constexpr (DL >= 0) {
+        const int c = DL == 0 ? i : (DL == 1 ? j : k);
+        if (c == -1 || c == N) {
+            const int lr = c == N ? 1 : 0;
+            const GFace f = a.gf[6 * X + lr + 2 * DL];
+            if (gface_filled(f.type, a.sel)) return ghost_pass_value<T, N, DL>(a, f, lr, X, i, j, k);
+        }
+        return ghost_value<T, N, DL - 1>(a, X, i, j, k);
+    } else {
+        return a.u[(int64_t)X * V + cidx(G, i, j, k)];
+    }
+}
+
+// the value pass D writes into cell (i,j,k) (on the D-ghost plane of side lr)
+template <class T, int N, int D>
+__device__ __forceinline__ T ghost_pass_value(const GhostLevelArgs<T, N> &a, const GFace &f, int lr, int X, int i, int j,
+                                              int k) {
+    constexpr int G = N + 2, NB2 = N / 2;
+    constexpr int64_t V = (int64_t)G * G * G;
+    if (f.type == 0) {   // fmg_ghfix_samelev: the neighbour's cell on the opposite boundary plane
+        const int xs = lr == 0 ? N - 1 : 0;
+        return ghost_value<T, N, D - 1>(a, f.src, D == 0 ? xs : i, D == 1 ? xs : j, D == 2 ? xs : k);
+    }
+    // fmg_ghfix_parentlev: transverse interpolation of the coarse layer, then
+    // the quadratic normal formula with the two inner fine cells
+    const int p = D == 0 ? j : i, q = D == 2 ? j : k;
+    const T *uc = a.u + (int64_t)f.src * V;
+    const int xc = lr == 0 ? N - 1 : 0;
+    const int oa = a.oct[3 * X + tra(D)] * NB2, ob = a.oct[3 * X + trb(D)] * NB2;
+    auto B = [&](int pb, int qb) -> T {
+        int ci, cj, ck;
+        put3(D, xc, pb + oa, qb + ob, ci, cj, ck);
+        return uc[cidx(G, ci, cj, ck)];
+    };
+    T uH;
+    if (a.bicubic) {
+        const int *cp = a.tab->c[p + 1], *cq = a.tab->c[q + 1];
+        const double *wp = a.tab->w[p + 1], *wq = a.tab->w[q + 1];
+        T bx[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            bx[m] = (T)wp[0] * B(cp[0], cq[m]) + (T)wp[1] * B(cp[1], cq[m]) + (T)wp[2] * B(cp[2], cq[m])
+                  + (T)wp[3] * B(cp[3], cq[m]);
+        uH = (T)wq[0] * bx[0] + (T)wq[1] * bx[1] + (T)wq[2] * bx[2] + (T)wq[3] * bx[3];
+    } else {
+        const int pc = fdiv2(p), qc = fdiv2(q);
+        const int p1 = near_(p, pc), q1 = near_(q, qc);
+        uH = ((T)9 * B(pc, qc) + B(p1, q1) + (T)3 * B(pc, q1) + (T)3 * B(p1, qc)) / (T)16;
+    }
+    const int xg = lr == 0 ? -1 : N, inner = lr == 0 ? 1 : -1;
+    const int x0 = xg + inner, xN = xg + 2 * inner;
+    const T u0 = ghost_value<T, N, D - 1>(a, X, D == 0 ? x0 : i, D == 1 ? x0 : j, D == 2 ? x0 : k);
+    const T uN = ghost_value<T, N, D - 1>(a, X, D == 0 ? xN : i, D == 1 ? xN : j, D == 2 ? xN : k);
+    return ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
+}
+
+// shell cells of one block, grouped by the highest ghost dimension D (the
+// pass that writes them last): D = 0 -> 2 N^2, D = 1 -> 2 (N+2) N, D = 2 -> 2 (N+2)^2
+template <int N>
+__host__ __device__ constexpr int ghost_shell() { return 2 * (N * N + (N + 2) * N + (N + 2) * (N + 2)); }
+constexpr int kGhostLevelK = 4;   // shell cells per thread, loads before stores
+template <int N>
+__host__ __device__ constexpr int ghost_level_ctas(int nblk) {
+    return (int)(((int64_t)nblk * ghost_shell<N>() + 256 * kGhostLevelK - 1) / (256 * kGhostLevelK));
+}
+
+template <class T, int N>
+__global__ void __launch_bounds__(256) k_ghost_level(T *u, const GFace *__restrict__ gf, const int8_t *__restrict__ oct,
+                                                     int first, int nblk, int sel, int cubic) {
+    pdl_enter();
+    constexpr int G = N + 2, NB2 = N / 2, SH = ghost_shell<N>(), K = kGhostLevelK;
+    constexpr int A0 = N * N, A1 = (N + 2) * N, A2 = (N + 2) * (N + 2);
+    constexpr int64_t V = (int64_t)G * G * G;
+    __shared__ GhostCubicTable<N> tab;
+    const bool bicubic = cubic && NB2 + 2 >= 4 && sel != 0;
+    if (bicubic) {
+        if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, tab.c[threadIdx.x], tab.w[threadIdx.x]);
+        __syncthreads();
+    }
+    const GhostLevelArgs<T, N> a{u, gf, oct, sel, bicubic, &tab};
+    const int64_t total = (int64_t)nblk * SH;
+    const int64_t g0 = (int64_t)blockIdx.x * 256 * K + threadIdx.x;
+    T val[K];
+    int64_t dst[K];
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+        const int64_t g = g0 + (int64_t)t * 256;
+        dst[t] = -1;
+        if (g >= total) continue;
+        const int bq = (int)(g / SH), r0 = (int)(g - (int64_t)bq * SH);
+        const int X = first + bq;
+        int i, j, k, D, side;
+        if (r0 < 2 * A0) {
+            side = r0 / A0;
+            const int t0 = r0 - side * A0;
+            D = 0; i = side ? N : -1; j = t0 % N; k = t0 / N;
+        } else if (r0 < 2 * A0 + 2 * A1) {
+            const int r = r0 - 2 * A0;
+            side = r / A1;
+            const int t1 = r - side * A1;
+            D = 1; i = t1 % (N + 2) - 1; j = side ? N : -1; k = t1 / (N + 2);
+        } else {
+            const int r = r0 - 2 * A0 - 2 * A1;
+            side = r / A2;
+            const int t2 = r - side * A2;
+            D = 2; i = t2 % (N + 2) - 1; j = t2 / (N + 2) - 1; k = side ? N : -1;
+        }
+        const GFace f = gf[6 * X + side + 2 * D];
+        if (!gface_filled(f.type, sel)) {
+            // the top face is not filled: the cell keeps the value of the
+            // highest lower pass that writes it, if any
+            bool any = false;
+            if (D >= 1 && (i == -1 || i == N)) any |= gface_filled(gf[6 * X + (i == N) + 0].type, sel);
+            if (D == 2 && (j == -1 || j == N)) any |= gface_filled(gf[6 * X + (j == N) + 2].type, sel);
+            if (!any) continue;
+            if (D == 2) val[t] = ghost_value<T, N, 1>(a, X, i, j, k);
+            else val[t] = ghost_value<T, N, 0>(a, X, i, j, k);
+        } else if (D == 0) {
+            val[t] = ghost_pass_value<T, N, 0>(a, f, side, X, i, j, k);
+        } else if (D == 1) {
+            val[t] = ghost_pass_value<T, N, 1>(a, f, side, X, i, j, k);
+        } else {
+            val[t] = ghost_pass_value<T, N, 2>(a, f, side, X, i, j, k);
+        }
+        dst[t] = (int64_t)X * V + cidx(G, i, j, k);
+    }
+#pragma unroll
+    for (int t = 0; t < K; t++)
+        if (dst[t] >= 0) u[dst[t]] = val[t];
+}
+
+// ---------------------------------------------------------------------------
 // staging of BPC consecutive listed blocks (G^3 each) into shared memory
 // ---------------------------------------------------------------------------
 template <int N>

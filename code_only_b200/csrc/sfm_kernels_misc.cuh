@@ -96,103 +96,120 @@ struct OpSphereMask {        // rho := 0 where x^2+y^2+z^2 >= rad2, all cells of
     }
 };
 
-// moments of one base block: one CTA per block, fixed-order tree reduction
-__global__ void k_moments_block(const double *R, const double *x0, const double *h0, int n, int G, int64_t V,
-                                int lmax, double *part /* [nbase][25] */) {
+// Multipole moments a_lm of the masked source over the base-level interior
+// cells (fmg_boundary_phys_sphere.F90:132-242; the l = 4 terms extend the
+// reference).  The reference accumulates every moment in one running sum
+// over the base blocks in list order and, inside a block, k, j, i; the two
+// kernels below keep that order, so the moments -- and with them the whole
+// isolated-boundary solve -- are bit-identical to a serial evaluation:
+// k_moment_terms evaluates each cell's 25 terms in parallel (the reference's
+// expressions, left to right), k_moments_ordered adds them in cell order,
+// one lane per moment, with the loads running ahead of the dependent adds.
+constexpr int kMomentTerms = 25;
+__global__ void k_moment_terms(const double *R, const double *x0, const double *h0, int n, int G, int64_t V,
+                               int nbase, int lmax, double *T /* [nbase n^3][25] */) {
     pdl_enter();
-    __shared__ double red[25][128];   // blockDim.x == 128
-    const int b = blockIdx.x;
+    const int64_t ncell = (int64_t)nbase * n * n * n;
     const double h = h0[0], dv = h * h * h;
-    double a[25];
-    for (int m = 0; m < 25; m++) a[m] = 0.0;
-    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-        int i = c % n, j = (c / n) % n, k = c / (n * n);
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x) {
+        const int per = n * n * n;
+        const int b = (int)(c / per), r = (int)(c - (int64_t)b * per);
+        const int i = r % n, j = (r / n) % n, k = r / (n * n);
         double x = x0[3 * b] + (double)i * h, y = x0[3 * b + 1] + (double)j * h, z = x0[3 * b + 2] + (double)k * h;
         double r2 = x * x + y * y + z * z;
-        double r = sqrt(r2);
-        double r3 = r2 * r;
+        double rr = sqrt(r2);
+        double r3 = r2 * rr;
         double rc = sqrt(x * x + y * y);
-        double ri = 1 / r, rci = 1 / rc;
+        double ri = 1 / rr, rci = 1 / rc;
         double cost = z * ri, sint = rc * ri, cosp = x * rci, sinp = y * rci;
         double rhodv = R[(int64_t)b * V + cidx(G, i, j, k)] * dv;
-        a[0] += rhodv;
-        a[1] += rhodv * r * cost;
-        a[2] += rhodv * r * sint * cosp;
-        a[3] += rhodv * r * sint * sinp;
-        a[4] += rhodv * r2 * (3 * (cost * cost) - 1);
-        a[5] += rhodv * r2 * sint * cost * cosp;
-        a[6] += rhodv * r2 * sint * cost * sinp;
-        a[7] += rhodv * r2 * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
-        a[8] += rhodv * r2 * (sint * sint) * 2 * sinp * cosp;
-        a[9] += rhodv * r3 * cost * (5 * (cost * cost) - 3);
-        a[10] += rhodv * r3 * sint * (5 * (cost * cost) - 1) * cosp;
-        a[11] += rhodv * r3 * sint * (5 * (cost * cost) - 1) * sinp;
-        a[12] += rhodv * r3 * cost * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
-        a[13] += rhodv * r3 * cost * (sint * sint) * 2 * sinp * cosp;
-        a[14] += rhodv * r3 * (sint * sint * sint) * cosp * ((cosp * cosp) - 3 * (sinp * sinp));
-        a[15] += rhodv * r3 * (sint * sint * sint) * sinp * (3 * (cosp * cosp) - (sinp * sinp));
+        double *t = T + c * kMomentTerms;
+        t[0] = rhodv;
+        t[1] = rhodv * rr * cost;
+        t[2] = rhodv * rr * sint * cosp;
+        t[3] = rhodv * rr * sint * sinp;
+        t[4] = rhodv * r2 * (3 * (cost * cost) - 1);
+        t[5] = rhodv * r2 * sint * cost * cosp;
+        t[6] = rhodv * r2 * sint * cost * sinp;
+        t[7] = rhodv * r2 * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
+        t[8] = rhodv * r2 * (sint * sint) * 2 * sinp * cosp;
+        t[9] = rhodv * r3 * cost * (5 * (cost * cost) - 3);
+        t[10] = rhodv * r3 * sint * (5 * (cost * cost) - 1) * cosp;
+        t[11] = rhodv * r3 * sint * (5 * (cost * cost) - 1) * sinp;
+        t[12] = rhodv * r3 * cost * (sint * sint) * ((cosp * cosp) - (sinp * sinp));
+        t[13] = rhodv * r3 * cost * (sint * sint) * 2 * sinp * cosp;
+        t[14] = rhodv * r3 * (sint * sint * sint) * cosp * ((cosp * cosp) - 3 * (sinp * sinp));
+        t[15] = rhodv * r3 * (sint * sint * sint) * sinp * (3 * (cosp * cosp) - (sinp * sinp));
         if (lmax >= 4) {
             double r4 = r2 * r2, c2 = cost * cost, s2 = sint * sint;
             double cos2p = (cosp * cosp) - (sinp * sinp), sin2p = 2 * sinp * cosp;
             double cos3p = cosp * ((cosp * cosp) - 3 * (sinp * sinp));
             double sin3p = sinp * (3 * (cosp * cosp) - (sinp * sinp));
             double cos4p = cos2p * cos2p - sin2p * sin2p, sin4p = 2 * sin2p * cos2p;
-            a[16] += rhodv * r4 * (35 * (c2 * c2) - 30 * c2 + 3);
-            a[17] += rhodv * r4 * sint * cost * (7 * c2 - 3) * cosp;
-            a[18] += rhodv * r4 * sint * cost * (7 * c2 - 3) * sinp;
-            a[19] += rhodv * r4 * s2 * (7 * c2 - 1) * cos2p;
-            a[20] += rhodv * r4 * s2 * (7 * c2 - 1) * sin2p;
-            a[21] += rhodv * r4 * s2 * sint * cost * cos3p;
-            a[22] += rhodv * r4 * s2 * sint * cost * sin3p;
-            a[23] += rhodv * r4 * (s2 * s2) * cos4p;
-            a[24] += rhodv * r4 * (s2 * s2) * sin4p;
+            t[16] = rhodv * r4 * (35 * (c2 * c2) - 30 * c2 + 3);
+            t[17] = rhodv * r4 * sint * cost * (7 * c2 - 3) * cosp;
+            t[18] = rhodv * r4 * sint * cost * (7 * c2 - 3) * sinp;
+            t[19] = rhodv * r4 * s2 * (7 * c2 - 1) * cos2p;
+            t[20] = rhodv * r4 * s2 * (7 * c2 - 1) * sin2p;
+            t[21] = rhodv * r4 * s2 * sint * cost * cos3p;
+            t[22] = rhodv * r4 * s2 * sint * cost * sin3p;
+            t[23] = rhodv * r4 * (s2 * s2) * cos4p;
+            t[24] = rhodv * r4 * (s2 * s2) * sin4p;
+        } else {
+            for (int m = 16; m < kMomentTerms; m++) t[m] = 0.0;
         }
     }
-    for (int m = 0; m < 25; m++) red[m][threadIdx.x] = a[m];
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s)
-            for (int m = 0; m < 25; m++) red[m][threadIdx.x] = red[m][threadIdx.x] + red[m][threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x < 25) part[(int64_t)b * 25 + threadIdx.x] = red[threadIdx.x][0];
 }
 
-// sum of the per-block moments in block order, then the normalisations of
-// sphere.F90:227-242 (and of the l = 4 extension)
-__global__ void k_moments_combine(const double *part, int nbase, double *mom) {
-    pdl_enter();
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double a[25];
-    for (int m = 0; m < 25; m++) a[m] = 0.0;
-    for (int b = 0; b < nbase; b++)
-        for (int m = 0; m < 25; m++) a[m] = a[m] + part[(int64_t)b * 25 + m];
+// normalisations (fmg_boundary_phys_sphere.F90:227-242; l = 4 extension)
+__device__ __forceinline__ double moment_norm(int m, double a) {
     const double pi = 3.141592653589793;
-    mom[0] = -a[0] / (4.0 * pi);
-    mom[1] = -a[1] / (4.0 * pi);
-    mom[2] = -a[2] / (8.0 * pi);
-    mom[3] = -a[3] / (8.0 * pi);
-    mom[4] = -a[4] / (16.0 * pi);
-    mom[5] = -a[5] / (8.0 * pi) * 3.0;
-    mom[6] = -a[6] / (8.0 * pi) * 3.0;
-    mom[7] = -a[7] / (32.0 * pi) * 3.0;
-    mom[8] = -a[8] / (32.0 * pi) * 3.0;
-    mom[9] = -a[9] / (16.0 * pi);
-    mom[10] = -a[10] / (64.0 * pi) * 3.0;
-    mom[11] = -a[11] / (64.0 * pi) * 3.0;
-    mom[12] = -a[12] / (32.0 * pi) * 15.0;
-    mom[13] = -a[13] / (32.0 * pi) * 15.0;
-    mom[14] = -a[14] / (64.0 * pi) * 5.0;
-    mom[15] = -a[15] / (64.0 * pi) * 5.0;
-    mom[16] = -a[16] / (4.0 * pi) * (1.0 / 64.0);
-    mom[17] = -a[17] / (4.0 * pi) * (5.0 / 8.0);
-    mom[18] = -a[18] / (4.0 * pi) * (5.0 / 8.0);
-    mom[19] = -a[19] / (4.0 * pi) * (5.0 / 16.0);
-    mom[20] = -a[20] / (4.0 * pi) * (5.0 / 16.0);
-    mom[21] = -a[21] / (4.0 * pi) * (35.0 / 8.0);
-    mom[22] = -a[22] / (4.0 * pi) * (35.0 / 8.0);
-    mom[23] = -a[23] / (4.0 * pi) * (35.0 / 64.0);
-    mom[24] = -a[24] / (4.0 * pi) * (35.0 / 64.0);
+    switch (m) {
+        case 0: return -a / (4.0 * pi);
+        case 1: return -a / (4.0 * pi);
+        case 2: return -a / (8.0 * pi);
+        case 3: return -a / (8.0 * pi);
+        case 4: return -a / (16.0 * pi);
+        case 5: return -a / (8.0 * pi) * 3.0;
+        case 6: return -a / (8.0 * pi) * 3.0;
+        case 7: return -a / (32.0 * pi) * 3.0;
+        case 8: return -a / (32.0 * pi) * 3.0;
+        case 9: return -a / (16.0 * pi);
+        case 10: return -a / (64.0 * pi) * 3.0;
+        case 11: return -a / (64.0 * pi) * 3.0;
+        case 12: return -a / (32.0 * pi) * 15.0;
+        case 13: return -a / (32.0 * pi) * 15.0;
+        case 14: return -a / (64.0 * pi) * 5.0;
+        case 15: return -a / (64.0 * pi) * 5.0;
+        case 16: return -a / (4.0 * pi) * (1.0 / 64.0);
+        case 17: return -a / (4.0 * pi) * (5.0 / 8.0);
+        case 18: return -a / (4.0 * pi) * (5.0 / 8.0);
+        case 19: return -a / (4.0 * pi) * (5.0 / 16.0);
+        case 20: return -a / (4.0 * pi) * (5.0 / 16.0);
+        case 21: return -a / (4.0 * pi) * (35.0 / 8.0);
+        case 22: return -a / (4.0 * pi) * (35.0 / 8.0);
+        case 23: return -a / (4.0 * pi) * (35.0 / 64.0);
+        default: return -a / (4.0 * pi) * (35.0 / 64.0);
+    }
+}
+
+// one warp; lane m < 25 sums term m over the cells in order
+__global__ void __launch_bounds__(32) k_moments_ordered(const double *__restrict__ T, int64_t ncell, double *mom) {
+    pdl_enter();
+    const int m = threadIdx.x;
+    if (m >= kMomentTerms) return;
+    constexpr int U = 16;   // loads issued ahead of the dependent adds
+    double a = 0.0;
+    int64_t c = 0;
+    for (; c + U <= ncell; c += U) {
+        double t[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) t[u] = T[(c + u) * kMomentTerms + m];
+#pragma unroll
+        for (int u = 0; u < U; u++) a = a + t[u];
+    }
+    for (; c < ncell; c++) a = a + T[c * kMomentTerms + m];
+    mom[m] = moment_norm(m, a);
 }
 
 // U00..U33 (sphere.F90:267-293) and the l = 4 terms

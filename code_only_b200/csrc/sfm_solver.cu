@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -240,6 +241,9 @@ public:
     int8_t *d_oct = nullptr, *d_skip = nullptr;
     double *d_h0 = nullptr, *d_x0 = nullptr;
     FaceItem *d_faces = nullptr;
+    GFace *d_gface = nullptr;              // [6 nb] face types and sources for the level fills
+    std::vector<std::array<bool, 3>> ghostMerge;   // [level][sel + 1]: one launch fills the level
+    bool ghostMergeOn = true;
     RefluxItem *d_reflux = nullptr;
     BFace *d_tfL = nullptr, *d_tfDL = nullptr, *d_crop = nullptr;
     std::vector<int64_t> faceOff, faceSplit, tfLOff, tfDLOff, cropOff, wcOff;
@@ -452,6 +456,20 @@ public:
         }
         cropOff[nlev] = (int64_t)crop.size();
 
+        // faces of every block for the level fills, and which fills of which
+        // level one launch can do
+        std::vector<GFace> gface(6 * (size_t)nb);
+        for (int b = 0; b < nb; b++)
+            for (int fc = 0; fc < 6; fc++) {
+                GFace g{};
+                g.src = H.nbrGid[6 * b + fc];
+                g.type = H.sameLev[6 * b + fc] ? 0 : (H.level[b] > 0 && H.parLev[6 * b + fc] ? 1 : 2);
+                if (g.type == 2) g.src = -1;
+                gface[6 * b + fc] = g;
+            }
+        ghostMerge.assign(nlev, {false, false, false});
+        for (int L = 0; L < nlev; L++)
+            for (int sel = -1; sel <= 1; sel++) ghostMerge[L][sel + 1] = ghost_merge_ok(gface, L, sel);
         d_level = mem.upload(std::vector<int32_t>(H.level.begin(), H.level.end()));
         d_parent = mem.upload(std::vector<int32_t>(H.parent.begin(), H.parent.end()));
         d_oct = mem.upload(H.oct);
@@ -463,6 +481,7 @@ public:
         d_leaves = mem.upload(std::vector<int32_t>(leafList.begin(), leafList.end()));
         d_withChild = mem.upload(withChild);
         d_faces = mem.upload(faces);
+        d_gface = mem.upload(gface);
         d_reflux = mem.upload(refl);
         d_tfL = mem.upload(tfL);
         d_tfDL = mem.upload(tfDL);
@@ -486,7 +505,8 @@ public:
         zeroList.push_back({d_err, sizeof(int)});
         for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], (void)bulk_grid<N>(), (void)0);
         d_mom = mem.alloc<double>(32);
-        d_part = mem.alloc<double>((size_t)(H.lstart[1]) * 25);
+        if (P.bc == SFM_BC_SPHERE)   // per-cell moment terms of the base level, summed in order
+            d_part = mem.alloc<double>((size_t)H.lstart[1] * H.NI * H.NI * H.NI * kMomentTerms);
         d_psum = mem.alloc<double>((size_t)nb);
         d_mgit = mem.alloc<int>(1);
         // ---- base grid (mg_data_init, mg_data.F90:45-90)
@@ -575,11 +595,59 @@ public:
     int cnt(int L) const { return H.lstart[L + 1] - H.lstart[L]; }
 
     // -----------------------------------------------------------------
+    // Whether k_ghost_level fills level L (fill kind sel) exactly as the
+    // three passes do.  The kernel evaluates each shell cell's final value
+    // by the composition the passes apply (highest filled ghost dimension
+    // first, then the cells that pass reads, dimension by dimension); where
+    // that composition reads a ghost cell no earlier pass wrote, it reads
+    // memory, which is exact only if no pass of this fill writes that cell
+    // at all.  The same recursion is walked here on every block of the level
+    // and for each of its 26 shell segments (a segment's cells share one
+    // recursion: which coordinates are ghosts and on which side).
+    bool ghost_merge_ok(const std::vector<GFace> &gf, int L, int sel) const {
+        auto filled = [&](int b, int d, int side) { return gface_filled(gf[6 * b + (side > 0) + 2 * d].type, sel); };
+        bool race = false;
+        // state of segment s (per dimension -1 low ghost, 0 interior, 1 high ghost) of block b after passes 0..dl
+        auto walk = [&](auto &&self, int b, std::array<int, 3> sg, int dl) -> void {
+            for (int d = dl; d >= 0; d--) {
+                if (sg[d] == 0 || !filled(b, d, sg[d])) continue;
+                const GFace &g = gf[6 * b + (sg[d] > 0) + 2 * d];
+                std::array<int, 3> s2 = sg;
+                s2[d] = 0;
+                self(self, g.type == 0 ? g.src : b, s2, d - 1);   // same level: the neighbour; coarse-fine: u0, uN
+                return;
+            }
+            for (int d = dl + 1; d < 3; d++)   // a memory read of a ghost cell a later pass rewrites
+                if (sg[d] != 0 && filled(b, d, sg[d])) race = true;
+        };
+        for (int b = H.lstart[L]; b < H.lstart[L + 1] && !race; b++)
+            for (int sz = -1; sz <= 1; sz++)
+                for (int sy = -1; sy <= 1; sy++)
+                    for (int sx = -1; sx <= 1; sx++)
+                        if (sx || sy || sz) walk(walk, b, {sx, sy, sz}, 2);
+        return !race;
+    }
+    // one fill of level L: k_ghost_level where exact, else the three passes
+    template <class TT>
+    void ghost_fill_level(int L, int f, TT *u, bool cubic, int sel) {
+        const int n = nf[f];
+        if (sel == 1 && L <= 0) return;
+        if (ghostMergeOn && ghostMerge[L][sel + 1] && (n == 2 || n == 4 || n == 8 || n == 16)) {
+            SFM_WITH_N(n,
+                       (launch_pdl(k_ghost_level<TT, N>, (unsigned)ghost_level_ctas<N>(cnt(L)), 256, 0, u, d_gface,
+                                   d_oct, H.lstart[L], cnt(L), sel, cubic ? 1 : 0),
+                        ++launches),
+                       (void)0)
+            return;
+        }
+        for (int dir = 0; dir < 3; dir++) ghost_pass(L, f, dir, u, cubic, sel);
+    }
+
+    // -----------------------------------------------------------------
     // ghost cells, convergence, boundary (any element type)
     template <class TT>
     void ghostcell_fix(int f, TT *u, bool cubic) {
-        for (int L = 0; L < H.nlev; L++)
-            for (int dir = 0; dir < 3; dir++) ghost_pass(L, f, dir, u, cubic);
+        for (int L = 0; L < H.nlev; L++) ghost_fill_level(L, f, u, cubic, -1);
     }
     template <class TT>
     void ghost_pass(int L, int f, int dir, TT *u, bool cubic, int sel = -1) {   // parentlev/samelev of (L, dir)
@@ -860,19 +928,12 @@ public:
     // vmg (vmg.F90) at fmg level FMax
     void vmg_ghostcell(int L, T *u) {
         const int F = H.FMax;
-        for (int dir = 0; dir < 3; dir++) ghost_pass_same(L, F, dir, u);
+        ghost_fill_level(L, F, u, false, 0);   // same-level faces, x then y then z
         boundary_fill0_level(L, F, u);
-    }
-    // same-level face copies of (L, dir) only (fmg_ghfix_samelev)
-    void ghost_pass_same(int L, int f, int dir, T *u) { ghost_pass(L, f, dir, u, false, 0); }
-    // coarse-fine faces of (L, dir) only (fmg_ghfix_parentlev)
-    void ghost_pass_parent(int L, int f, int dir, T *u, bool cubic) {
-        if (L <= 0) return;
-        ghost_pass(L, f, dir, u, cubic, 1);
     }
     void vmg_gridboundary(int L, T *u) {
         const int F = H.FMax;
-        for (int dir = 0; dir < 3; dir++) ghost_pass_parent(L, F, dir, u, false);
+        ghost_fill_level(L, F, u, false, 1);   // coarse-fine faces, x then y then z
         boundary_fill0_level(L, F, u);
     }
     void vmg_relax(int L, T *u, const T *rhs) {
@@ -885,11 +946,7 @@ public:
     }
     void vmg_rstrct(int Lc, T *u, bool cubic) {
         const int F = H.FMax;
-        if (cubic)
-            for (int dir = 0; dir < 3; dir++) {
-                ghost_pass_parent(Lc + 1, F, dir, u, true);
-                ghost_pass_same(Lc + 1, F, dir, u);
-            }
+        if (cubic) ghost_fill_level(Lc + 1, F, u, true, -1);   // per direction: coarse-fine, then same level
         converge_c2p_lev(Lc, F, u, cubic);
     }
     void vmg_copy_level(int L, T *o, const T *a) {
@@ -982,8 +1039,10 @@ public:
         double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
         double rad2 = rr * rr;
         run(OpSphereMask{SRC0, d_x0, d_h0, d_level, n, Gf[0], Vf[0], rad2}, (int64_t)H.nb * Vf[0]);
-        launch_pdl(k_moments_block, (unsigned)cnt(0), 128, 0, SRC0, d_x0, d_h0, n, Gf[0], Vf[0], P.lmax, d_part);
-        launch_pdl(k_moments_combine, 1, 1, 0, d_part, cnt(0), d_mom);
+        const int64_t ncell = (int64_t)cnt(0) * n * n * n;
+        launch_pdl(k_moment_terms, (unsigned)std::min<int64_t>((ncell + 255) / 256, (int64_t)nSM * 8), 256, 0, SRC0,
+                   d_x0, d_h0, n, Gf[0], Vf[0], cnt(0), P.lmax, d_part);
+        launch_pdl(k_moments_ordered, 1, 32, 0, d_part, ncell, d_mom);
         launches += 2;
         int GT = n + 2;
         run(OpSphereGhost{PSI0, d_tfL, d_mom, d_x0, d_h0, d_level, n, Gf[0], Vf[0], P.lmax}, tfLOff[H.nlev] * GT * GT);
