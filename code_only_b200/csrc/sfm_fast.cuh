@@ -230,13 +230,15 @@ struct GhostLevelArgs {
 };
 
 template <class T, int N, int D>
-__device__ __forceinline__ T ghost_pass_value(const GhostLevelArgs<T, N> &a, const GFace &f, int lr, int X, int i, int j,
-                                              int k);
+__device__ __noinline__ T ghost_pass_value(const GhostLevelArgs<T, N> &a, GFace f, int lr, int X, int i, int j, int k);
 
 // state of cell (i,j,k) of block X after passes 0..DL of the fill; the
-// coordinates of dimensions above DL are interior
+// coordinates of dimensions above DL are interior.  Not inlined: one copy
+// of each depth keeps the code small (inlined, the three-deep composition
+// multiplied the interpolation code and the kernel ran from instruction
+// cache misses on levels with many coarse-fine faces).
 template <class T, int N, int DL>
-__device__ __forceinline__ T ghost_value(const GhostLevelArgs<T, N> &a, int X, int i, int j, int k) {
+__device__ __noinline__ T ghost_value(const GhostLevelArgs<T, N> &a, int X, int i, int j, int k) {
     constexpr int G = N + 2;
     constexpr int64_t V = (int64_t)G * G * G;
     if constexpr (DL >= 0) {
@@ -254,8 +256,7 @@ __device__ __forceinline__ T ghost_value(const GhostLevelArgs<T, N> &a, int X, i
 
 // the value pass D writes into cell (i,j,k) (on the D-ghost plane of side lr)
 template <class T, int N, int D>
-__device__ __forceinline__ T ghost_pass_value(const GhostLevelArgs<T, N> &a, const GFace &f, int lr, int X, int i, int j,
-                                              int k) {
+__device__ __noinline__ T ghost_pass_value(const GhostLevelArgs<T, N> &a, GFace f, int lr, int X, int i, int j, int k) {
     constexpr int G = N + 2, NB2 = N / 2;
     constexpr int64_t V = (int64_t)G * G * G;
     if (f.type == 0) {   // fmg_ghfix_samelev: the neighbour's cell on the opposite boundary plane
@@ -295,6 +296,34 @@ __device__ __forceinline__ T ghost_pass_value(const GhostLevelArgs<T, N> &a, con
     return ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
 }
 
+// the final value of shell cell (i,j,k) of block X, or false when no pass of
+// the fill writes it (general composition, for cells whose chain meets a
+// coarse-fine or an unfilled face)
+template <class T, int N>
+__device__ __noinline__ bool ghost_cell_general(const GhostLevelArgs<T, N> &a, int X, int i, int j, int k, T &out) {
+    const int cs[3] = {i, j, k};
+#pragma unroll
+    for (int d = 2; d >= 0; d--) {
+        if (cs[d] != -1 && cs[d] != N) continue;
+        const int lr = cs[d] == N ? 1 : 0;
+        const GFace f = a.gf[6 * X + lr + 2 * d];
+        if (!gface_filled(f.type, a.sel)) continue;
+        out = d == 2 ? ghost_pass_value<T, N, 2>(a, f, lr, X, i, j, k)
+                     : (d == 1 ? ghost_pass_value<T, N, 1>(a, f, lr, X, i, j, k)
+                               : ghost_pass_value<T, N, 0>(a, f, lr, X, i, j, k));
+        return true;
+    }
+    return false;
+}
+
+// shell segment of a cell: 3^3 pattern of (low ghost, interior, high ghost)
+// per dimension, (sx+1) + 3 (sy+1) + 9 (sz+1), the interior 13 excluded:
+// entries 0..12 and 14..26 map to 0..25
+__host__ __device__ __forceinline__ int shell_segment(int sx, int sy, int sz) {
+    const int s = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+    return s < 13 ? s : s - 1;
+}
+
 // shell cells of one block, grouped by the highest ghost dimension D (the
 // pass that writes them last): D = 0 -> 2 N^2, D = 1 -> 2 (N+2) N, D = 2 -> 2 (N+2)^2
 template <int N>
@@ -305,9 +334,18 @@ __host__ __device__ constexpr int ghost_level_ctas(int nblk) {
     return (int)(((int64_t)nblk * ghost_shell<N>() + 256 * kGhostLevelK - 1) / (256 * kGhostLevelK));
 }
 
+// src26[26 X + segment]: for a segment whose composition runs through
+// same-level faces only (every one filled), the block whose interior cell
+// the passes end up copying -- the neighbour across the highest ghost
+// dimension, then its neighbour across the next, and so on -- at the cell's
+// coordinates wrapped into the block (-1 -> N-1, N -> 0); -1 otherwise.
+// Such cells (all of them on a level without coarse-fine or boundary faces)
+// cost one table load and one value load.  A fill of coarse-fine faces only
+// (sel 1) passes no table: its same-level faces are not filled.
 template <class T, int N>
 __global__ void __launch_bounds__(256) k_ghost_level(T *u, const GFace *__restrict__ gf, const int8_t *__restrict__ oct,
-                                                     int first, int nblk, int sel, int cubic) {
+                                                     const int32_t *__restrict__ src26, int first, int nblk, int sel,
+                                                     int cubic) {
     pdl_enter();
     constexpr int G = N + 2, NB2 = N / 2, SH = ghost_shell<N>(), K = kGhostLevelK;
     constexpr int A0 = N * N, A1 = (N + 2) * N, A2 = (N + 2) * (N + 2);
@@ -318,56 +356,57 @@ __global__ void __launch_bounds__(256) k_ghost_level(T *u, const GFace *__restri
         if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, tab.c[threadIdx.x], tab.w[threadIdx.x]);
         __syncthreads();
     }
-    const GhostLevelArgs<T, N> a{u, gf, oct, sel, bicubic, &tab};
     const int64_t total = (int64_t)nblk * SH;
     const int64_t g0 = (int64_t)blockIdx.x * 256 * K + threadIdx.x;
-    T val[K];
-    int64_t dst[K];
+    int cX[K], ci[K], cj[K], ck[K], src[K];
 #pragma unroll
     for (int t = 0; t < K; t++) {
         const int64_t g = g0 + (int64_t)t * 256;
-        dst[t] = -1;
+        cX[t] = -1;
+        src[t] = -1;
+        ci[t] = cj[t] = ck[t] = 0;
         if (g >= total) continue;
         const int bq = (int)(g / SH), r0 = (int)(g - (int64_t)bq * SH);
-        const int X = first + bq;
-        int i, j, k, D, side;
+        int i, j, k;
         if (r0 < 2 * A0) {
-            side = r0 / A0;
-            const int t0 = r0 - side * A0;
-            D = 0; i = side ? N : -1; j = t0 % N; k = t0 / N;
+            const int side = r0 / A0, t0 = r0 - side * A0;
+            i = side ? N : -1; j = t0 % N; k = t0 / N;
         } else if (r0 < 2 * A0 + 2 * A1) {
-            const int r = r0 - 2 * A0;
-            side = r / A1;
-            const int t1 = r - side * A1;
-            D = 1; i = t1 % (N + 2) - 1; j = side ? N : -1; k = t1 / (N + 2);
+            const int r = r0 - 2 * A0, side = r / A1, t1 = r - side * A1;
+            i = t1 % (N + 2) - 1; j = side ? N : -1; k = t1 / (N + 2);
         } else {
-            const int r = r0 - 2 * A0 - 2 * A1;
-            side = r / A2;
-            const int t2 = r - side * A2;
-            D = 2; i = t2 % (N + 2) - 1; j = t2 / (N + 2) - 1; k = side ? N : -1;
+            const int r = r0 - 2 * A0 - 2 * A1, side = r / A2, t2 = r - side * A2;
+            i = t2 % (N + 2) - 1; j = t2 / (N + 2) - 1; k = side ? N : -1;
         }
-        const GFace f = gf[6 * X + side + 2 * D];
-        if (!gface_filled(f.type, sel)) {
-            // the top face is not filled: the cell keeps the value of the
-            // highest lower pass that writes it, if any
-            bool any = false;
-            if (D >= 1 && (i == -1 || i == N)) any |= gface_filled(gf[6 * X + (i == N) + 0].type, sel);
-            if (D == 2 && (j == -1 || j == N)) any |= gface_filled(gf[6 * X + (j == N) + 2].type, sel);
-            if (!any) continue;
-            if (D == 2) val[t] = ghost_value<T, N, 1>(a, X, i, j, k);
-            else val[t] = ghost_value<T, N, 0>(a, X, i, j, k);
-        } else if (D == 0) {
-            val[t] = ghost_pass_value<T, N, 0>(a, f, side, X, i, j, k);
-        } else if (D == 1) {
-            val[t] = ghost_pass_value<T, N, 1>(a, f, side, X, i, j, k);
-        } else {
-            val[t] = ghost_pass_value<T, N, 2>(a, f, side, X, i, j, k);
-        }
-        dst[t] = (int64_t)X * V + cidx(G, i, j, k);
+        cX[t] = first + bq;
+        ci[t] = i; cj[t] = j; ck[t] = k;
+        const int sx = i < 0 ? -1 : (i >= N ? 1 : 0), sy = j < 0 ? -1 : (j >= N ? 1 : 0),
+                  sz = k < 0 ? -1 : (k >= N ? 1 : 0);
+        src[t] = src26 ? src26[26 * (int64_t)cX[t] + shell_segment(sx, sy, sz)] : -1;
     }
+    T val[K];
+    bool wr[K];
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+        wr[t] = false;
+        if (cX[t] < 0) continue;
+        if (src[t] >= 0) {
+            auto wrap = [](int x) { return x < 0 ? N - 1 : (x >= N ? 0 : x); };
+            val[t] = u[(int64_t)src[t] * V + cidx(G, wrap(ci[t]), wrap(cj[t]), wrap(ck[t]))];
+            wr[t] = true;
+        }
+    }
+    const GhostLevelArgs<T, N> a{u, gf, oct, sel, bicubic, &tab};
 #pragma unroll
     for (int t = 0; t < K; t++)
-        if (dst[t] >= 0) u[dst[t]] = val[t];
+        if (cX[t] >= 0 && src[t] < 0) {
+            T v;
+            wr[t] = ghost_cell_general<T, N>(a, cX[t], ci[t], cj[t], ck[t], v);
+            val[t] = v;
+        }
+#pragma unroll
+    for (int t = 0; t < K; t++)
+        if (wr[t]) u[(int64_t)cX[t] * V + cidx(G, ci[t], cj[t], ck[t])] = val[t];
 }
 
 // ---------------------------------------------------------------------------
@@ -545,6 +584,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+// bounded wait that also gives up as soon as *abort is set
+__device__ __forceinline__ bool mbar_wait_bounded_abort(uint64_t *bar, uint32_t parity, uint32_t limit,
+                                                        const int *abort) {
+    for (uint32_t t = 0; t < limit; t++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*(const volatile int *)abort) return false;
+    }
+    return false;
+}
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_addr(dst)),
@@ -594,8 +642,15 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // block (the arithmetic of k_relax_tiled), stores the new values straight to
 // u and releases the stage -- so a stage can be refilled as soon as it has
 // been read, and the producer's latencies stay off the consumers' path.
-// Every mbarrier wait is bounded (kWaitPolls): a wait that gives up sets
-// *err, the warp leaves, and the producer stops issuing.
+// Every mbarrier wait is bounded: a wait that gives up sets *err, the warp
+// leaves, and the producer stops issuing.  The consumers' wait for a stage
+// polls at most `cpolls` times (kWaitPolls in a solve; a test sets it to 0
+// to make every such wait give up and check the error path); the
+// producer's wait for a free stage gives up at kWaitPolls or as soon as a
+// consumer has given up; the final drain of copies still in flight always
+// polls up to kWaitPolls, so no bulk copy writes shared memory after the
+// CTA exits.  Every give-up decision is made warp-uniform (vote), so no
+// lane waits at a warp barrier for a lane that has left.
 // resident CTAs per SM the bulk ring's shared memory allows: the register
 // budget that leaves (at 4^3 blocks ptxas otherwise settles on 32 registers
 // and spills)
@@ -614,7 +669,8 @@ __global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T
                                                     const int32_t *__restrict__ blocks, int nblk,
                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
                                                     const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
-                                                    int f, int ipass, unsigned long long *out, int *err) {
+                                                    int f, int ipass, unsigned long long *out, int *err,
+                                                    uint32_t cpolls) {
     pdl_enter();
     using Tl = Tile<N>;
     using Pl = BulkPlan<T, N>;
@@ -684,11 +740,15 @@ __global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T
         int it = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
-            if (it >= S && !mbar_wait_bounded(&empty[s], (uint32_t)((it / S - 1) & 1), kWaitPolls)) {
-                if (lane == 0) pab = 1;
-                break;
+            if (it >= S) {
+                const bool ok =
+                    __all_sync(0xffffffffu, mbar_wait_bounded_abort(&empty[s], (uint32_t)((it / S - 1) & 1), kWaitPolls, &cab));
+                if (!ok) {
+                    if (lane == 0) pab = 1;
+                    break;
+                }
             }
-            if (*(volatile int *)&cab) break;
+            if (__any_sync(0xffffffffu, *(volatile int *)&cab)) break;
             if (it % R == S && (it / R + 1) * R < nsteps) fill_window(it / R + 1);
             const int first = tile * BPC;
             const int cnt = nblk - first < BPC ? nblk - first : BPC;
@@ -714,8 +774,8 @@ __global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T
         int it = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
-            if (!mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), kWaitPolls)) {
-                atomicExch(&cab, 1);
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), cpolls))) {
+                if (lane == 0) atomicExch(&cab, 1);
                 break;
             }
             const int first = tile * BPC;

@@ -216,6 +216,7 @@ public:
     virtual int adjoint(const double *dJdphi, double *dJdrho, sfm_stats *st, cudaStream_t s) = 0;
     virtual int64_t device_bytes() const = 0;
     virtual int fmg_levels() const = 0;
+    virtual void set_wait_polls(uint32_t polls) = 0;
     std::string last_error;
     // g written as [nblocks][3][ni^3] (block interiors only, no io ghost
     // layers) instead of the caller's layout: the host-array entry point
@@ -242,6 +243,7 @@ public:
     double *d_h0 = nullptr, *d_x0 = nullptr;
     FaceItem *d_faces = nullptr;
     GFace *d_gface = nullptr;              // [6 nb] face types and sources for the level fills
+    int32_t *d_src26 = nullptr;            // [26 nb] same-level composition sources (k_ghost_level)
     std::vector<std::array<bool, 3>> ghostMerge;   // [level][sel + 1]: one launch fills the level
     bool ghostMergeOn = true;
     RefluxItem *d_reflux = nullptr;
@@ -262,6 +264,7 @@ public:
     double *d_scal = nullptr;              // [8]
     int *d_bad = nullptr;
     int *d_err = nullptr;                  // set by a device wait that gave up
+    uint32_t waitPolls = kWaitPolls;       // poll limit of the smoother's stage waits (tests lower it)
     int nSM = 148;
     int bulkGrid[5] = {0, 0, 0, 0, 0};     // persistent CTAs of k_relax_bulk<T, N>, by log2(N)
     double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
@@ -332,6 +335,15 @@ public:
         mem.release();
     }
     int64_t device_bytes() const override { return mem.bytes; }
+    // the iteration graph holds the kernel parameters it was captured with:
+    // a new limit drops it, and the next outer iteration captures again
+    void set_wait_polls(uint32_t polls) override {
+        waitPolls = polls;
+        if (iterExec) {
+            cudaGraphExecDestroy(iterExec);
+            iterExec = nullptr;
+        }
+    }
     int fmg_levels() const override { return H.FMax + 1; }
 
     // -----------------------------------------------------------------
@@ -467,6 +479,24 @@ public:
                 if (g.type == 2) g.src = -1;
                 gface[6 * b + fc] = g;
             }
+        // per block and shell segment: the block whose interior the passes
+        // copy when every face on the way is a same-level one (filled by the
+        // fills of kinds -1 and 0), else -1
+        std::vector<int32_t> src26(26 * (size_t)nb, -1);
+        for (int b = 0; b < nb; b++)
+            for (int sz = -1; sz <= 1; sz++)
+                for (int sy = -1; sy <= 1; sy++)
+                    for (int sx = -1; sx <= 1; sx++) {
+                        if (!sx && !sy && !sz) continue;
+                        const int sg[3] = {sx, sy, sz};
+                        int cur = b;
+                        for (int d = 2; d >= 0 && cur >= 0; d--) {
+                            if (!sg[d]) continue;
+                            const GFace &g = gface[6 * cur + (sg[d] > 0) + 2 * d];
+                            cur = g.type == 0 ? g.src : -1;
+                        }
+                        src26[26 * (size_t)b + shell_segment(sx, sy, sz)] = cur;
+                    }
         ghostMerge.assign(nlev, {false, false, false});
         for (int L = 0; L < nlev; L++)
             for (int sel = -1; sel <= 1; sel++) ghostMerge[L][sel + 1] = ghost_merge_ok(gface, L, sel);
@@ -482,6 +512,7 @@ public:
         d_withChild = mem.upload(withChild);
         d_faces = mem.upload(faces);
         d_gface = mem.upload(gface);
+        d_src26 = mem.upload(src26);
         d_reflux = mem.upload(refl);
         d_tfL = mem.upload(tfL);
         d_tfDL = mem.upload(tfDL);
@@ -635,7 +666,7 @@ public:
         if (ghostMergeOn && ghostMerge[L][sel + 1] && (n == 2 || n == 4 || n == 8 || n == 16)) {
             SFM_WITH_N(n,
                        (launch_pdl(k_ghost_level<TT, N>, (unsigned)ghost_level_ctas<N>(cnt(L)), 256, 0, u, d_gface,
-                                   d_oct, H.lstart[L], cnt(L), sel, cubic ? 1 : 0),
+                                   d_oct, sel == 1 ? nullptr : d_src26, H.lstart[L], cnt(L), sel, cubic ? 1 : 0),
                         ++launches),
                        (void)0)
             return;
@@ -775,7 +806,7 @@ public:
                                               (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N>()),
                                               relax_bulk_threads<N>(), BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0,
                                               d_level, rslot,
-                                              rb, f, ipass, out, d_err)
+                                              rb, f, ipass, out, d_err, waitPolls)
                                  : launch_pdl(k_relax_tiled<T, N>,
                                               (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
                                               256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
@@ -1690,6 +1721,15 @@ int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes) {
     if (!c || !c->s) return SFM_EINVAL;
     if (fmg_levels) *fmg_levels = c->s->fmg_levels();
     if (device_bytes) *device_bytes = c->s->device_bytes();
+    return SFM_OK;
+}
+
+// Test hook (not part of include/sfmg.h): poll limit of the smoother's
+// consumer stage waits (k_relax_bulk); 0 makes every such wait give up at
+// once, so a solve exercises the bounded-wait error path (SFM_ETIMEOUT).
+int sfm_debug_set_wait_polls(sfm_ctx *c, uint32_t polls) {
+    if (!c || !c->s) return SFM_EINVAL;
+    c->s->set_wait_polls(polls);
     return SFM_OK;
 }
 

@@ -174,3 +174,28 @@ def test_solve_device_rejects_host_pointers():
         st = s.solve_device(rho_d.data_ptr(), psi_d.data_ptr())
         torch.cuda.synchronize()
         assert st.outer_iters > 0 and torch.cuda.current_device() == dev
+
+
+def test_bounded_smoother_wait_reports_timeout():
+    """Every mbarrier wait of the bulk-copy smoother is bounded.  With the
+    consumers' poll limit set to zero every stage wait gives up at once: the
+    CTA drains the copies it issued (their own wait keeps its full limit),
+    sets the error flag and leaves, and the solve returns SFM_ETIMEOUT instead
+    of hanging.  A fresh context afterwards solves bit-identically to the
+    oracle, so the give-up left the GPU and the library usable."""
+    lib = abi.load_library()
+    lib.sfm_debug_set_wait_polls.argtypes = [C.c_void_p, C.c_uint32]
+    lib.sfm_debug_set_wait_polls.restype = C.c_int
+    h = w.small_periodic(2, 8, 2, 0)
+    p = abi.default_params(abi.SFM_BC_PERIODIC, max_outer=1)
+    rho = w.block_field(h, p.ngh_io, w.gaussian_peak)
+    with FMGPoisson(h, params=p) as s:
+        assert lib.sfm_debug_set_wait_polls(s.ctx, 0) == abi.SFM_OK
+        psi = np.zeros_like(rho)
+        rc = lib.sfm_solve(s.ctx, rho.ctypes.data, psi.ctypes.data, None, None)
+        assert rc == abi.SFM_ETIMEOUT
+    p = abi.default_params(abi.SFM_BC_PERIODIC)
+    rc1, psi1, g1, st1, _ = oracle_solve(h, rho, p)
+    with FMGPoisson(h, params=p) as s:
+        psi2, g2, st2 = s.solve(rho)
+    assert rel(psi2, psi1) == 0.0 and rel(interior(h, g2, 2), interior(h, g1, 2)) == 0.0
