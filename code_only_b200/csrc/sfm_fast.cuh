@@ -202,16 +202,26 @@ __global__ void __launch_bounds__(256) k_ghost_faces(T *u, const FaceItem *__res
 // interior along D of the same level -- which hold either interior values or
 // ghost values of dimensions below D, themselves final after passes < D --
 // and (b) coarse cells of the level above, complete before this level
-// starts.  k_ghost_level evaluates that composition for every shell cell of
-// the level's blocks (depth <= 3: gval<D> calls gval<D-1>), reading only
-// interior cells, coarse cells and ghost cells no pass of this fill writes,
-// and writing only ghost cells of the level: no read meets a write of the
-// same launch.  The same expressions as ghost_face / ghost_copy give
-// bit-identical values.  A ghost cell that no pass writes is left alone; a
-// composition that would read a ghost cell some later pass of the same fill
-// rewrites (possible next to the physical boundary or when one kind of face
-// is filled alone) is detected on the host, and such a level keeps the three
-// passes (Solver::ghost_merge_ok).
+// starts.  k_ghost_level writes those final values for a whole level in one
+// launch.  Its work comes as host-built item lists (GItem), one list per
+// kind of cell so that no warp mixes kinds:
+//   - a face, edge or corner segment whose chain of passes runs through
+//     same-level faces only ends up holding an interior cell of one block
+//     (the neighbour across the highest ghost dimension, then its
+//     neighbour across the next...): a flat copy;
+//   - the face part of a coarse-fine face is the parentlev formula of its
+//     coarse layer and two interior cells, as in ghost_face;
+//   - the few edges and corners whose chain meets a coarse-fine or an
+//     unfilled face follow the composition (ghost_value / ghost_pass_value,
+//     depth <= 3).
+// Every read is of an interior cell, a coarse cell or a ghost cell no pass
+// of this fill writes; every write is a ghost cell of the level: no read
+// meets a write of the same launch, and the same expressions as ghost_face /
+// ghost_copy give bit-identical values.  A cell no pass writes is left
+// alone.  Where the composition would read a ghost cell that a later pass of
+// the same fill rewrites (possible next to the physical boundary, or when
+// only one kind of face is filled), the host keeps the three passes for
+// that level (Solver::ghost_merge_ok).
 struct GFace {             // one face of one block for the level fills
     int32_t src;           // same-level neighbour, parent-level neighbour, or -1
     int8_t type;           // 0 same level, 1 coarse-fine, 2 physical boundary
@@ -323,90 +333,183 @@ __host__ __device__ __forceinline__ int shell_segment(int sx, int sy, int sz) {
     const int s = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
     return s < 13 ? s : s - 1;
 }
-
-// shell cells of one block, grouped by the highest ghost dimension D (the
-// pass that writes them last): D = 0 -> 2 N^2, D = 1 -> 2 (N+2) N, D = 2 -> 2 (N+2)^2
-template <int N>
-__host__ __device__ constexpr int ghost_shell() { return 2 * (N * N + (N + 2) * N + (N + 2) * (N + 2)); }
-constexpr int kGhostLevelK = 4;   // shell cells per thread, loads before stores
-template <int N>
-__host__ __device__ constexpr int ghost_level_ctas(int nblk) {
-    return (int)(((int64_t)nblk * ghost_shell<N>() + 256 * kGhostLevelK - 1) / (256 * kGhostLevelK));
+__host__ __device__ __forceinline__ void segment_sides(int seg, int &sx, int &sy, int &sz) {
+    const int s = seg < 13 ? seg : seg + 1;
+    sx = s % 3 - 1;
+    sy = (s / 3) % 3 - 1;
+    sz = s / 9 - 1;
 }
 
-// src26[26 X + segment]: for a segment whose composition runs through
-// same-level faces only (every one filled), the block whose interior cell
-// the passes end up copying -- the neighbour across the highest ghost
-// dimension, then its neighbour across the next, and so on -- at the cell's
-// coordinates wrapped into the block (-1 -> N-1, N -> 0); -1 otherwise.
-// Such cells (all of them on a level without coarse-fine or boundary faces)
-// cost one table load and one value load.  A fill of coarse-fine faces only
-// (sel 1) passes no table: its same-level faces are not filled.
+// One item of a level fill: a face, edge or corner segment of a block.
+// Ranges of one launch (cells per item):
+//   0 same-level faces   (N^2): the chain of the passes runs through
+//   1 same-level edges   (N)    same-level faces only; `src` is the block
+//   2 same-level corners (1)    whose interior cell the passes copy
+//   3 coarse-fine faces  (N^2): the parentlev formula, `src` the coarse block
+//   4 other edges        (N)    the general composition (a coarse-fine or an
+//   5 other corners      (1)    unfilled face on the way)
+struct GItem {
+    int32_t dst, src;
+    int8_t seg, pad[3];
+};
+constexpr int kGhostRanges = 6;
+struct GhostLevelPlan {
+    int cta0[kGhostRanges + 1];   // first CTA of each range; cta0[6] = grid size
+    int64_t off[kGhostRanges];    // first item of each range
+    int cnt[kGhostRanges];        // items of each range
+};
+template <int N>
+__host__ __device__ constexpr int ghost_range_cells(int r) { return (r == 0 || r == 3) ? N * N : ((r == 1 || r == 4) ? N : 1); }
+constexpr int kGhostLevelK = 4;   // cells per thread, loads before stores
+template <int N>
+__host__ __device__ constexpr int ghost_range_ctas(int r, int items) {
+    return (int)(((int64_t)items * ghost_range_cells<N>(r) + 256 * kGhostLevelK - 1) / (256 * kGhostLevelK));
+}
+
+// cell `c` of segment `seg`: the ghost coordinate of each nonzero side, the
+// free coordinates from c (lower dimension fastest)
+template <int N>
+__device__ __forceinline__ void segment_cell(int seg, int c, int &i, int &j, int &k) {
+    int sx, sy, sz;
+    segment_sides(seg, sx, sy, sz);
+    const int sd[3] = {sx, sy, sz};
+    int o[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (sd[d] != 0) {
+            o[d] = sd[d] < 0 ? -1 : N;
+        } else {
+            o[d] = c % N;
+            c /= N;
+        }
+    }
+    i = o[0]; j = o[1]; k = o[2];
+}
+
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_ghost_level(T *u, const GFace *__restrict__ gf, const int8_t *__restrict__ oct,
-                                                     const int32_t *__restrict__ src26, int first, int nblk, int sel,
-                                                     int cubic) {
+__global__ void __launch_bounds__(256) k_ghost_level(T *u, const GItem *__restrict__ items, GhostLevelPlan plan,
+                                                     const GFace *__restrict__ gf, const int8_t *__restrict__ oct,
+                                                     int sel, int cubic) {
     pdl_enter();
-    constexpr int G = N + 2, NB2 = N / 2, SH = ghost_shell<N>(), K = kGhostLevelK;
-    constexpr int A0 = N * N, A1 = (N + 2) * N, A2 = (N + 2) * (N + 2);
+    constexpr int G = N + 2, NB2 = N / 2, K = kGhostLevelK;
     constexpr int64_t V = (int64_t)G * G * G;
     __shared__ GhostCubicTable<N> tab;
-    const bool bicubic = cubic && NB2 + 2 >= 4 && sel != 0;
-    if (bicubic) {
+    // this CTA's range, its first CTA, first item and item count (unrolled
+    // selects: no run-time indexing of the parameter arrays)
+    int r = 0, rc0 = 0, rcnt = 0;
+    int64_t roff = 0;
+#pragma unroll
+    for (int q = 1; q < kGhostRanges; q++)
+        if ((int)blockIdx.x >= plan.cta0[q]) r = q;
+#pragma unroll
+    for (int q = 0; q < kGhostRanges; q++)
+        if (q == r) {
+            rc0 = plan.cta0[q];
+            roff = plan.off[q];
+            rcnt = plan.cnt[q];
+        }
+    const bool bicubic = cubic && NB2 + 2 >= 4 && sel != 0 && r >= 3;
+    if (bicubic) {   // CTA-uniform
         if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, tab.c[threadIdx.x], tab.w[threadIdx.x]);
         __syncthreads();
     }
-    const int64_t total = (int64_t)nblk * SH;
-    const int64_t g0 = (int64_t)blockIdx.x * 256 * K + threadIdx.x;
-    int cX[K], ci[K], cj[K], ck[K], src[K];
-#pragma unroll
-    for (int t = 0; t < K; t++) {
-        const int64_t g = g0 + (int64_t)t * 256;
-        cX[t] = -1;
-        src[t] = -1;
-        ci[t] = cj[t] = ck[t] = 0;
-        if (g >= total) continue;
-        const int bq = (int)(g / SH), r0 = (int)(g - (int64_t)bq * SH);
-        int i, j, k;
-        if (r0 < 2 * A0) {
-            const int side = r0 / A0, t0 = r0 - side * A0;
-            i = side ? N : -1; j = t0 % N; k = t0 / N;
-        } else if (r0 < 2 * A0 + 2 * A1) {
-            const int r = r0 - 2 * A0, side = r / A1, t1 = r - side * A1;
-            i = t1 % (N + 2) - 1; j = side ? N : -1; k = t1 / (N + 2);
-        } else {
-            const int r = r0 - 2 * A0 - 2 * A1, side = r / A2, t2 = r - side * A2;
-            i = t2 % (N + 2) - 1; j = t2 / (N + 2) - 1; k = side ? N : -1;
-        }
-        cX[t] = first + bq;
-        ci[t] = i; cj[t] = j; ck[t] = k;
-        const int sx = i < 0 ? -1 : (i >= N ? 1 : 0), sy = j < 0 ? -1 : (j >= N ? 1 : 0),
-                  sz = k < 0 ? -1 : (k >= N ? 1 : 0);
-        src[t] = src26 ? src26[26 * (int64_t)cX[t] + shell_segment(sx, sy, sz)] : -1;
-    }
+    const int CP = ghost_range_cells<N>(r);
+    const int64_t total = (int64_t)rcnt * CP;
+    const GItem *it = items + roff;
+    const int64_t g0 = (int64_t)((int)blockIdx.x - rc0) * 256 * K + threadIdx.x;
     T val[K];
-    bool wr[K];
+    int64_t dst[K];
+    if (r <= 2) {
+        // same-level compositions: item load, then value load
+        int64_t src[K];
 #pragma unroll
-    for (int t = 0; t < K; t++) {
-        wr[t] = false;
-        if (cX[t] < 0) continue;
-        if (src[t] >= 0) {
+        for (int t = 0; t < K; t++) {
+            const int64_t g = g0 + (int64_t)t * 256;
+            dst[t] = -1;
+            src[t] = 0;
+            if (g >= total) continue;
+            const int q = (int)(g / CP), c = (int)(g - (int64_t)q * CP);
+            const GItem e = it[q];
+            int i, j, k;
+            segment_cell<N>(e.seg, c, i, j, k);
             auto wrap = [](int x) { return x < 0 ? N - 1 : (x >= N ? 0 : x); };
-            val[t] = u[(int64_t)src[t] * V + cidx(G, wrap(ci[t]), wrap(cj[t]), wrap(ck[t]))];
-            wr[t] = true;
+            dst[t] = (int64_t)e.dst * V + cidx(G, i, j, k);
+            src[t] = (int64_t)e.src * V + cidx(G, wrap(i), wrap(j), wrap(k));
+        }
+#pragma unroll
+        for (int t = 0; t < K; t++)
+            if (dst[t] >= 0) val[t] = u[src[t]];
+    } else if (r == 3) {
+        // coarse-fine face parts: transverse interior, so u0 and uN are
+        // interior cells (fmg_ghfix_parentlev, as ghost_face)
+#pragma unroll
+        for (int t = 0; t < K; t++) {
+            const int64_t g = g0 + (int64_t)t * 256;
+            dst[t] = -1;
+            if (g >= total) continue;
+            const int q = (int)(g / CP), c = (int)(g - (int64_t)q * CP);
+            const GItem e = it[q];
+            int sx, sy, sz;
+            segment_sides(e.seg, sx, sy, sz);
+            const int D = sx ? 0 : (sy ? 1 : 2), lr = (sx + sy + sz) > 0 ? 1 : 0;
+            const int p = c % N, qq = c / N;   // lower, upper transverse coordinate
+            int i, j, k;
+            put3(D, lr ? N : -1, p, qq, i, j, k);
+            const T *uc = u + (int64_t)e.src * V;
+            const T *ud = u + (int64_t)e.dst * V;
+            const int xc = lr == 0 ? N - 1 : 0;
+            const int oa = oct[3 * e.dst + tra(D)] * NB2, ob = oct[3 * e.dst + trb(D)] * NB2;
+            auto B = [&](int pb, int qb) -> T {
+                int ci, cj, ck;
+                put3(D, xc, pb + oa, qb + ob, ci, cj, ck);
+                return uc[cidx(G, ci, cj, ck)];
+            };
+            T uH;
+            if (bicubic) {
+                const int *cp = tab.c[p + 1], *cq = tab.c[qq + 1];
+                const double *wp = tab.w[p + 1], *wq = tab.w[qq + 1];
+                T bx[4];
+#pragma unroll
+                for (int m = 0; m < 4; m++)
+                    bx[m] = (T)wp[0] * B(cp[0], cq[m]) + (T)wp[1] * B(cp[1], cq[m]) + (T)wp[2] * B(cp[2], cq[m])
+                          + (T)wp[3] * B(cp[3], cq[m]);
+                uH = (T)wq[0] * bx[0] + (T)wq[1] * bx[1] + (T)wq[2] * bx[2] + (T)wq[3] * bx[3];
+            } else {
+                const int pc = fdiv2(p), qc = fdiv2(qq);
+                const int p1 = near_(p, pc), q1 = near_(qq, qc);
+                uH = ((T)9 * B(pc, qc) + B(p1, q1) + (T)3 * B(pc, q1) + (T)3 * B(p1, qc)) / (T)16;
+            }
+            const int xg = lr ? N : -1, inner = lr ? -1 : 1;
+            int i0, j0, k0, iN, jN, kN;
+            put3(D, xg + inner, p, qq, i0, j0, k0);
+            put3(D, xg + 2 * inner, p, qq, iN, jN, kN);
+            const T u0 = ud[cidx(G, i0, j0, k0)], uN = ud[cidx(G, iN, jN, kN)];
+            val[t] = ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
+            dst[t] = (int64_t)e.dst * V + cidx(G, i, j, k);
+        }
+    } else {
+        // edges and corners whose composition meets a coarse-fine or an
+        // unfilled face: evaluated through the passes' composition
+        const GhostLevelArgs<T, N> a{u, gf, oct, sel, bicubic, &tab};
+#pragma unroll
+        for (int t = 0; t < K; t++) {
+            const int64_t g = g0 + (int64_t)t * 256;
+            dst[t] = -1;
+            if (g >= total) continue;
+            const int q = (int)(g / CP), c = (int)(g - (int64_t)q * CP);
+            const GItem e = it[q];
+            int i, j, k;
+            segment_cell<N>(e.seg, c, i, j, k);
+            T v;
+            if (ghost_cell_general<T, N>(a, e.dst, i, j, k, v)) {
+                val[t] = v;
+                dst[t] = (int64_t)e.dst * V + cidx(G, i, j, k);
+            }
         }
     }
-    const GhostLevelArgs<T, N> a{u, gf, oct, sel, bicubic, &tab};
 #pragma unroll
     for (int t = 0; t < K; t++)
-        if (cX[t] >= 0 && src[t] < 0) {
-            T v;
-            wr[t] = ghost_cell_general<T, N>(a, cX[t], ci[t], cj[t], ck[t], v);
-            val[t] = v;
-        }
-#pragma unroll
-    for (int t = 0; t < K; t++)
-        if (wr[t]) u[(int64_t)cX[t] * V + cidx(G, ci[t], cj[t], ck[t])] = val[t];
+        if (dst[t] >= 0) u[dst[t]] = val[t];
 }
 
 // ---------------------------------------------------------------------------

@@ -243,7 +243,9 @@ public:
     double *d_h0 = nullptr, *d_x0 = nullptr;
     FaceItem *d_faces = nullptr;
     GFace *d_gface = nullptr;              // [6 nb] face types and sources for the level fills
-    int32_t *d_src26 = nullptr;            // [26 nb] same-level composition sources (k_ghost_level)
+    GItem *d_gitems = nullptr;             // item lists of the level fills (k_ghost_level)
+    std::vector<std::array<std::array<int64_t, kGhostRanges>, 3>> gOff;   // [level][sel + 1][range]
+    std::vector<std::array<std::array<int, kGhostRanges>, 3>> gCnt;
     std::vector<std::array<bool, 3>> ghostMerge;   // [level][sel + 1]: one launch fills the level
     bool ghostMergeOn = true;
     RefluxItem *d_reflux = nullptr;
@@ -479,27 +481,53 @@ public:
                 if (g.type == 2) g.src = -1;
                 gface[6 * b + fc] = g;
             }
-        // per block and shell segment: the block whose interior the passes
-        // copy when every face on the way is a same-level one (filled by the
-        // fills of kinds -1 and 0), else -1
-        std::vector<int32_t> src26(26 * (size_t)nb, -1);
-        for (int b = 0; b < nb; b++)
-            for (int sz = -1; sz <= 1; sz++)
-                for (int sy = -1; sy <= 1; sy++)
-                    for (int sx = -1; sx <= 1; sx++) {
-                        if (!sx && !sy && !sz) continue;
-                        const int sg[3] = {sx, sy, sz};
-                        int cur = b;
-                        for (int d = 2; d >= 0 && cur >= 0; d--) {
-                            if (!sg[d]) continue;
-                            const GFace &g = gface[6 * cur + (sg[d] > 0) + 2 * d];
-                            cur = g.type == 0 ? g.src : -1;
-                        }
-                        src26[26 * (size_t)b + shell_segment(sx, sy, sz)] = cur;
-                    }
         ghostMerge.assign(nlev, {false, false, false});
         for (int L = 0; L < nlev; L++)
             for (int sel = -1; sel <= 1; sel++) ghostMerge[L][sel + 1] = ghost_merge_ok(gface, L, sel);
+        // item lists of the exact level fills, by range (see GItem)
+        std::vector<GItem> gitems;
+        gOff.assign(nlev, {});
+        gCnt.assign(nlev, {});
+        for (int L = 0; L < nlev; L++)
+            for (int sel = -1; sel <= 1; sel++) {
+                std::array<std::vector<GItem>, kGhostRanges> rg;
+                if (ghostMerge[L][sel + 1])
+                    for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                        for (int seg = 0; seg < 26; seg++) {
+                            int sg[3];
+                            segment_sides(seg, sg[0], sg[1], sg[2]);
+                            const int nz = (sg[0] != 0) + (sg[1] != 0) + (sg[2] != 0);
+                            bool written = false;
+                            for (int d = 0; d < 3; d++)
+                                if (sg[d] && gface_filled(gface[6 * b + (sg[d] > 0) + 2 * d].type, sel)) written = true;
+                            if (!written) continue;   // no pass writes the segment
+                            int cur = b;   // the chain of the passes through same-level faces only
+                            for (int d = 2; d >= 0 && cur >= 0; d--) {
+                                if (!sg[d]) continue;
+                                const GFace &g = gface[6 * cur + (sg[d] > 0) + 2 * d];
+                                cur = (g.type == 0 && gface_filled(0, sel)) ? g.src : -1;
+                            }
+                            GItem e{};
+                            e.dst = b;
+                            e.seg = (int8_t)seg;
+                            if (cur >= 0) {
+                                e.src = cur;
+                                rg[nz - 1].push_back(e);
+                            } else if (nz == 1) {   // a filled coarse-fine face
+                                const int d = sg[0] ? 0 : (sg[1] ? 1 : 2);
+                                e.src = gface[6 * b + (sg[d] > 0) + 2 * d].src;
+                                rg[3].push_back(e);
+                            } else {
+                                e.src = -1;
+                                rg[nz == 2 ? 4 : 5].push_back(e);
+                            }
+                        }
+                for (int r = 0; r < kGhostRanges; r++) {
+                    gOff[L][sel + 1][r] = (int64_t)gitems.size();
+                    gCnt[L][sel + 1][r] = (int)rg[r].size();
+                    gitems.insert(gitems.end(), rg[r].begin(), rg[r].end());
+                }
+            }
         d_level = mem.upload(std::vector<int32_t>(H.level.begin(), H.level.end()));
         d_parent = mem.upload(std::vector<int32_t>(H.parent.begin(), H.parent.end()));
         d_oct = mem.upload(H.oct);
@@ -512,7 +540,7 @@ public:
         d_withChild = mem.upload(withChild);
         d_faces = mem.upload(faces);
         d_gface = mem.upload(gface);
-        d_src26 = mem.upload(src26);
+        d_gitems = mem.upload(gitems);
         d_reflux = mem.upload(refl);
         d_tfL = mem.upload(tfL);
         d_tfDL = mem.upload(tfDL);
@@ -658,17 +686,29 @@ public:
                         if (sx || sy || sz) walk(walk, b, {sx, sy, sz}, 2);
         return !race;
     }
+    template <class TT, int N>
+    void ghost_level_launch(int L, TT *u, bool cubic, int sel) {
+        GhostLevelPlan pl{};
+        int ctas = 0;
+        for (int r = 0; r < kGhostRanges; r++) {
+            pl.cta0[r] = ctas;
+            pl.off[r] = gOff[L][sel + 1][r];
+            pl.cnt[r] = gCnt[L][sel + 1][r];
+            ctas += ghost_range_ctas<N>(r, pl.cnt[r]);
+        }
+        pl.cta0[kGhostRanges] = ctas;
+        if (ctas == 0) return;
+        launch_pdl(k_ghost_level<TT, N>, (unsigned)ctas, 256, 0, u, (const GItem *)d_gitems, pl,
+                   (const GFace *)d_gface, (const int8_t *)d_oct, sel, cubic ? 1 : 0);
+        ++launches;
+    }
     // one fill of level L: k_ghost_level where exact, else the three passes
     template <class TT>
     void ghost_fill_level(int L, int f, TT *u, bool cubic, int sel) {
         const int n = nf[f];
         if (sel == 1 && L <= 0) return;
         if (ghostMergeOn && ghostMerge[L][sel + 1] && (n == 2 || n == 4 || n == 8 || n == 16)) {
-            SFM_WITH_N(n,
-                       (launch_pdl(k_ghost_level<TT, N>, (unsigned)ghost_level_ctas<N>(cnt(L)), 256, 0, u, d_gface,
-                                   d_oct, sel == 1 ? nullptr : d_src26, H.lstart[L], cnt(L), sel, cubic ? 1 : 0),
-                        ++launches),
-                       (void)0)
+            SFM_WITH_N(n, (ghost_level_launch<TT, N>(L, u, cubic, sel)), (void)0)
             return;
         }
         for (int dir = 0; dir < 3; dir++) ghost_pass(L, f, dir, u, cubic, sel);
