@@ -340,176 +340,182 @@ __host__ __device__ __forceinline__ void segment_sides(int seg, int &sx, int &sy
     sz = s / 9 - 1;
 }
 
-// One item of a level fill: a face, edge or corner segment of a block.
-// Ranges of one launch (cells per item):
-//   0 same-level faces   (N^2): the chain of the passes runs through
-//   1 same-level edges   (N)    same-level faces only; `src` is the block
-//   2 same-level corners (1)    whose interior cell the passes copy
-//   3 coarse-fine faces  (N^2): the parentlev formula, `src` the coarse block
-//   4 other edges        (N)    the general composition (a coarse-fine or an
-//   5 other corners      (1)    unfilled face on the way)
+// Kind of a shell segment of a block in one level fill (kind26[26 X + seg]):
+//   >= 0  the chain of the passes runs through filled same-level faces only
+//         and the segment ends up holding interior cells of that block (the
+//         neighbour across the highest ghost dimension, then its neighbour
+//         across the next...), at the cell's coordinates wrapped into it;
+//   -1    no pass of the fill writes the segment;
+//   -2    a filled coarse-fine face (face segment): the parentlev formula;
+//   -3    anything else (edges and corners whose chain meets a coarse-fine
+//         or an unfilled face): the general composition, done by the
+//         trailing CTAs of the launch from a list of (block, segment) items.
+constexpr int kSegSkip = -1, kSegCF = -2, kSegGeneral = -3;
 struct GItem {
-    int32_t dst, src;
+    int32_t dst;
     int8_t seg, pad[3];
 };
-constexpr int kGhostRanges = 6;
-struct GhostLevelPlan {
-    int cta0[kGhostRanges + 1];   // first CTA of each range; cta0[6] = grid size
-    int64_t off[kGhostRanges];    // first item of each range
-    int cnt[kGhostRanges];        // items of each range
-};
-template <int N>
-__host__ __device__ constexpr int ghost_range_cells(int r) { return (r == 0 || r == 3) ? N * N : ((r == 1 || r == 4) ? N : 1); }
-constexpr int kGhostLevelK = 4;   // cells per thread, loads before stores
-template <int N>
-__host__ __device__ constexpr int ghost_range_ctas(int r, int items) {
-    return (int)(((int64_t)items * ghost_range_cells<N>(r) + 256 * kGhostLevelK - 1) / (256 * kGhostLevelK));
-}
 
-// cell `c` of segment `seg`: the ghost coordinate of each nonzero side, the
-// free coordinates from c (lower dimension fastest)
+// shell cells of one block, grouped by the highest ghost dimension (the
+// pass that writes them last): 2 N^2 on x planes, 2 (N+2) N on y planes,
+// 2 (N+2)^2 on z planes -- every cell once, all of a block's together
 template <int N>
-__device__ __forceinline__ void segment_cell(int seg, int c, int &i, int &j, int &k) {
-    int sx, sy, sz;
-    segment_sides(seg, sx, sy, sz);
-    const int sd[3] = {sx, sy, sz};
-    int o[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        if (sd[d] != 0) {
-            o[d] = sd[d] < 0 ? -1 : N;
-        } else {
-            o[d] = c % N;
-            c /= N;
-        }
-    }
-    i = o[0]; j = o[1]; k = o[2];
-}
-
+__host__ __device__ constexpr int ghost_shell() { return 2 * (N * N + (N + 2) * N + (N + 2) * (N + 2)); }
+// cells per thread (eight 4-byte cells fit the 64-register budget, eight doubles do not)
 template <class T, int N>
-__global__ void __launch_bounds__(256) k_ghost_level(T *u, const GItem *__restrict__ items, GhostLevelPlan plan,
-                                                     const GFace *__restrict__ gf, const int8_t *__restrict__ oct,
-                                                     int sel, int cubic) {
+__host__ __device__ constexpr int ghost_level_k() { return N >= 8 && sizeof(T) == 4 ? 8 : 4; }
+template <class T, int N>
+__host__ __device__ constexpr int ghost_sweep_ctas(int nblk) {
+    return (int)(((int64_t)nblk * ghost_shell<N>() + 256 * ghost_level_k<T, N>() - 1) / (256 * ghost_level_k<T, N>()));
+}
+template <int N>
+__host__ __device__ constexpr int ghost_general_ctas(int items) {
+    return (int)(((int64_t)items * N + 255) / 256);   // N cells per item (corners use the first)
+}
+
+// cell r (0 .. ghost_shell - 1) of a block's shell
+template <int N>
+__device__ __forceinline__ void shell_cell(int r0, int &i, int &j, int &k) {
+    constexpr int A0 = N * N, A1 = (N + 2) * N, A2 = (N + 2) * (N + 2);
+    if (r0 < 2 * A0) {
+        const int side = r0 / A0, t0 = r0 - side * A0;
+        i = side ? N : -1; j = t0 % N; k = t0 / N;
+    } else if (r0 < 2 * A0 + 2 * A1) {
+        const int r = r0 - 2 * A0, side = r / A1, t1 = r - side * A1;
+        i = t1 % (N + 2) - 1; j = side ? N : -1; k = t1 / (N + 2);
+    } else {
+        const int r = r0 - 2 * A0 - 2 * A1, side = r / A2, t2 = r - side * A2;
+        i = t2 % (N + 2) - 1; j = t2 / (N + 2) - 1; k = side ? N : -1;
+    }
+}
+
+// the parentlev value of cell (i,j,k) on the face part (transverse interior)
+// of coarse-fine face (D, lr) of block X, coarse block C (as ghost_face)
+template <class T, int N>
+__device__ __noinline__ T ghost_cf_face(const T *u, const int8_t *oct, int X, int C, int D, int lr, int i, int j, int k,
+                                        bool bicubic, const GhostCubicTable<N> *tab) {
+    constexpr int G = N + 2, NB2 = N / 2;
+    constexpr int64_t V = (int64_t)G * G * G;
+    const int p = D == 0 ? j : i, q = D == 2 ? j : k;
+    const T *uc = u + (int64_t)C * V;
+    const T *ud = u + (int64_t)X * V;
+    const int xc = lr == 0 ? N - 1 : 0;
+    const int oa = oct[3 * X + tra(D)] * NB2, ob = oct[3 * X + trb(D)] * NB2;
+    auto B = [&](int pb, int qb) -> T {
+        int ci, cj, ck;
+        put3(D, xc, pb + oa, qb + ob, ci, cj, ck);
+        return uc[cidx(G, ci, cj, ck)];
+    };
+    T uH;
+    if (bicubic) {
+        const int *cp = tab->c[p + 1], *cq = tab->c[q + 1];
+        const double *wp = tab->w[p + 1], *wq = tab->w[q + 1];
+        T bx[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            bx[m] = (T)wp[0] * B(cp[0], cq[m]) + (T)wp[1] * B(cp[1], cq[m]) + (T)wp[2] * B(cp[2], cq[m])
+                  + (T)wp[3] * B(cp[3], cq[m]);
+        uH = (T)wq[0] * bx[0] + (T)wq[1] * bx[1] + (T)wq[2] * bx[2] + (T)wq[3] * bx[3];
+    } else {
+        const int pc = fdiv2(p), qc = fdiv2(q);
+        const int p1 = near_(p, pc), q1 = near_(q, qc);
+        uH = ((T)9 * B(pc, qc) + B(p1, q1) + (T)3 * B(pc, q1) + (T)3 * B(p1, qc)) / (T)16;
+    }
+    const int xg = lr ? N : -1, inner = lr ? -1 : 1;
+    int i0, j0, k0, iN, jN, kN;
+    put3(D, xg + inner, p, q, i0, j0, k0);
+    put3(D, xg + 2 * inner, p, q, iN, jN, kN);
+    const T u0 = ud[cidx(G, i0, j0, k0)], uN = ud[cidx(G, iN, jN, kN)];
+    return ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
+}
+
+// One fill of the level's blocks first .. first+nblk-1: the first `sweep`
+// CTAs walk every block's shell (K cells per thread: kind loads, value
+// loads, then stores), the rest take the general items.
+template <class T, int N>
+__global__ void __launch_bounds__(256, 4) k_ghost_level(T *u, const int32_t *__restrict__ kind26,
+                                                        const GItem *__restrict__ gen, int ngen, int first, int nblk,
+                                                        int sweep, const GFace *__restrict__ gf,
+                                                        const int8_t *__restrict__ oct, int sel, int cubic) {
     pdl_enter();
-    constexpr int G = N + 2, NB2 = N / 2, K = kGhostLevelK;
+    constexpr int G = N + 2, NB2 = N / 2, SH = ghost_shell<N>(), K = ghost_level_k<T, N>();
     constexpr int64_t V = (int64_t)G * G * G;
     __shared__ GhostCubicTable<N> tab;
-    // this CTA's range, its first CTA, first item and item count (unrolled
-    // selects: no run-time indexing of the parameter arrays)
-    int r = 0, rc0 = 0, rcnt = 0;
-    int64_t roff = 0;
-#pragma unroll
-    for (int q = 1; q < kGhostRanges; q++)
-        if ((int)blockIdx.x >= plan.cta0[q]) r = q;
-#pragma unroll
-    for (int q = 0; q < kGhostRanges; q++)
-        if (q == r) {
-            rc0 = plan.cta0[q];
-            roff = plan.off[q];
-            rcnt = plan.cnt[q];
-        }
-    const bool bicubic = cubic && NB2 + 2 >= 4 && sel != 0 && r >= 3;
-    if (bicubic) {   // CTA-uniform
+    const bool bicubic = cubic && NB2 + 2 >= 4 && sel != 0;
+    if (bicubic) {   // launch-uniform
         if (threadIdx.x < G) cubic_weights((int)threadIdx.x - 1, -1, NB2, tab.c[threadIdx.x], tab.w[threadIdx.x]);
         __syncthreads();
     }
-    const int CP = ghost_range_cells<N>(r);
-    const int64_t total = (int64_t)rcnt * CP;
-    const GItem *it = items + roff;
-    const int64_t g0 = (int64_t)((int)blockIdx.x - rc0) * 256 * K + threadIdx.x;
-    T val[K];
-    int64_t dst[K];
-    if (r <= 2) {
-        // same-level compositions: item load, then value load
-        int64_t src[K];
+    if ((int)blockIdx.x < sweep) {
+        const int64_t total = (int64_t)nblk * SH;
+        const int64_t g0 = (int64_t)blockIdx.x * 256 * K + threadIdx.x;
+        // per cell: block, packed coordinates (i+1) | (j+1) << 8 | (k+1) << 16, kind
+        int X[K], pk[K], kd[K];
+        auto unpack = [](int v, int &i, int &j, int &k) {
+            i = (v & 255) - 1;
+            j = ((v >> 8) & 255) - 1;
+            k = (v >> 16) - 1;
+        };
 #pragma unroll
         for (int t = 0; t < K; t++) {
             const int64_t g = g0 + (int64_t)t * 256;
-            dst[t] = -1;
-            src[t] = 0;
+            kd[t] = kSegSkip;
+            X[t] = 0;
+            pk[t] = 0;
             if (g >= total) continue;
-            const int q = (int)(g / CP), c = (int)(g - (int64_t)q * CP);
-            const GItem e = it[q];
+            const int bq = (int)(g / SH);
             int i, j, k;
-            segment_cell<N>(e.seg, c, i, j, k);
+            shell_cell<N>((int)(g - (int64_t)bq * SH), i, j, k);
+            X[t] = first + bq;
+            pk[t] = (i + 1) | ((j + 1) << 8) | ((k + 1) << 16);
+            const int sx = i < 0 ? -1 : (i >= N ? 1 : 0), sy = j < 0 ? -1 : (j >= N ? 1 : 0),
+                      sz = k < 0 ? -1 : (k >= N ? 1 : 0);
+            kd[t] = kind26[26 * (int64_t)X[t] + shell_segment(sx, sy, sz)];
+        }
+        T val[K];
+#pragma unroll
+        for (int t = 0; t < K; t++) {
+            if (kd[t] < 0) continue;
             auto wrap = [](int x) { return x < 0 ? N - 1 : (x >= N ? 0 : x); };
-            dst[t] = (int64_t)e.dst * V + cidx(G, i, j, k);
-            src[t] = (int64_t)e.src * V + cidx(G, wrap(i), wrap(j), wrap(k));
+            int i, j, k;
+            unpack(pk[t], i, j, k);
+            val[t] = u[(int64_t)kd[t] * V + cidx(G, wrap(i), wrap(j), wrap(k))];
+        }
+#pragma unroll
+        for (int t = 0; t < K; t++) {
+            if (kd[t] != kSegCF) continue;
+            int i, j, k;
+            unpack(pk[t], i, j, k);
+            const int D = (i == -1 || i == N) ? 0 : ((j == -1 || j == N) ? 1 : 2);
+            const int c = D == 0 ? i : (D == 1 ? j : k);
+            const int lr = c == N ? 1 : 0;
+            val[t] = ghost_cf_face<T, N>(u, oct, X[t], gf[6 * X[t] + lr + 2 * D].src, D, lr, i, j, k, bicubic, &tab);
         }
 #pragma unroll
         for (int t = 0; t < K; t++)
-            if (dst[t] >= 0) val[t] = u[src[t]];
-    } else if (r == 3) {
-        // coarse-fine face parts: transverse interior, so u0 and uN are
-        // interior cells (fmg_ghfix_parentlev, as ghost_face)
-#pragma unroll
-        for (int t = 0; t < K; t++) {
-            const int64_t g = g0 + (int64_t)t * 256;
-            dst[t] = -1;
-            if (g >= total) continue;
-            const int q = (int)(g / CP), c = (int)(g - (int64_t)q * CP);
-            const GItem e = it[q];
-            int sx, sy, sz;
-            segment_sides(e.seg, sx, sy, sz);
-            const int D = sx ? 0 : (sy ? 1 : 2), lr = (sx + sy + sz) > 0 ? 1 : 0;
-            const int p = c % N, qq = c / N;   // lower, upper transverse coordinate
-            int i, j, k;
-            put3(D, lr ? N : -1, p, qq, i, j, k);
-            const T *uc = u + (int64_t)e.src * V;
-            const T *ud = u + (int64_t)e.dst * V;
-            const int xc = lr == 0 ? N - 1 : 0;
-            const int oa = oct[3 * e.dst + tra(D)] * NB2, ob = oct[3 * e.dst + trb(D)] * NB2;
-            auto B = [&](int pb, int qb) -> T {
-                int ci, cj, ck;
-                put3(D, xc, pb + oa, qb + ob, ci, cj, ck);
-                return uc[cidx(G, ci, cj, ck)];
-            };
-            T uH;
-            if (bicubic) {
-                const int *cp = tab.c[p + 1], *cq = tab.c[qq + 1];
-                const double *wp = tab.w[p + 1], *wq = tab.w[qq + 1];
-                T bx[4];
-#pragma unroll
-                for (int m = 0; m < 4; m++)
-                    bx[m] = (T)wp[0] * B(cp[0], cq[m]) + (T)wp[1] * B(cp[1], cq[m]) + (T)wp[2] * B(cp[2], cq[m])
-                          + (T)wp[3] * B(cp[3], cq[m]);
-                uH = (T)wq[0] * bx[0] + (T)wq[1] * bx[1] + (T)wq[2] * bx[2] + (T)wq[3] * bx[3];
-            } else {
-                const int pc = fdiv2(p), qc = fdiv2(qq);
-                const int p1 = near_(p, pc), q1 = near_(qq, qc);
-                uH = ((T)9 * B(pc, qc) + B(p1, q1) + (T)3 * B(pc, q1) + (T)3 * B(p1, qc)) / (T)16;
+            if (kd[t] >= 0 || kd[t] == kSegCF) {
+                int i, j, k;
+                unpack(pk[t], i, j, k);
+                u[(int64_t)X[t] * V + cidx(G, i, j, k)] = val[t];
             }
-            const int xg = lr ? N : -1, inner = lr ? -1 : 1;
-            int i0, j0, k0, iN, jN, kN;
-            put3(D, xg + inner, p, qq, i0, j0, k0);
-            put3(D, xg + 2 * inner, p, qq, iN, jN, kN);
-            const T u0 = ud[cidx(G, i0, j0, k0)], uN = ud[cidx(G, iN, jN, kN)];
-            val[t] = ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
-            dst[t] = (int64_t)e.dst * V + cidx(G, i, j, k);
-        }
-    } else {
-        // edges and corners whose composition meets a coarse-fine or an
-        // unfilled face: evaluated through the passes' composition
-        const GhostLevelArgs<T, N> a{u, gf, oct, sel, bicubic, &tab};
-#pragma unroll
-        for (int t = 0; t < K; t++) {
-            const int64_t g = g0 + (int64_t)t * 256;
-            dst[t] = -1;
-            if (g >= total) continue;
-            const int q = (int)(g / CP), c = (int)(g - (int64_t)q * CP);
-            const GItem e = it[q];
-            int i, j, k;
-            segment_cell<N>(e.seg, c, i, j, k);
-            T v;
-            if (ghost_cell_general<T, N>(a, e.dst, i, j, k, v)) {
-                val[t] = v;
-                dst[t] = (int64_t)e.dst * V + cidx(G, i, j, k);
-            }
-        }
+        return;
     }
+    // general items: N cells per item (the free coordinate of an edge; a
+    // corner uses cell 0 only); loads happen in the composition, then one store
+    const int64_t g = (int64_t)((int)blockIdx.x - sweep) * 256 + threadIdx.x;
+    const int q = (int)(g / N), c = (int)(g - (int64_t)q * N);
+    if (q >= ngen) return;
+    const GItem e = gen[q];
+    int sx, sy, sz;
+    segment_sides(e.seg, sx, sy, sz);
+    if (sx && sy && sz && c != 0) return;
+    const int sd[3] = {sx, sy, sz};
+    int o[3];
 #pragma unroll
-    for (int t = 0; t < K; t++)
-        if (dst[t] >= 0) u[dst[t]] = val[t];
+    for (int d = 0; d < 3; d++) o[d] = sd[d] < 0 ? -1 : (sd[d] > 0 ? N : c);
+    const GhostLevelArgs<T, N> a{u, gf, oct, sel, bicubic, &tab};
+    T v;
+    if (ghost_cell_general<T, N>(a, e.dst, o[0], o[1], o[2], v)) u[(int64_t)e.dst * V + cidx(G, o[0], o[1], o[2])] = v;
 }
 
 // ---------------------------------------------------------------------------

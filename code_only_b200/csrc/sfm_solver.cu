@@ -243,9 +243,10 @@ public:
     double *d_h0 = nullptr, *d_x0 = nullptr;
     FaceItem *d_faces = nullptr;
     GFace *d_gface = nullptr;              // [6 nb] face types and sources for the level fills
-    GItem *d_gitems = nullptr;             // item lists of the level fills (k_ghost_level)
-    std::vector<std::array<std::array<int64_t, kGhostRanges>, 3>> gOff;   // [level][sel + 1][range]
-    std::vector<std::array<std::array<int, kGhostRanges>, 3>> gCnt;
+    int32_t *d_kind26[3] = {nullptr, nullptr, nullptr};   // [sel + 1][26 nb] segment kinds (k_ghost_level)
+    GItem *d_gitems = nullptr;             // general items of the level fills
+    std::vector<std::array<int64_t, 3>> gOff;   // [level][sel + 1]: first general item
+    std::vector<std::array<int, 3>> gCnt;       // [level][sel + 1]: general items
     std::vector<std::array<bool, 3>> ghostMerge;   // [level][sel + 1]: one launch fills the level
     bool ghostMergeOn = true;
     RefluxItem *d_reflux = nullptr;
@@ -484,13 +485,15 @@ public:
         ghostMerge.assign(nlev, {false, false, false});
         for (int L = 0; L < nlev; L++)
             for (int sel = -1; sel <= 1; sel++) ghostMerge[L][sel + 1] = ghost_merge_ok(gface, L, sel);
-        // item lists of the exact level fills, by range (see GItem)
+        // segment kinds and general items of the exact level fills (see kind26)
         std::vector<GItem> gitems;
+        std::array<std::vector<int32_t>, 3> kind26;
         gOff.assign(nlev, {});
         gCnt.assign(nlev, {});
+        for (int sel = -1; sel <= 1; sel++) kind26[sel + 1].assign(26 * (size_t)nb, kSegSkip);
         for (int L = 0; L < nlev; L++)
             for (int sel = -1; sel <= 1; sel++) {
-                std::array<std::vector<GItem>, kGhostRanges> rg;
+                gOff[L][sel + 1] = (int64_t)gitems.size();
                 if (ghostMerge[L][sel + 1])
                     for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
                         for (int seg = 0; seg < 26; seg++) {
@@ -500,33 +503,29 @@ public:
                             bool written = false;
                             for (int d = 0; d < 3; d++)
                                 if (sg[d] && gface_filled(gface[6 * b + (sg[d] > 0) + 2 * d].type, sel)) written = true;
-                            if (!written) continue;   // no pass writes the segment
-                            int cur = b;   // the chain of the passes through same-level faces only
-                            for (int d = 2; d >= 0 && cur >= 0; d--) {
-                                if (!sg[d]) continue;
-                                const GFace &g = gface[6 * cur + (sg[d] > 0) + 2 * d];
-                                cur = (g.type == 0 && gface_filled(0, sel)) ? g.src : -1;
+                            int32_t kind = kSegSkip;
+                            if (written) {
+                                int cur = b;   // the chain of the passes through same-level faces only
+                                for (int d = 2; d >= 0 && cur >= 0; d--) {
+                                    if (!sg[d]) continue;
+                                    const GFace &g = gface[6 * cur + (sg[d] > 0) + 2 * d];
+                                    cur = (g.type == 0 && gface_filled(0, sel)) ? g.src : -1;
+                                }
+                                if (cur >= 0) {
+                                    kind = cur;
+                                } else if (nz == 1) {   // a filled coarse-fine face
+                                    kind = kSegCF;
+                                } else {
+                                    kind = kSegGeneral;
+                                    GItem e{};
+                                    e.dst = b;
+                                    e.seg = (int8_t)seg;
+                                    gitems.push_back(e);
+                                }
                             }
-                            GItem e{};
-                            e.dst = b;
-                            e.seg = (int8_t)seg;
-                            if (cur >= 0) {
-                                e.src = cur;
-                                rg[nz - 1].push_back(e);
-                            } else if (nz == 1) {   // a filled coarse-fine face
-                                const int d = sg[0] ? 0 : (sg[1] ? 1 : 2);
-                                e.src = gface[6 * b + (sg[d] > 0) + 2 * d].src;
-                                rg[3].push_back(e);
-                            } else {
-                                e.src = -1;
-                                rg[nz == 2 ? 4 : 5].push_back(e);
-                            }
+                            kind26[sel + 1][26 * (size_t)b + seg] = kind;
                         }
-                for (int r = 0; r < kGhostRanges; r++) {
-                    gOff[L][sel + 1][r] = (int64_t)gitems.size();
-                    gCnt[L][sel + 1][r] = (int)rg[r].size();
-                    gitems.insert(gitems.end(), rg[r].begin(), rg[r].end());
-                }
+                gCnt[L][sel + 1] = (int)((int64_t)gitems.size() - gOff[L][sel + 1]);
             }
         d_level = mem.upload(std::vector<int32_t>(H.level.begin(), H.level.end()));
         d_parent = mem.upload(std::vector<int32_t>(H.parent.begin(), H.parent.end()));
@@ -541,6 +540,7 @@ public:
         d_faces = mem.upload(faces);
         d_gface = mem.upload(gface);
         d_gitems = mem.upload(gitems);
+        for (int q = 0; q < 3; q++) d_kind26[q] = mem.upload(kind26[q]);
         d_reflux = mem.upload(refl);
         d_tfL = mem.upload(tfL);
         d_tfDL = mem.upload(tfDL);
@@ -688,17 +688,11 @@ public:
     }
     template <class TT, int N>
     void ghost_level_launch(int L, TT *u, bool cubic, int sel) {
-        GhostLevelPlan pl{};
-        int ctas = 0;
-        for (int r = 0; r < kGhostRanges; r++) {
-            pl.cta0[r] = ctas;
-            pl.off[r] = gOff[L][sel + 1][r];
-            pl.cnt[r] = gCnt[L][sel + 1][r];
-            ctas += ghost_range_ctas<N>(r, pl.cnt[r]);
-        }
-        pl.cta0[kGhostRanges] = ctas;
+        const int sweep = ghost_sweep_ctas<TT, N>(cnt(L)), ngen = gCnt[L][sel + 1];
+        const int ctas = sweep + ghost_general_ctas<N>(ngen);
         if (ctas == 0) return;
-        launch_pdl(k_ghost_level<TT, N>, (unsigned)ctas, 256, 0, u, (const GItem *)d_gitems, pl,
+        launch_pdl(k_ghost_level<TT, N>, (unsigned)ctas, 256, 0, u, (const int32_t *)d_kind26[sel + 1],
+                   (const GItem *)(d_gitems + gOff[L][sel + 1]), ngen, H.lstart[L], cnt(L), sweep,
                    (const GFace *)d_gface, (const int8_t *)d_oct, sel, cubic ? 1 : 0);
         ++launches;
     }
