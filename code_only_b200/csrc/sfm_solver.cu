@@ -217,6 +217,7 @@ public:
     virtual int64_t device_bytes() const = 0;
     virtual int fmg_levels() const = 0;
     virtual void set_wait_polls(uint32_t polls) = 0;
+    virtual void set_ghost_merge(bool on) = 0;
     std::string last_error;
     // g written as [nblocks][3][ni^3] (block interiors only, no io ghost
     // layers) instead of the caller's layout: the host-array entry point
@@ -340,6 +341,13 @@ public:
     int64_t device_bytes() const override { return mem.bytes; }
     // the iteration graph holds the kernel parameters it was captured with:
     // a new limit drops it, and the next outer iteration captures again
+    void set_ghost_merge(bool on) override {
+        ghostMergeOn = on;
+        if (iterExec) {
+            cudaGraphExecDestroy(iterExec);
+            iterExec = nullptr;
+        }
+    }
     void set_wait_polls(uint32_t polls) override {
         waitPolls = polls;
         if (iterExec) {
@@ -1764,6 +1772,15 @@ int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes) {
 int sfm_debug_set_wait_polls(sfm_ctx *c, uint32_t polls) {
     if (!c || !c->s) return SFM_EINVAL;
     c->s->set_wait_polls(polls);
+    return SFM_OK;
+}
+
+// Test hook (not part of include/sfmg.h): 0 fills every level's ghost
+// cells by the three directional passes, 1 (the default) by one launch per
+// level where that is exact.  Both give bit-identical fields.
+int sfm_debug_set_ghost_merge(sfm_ctx *c, int on) {
+    if (!c || !c->s) return SFM_EINVAL;
+    c->s->set_ghost_merge(on != 0);
     return SFM_OK;
 }
 
