@@ -1,0 +1,103 @@
+// sfm_tune.h -- the launch-shape table of the autotuner (host code only).
+//
+// The solver's kernels come in variants that differ only in how the work
+// is spread over threads and CTAs; every variant evaluates the same
+// expressions in the same order, so the choice never changes a result bit.
+// A table maps (knob, element size, block edge, AMR level, fill kind) to the
+// chosen variant; Solver::autotune fills it by timing the candidates on the
+// context's own hierarchy, sfm_tune_save / sfm_tune_load keep it across
+// runs.  Knobs:
+//   ghost_fill    level fill by the three directional passes (0) or by one
+//                 launch per level (1; only where Solver::ghost_merge_ok);
+//                 key: element size, block edge n, AMR level, fill kind
+//   relax_threads threads of the bulk-copy smoother CTA (256 or 512);
+//                 key: element size, block edge n
+//   resid_bpc     blocks per CTA of the tiled residual (1, 2 or 4);
+//                 key: element size, block edge n
+// Text form, one entry per line (blank lines and lines starting with '#'
+// are skipped):
+//   <knob> <element bytes> <n> <level> <kind> <choice>
+// e.g. "ghost_fill 4 8 2 -1 1".  Unknown knobs, malformed lines and choices
+// outside a knob's candidates are rejected.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace sfm {
+
+enum TuneKnob { kKnobGhostFill = 0, kKnobRelaxThreads = 1, kKnobResidBpc = 2, kKnobCount = 3 };
+inline const char *tune_knob_name(int k) {
+    switch (k) {
+        case kKnobGhostFill: return "ghost_fill";
+        case kKnobRelaxThreads: return "relax_threads";
+        case kKnobResidBpc: return "resid_bpc";
+        default: return nullptr;
+    }
+}
+inline bool tune_choice_ok(int knob, int v) {
+    switch (knob) {
+        case kKnobGhostFill: return v == 0 || v == 1;
+        case kKnobRelaxThreads: return v == 256 || v == 512;
+        case kKnobResidBpc: return v == 1 || v == 2 || v == 4;
+        default: return false;
+    }
+}
+
+struct TuneTable {
+    // (knob, element bytes, n, level, kind) -> choice
+    using Key = std::tuple<int, int, int, int, int>;
+    std::map<Key, int> v;
+
+    int get(int knob, int elem, int n, int level, int kind, int dflt) const {
+        auto it = v.find(Key{knob, elem, n, level, kind});
+        return it == v.end() ? dflt : it->second;
+    }
+    void set(int knob, int elem, int n, int level, int kind, int choice) { v[Key{knob, elem, n, level, kind}] = choice; }
+
+    std::string text() const {
+        std::string s = "# knob elem_bytes n level kind choice\n";
+        char line[128];
+        for (const auto &e : v) {
+            std::snprintf(line, sizeof line, "%s %d %d %d %d %d\n", tune_knob_name(std::get<0>(e.first)),
+                          std::get<1>(e.first), std::get<2>(e.first), std::get<3>(e.first), std::get<4>(e.first),
+                          e.second);
+            s += line;
+        }
+        return s;
+    }
+    // replaces the table with the entries of `t`; false (table unchanged) on
+    // any malformed or out-of-range line
+    bool parse(const char *t) {
+        std::map<Key, int> nv;
+        std::istringstream in(t ? t : "");
+        std::string line;
+        while (std::getline(in, line)) {
+            size_t a = line.find_first_not_of(" \t\r");
+            if (a == std::string::npos || line[a] == '#') continue;
+            std::istringstream ls(line);
+            std::string name;
+            long elem, n, level, kind, choice;
+            if (!(ls >> name >> elem >> n >> level >> kind >> choice)) return false;
+            std::string rest;
+            if (ls >> rest) return false;
+            int knob = -1;
+            for (int k = 0; k < kKnobCount; k++)
+                if (name == tune_knob_name(k)) knob = k;
+            if (knob < 0) return false;
+            if ((elem != 4 && elem != 8) || n < 2 || n > 64 || (n & (n - 1)) || level < -1 || level > 30 || kind < -1 ||
+                kind > 1 || !tune_choice_ok(knob, (int)choice))
+                return false;
+            nv[Key{knob, (int)elem, (int)n, (int)level, (int)kind}] = (int)choice;
+        }
+        v.swap(nv);
+        return true;
+    }
+};
+
+}  // namespace sfm

@@ -434,6 +434,9 @@ def config_hierarchy(name: str):
                    126 MB L2, used for kernel profiles of the 8^3-block sweeps
     'uniform128' : 128^3 periodic, 16^3 blocks of 8^3: the smallest uniform grid
                    with jeans6's 32^3 base grid, used to profile the base-grid CTA
+    'jeans3'     : the jeans6 density refined to 3 levels (89,800 blocks; the finest
+                   level's FP32 field, 224 MB, exceeds L2): kernel profiles of
+                   AMR-level operations at a few GB of device memory
     """
     if name == "uniform64":
         return uniform_periodic(8, 8), gaussian_peak, 0
@@ -443,6 +446,9 @@ def config_hierarchy(name: str):
         return uniform_periodic(32, 8), gaussian_peak, 0
     if name == "uniform128":
         return uniform_periodic(16, 8), gaussian_peak, 0
+    if name == "jeans3":
+        h, fn = jeans_cloud(nlev=3, nbase=16, ni=8)
+        return h, fn, 0
     if name == "jeans6":
         h, fn = jeans_cloud(nlev=6, nbase=16, ni=8)
         return h, fn, 0
