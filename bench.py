@@ -245,15 +245,23 @@ def run_ours(args):
 
     sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     results = {}
+    tables = {}
     for prec, key in ((abi.SFM_PREC_MIXED, "mixed"), (abi.SFM_PREC_FP64, "fp64")):
         with FMGPoisson(h, params=params_for(bc, prec, profile=1)) as s:
+            # the built-in launch shapes, then the autotuned ones (sfm_autotune;
+            # the results are bit-identical, only the launch shapes differ)
+            ms_default = time_device(s, rho_d, psi_d, g_d, max(2, args.steps // 4), 1, info)[0]
+            t0 = time.perf_counter()
+            s.autotune(3)
+            tune_s = time.perf_counter() - t0
+            tables[key] = s.tune_table()
             if key == "mixed" and sampler:
                 sampler.start()
             ms, st, launches, smo, iters = time_device(s, rho_d, psi_d, g_d, args.steps, args.warmup, info)
             if key == "mixed" and sampler:
                 clocks = sampler.stop()
             results[key] = dict(ms=ms, st=st, launches=launches, smo=smo, iters=iters,
-                                resid=st.true_rel_residual, info=s.info())
+                                resid=st.true_rel_residual, info=s.info(), ms_default=ms_default, tune_s=tune_s)
             if rank == 0 and not args.no_cpu:   # kept on the host for the oracle comparison
                 ng = (G - h.ni) // 2
                 sl = slice(ng, ng + h.ni)
@@ -275,6 +283,7 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         with FMGPoisson(h, params=params_for(bc, abi.SFM_PREC_MIXED)) as s:
+            s.load_tune_table(tables["mixed"])
             rho_h = torch.from_numpy(rho).pin_memory().numpy()
             psi_h = torch.zeros(rho.shape, dtype=torch.float64).pin_memory().numpy()
             g_h = torch.zeros((h.nblocks, 3, G, G, G), dtype=torch.float64).pin_memory().numpy()
@@ -344,6 +353,12 @@ def run_ours(args):
         "true_rel_residual": {"mixed": mx["resid"], "fp64": fp["resid"]},
         "fp64": {"value": round(world * 1e3 / fp["ms"], 4), "unit": "solves/s", "ms_per_step": round(fp["ms"], 4)},
         "mixed_over_fp64": round(fp["ms"] / mx["ms"], 3),
+        "autotune": {
+            "mixed_default_ms_per_step": round(mx["ms_default"], 3), "mixed_tuned_ms_per_step": round(mx["ms"], 3),
+            "fp64_default_ms_per_step": round(fp["ms_default"], 3), "fp64_tuned_ms_per_step": round(fp["ms"], 3),
+            "tuning_s": {"mixed": round(mx["tune_s"], 2), "fp64": round(fp["tune_s"], 2)},
+            "choices_mixed": tune_summary(tables["mixed"]),
+        },
         "phi_rel_err_mixed_vs_fp64": phi_err,
         "roofline": {
             "kernel": f"k_relax_bulk<float, {h.ni}>: one red-black colour over the leaf cells, fmg level 0",
@@ -368,6 +383,17 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
     from code_only_b200 import replicas
     replicas.teardown(info)
+
+
+def tune_summary(text):
+    """Counts of the tuned choices per knob, e.g. {"ghost_fill": {"0": 9, "1": 6}, ...}."""
+    out = {}
+    for ln in text.splitlines():
+        f = ln.split()
+        if len(f) == 6 and not ln.startswith("#"):
+            out.setdefault(f[0], {}).setdefault(f[5], 0)
+            out[f[0]][f[5]] += 1
+    return out
 
 
 def time_adjoint(h, rho, bc):

@@ -34,7 +34,8 @@ SFM_MAX_HISTORY = 64
 
 # every exported symbol of include/sfmg.h
 EXPORTED = ("sfm_default_params", "sfm_create", "sfm_solve", "sfm_solve_device",
-            "sfm_adjoint", "sfm_destroy", "sfm_strerror", "sfm_info", "sfm_uniform_solve_noalloc")
+            "sfm_adjoint", "sfm_destroy", "sfm_strerror", "sfm_info", "sfm_autotune", "sfm_tune_save",
+            "sfm_tune_load", "sfm_uniform_solve_noalloc")
 SFM_NOALLOC_MAX_N = 32
 
 
@@ -153,6 +154,14 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.sfm_strerror.restype = C.c_char_p
     lib.sfm_info.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     lib.sfm_info.restype = C.c_int
+    lib.sfm_autotune.argtypes = [C.c_void_p, C.c_int32]
+    lib.sfm_autotune.restype = C.c_int
+    lib.sfm_tune_save.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    lib.sfm_tune_save.restype = C.c_int
+    lib.sfm_tune_load.argtypes = [C.c_void_p, C.c_char_p]
+    lib.sfm_tune_load.restype = C.c_int
+    lib.sfm_tune_text_check.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t]
+    lib.sfm_tune_text_check.restype = C.c_int
     if path is None:
         _lib = lib
     return lib

@@ -361,17 +361,6 @@ struct GItem {
 // 2 (N+2)^2 on z planes -- every cell once, all of a block's together
 template <int N>
 __host__ __device__ constexpr int ghost_shell() { return 2 * (N * N + (N + 2) * N + (N + 2) * (N + 2)); }
-// cells per thread (eight 4-byte cells fit the 64-register budget, eight doubles do not)
-template <class T, int N>
-__host__ __device__ constexpr int ghost_level_k() { return N >= 8 && sizeof(T) == 4 ? 8 : 4; }
-template <class T, int N>
-__host__ __device__ constexpr int ghost_sweep_ctas(int nblk) {
-    return (int)(((int64_t)nblk * ghost_shell<N>() + 256 * ghost_level_k<T, N>() - 1) / (256 * ghost_level_k<T, N>()));
-}
-template <int N>
-__host__ __device__ constexpr int ghost_general_ctas(int items) {
-    return (int)(((int64_t)items * N + 255) / 256);   // N cells per item (corners use the first)
-}
 
 // cell r (0 .. ghost_shell - 1) of a block's shell
 template <int N>
@@ -429,17 +418,35 @@ __device__ __noinline__ T ghost_cf_face(const T *u, const int8_t *oct, int X, in
     return ((T)10 * u0 + (T)8 * uH - (T)3 * uN) / (T)15;
 }
 
-// One fill of the level's blocks first .. first+nblk-1: the first `sweep`
-// CTAs walk every block's shell (K cells per thread: kind loads, value
-// loads, then stores), the rest take the general items.
+// One fill of the level's blocks first .. first+nblk-1.  The first `sweep`
+// CTAs give each warp one block: the block's 26 segment kinds go to shared
+// memory, and the warp walks the block's shell through a per-CTA table of
+// (destination offset, wrapped source offset, segment) for every shell
+// cell, so a copied cell costs two shared loads, one load and one store
+// (decoding the cell from a flat index each time measured issue-bound).
+// The remaining CTAs take the general items.
+constexpr int kGhostWarps = 8;   // blocks per sweep CTA (one per warp)
+template <int N>
+__host__ __device__ constexpr int ghost_sweep_ctas(int nblk) { return (nblk + kGhostWarps - 1) / kGhostWarps; }
+template <int N>
+__host__ __device__ constexpr int ghost_general_ctas(int items) {
+    return (int)(((int64_t)items * N + 255) / 256);   // N cells per item (corners use the first)
+}
+template <int N>
+struct ShellTable {
+    uint32_t off[ghost_shell<N>()];   // in-block offset of the cell | wrapped offset << 16 (G^3 < 2^16)
+    uint8_t seg[ghost_shell<N>()];
+};
+
 template <class T, int N>
-__global__ void __launch_bounds__(256, 4) k_ghost_level(T *u, const int32_t *__restrict__ kind26,
-                                                        const GItem *__restrict__ gen, int ngen, int first, int nblk,
-                                                        int sweep, const GFace *__restrict__ gf,
-                                                        const int8_t *__restrict__ oct, int sel, int cubic) {
+__global__ void __launch_bounds__(256) k_ghost_level(T *u, const int32_t *__restrict__ kind26,
+                                                     const GItem *__restrict__ gen, int ngen, int first, int nblk,
+                                                     int sweep, const GFace *__restrict__ gf,
+                                                     const int8_t *__restrict__ oct, int sel, int cubic) {
     pdl_enter();
-    constexpr int G = N + 2, NB2 = N / 2, SH = ghost_shell<N>(), K = ghost_level_k<T, N>();
+    constexpr int G = N + 2, NB2 = N / 2, SH = ghost_shell<N>(), U = 4;
     constexpr int64_t V = (int64_t)G * G * G;
+    static_assert(G * G * G < 65536, "offsets fit 16 bits");
     __shared__ GhostCubicTable<N> tab;
     const bool bicubic = cubic && NB2 + 2 >= 4 && sel != 0;
     if (bicubic) {   // launch-uniform
@@ -447,57 +454,52 @@ __global__ void __launch_bounds__(256, 4) k_ghost_level(T *u, const int32_t *__r
         __syncthreads();
     }
     if ((int)blockIdx.x < sweep) {
-        const int64_t total = (int64_t)nblk * SH;
-        const int64_t g0 = (int64_t)blockIdx.x * 256 * K + threadIdx.x;
-        // per cell: block, packed coordinates (i+1) | (j+1) << 8 | (k+1) << 16, kind
-        int X[K], pk[K], kd[K];
-        auto unpack = [](int v, int &i, int &j, int &k) {
-            i = (v & 255) - 1;
-            j = ((v >> 8) & 255) - 1;
-            k = (v >> 16) - 1;
-        };
-#pragma unroll
-        for (int t = 0; t < K; t++) {
-            const int64_t g = g0 + (int64_t)t * 256;
-            kd[t] = kSegSkip;
-            X[t] = 0;
-            pk[t] = 0;
-            if (g >= total) continue;
-            const int bq = (int)(g / SH);
+        __shared__ ShellTable<N> st;
+        __shared__ int wk[kGhostWarps][26];
+        for (int r = threadIdx.x; r < SH; r += blockDim.x) {
             int i, j, k;
-            shell_cell<N>((int)(g - (int64_t)bq * SH), i, j, k);
-            X[t] = first + bq;
-            pk[t] = (i + 1) | ((j + 1) << 8) | ((k + 1) << 16);
+            shell_cell<N>(r, i, j, k);
+            auto wrap = [](int x) { return x < 0 ? N - 1 : (x >= N ? 0 : x); };
+            st.off[r] = (uint32_t)cidx(G, i, j, k) | ((uint32_t)cidx(G, wrap(i), wrap(j), wrap(k)) << 16);
             const int sx = i < 0 ? -1 : (i >= N ? 1 : 0), sy = j < 0 ? -1 : (j >= N ? 1 : 0),
                       sz = k < 0 ? -1 : (k >= N ? 1 : 0);
-            kd[t] = kind26[26 * (int64_t)X[t] + shell_segment(sx, sy, sz)];
+            st.seg[r] = (uint8_t)shell_segment(sx, sy, sz);
         }
-        T val[K];
+        __syncthreads();
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int bq = (int)blockIdx.x * kGhostWarps + w;
+        if (bq >= nblk) return;
+        const int X = first + bq;
+        if (lane < 26) wk[w][lane] = kind26[26 * (int64_t)X + lane];
+        __syncwarp();
+        T *ud = u + (int64_t)X * V;
+        for (int r0 = 0; r0 < SH; r0 += 32 * U) {
+            T val[U];
+            int dof[U];
 #pragma unroll
-        for (int t = 0; t < K; t++) {
-            if (kd[t] < 0) continue;
-            auto wrap = [](int x) { return x < 0 ? N - 1 : (x >= N ? 0 : x); };
-            int i, j, k;
-            unpack(pk[t], i, j, k);
-            val[t] = u[(int64_t)kd[t] * V + cidx(G, wrap(i), wrap(j), wrap(k))];
-        }
-#pragma unroll
-        for (int t = 0; t < K; t++) {
-            if (kd[t] != kSegCF) continue;
-            int i, j, k;
-            unpack(pk[t], i, j, k);
-            const int D = (i == -1 || i == N) ? 0 : ((j == -1 || j == N) ? 1 : 2);
-            const int c = D == 0 ? i : (D == 1 ? j : k);
-            const int lr = c == N ? 1 : 0;
-            val[t] = ghost_cf_face<T, N>(u, oct, X[t], gf[6 * X[t] + lr + 2 * D].src, D, lr, i, j, k, bicubic, &tab);
-        }
-#pragma unroll
-        for (int t = 0; t < K; t++)
-            if (kd[t] >= 0 || kd[t] == kSegCF) {
-                int i, j, k;
-                unpack(pk[t], i, j, k);
-                u[(int64_t)X[t] * V + cidx(G, i, j, k)] = val[t];
+            for (int q = 0; q < U; q++) {
+                const int r = r0 + q * 32 + lane;
+                dof[q] = -1;
+                if (r >= SH) continue;
+                const uint32_t o = st.off[r];
+                const int kd = wk[w][st.seg[r]];
+                if (kd >= 0) {
+                    val[q] = u[(int64_t)kd * V + (o >> 16)];
+                    dof[q] = (int)(o & 0xffffu);
+                } else if (kd == kSegCF) {
+                    const int c = (int)(o & 0xffffu);
+                    const int i = c % G - 1, j = (c / G) % G - 1, k = c / (G * G) - 1;
+                    const int D = (i == -1 || i == N) ? 0 : ((j == -1 || j == N) ? 1 : 2);
+                    const int cc = D == 0 ? i : (D == 1 ? j : k);
+                    const int lr = cc == N ? 1 : 0;
+                    val[q] = ghost_cf_face<T, N>(u, oct, X, gf[6 * X + lr + 2 * D].src, D, lr, i, j, k, bicubic, &tab);
+                    dof[q] = c;
+                }
             }
+#pragma unroll
+            for (int q = 0; q < U; q++)
+                if (dof[q] >= 0) ud[dof[q]] = val[q];
+        }
         return;
     }
     // general items: N cells per item (the free coordinate of an edge; a
@@ -763,17 +765,21 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // resident CTAs per SM the bulk ring's shared memory allows: the register
 // budget that leaves (at 4^3 blocks ptxas otherwise settles on 32 registers
 // and spills)
-template <class T, int N>
+template <class T, int N, int NT = 256>
 __host__ __device__ constexpr int relax_bulk_min_ctas() {
-    return (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024) < 8 ? (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024) : 8;
+    // bounded by the ring's shared memory, 8, and the 2048 threads of an SM
+    return (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024) < (2048 / NT < 8 ? 2048 / NT : 8)
+               ? (228 * 1024) / (BulkPlan<T, N>::SMEM + 1024)
+               : (2048 / NT < 8 ? 2048 / NT : 8);
 }
 // threads of k_relax_bulk: warp 0 produces, the others consume.  A 16^3
 // block's stages allow only one or two CTAs per SM, so those CTAs get 15
 // consumer warps instead of 7.
+// (the default; the autotuner may choose the other count per block edge)
 template <int N>
 __host__ __device__ constexpr int relax_bulk_threads() { return N >= 16 ? 512 : 256; }
-template <class T, int N>
-__global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T, N>())
+template <class T, int N, int NT = relax_bulk_threads<N>()>
+__global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
     k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
                                                     const int32_t *__restrict__ blocks, int nblk,
                                                     const double *__restrict__ h0, const int32_t *__restrict__ level,
@@ -784,7 +790,7 @@ __global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T
     using Tl = Tile<N>;
     using Pl = BulkPlan<T, N>;
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2, S = Pl::S;
-    constexpr int NCW = relax_bulk_threads<N>() / 32 - 1, NCT = 32 * NCW;   // consumer warps / threads
+    constexpr int NCW = NT / 32 - 1, NCT = 32 * NCW;   // consumer warps / threads
     constexpr uint32_t BB = (uint32_t)(V * sizeof(T));
     constexpr int LO = Pl::LO;
     constexpr uint32_t SB = (uint32_t)(Pl::SPAN * sizeof(T));
@@ -928,9 +934,10 @@ __global__ void __launch_bounds__(relax_bulk_threads<N>(), relax_bulk_min_ctas<T
 // residual res = rhs - div F / h on listed blocks (fmg_poisson_resid)
 // blocks per CTA of k_resid_tiled: two 8^3 blocks (1024 cells) measured
 // faster than one
+// (the default; the autotuner may choose 1, 2 or 4 for 8^3 blocks)
 template <int N>
 __host__ __device__ constexpr int resid_bpc() { return N == 8 ? 2 : Tile<N>::BPC; }
-template <class TU, class TR, class TO, int N>
+template <class TU, class TR, class TO, int N, int BPCX = resid_bpc<N>()>
 __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const TU *__restrict__ u,
                                                      const TR *__restrict__ rhs, const int32_t *__restrict__ blocks,
                                                      int nblk, const double *__restrict__ h0,
@@ -938,7 +945,7 @@ __global__ void __launch_bounds__(256) k_resid_tiled(TO *__restrict__ res, const
                                                      const double *__restrict__ rbuf, int f) {
     pdl_enter();
     using Tl = Tile<N>;
-    constexpr int G = Tl::G, V = Tl::V, BPC = resid_bpc<N>();
+    constexpr int G = Tl::G, V = Tl::V, BPC = BPCX;
     __shared__ TU sh[BPC * V];
     __shared__ int ssl[BPC][6];
     __shared__ int sbid[BPC];

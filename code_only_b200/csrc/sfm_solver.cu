@@ -35,6 +35,7 @@
 #include "sfm_fast.cuh"
 #include "sfm_noalloc.cuh"
 #include "sfm_adjoint.cuh"
+#include "sfm_tune.h"
 
 namespace sfm {
 
@@ -218,6 +219,9 @@ public:
     virtual int fmg_levels() const = 0;
     virtual void set_wait_polls(uint32_t polls) = 0;
     virtual void set_ghost_merge(bool on) = 0;
+    virtual int autotune(int reps) = 0;
+    virtual std::string tune_text() const = 0;
+    virtual bool tune_load(const char *text) = 0;
     std::string last_error;
     // g written as [nblocks][3][ni^3] (block interiors only, no io ghost
     // layers) instead of the caller's layout: the host-array entry point
@@ -249,7 +253,8 @@ public:
     std::vector<std::array<int64_t, 3>> gOff;   // [level][sel + 1]: first general item
     std::vector<std::array<int, 3>> gCnt;       // [level][sel + 1]: general items
     std::vector<std::array<bool, 3>> ghostMerge;   // [level][sel + 1]: one launch fills the level
-    bool ghostMergeOn = true;
+    int ghostForce = -1;                   // test hook: 1 / 0 forces the one-launch fill on / off, -1 the table
+    TuneTable tune;                        // launch-shape choices (sfm_tune.h); empty = defaults
     RefluxItem *d_reflux = nullptr;
     BFace *d_tfL = nullptr, *d_tfDL = nullptr, *d_crop = nullptr;
     std::vector<int64_t> faceOff, faceSplit, tfLOff, tfDLOff, cropOff, wcOff;
@@ -270,7 +275,7 @@ public:
     int *d_err = nullptr;                  // set by a device wait that gave up
     uint32_t waitPolls = kWaitPolls;       // poll limit of the smoother's stage waits (tests lower it)
     int nSM = 148;
-    int bulkGrid[5] = {0, 0, 0, 0, 0};     // persistent CTAs of k_relax_bulk<T, N>, by log2(N)
+    int bulkGrid[5][2] = {};               // persistent CTAs of k_relax_bulk<T, N, NT>, by log2(N) and NT / 512
     double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
     int *d_mgit = nullptr;
     // base grid
@@ -342,11 +347,122 @@ public:
     // the iteration graph holds the kernel parameters it was captured with:
     // a new limit drops it, and the next outer iteration captures again
     void set_ghost_merge(bool on) override {
-        ghostMergeOn = on;
+        ghostForce = on ? 1 : 0;
         if (iterExec) {
             cudaGraphExecDestroy(iterExec);
             iterExec = nullptr;
         }
+    }
+    // -----------------------------------------------------------------
+    // Autotuner: times every candidate of every knob in use on this
+    // context's hierarchy (each candidate `reps` times after one warm-up
+    // launch, CUDA events on the context's stream, minimum kept) and keeps
+    // the fastest in the table.  All candidates give bit-identical fields,
+    // so the choice never changes a result; the reference's sweep counts and
+    // coarse-level cutoff (fmg.F90:280-288, mg.F90:50-52, vmg.F90:85-91) are
+    // not knobs, since they change the iterates.
+    template <class F>
+    float time_min(F &&op, int reps) {
+        op();   // warm-up
+        float best = std::numeric_limits<float>::max();
+        for (int r = 0; r < reps; r++) {
+            cudaEventRecord(ev0, st_);
+            op();
+            cudaEventRecord(ev1, st_);
+            cudaEventSynchronize(ev1);
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess && ms < best) best = ms;
+        }
+        return best;
+    }
+    template <class TT>
+    void tune_ghost(TT *u, int f, int sel, int reps) {
+        const int n = nf[f];
+        if (!(n == 2 || n == 4 || n == 8 || n == 16)) return;
+        for (int L = 0; L < H.nlev; L++) {
+            if (!ghostMerge[L][sel + 1] || (sel == 1 && L == 0)) continue;
+            float t[2];
+            for (int m = 0; m < 2; m++) {
+                tune.set(kKnobGhostFill, (int)sizeof(TT), n, L, sel, m);
+                t[m] = time_min([&] { ghost_fill_level(L, f, u, false, sel); }, reps);
+            }
+            tune.set(kKnobGhostFill, (int)sizeof(TT), n, L, sel, t[1] < t[0] ? 1 : 0);
+        }
+    }
+    int autotune(int reps) override {
+        st_ = own_;
+        const int saveForce = ghostForce;
+        ghostForce = -1;
+        for (auto &z : zeroList) cudaMemsetAsync(z.first, 0, z.second, st_);
+        FmgLevel_fill0 = Undef;
+        const int FMax = H.FMax;
+        // ghost fills: inner fields at every fmg level (both kinds), the
+        // same-level and coarse-fine fills of the AMR-level V-cycle, and the
+        // FP64 outer fields at fmg level 0
+        for (int f = 0; f <= FMax; f++) tune_ghost<T>(U[f], f, -1, reps);
+        tune_ghost<T>(U[FMax], FMax, 0, reps);
+        tune_ghost<T>(U[FMax], FMax, 1, reps);
+        if (sizeof(T) != sizeof(double)) tune_ghost<double>(PSI0, 0, -1, reps);
+        // smoother CTA size on the bulk-copy levels
+        for (int f = 0; f <= FMax; f++) {
+            const int n = nf[f];
+            if (n < 4 || nLeaves <= 0) continue;
+            float t[2];
+            const int cand[2] = {256, 512};
+            for (int c = 0; c < 2; c++) {
+                tune.set(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, cand[c]);
+                t[c] = time_min([&] {
+                    for (int ipass = 1; ipass <= 2; ipass++)
+                        relax_launch(U[f], RHS[f], d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max);
+                }, reps);
+            }
+            tune.set(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, t[1] < t[0] ? 512 : 256);
+        }
+        // residual blocks per CTA on 8^3 blocks (inner and outer precision)
+        for (int f = 0; f <= FMax; f++) {
+            if (nf[f] != 8) continue;
+            const int cand[3] = {1, 2, 4};
+            float best = std::numeric_limits<float>::max();
+            int pick = 2;
+            for (int c = 0; c < 3; c++) {
+                tune.set(kKnobResidBpc, (int)sizeof(T), 8, -1, -1, cand[c]);
+                const float t = time_min([&] {
+                    FmgLevel_fill0 = f;   // time the residual kernel alone, not its ghost fill
+                    resid<T, T, T>(f, RES[f], U[f], RHS[f], false);
+                }, reps);
+                if (t < best) { best = t; pick = cand[c]; }
+            }
+            tune.set(kKnobResidBpc, (int)sizeof(T), 8, -1, -1, pick);
+            if (sizeof(T) != sizeof(double) && f == 0) {
+                best = std::numeric_limits<float>::max();
+                pick = 2;
+                for (int c = 0; c < 3; c++) {
+                    tune.set(kKnobResidBpc, 8, 8, -1, -1, cand[c]);
+                    const float t = time_min([&] {
+                        FmgLevel_fill0 = 0;
+                        resid<double, double, T>(0, RHO[0], PSI0, SRC0, false);
+                    }, reps);
+                    if (t < best) { best = t; pick = cand[c]; }
+                }
+                tune.set(kKnobResidBpc, 8, 8, -1, -1, pick);
+            }
+        }
+        FmgLevel_fill0 = Undef;
+        ghostForce = saveForce;
+        if (iterExec) {   // the graph holds the old launch shapes
+            cudaGraphExecDestroy(iterExec);
+            iterExec = nullptr;
+        }
+        return check("autotune");
+    }
+    std::string tune_text() const override { return tune.text(); }
+    bool tune_load(const char *text) override {
+        if (!tune.parse(text)) return false;
+        if (iterExec) {
+            cudaGraphExecDestroy(iterExec);
+            iterExec = nullptr;
+        }
+        return true;
     }
     void set_wait_polls(uint32_t polls) override {
         waitPolls = polls;
@@ -570,7 +686,7 @@ public:
         d_bad = mem.alloc<int>(1);
         d_err = mem.alloc<int>(1);
         zeroList.push_back({d_err, sizeof(int)});
-        for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], (void)bulk_grid<N>(), (void)0);
+        for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], ((void)bulk_grid<N, 256>(), (void)bulk_grid<N, 512>()), (void)0);
         d_mom = mem.alloc<double>(32);
         if (P.bc == SFM_BC_SPHERE)   // per-cell moment terms of the base level, summed in order
             d_part = mem.alloc<double>((size_t)H.lstart[1] * H.NI * H.NI * H.NI * kMomentTerms);
@@ -696,7 +812,7 @@ public:
     }
     template <class TT, int N>
     void ghost_level_launch(int L, TT *u, bool cubic, int sel) {
-        const int sweep = ghost_sweep_ctas<TT, N>(cnt(L)), ngen = gCnt[L][sel + 1];
+        const int sweep = ghost_sweep_ctas<N>(cnt(L)), ngen = gCnt[L][sel + 1];
         const int ctas = sweep + ghost_general_ctas<N>(ngen);
         if (ctas == 0) return;
         launch_pdl(k_ghost_level<TT, N>, (unsigned)ctas, 256, 0, u, (const int32_t *)d_kind26[sel + 1],
@@ -709,7 +825,9 @@ public:
     void ghost_fill_level(int L, int f, TT *u, bool cubic, int sel) {
         const int n = nf[f];
         if (sel == 1 && L <= 0) return;
-        if (ghostMergeOn && ghostMerge[L][sel + 1] && (n == 2 || n == 4 || n == 8 || n == 16)) {
+        const int mode = tune.get(kKnobGhostFill, (int)sizeof(TT), n, L, sel, 0);   // default: three passes
+        const bool one = ghostForce >= 0 ? ghostForce == 1 : mode == 1;
+        if (one && ghostMerge[L][sel + 1] && (n == 2 || n == 4 || n == 8 || n == 16)) {
             SFM_WITH_N(n, (ghost_level_launch<TT, N>(L, u, cubic, sel)), (void)0)
             return;
         }
@@ -820,35 +938,40 @@ public:
     // (on 2^3 blocks it measured slower than k_relax_tiled)
     template <int N>
     static constexpr bool bulk_ok() { return N >= 4 && BulkPlan<T, N>::SMEM <= 220 * 1024; }
-    template <int N>
+    template <int N, int NT>
     int bulk_grid() {
         if (!bulk_ok<N>()) return 0;
         constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : (N >= 4 ? 2 : 1));   // log2(N), capped
-        if (!bulkGrid[li]) {
+        constexpr int ti = NT == 512 ? 1 : 0;
+        if (!bulkGrid[li][ti]) {
             const int smem = BulkPlan<T, N>::SMEM;
             // opt in whatever the size: static and dynamic shared memory together may pass 48 KB
-            cudaFuncSetAttribute(k_relax_bulk<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaFuncSetAttribute(k_relax_bulk<T, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             int per = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N>, relax_bulk_threads<N>(), smem) !=
-                    cudaSuccess ||
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N, NT>, NT, smem) != cudaSuccess ||
                 per < 1) {
                 cudaGetLastError();
                 per = 1;
             }
-            bulkGrid[li] = nSM * per;
+            bulkGrid[li][ti] = nSM * per;
         }
-        return bulkGrid[li];
+        return bulkGrid[li][ti];
+    }
+    template <int N, int NT>
+    void relax_bulk_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
+                           int f, int ipass, unsigned long long *out) {
+        launch_pdl(k_relax_bulk<T, N, NT>,
+                   (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N, NT>()), NT,
+                   BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out, d_err, waitPolls);
     }
     void relax_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
                       int f, int ipass, unsigned long long *out) {
         const int n = nf[f];
         if (nblk <= 0) return;
+        const int nt = tune.get(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, n >= 16 ? 512 : 256);
         SFM_WITH_N(n,
-                   (bulk_ok<N>() ? launch_pdl(k_relax_bulk<T, N>,
-                                              (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N>()),
-                                              relax_bulk_threads<N>(), BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0,
-                                              d_level, rslot,
-                                              rb, f, ipass, out, d_err, waitPolls)
+                   (bulk_ok<N>() ? (nt == 512 ? relax_bulk_launch<N, 512>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out)
+                                              : relax_bulk_launch<N, 256>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out))
                                  : launch_pdl(k_relax_tiled<T, N>,
                                               (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
                                               256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
@@ -924,6 +1047,18 @@ public:
     void resid(int f, TO *res, TU *u, const TR *rhs, bool bf0) {   // fmg_poisson_resid
         poisson_flux(f, u, bf0);
         const int n = nf[f];
+        if (n == 8) {   // blocks per CTA from the tuning table (default 2)
+            const int bpc = tune.get(kKnobResidBpc, (int)sizeof(TU), 8, -1, -1, resid_bpc<8>());
+            auto go = [&](auto kern, int b) {
+                launch_pdl(kern, (unsigned)((nLeaves + b - 1) / b), 256, 0, res, u, rhs, d_leaves, nLeaves, d_h0, d_level,
+                           d_rslot, rbuf[f], f);
+            };
+            if (bpc == 1) go(k_resid_tiled<TU, TR, TO, 8, 1>, 1);
+            else if (bpc == 4) go(k_resid_tiled<TU, TR, TO, 8, 4>, 4);
+            else go(k_resid_tiled<TU, TR, TO, 8, 2>, 2);
+            ++launches;
+            return;
+        }
         SFM_WITH_N(n,
                    (launch_pdl(k_resid_tiled<TU, TR, TO, N>, (unsigned)((nLeaves + resid_bpc<N>() - 1) / resid_bpc<N>()),
                                256, 0, res, u, rhs, d_leaves, nLeaves, d_h0, d_level, d_rslot, rbuf[f], f),
@@ -1757,6 +1892,47 @@ const char *sfm_strerror(int code) {
         case SFM_ESIZE: return "size exceeds a fixed maximum";
         default: return "unknown error";
     }
+}
+
+int sfm_autotune(sfm_ctx *c, int32_t reps) {
+    if (!c || !c->s || reps < 1 || reps > 100) return SFM_EINVAL;
+    DeviceGuard dg(c->device);
+    return sfm_guard([&] { return c->s->autotune(reps); });
+}
+
+int sfm_tune_save(const sfm_ctx *c, char *buf, size_t cap, size_t *len) {
+    if (!c || !c->s) return SFM_EINVAL;
+    return sfm_guard([&] {
+        const std::string t = c->s->tune_text();
+        if (len) *len = t.size();
+        if (!buf) return SFM_OK;
+        if (cap < t.size() + 1) return SFM_ESIZE;
+        std::memcpy(buf, t.c_str(), t.size() + 1);
+        return SFM_OK;
+    });
+}
+
+int sfm_tune_load(sfm_ctx *c, const char *text) {
+    if (!c || !c->s || !text) return SFM_EINVAL;
+    DeviceGuard dg(c->device);
+    return sfm_guard([&] { return c->s->tune_load(text) ? SFM_OK : SFM_EINVAL; });
+}
+
+// Test hook (not part of include/sfmg.h; host code only, no device): parses
+// a tuning table and writes it back in canonical form.  Returns the number
+// of entries, SFM_EINVAL for a malformed table or SFM_ESIZE when `out` is
+// too small.
+int sfm_tune_text_check(const char *in, char *out, size_t cap) {
+    return sfm_guard([&] {
+        sfm::TuneTable t;
+        if (!in || !t.parse(in)) return SFM_EINVAL;
+        const std::string s = t.text();
+        if (out) {
+            if (cap < s.size() + 1) return SFM_ESIZE;
+            std::memcpy(out, s.c_str(), s.size() + 1);
+        }
+        return (int)t.v.size();
+    });
 }
 
 int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes) {

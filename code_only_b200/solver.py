@@ -93,6 +93,31 @@ class FMGPoisson:
             raise SFMError(rc, "sfm_adjoint")
         return out, st
 
+    def autotune(self, reps: int = 3):
+        """Times every launch-shape candidate on this hierarchy and keeps the
+        fastest (sfm_autotune); results stay bit-identical whatever is chosen."""
+        rc = self.lib.sfm_autotune(self.ctx, reps)
+        if rc != abi.SFM_OK:
+            raise SFMError(rc, "sfm_autotune")
+
+    def tune_table(self) -> str:
+        """The tuning table as text (sfm_tune_save)."""
+        n = C.c_size_t()
+        rc = self.lib.sfm_tune_save(self.ctx, None, 0, C.byref(n))
+        if rc != abi.SFM_OK:
+            raise SFMError(rc, "sfm_tune_save")
+        buf = C.create_string_buffer(n.value + 1)
+        rc = self.lib.sfm_tune_save(self.ctx, buf, n.value + 1, None)
+        if rc != abi.SFM_OK:
+            raise SFMError(rc, "sfm_tune_save")
+        return buf.value.decode()
+
+    def load_tune_table(self, text: str):
+        """Replaces the tuning table (sfm_tune_load); '' restores the defaults."""
+        rc = self.lib.sfm_tune_load(self.ctx, text.encode())
+        if rc != abi.SFM_OK:
+            raise SFMError(rc, "sfm_tune_load")
+
     def info(self):
         lv = C.c_int32()
         by = C.c_int64()

@@ -182,6 +182,34 @@ const char *sfm_strerror(int code);
  * bytes of device memory held by the context. */
 int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes);
 
+/* ---- autotuner (no counterpart in the reference) -----------------------
+ * The solver's kernels come in launch-shape variants (ghost fill of a level
+ * by three directional passes or by one launch; threads of the smoother
+ * CTA; blocks per residual CTA) that evaluate the same expressions in the
+ * same order, so no choice changes a result bit.  The reference has no such
+ * knobs; its sweep counts and coarse-level cutoff (fmg.F90:280-288,
+ * mg.F90:50-52, vmg.F90:85-91) stay fixed here because they change the
+ * iterates.
+ *
+ * sfm_autotune times every candidate of every knob the context's hierarchy
+ * uses (each `reps` times, 1 <= reps <= 100, on the context's own stream and
+ * fields; the fields are zeroed first) and keeps the fastest.  Call it
+ * between solves, outside stream capture; it takes about a second for a
+ * hierarchy of 1e5 blocks.  Without it (or after sfm_tune_load(c, "")) the
+ * built-in defaults apply. */
+int sfm_autotune(sfm_ctx *c, int32_t reps);
+
+/* The tuning table as text, one choice per line
+ *   "<knob> <element bytes> <block edge> <AMR level> <fill kind> <choice>",
+ * '#' starting a comment line.  sfm_tune_save writes it NUL-terminated into
+ * buf (when buf is not NULL) and its length without the NUL into *len (when
+ * len is not NULL); SFM_ESIZE if cap is too small.  sfm_tune_load replaces
+ * the table; a malformed table returns SFM_EINVAL and leaves it unchanged.
+ * A table saved for one hierarchy and GPU may be loaded into a context of
+ * another: unused entries are ignored, missing ones take the defaults. */
+int sfm_tune_save(const sfm_ctx *c, char *buf, size_t cap, size_t *len);
+int sfm_tune_load(sfm_ctx *c, const char *text);
+
 /* Uniform periodic base-grid solve that allocates nothing.  No counterpart
  * in the reference: it runs the reference's base-grid multigrid (mg_cycle's
  * residual / mg_lin / correction loop, mg.F90:42-94, with mg_lin of

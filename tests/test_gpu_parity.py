@@ -1,10 +1,10 @@
 """CUDA solver versus the CPU restatement (oracle) on the same seeded inputs.
 
 FP64 path: the device kernels evaluate the reference's expressions in the
-same order with --fmad=false, so with periodic boundaries every field must
-agree to the last bit; with the isolated-sphere boundary the multipole
-moments are summed in a different order (per-block partial sums), so the
-tolerance is 1e-13 relative (max norm).  Mixed path: the FP32 inner solve
+same order with --fmad=false (the multipole moments of the isolated boundary
+included: one running sum per moment in the reference's cell order), so
+every field must agree to the last bit, with the ghost cells filled by the
+three directional passes or by one launch per level.  Mixed path: the FP32 inner solve
 inside the FP64 defect correction must reach the same solution as the FP64
 oracle to 1e-9 relative in phi (phi minus its mean for periodic boxes, whose
 constant is free) and in g, at relative residual <= 1e-10.
@@ -44,19 +44,32 @@ CASES = {
 }
 
 
+def force_ghost_fill(s, mode):
+    """mode None: the tuning table (three passes by default); 1: one launch
+    per level wherever that is exact; 0: always the three passes"""
+    if mode is None:
+        return
+    lib = s.lib
+    lib.sfm_debug_set_ghost_merge.argtypes = [C.c_void_p, C.c_int]
+    lib.sfm_debug_set_ghost_merge.restype = C.c_int
+    assert lib.sfm_debug_set_ghost_merge(s.ctx, mode) == abi.SFM_OK
+
+
+@pytest.mark.parametrize("ghost", [None, 1], ids=["default", "one_launch_fill"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_fp64_matches_oracle(name):
+def test_fp64_matches_oracle(name, ghost):
     mk, fn, bc, kw = CASES[name]
     h = mk()
     p = abi.default_params(bc, **kw)
     rho = w.block_field(h, p.ngh_io, fn)
     rc1, psi1, g1, st1, _ = oracle_solve(h, rho, p)
     with FMGPoisson(h, params=p) as s:
+        force_ghost_fill(s, ghost)
         psi2, g2, st2 = s.solve(rho)
         # a second call on the same context must start from fresh arrays
         psi3, g3, st3 = s.solve(rho)
     assert rc1 == abi.SFM_OK and st1.outer_iters == st2.outer_iters
-    tol = 0.0 if bc == abi.SFM_BC_PERIODIC else 1e-13
+    tol = 0.0   # bit-identical: the isolated boundary's moments are summed in the reference's order too
     assert rel(interior(h, psi2, 2), interior(h, psi1, 2)) <= tol
     assert rel(psi2[:, 1:-1, 1:-1, 1:-1], psi1[:, 1:-1, 1:-1, 1:-1]) <= tol
     assert rel(interior(h, g2, 2), interior(h, g1, 2)) <= tol
@@ -93,8 +106,9 @@ def test_warm_start_matches_oracle():
     assert rel(psi2, psi1) == 0.0 and rel(interior(h, g2, 2), interior(h, g1, 2)) == 0.0
 
 
+@pytest.mark.parametrize("ghost", [None, 1], ids=["default", "one_launch_fill"])
 @pytest.mark.parametrize("name", ["amr3_periodic", "amr3_sphere_l4", "amr3_periodic_ni16"])
-def test_mixed_precision_reaches_fp64_solution(name):
+def test_mixed_precision_reaches_fp64_solution(name, ghost):
     mk, fn, bc, kw = CASES[name]
     h = mk()
     p64 = abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw)
@@ -102,6 +116,7 @@ def test_mixed_precision_reaches_fp64_solution(name):
     rho = w.block_field(h, p64.ngh_io, fn)
     _, psi1, g1, st1, _ = oracle_solve(h, rho, p64)
     with FMGPoisson(h, params=pmx) as s:
+        force_ghost_fill(s, ghost)
         psi2, g2, st2 = s.solve(rho)
     assert st2.true_rel_residual <= 1e-10
     a, b = interior(h, psi2, 2), interior(h, psi1, 2)

@@ -1,0 +1,48 @@
+"""The autotuner on the GPU: every launch-shape candidate evaluates the same
+expressions in the same order, so a tuned solve must be bit-identical to the
+untuned one (and, in FP64, to the oracle); the table survives a save/load
+round trip and an empty table restores the defaults."""
+import numpy as np
+import pytest
+
+from code_only_b200 import abi, workloads as w
+from code_only_b200.solver import FMGPoisson, SFMError
+from tests.oracle_lib import oracle_solve
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "amr3_periodic": (lambda: w.small_periodic(2, 8, 3, 1), w.gaussian_peak, abi.SFM_BC_PERIODIC, {}),
+    "amr3_sphere_l4": (lambda: w.small_sphere(2, 8, 3, 2), w.softened_sphere, abi.SFM_BC_SPHERE,
+                       {"zero_mean": 0, "lmax": 4}),
+    "amr3_periodic_ni16": (lambda: w.small_periodic(2, 16, 3, 4), w.gaussian_peak, abi.SFM_BC_PERIODIC, {}),
+}
+
+
+@pytest.mark.parametrize("prec", [abi.SFM_PREC_FP64, abi.SFM_PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("name", list(CASES))
+def test_tuned_solve_is_bitwise_unchanged(name, prec):
+    mk, fn, bc, kw = CASES[name]
+    h = mk()
+    p = abi.default_params(bc, rel_tol=1e-10, max_outer=40, precision=prec, **kw)
+    rho = w.block_field(h, p.ngh_io, fn)
+    with FMGPoisson(h, params=p) as s:
+        psi0, g0, st0 = s.solve(rho)
+        s.autotune(2)
+        table = s.tune_table()
+        assert any(ln.startswith(("ghost_fill", "relax_threads", "resid_bpc")) for ln in table.splitlines())
+        psi1, g1, st1 = s.solve(rho)
+        s.load_tune_table("")
+        assert s.tune_table().strip().splitlines()[1:] == []
+        s.load_tune_table(table)
+        assert s.tune_table() == table
+        psi2, g2, st2 = s.solve(rho)
+        with pytest.raises(SFMError):
+            s.load_tune_table("relax_threads 4 8 -1 -1 100\n")
+        assert s.tune_table() == table            # a rejected table leaves the old one
+    assert np.array_equal(psi0, psi1) and np.array_equal(g0, g1)
+    assert np.array_equal(psi0, psi2) and np.array_equal(g0, g2)
+    assert st0.outer_iters == st1.outer_iters
+    if prec == abi.SFM_PREC_FP64:
+        _, psi_o, g_o, _, _ = oracle_solve(h, rho, abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw))
+        assert np.array_equal(psi1[:, 1:-1, 1:-1, 1:-1], psi_o[:, 1:-1, 1:-1, 1:-1])
