@@ -119,6 +119,26 @@ __global__ void __launch_bounds__(256) k_blocks(Op op, int nblk, int bpc) {
         }
 }
 
+// Serial reference order for race checks: one thread per listed block
+// applies op to the block's items per_block*q .. per_block*(q+1)-1 in order
+// (the cell order of a single-threaded sweep), max of the results folded
+// into *out as k_apply_max does.
+template <class Op>
+__global__ void k_serial_blocks(Op op, int nblk, int per_block, unsigned long long *out) {
+    pdl_enter();
+    double m = 0.0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nblk; q += gridDim.x * blockDim.x)
+        for (int r = 0; r < per_block; r++) {
+            const double v = op((int64_t)q * per_block + r);
+            m = v > m ? v : m;
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        double t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
 // max over items of op(i) >= 0, folded into *out by atomicMax on the IEEE
 // bit pattern (order-preserving for non-negative doubles)
 template <class Op>

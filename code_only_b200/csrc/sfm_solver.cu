@@ -13,6 +13,7 @@
 // FP32 inside the FP64 defect-correction loop, with the outer residual, the
 // accumulation into phi, the reflux flux sums and the base-grid solve in FP64.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <array>
@@ -219,6 +220,7 @@ public:
     virtual int fmg_levels() const = 0;
     virtual void set_wait_polls(uint32_t polls) = 0;
     virtual void set_ghost_merge(bool on) = 0;
+    virtual void set_serial_relax(bool on) = 0;
     virtual int autotune(int reps) = 0;
     virtual std::string tune_text() const = 0;
     virtual bool tune_load(const char *text) = 0;
@@ -254,6 +256,7 @@ public:
     std::vector<std::array<int, 3>> gCnt;       // [level][sel + 1]: general items
     std::vector<std::array<bool, 3>> ghostMerge;   // [level][sel + 1]: one launch fills the level
     int ghostForce = -1;                   // test hook: 1 / 0 forces the one-launch fill on / off, -1 the table
+    bool serialRelax = false;              // test hook: colour sweeps one thread per block, in cell order
     TuneTable tune;                        // launch-shape choices (sfm_tune.h); empty = defaults
     RefluxItem *d_reflux = nullptr;
     BFace *d_tfL = nullptr, *d_tfDL = nullptr, *d_crop = nullptr;
@@ -297,11 +300,13 @@ public:
     int64_t iterLaunches = 0;
     bool graphsOff = false;
     void outer_iteration_body() {
+        nvtxRangePushA("sfm outer iteration");
         profNext = 0;
         resid<double, double, T>(0, RHO[0], PSI0, SRC0, false);
         fmg_lin();
         add(0, PSI0, U[0]);
         profPairs = profNext;
+        nvtxRangePop();
     }
     void outer_iteration() {
         if (graphsOff) { outer_iteration_body(); return; }
@@ -346,6 +351,13 @@ public:
     int64_t device_bytes() const override { return mem.bytes; }
     // the iteration graph holds the kernel parameters it was captured with:
     // a new limit drops it, and the next outer iteration captures again
+    void set_serial_relax(bool on) override {
+        serialRelax = on;
+        if (iterExec) {
+            cudaGraphExecDestroy(iterExec);
+            iterExec = nullptr;
+        }
+    }
     void set_ghost_merge(bool on) override {
         ghostForce = on ? 1 : 0;
         if (iterExec) {
@@ -968,6 +980,13 @@ public:
                       int f, int ipass, unsigned long long *out) {
         const int n = nf[f];
         if (nblk <= 0) return;
+        if (serialRelax) {   // race check: the same cells in a single-threaded sweep's order
+            const int per = n * n * n / 2;
+            launch_pdl(k_serial_blocks<OpRelax<T, T>>, (unsigned)((nblk + 127) / 128), 128, 0,
+                       OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass}, nblk, per, out);
+            ++launches;
+            return;
+        }
         const int nt = tune.get(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, n >= 16 ? 512 : 256);
         SFM_WITH_N(n,
                    (bulk_ok<N>() ? (nt == 512 ? relax_bulk_launch<N, 512>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out)
@@ -1106,6 +1125,7 @@ public:
 
     // fmg_lin (fmg.F90:270-377)
     void fmg_lin() {
+        nvtxRangePushA("sfm fmg_lin");
         const int FMax = H.FMax;
         for (int f = 1; f <= FMax; f++) fmg_rstrct(f, RHO[f], RHO[f - 1]);
         fill0(FMax, U[FMax]);
@@ -1130,6 +1150,7 @@ public:
             }
         }
         converge_c2p(0, U[0]);
+        nvtxRangePop();
     }
 
     // -----------------------------------------------------------------
@@ -1206,6 +1227,7 @@ public:
     }
     // vmg_fas (vmg.F90:116-243); jrho = IRHS when copy_rhs (second and later calls)
     void vmg_fas(bool copy_rhs) {
+        nvtxRangePushA("sfm vmg_fas");
         const int F = H.FMax, nlev = H.nlev;
         // the level lists are consecutive ranges of d_all: the per-level
         // copies of vmg_fas are one launch over all blocks
@@ -1233,6 +1255,7 @@ public:
             vmg_gridboundary(v, U[F]);
             for (int q = 0; q < 2; q++) vmg_relax(v, U[F], RHS[F]);
         }
+        nvtxRangePop();
     }
 
     // -----------------------------------------------------------------
@@ -1948,6 +1971,16 @@ int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes) {
 int sfm_debug_set_wait_polls(sfm_ctx *c, uint32_t polls) {
     if (!c || !c->s) return SFM_EINVAL;
     c->s->set_wait_polls(polls);
+    return SFM_OK;
+}
+
+// Test hook (not part of include/sfmg.h): 1 runs every red-black colour
+// sweep one thread per block, the block's cells in the order of a serial
+// sweep; a result bit-identical to the parallel kernels shows that no cell
+// of a colour depends on another cell of the same colour (race check).
+int sfm_debug_set_serial_relax(sfm_ctx *c, int on) {
+    if (!c || !c->s) return SFM_EINVAL;
+    c->s->set_serial_relax(on != 0);
     return SFM_OK;
 }
 

@@ -214,3 +214,25 @@ def test_bounded_smoother_wait_reports_timeout():
     with FMGPoisson(h, params=p) as s:
         psi2, g2, st2 = s.solve(rho)
     assert rel(psi2, psi1) == 0.0 and rel(interior(h, g2, 2), interior(h, g1, 2)) == 0.0
+
+
+@pytest.mark.parametrize("name", ["amr3_periodic", "amr3_sphere_l4", "amr3_periodic_ni16"])
+def test_red_black_sweeps_have_no_intra_colour_race(name):
+    """Race check of the red-black smoother: with every colour sweep run one
+    thread per block, the block's cells in the order of a serial sweep
+    (sfm_debug_set_serial_relax), the solve must be bit-identical to the
+    parallel kernels.  A cell of one colour that read another cell of the
+    same colour while it was being updated would make the two differ."""
+    mk, fn, bc, kw = CASES[name]
+    h = mk()
+    for prec in (abi.SFM_PREC_FP64, abi.SFM_PREC_MIXED):
+        p = abi.default_params(bc, rel_tol=1e-10, max_outer=40, precision=prec, **kw)
+        rho = w.block_field(h, p.ngh_io, fn)
+        with FMGPoisson(h, params=p) as s:
+            psi_par, g_par, st_par = s.solve(rho)
+            s.lib.sfm_debug_set_serial_relax.argtypes = [C.c_void_p, C.c_int]
+            s.lib.sfm_debug_set_serial_relax.restype = C.c_int
+            assert s.lib.sfm_debug_set_serial_relax(s.ctx, 1) == abi.SFM_OK
+            psi_ser, g_ser, st_ser = s.solve(rho)
+        assert st_par.outer_iters == st_ser.outer_iters
+        assert np.array_equal(psi_par, psi_ser) and np.array_equal(g_par, g_ser)
