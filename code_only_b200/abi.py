@@ -154,7 +154,7 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.sfm_strerror.restype = C.c_char_p
     lib.sfm_info.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     lib.sfm_info.restype = C.c_int
-    lib.sfm_autotune.argtypes = [C.c_void_p, C.c_int32]
+    lib.sfm_autotune.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     lib.sfm_autotune.restype = C.c_int
     lib.sfm_tune_save.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     lib.sfm_tune_save.restype = C.c_int

@@ -266,7 +266,8 @@ __host__ __device__ inline int mg_smem_from(int N, int MMax, size_t budget_doubl
 }
 
 // mg_cycle (mg.F90:42-94) with ju = PSI, jrho = SRC; one CTA
-__global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, int *iters_out) {
+// (nmax: cap on the defect corrections, 10 in the reference)
+__global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, int *iters_out, int nmax) {
     pdl_enter();
     __shared__ double sh[32];
     MgData d = dg;
@@ -288,7 +289,7 @@ __global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, i
     mg_boundary_u(d, 0, d.PSI);
     double rhomax = 0.0;
     int it;
-    for (it = 1; it <= 10; it++) {
+    for (it = 1; it <= nmax; it++) {
         mg_resid(d, 0, d.RHO[0], d.PSI, d.SRC);
         if (it == 1) {
             const int n = d.N, G = n + 2;
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, i
         mg_addw(d, 0, d.PSI, d.U[0]);
         if (res / rhomax < errmax) break;
     }
-    if (threadIdx.x == 0 && iters_out) *iters_out = it > 10 ? 10 : it;
+    if (threadIdx.x == 0 && iters_out) *iters_out = it > nmax ? nmax : it;
 }
 
 }  // namespace sfm

@@ -221,7 +221,7 @@ public:
     virtual void set_wait_polls(uint32_t polls) = 0;
     virtual void set_ghost_merge(bool on) = 0;
     virtual void set_serial_relax(bool on) = 0;
-    virtual int autotune(int reps) = 0;
+    virtual int autotune(int reps, const double *d_rho) = 0;
     virtual std::string tune_text() const = 0;
     virtual bool tune_load(const char *text) = 0;
     std::string last_error;
@@ -258,6 +258,12 @@ public:
     int ghostForce = -1;                   // test hook: 1 / 0 forces the one-launch fill on / off, -1 the table
     bool serialRelax = false;              // test hook: colour sweeps one thread per block, in cell order
     TuneTable tune;                        // launch-shape choices (sfm_tune.h); empty = defaults
+    // schedule of the inner solve: the reference's in FP64, the table's (if
+    // any) in the mixed path, where the inner solve only preconditions the
+    // FP64 defect correction
+    int sched(int knob, int reference) const {
+        return sizeof(T) == 4 ? tune.get(knob, 4, H.NI, -1, -1, reference) : reference;
+    }
     RefluxItem *d_reflux = nullptr;
     BFace *d_tfL = nullptr, *d_tfDL = nullptr, *d_crop = nullptr;
     std::vector<int64_t> faceOff, faceSplit, tfLOff, tfDLOff, cropOff, wcOff;
@@ -401,7 +407,59 @@ public:
             tune.set(kKnobGhostFill, (int)sizeof(TT), n, L, sel, t[1] < t[0] ? 1 : 0);
         }
     }
-    int autotune(int reps) override {
+    // Schedule of the mixed path's inner solve (see sfm_tune.h): coordinate
+    // descent from the reference schedule over complete solves of the
+    // caller's density, keeping a change only when the solve still reaches
+    // rel_tol (stagnation exit and true residual as configured) and is at
+    // least 2% faster.  The FP64 path keeps the reference's schedule.
+    int tune_schedule(const double *d_rho, int reps) {
+        auto solve_ms = [&](float &ms) -> bool {
+            if (iterExec) {   // the graph holds the old schedule
+                cudaGraphExecDestroy(iterExec);
+                iterExec = nullptr;
+            }
+            sfm_stats st;
+            const int rc = solve(d_rho, nullptr, nullptr, &st, own_, 0, nullptr);
+            if (rc != SFM_OK || !(st.true_rel_residual <= P.rel_tol) || !st.converged) return false;
+            ms = (float)st.device_ms;
+            return true;
+        };
+        auto candidate = [&]() -> float {
+            float ms = 0.f, best = std::numeric_limits<float>::max();
+            if (!solve_ms(ms)) return best;   // the first solve also captures the graph
+            for (int r = 0; r < reps; r++)
+                if (solve_ms(ms) && ms < best) best = ms;
+            return best;
+        };
+        struct Knob { int knob; int ref; std::vector<int> vals; };
+        const Knob ks[] = {{kKnobBaseCorr, 10, {10, 4, 2, 1}},
+                           {kKnobFmgCycles, 2, {2, 1}},
+                           {kKnobFmgSweeps, 2, {2, 1, 3}},
+                           {kKnobVmgSweeps, 2, {2, 1}}};
+        for (const Knob &k : ks) tune.set(k.knob, 4, H.NI, -1, -1, k.ref);
+        float best = candidate();
+        if (best == std::numeric_limits<float>::max()) return SFM_ENOTCONVERGED;   // not even the reference
+        for (const Knob &k : ks) {
+            const int cur = tune.get(k.knob, 4, H.NI, -1, -1, k.ref);
+            int pick = cur;
+            for (int v : k.vals) {
+                if (v == cur) continue;
+                tune.set(k.knob, 4, H.NI, -1, -1, v);
+                const float t = candidate();
+                if (t < 0.98f * best) {
+                    best = t;
+                    pick = v;
+                }
+            }
+            tune.set(k.knob, 4, H.NI, -1, -1, pick);
+        }
+        if (iterExec) {
+            cudaGraphExecDestroy(iterExec);
+            iterExec = nullptr;
+        }
+        return SFM_OK;
+    }
+    int autotune(int reps, const double *d_rho) override {
         st_ = own_;
         const int saveForce = ghostForce;
         ghostForce = -1;
@@ -460,12 +518,17 @@ public:
             }
         }
         FmgLevel_fill0 = Undef;
-        ghostForce = saveForce;
         if (iterExec) {   // the graph holds the old launch shapes
             cudaGraphExecDestroy(iterExec);
             iterExec = nullptr;
         }
-        return check("autotune");
+        int rc = check("autotune");
+        if (rc == SFM_OK && d_rho && sizeof(T) == 4) {
+            rc = tune_schedule(d_rho, std::min(reps, 2));
+            if (rc == SFM_OK) rc = check("autotune schedule");
+        }
+        ghostForce = saveForce;
+        return rc;
     }
     std::string tune_text() const override { return tune.text(); }
     bool tune_load(const char *text) override {
@@ -1133,9 +1196,10 @@ public:
         for (int f = FMax - 1; f >= 0; f--) {
             fmg_interp(f, U[f], U[f + 1], true);
             copy(f, RHS[f], RHO[f], false);
-            for (int jc = 1; jc <= 2; jc++) {
+            const int ncycle = sched(kKnobFmgCycles, 2), nsweep = sched(kKnobFmgSweeps, 2);
+            for (int jc = 1; jc <= ncycle; jc++) {
                 for (int v = f; v <= FMax - 1; v++) {
-                    for (int q = 0; q < 2; q++) relax(v, U[v], RHS[v], true, 0);
+                    for (int q = 0; q < nsweep; q++) relax(v, U[v], RHS[v], true, 0);
                     resid(v, RES[v], U[v], RHS[v], true);
                     fmg_rstrct(v + 1, RHS[v + 1], RES[v]);
                     fill0(v + 1, U[v + 1]);
@@ -1145,7 +1209,7 @@ public:
                 for (int v = FMax - 1; v >= f; v--) {
                     fmg_interp(v, RES[v], U[v + 1], false);   // fmg_addint
                     add(v, U[v], RES[v]);
-                    for (int q = 0; q < 2; q++) relax(v, U[v], RHS[v], true, 0);
+                    for (int q = 0; q < nsweep; q++) relax(v, U[v], RHS[v], true, 0);
                 }
             }
         }
@@ -1221,7 +1285,7 @@ public:
         const int F = H.FMax;
         int64_t N3 = (int64_t)NBc * NBc * NBc;
         run(OpMgGather<T>{mg.SRC, mg.PSI, rhs, u, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
-        launch_pdl(k_mg_cycle, 1, 512, mgSmemBytes, mg, mgSmemFrom, d_mgit);
+        launch_pdl(k_mg_cycle, 1, 512, mgSmemBytes, mg, mgSmemFrom, d_mgit, sched(kKnobBaseCorr, 10));
         ++launches;
         run(OpMgScatter<T>{u, mg.PSI, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
     }
@@ -1236,9 +1300,10 @@ public:
         converge_c2p(F, RHO[F]);
         boundary_fill0(F, U[F]);
         runB(OpCopy<T, T>{RHS[F], RHO[F], d_all, Vf[F]}, H.nb);
+        const int nvs = sched(kKnobVmgSweeps, 2);
         for (int v = nlev - 1; v >= 1; v--) {
             vmg_gridboundary(v, U[F]);
-            for (int q = 0; q < 2; q++) vmg_relax(v, U[F], RHS[F]);
+            for (int q = 0; q < nvs; q++) vmg_relax(v, U[F], RHS[F]);
             vmg_rstrct(v - 1, U[F], true);
             vmg_copy_level(v - 1, RUF, U[F]);
             vmg_rstrct(v - 1, RHS[F], false);
@@ -1253,7 +1318,7 @@ public:
             vmg_interp(v, RES[F], RES[F]);
             runB(OpAdd<T, T>{U[F], RES[F], d_all + H.lstart[v], Vf[F]}, cnt(v));
             vmg_gridboundary(v, U[F]);
-            for (int q = 0; q < 2; q++) vmg_relax(v, U[F], RHS[F]);
+            for (int q = 0; q < nvs; q++) vmg_relax(v, U[F], RHS[F]);
         }
         nvtxRangePop();
     }
@@ -1917,10 +1982,11 @@ const char *sfm_strerror(int code) {
     }
 }
 
-int sfm_autotune(sfm_ctx *c, int32_t reps) {
+int sfm_autotune(sfm_ctx *c, int32_t reps, const double *d_rho) {
     if (!c || !c->s || reps < 1 || reps > 100) return SFM_EINVAL;
     DeviceGuard dg(c->device);
-    return sfm_guard([&] { return c->s->autotune(reps); });
+    if (d_rho && !device_pointer_on(d_rho, c->device)) return SFM_EINVAL;
+    return sfm_guard([&] { return c->s->autotune(reps, d_rho); });
 }
 
 int sfm_tune_save(const sfm_ctx *c, char *buf, size_t cap, size_t *len) {

@@ -1,12 +1,12 @@
-// sfm_tune.h -- the launch-shape table of the autotuner (host code only).
+// sfm_tune.h -- the table of the autotuner (host code only).
 //
-// The solver's kernels come in variants that differ only in how the work
-// is spread over threads and CTAs; every variant evaluates the same
-// expressions in the same order, so the choice never changes a result bit.
+// The solver's kernels come in launch-shape variants that differ only in how
+// the work is spread over threads and CTAs; every variant evaluates the same
+// expressions in the same order, so that choice never changes a result bit.
 // A table maps (knob, element size, block edge, AMR level, fill kind) to the
 // chosen variant; Solver::autotune fills it by timing the candidates on the
 // context's own hierarchy, sfm_tune_save / sfm_tune_load keep it across
-// runs.  Knobs:
+// runs.  Launch-shape knobs:
 //   ghost_fill    level fill by the three directional passes (0) or by one
 //                 launch per level (1; only where Solver::ghost_merge_ok);
 //                 key: element size, block edge n, AMR level, fill kind
@@ -14,6 +14,16 @@
 //                 key: element size, block edge n
 //   resid_bpc     blocks per CTA of the tiled residual (1, 2 or 4);
 //                 key: element size, block edge n
+// and, for the mixed-precision path only (element size 4), the schedule of
+// the FP32 inner solve, which is a preconditioner inside the FP64 defect
+// correction: the outer loop converges to the same potential whatever the
+// schedule, only its cost and the number of outer iterations change (the
+// FP64 path always runs the reference's schedule):
+//   fmg_ncycle      V-cycles per fmg level in fmg_lin (reference 2, fmg.F90:280-288)
+//   fmg_sweeps      pre- and post-smoothing sweeps in fmg_lin (reference 2)
+//   vmg_sweeps      pre- and post-smoothing sweeps in vmg_fas (reference 2, vmg.F90:125-135)
+//   base_corrections  cap on mg_cycle's defect corrections (reference 10, mg.F90:50-52)
+//   key: element size 4, block edge NI, level -1, kind -1
 // Text form, one entry per line (blank lines and lines starting with '#'
 // are skipped):
 //   <knob> <element bytes> <n> <level> <kind> <choice>
@@ -31,12 +41,19 @@
 
 namespace sfm {
 
-enum TuneKnob { kKnobGhostFill = 0, kKnobRelaxThreads = 1, kKnobResidBpc = 2, kKnobCount = 3 };
+enum TuneKnob {
+    kKnobGhostFill = 0, kKnobRelaxThreads = 1, kKnobResidBpc = 2,
+    kKnobFmgCycles = 3, kKnobFmgSweeps = 4, kKnobVmgSweeps = 5, kKnobBaseCorr = 6, kKnobCount = 7
+};
 inline const char *tune_knob_name(int k) {
     switch (k) {
         case kKnobGhostFill: return "ghost_fill";
         case kKnobRelaxThreads: return "relax_threads";
         case kKnobResidBpc: return "resid_bpc";
+        case kKnobFmgCycles: return "fmg_ncycle";
+        case kKnobFmgSweeps: return "fmg_sweeps";
+        case kKnobVmgSweeps: return "vmg_sweeps";
+        case kKnobBaseCorr: return "base_corrections";
         default: return nullptr;
     }
 }
@@ -45,6 +62,10 @@ inline bool tune_choice_ok(int knob, int v) {
         case kKnobGhostFill: return v == 0 || v == 1;
         case kKnobRelaxThreads: return v == 256 || v == 512;
         case kKnobResidBpc: return v == 1 || v == 2 || v == 4;
+        case kKnobFmgCycles: return v >= 1 && v <= 3;
+        case kKnobFmgSweeps: return v >= 1 && v <= 3;
+        case kKnobVmgSweeps: return v >= 1 && v <= 3;
+        case kKnobBaseCorr: return v >= 1 && v <= 10;
         default: return false;
     }
 }

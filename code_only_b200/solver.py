@@ -93,10 +93,13 @@ class FMGPoisson:
             raise SFMError(rc, "sfm_adjoint")
         return out, st
 
-    def autotune(self, reps: int = 3):
+    def autotune(self, reps: int = 3, rho_ptr: Optional[int] = None):
         """Times every launch-shape candidate on this hierarchy and keeps the
-        fastest (sfm_autotune); results stay bit-identical whatever is chosen."""
-        rc = self.lib.sfm_autotune(self.ctx, reps)
+        fastest (sfm_autotune; bit-identical results whatever is chosen).  With
+        rho_ptr (device array of the density, sfm_solve_device's layout) a
+        mixed-precision context also tunes its inner-solve schedule by complete
+        solves of that density."""
+        rc = self.lib.sfm_autotune(self.ctx, reps, C.c_void_p(rho_ptr) if rho_ptr else None)
         if rc != abi.SFM_OK:
             raise SFMError(rc, "sfm_autotune")
 

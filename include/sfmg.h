@@ -183,21 +183,31 @@ const char *sfm_strerror(int code);
 int sfm_info(const sfm_ctx *c, int32_t *fmg_levels, int64_t *device_bytes);
 
 /* ---- autotuner (no counterpart in the reference) -----------------------
- * The solver's kernels come in launch-shape variants (ghost fill of a level
- * by three directional passes or by one launch; threads of the smoother
- * CTA; blocks per residual CTA) that evaluate the same expressions in the
- * same order, so no choice changes a result bit.  The reference has no such
- * knobs; its sweep counts and coarse-level cutoff (fmg.F90:280-288,
- * mg.F90:50-52, vmg.F90:85-91) stay fixed here because they change the
- * iterates.
+ * Two kinds of knobs.
+ *  - Launch shapes: ghost fill of a level by three directional passes or by
+ *    one launch, threads of the smoother CTA, blocks per residual CTA.  Every
+ *    variant evaluates the same expressions in the same order, so no choice
+ *    changes a result bit.
+ *  - The schedule of the mixed path's FP32 inner solve: V-cycles per level
+ *    and sweeps of fmg_lin (the reference's fixed Ncycle = 2, Npre = Npost =
+ *    2, fmg.F90:280-288), sweeps of vmg_fas (vmg.F90:125-135) and the cap on
+ *    the base-grid defect corrections (mg.F90:50-52).  That solve only
+ *    preconditions the FP64 defect correction, which converges to the same
+ *    potential (within rel_tol) whatever the schedule; only its cost and the
+ *    number of outer iterations change.  The FP64 path always runs the
+ *    reference's schedule.
  *
- * sfm_autotune times every candidate of every knob the context's hierarchy
+ * sfm_autotune times every launch-shape candidate the context's hierarchy
  * uses (each `reps` times, 1 <= reps <= 100, on the context's own stream and
- * fields; the fields are zeroed first) and keeps the fastest.  Call it
- * between solves, outside stream capture; it takes about a second for a
- * hierarchy of 1e5 blocks.  Without it (or after sfm_tune_load(c, "")) the
- * built-in defaults apply. */
-int sfm_autotune(sfm_ctx *c, int32_t reps);
+ * fields; the fields are zeroed first) and keeps the fastest.  With d_rho (a
+ * density in sfm_solve_device's layout, device memory of the context's
+ * device) a mixed-precision context also tunes the schedule by complete
+ * solves of that density: from the reference's schedule, one knob at a
+ * time, a change is kept only when the solve still converges to rel_tol and
+ * is at least 2% faster (a few seconds for 1e5 blocks).  Call it between
+ * solves, outside stream capture.  Without it (or after sfm_tune_load(c,
+ * "")) the built-in launch shapes and the reference's schedule apply. */
+int sfm_autotune(sfm_ctx *c, int32_t reps, const double *d_rho);
 
 /* The tuning table as text, one choice per line
  *   "<knob> <element bytes> <block edge> <AMR level> <fill kind> <choice>",

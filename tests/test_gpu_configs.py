@@ -83,9 +83,14 @@ def _check_fp64(h, rho, bc, kw, oracle_out):
     assert st2.true_rel_residual <= REL_TOL
 
 
-def _check_mixed(h, rho, bc, kw, oracle_out):
+def _check_mixed(h, rho, bc, kw, oracle_out, tuned=False):
     _, psi1, g1, _, _ = oracle_out
     with FMGPoisson(h, params=params(bc, abi.SFM_PREC_MIXED, **kw)) as s:
+        if tuned:   # launch shapes and the inner-solve schedule tuned on this density
+            import torch
+            rho_d = torch.from_numpy(rho).cuda()
+            s.autotune(2, rho_d.data_ptr())
+            del rho_d
         psi2, g2, st2 = s.solve(rho)
     assert st2.true_rel_residual <= REL_TOL
     a, b = interior(h, psi2, 2), interior(h, psi1, 2)
@@ -125,3 +130,11 @@ def test_jeans6_fp64_bitwise(jeans6):
 def test_jeans6_mixed_within_1e9(jeans6):
     h, rho, bc, out = jeans6
     _check_mixed(h, rho, bc, {}, out)
+
+
+def test_jeans6_mixed_tuned_within_1e9(jeans6):
+    """The benchmark's configuration: launch shapes and the mixed path's
+    inner-solve schedule tuned on the jeans6 density, then phi and g against
+    the FP64 oracle at the north-star bar."""
+    h, rho, bc, out = jeans6
+    _check_mixed(h, rho, bc, {}, out, tuned=True)

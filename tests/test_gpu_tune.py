@@ -46,3 +46,52 @@ def test_tuned_solve_is_bitwise_unchanged(name, prec):
     if prec == abi.SFM_PREC_FP64:
         _, psi_o, g_o, _, _ = oracle_solve(h, rho, abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw))
         assert np.array_equal(psi1[:, 1:-1, 1:-1, 1:-1], psi_o[:, 1:-1, 1:-1, 1:-1])
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_tuned_mixed_schedule_keeps_the_fp64_solution(name):
+    """With a density, sfm_autotune also tunes the schedule of the mixed
+    path's FP32 inner solve (V-cycles, sweeps, base-grid corrections).  The
+    FP64 defect correction still converges to the same potential: within
+    1e-9 (max norm, relative; phi's mean removed on periodic boxes) of the
+    FP64 oracle in phi and g, at relative residual <= 1e-10."""
+    import torch
+    mk, fn, bc, kw = CASES[name]
+    h = mk()
+    p = abi.default_params(bc, rel_tol=1e-10, max_outer=40, precision=abi.SFM_PREC_MIXED, **kw)
+    rho = w.block_field(h, p.ngh_io, fn)
+    rho_d = torch.from_numpy(rho).cuda()
+    with FMGPoisson(h, params=p) as s:
+        s.autotune(2, rho_d.data_ptr())
+        table = s.tune_table()
+        for knob in ("fmg_ncycle", "fmg_sweeps", "vmg_sweeps", "base_corrections"):
+            assert any(ln.startswith(knob + " 4 ") for ln in table.splitlines()), knob
+        psi2, g2, st2 = s.solve(rho)
+    assert st2.converged and st2.true_rel_residual <= 1e-10
+    _, psi1, g1, _, _ = oracle_solve(h, rho, abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw))
+    n = h.ni
+    a, b = psi2[:, 2:2 + n, 2:2 + n, 2:2 + n], psi1[:, 2:2 + n, 2:2 + n, 2:2 + n]
+    if bc == abi.SFM_BC_PERIODIC:
+        a, b = a - a.mean(), b - b.mean()
+    assert np.abs(a - b).max() / np.abs(b).max() <= 1e-9
+    ga, gb = g2[:, :, 2:2 + n, 2:2 + n, 2:2 + n], g1[:, :, 2:2 + n, 2:2 + n, 2:2 + n]
+    assert np.abs(ga - gb).max() / np.abs(gb).max() <= 1e-9
+
+
+def test_fp64_context_keeps_the_reference_schedule():
+    """The schedule knobs exist only for the mixed path: tuning an FP64
+    context with a density adds none, and its solve stays bit-identical to
+    the oracle."""
+    import torch
+    mk, fn, bc, kw = CASES["amr3_periodic"]
+    h = mk()
+    p = abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw)
+    rho = w.block_field(h, p.ngh_io, fn)
+    rho_d = torch.from_numpy(rho).cuda()
+    with FMGPoisson(h, params=p) as s:
+        s.autotune(2, rho_d.data_ptr())
+        assert not any(ln.startswith(("fmg_ncycle", "fmg_sweeps", "vmg_sweeps", "base_corrections"))
+                       for ln in s.tune_table().splitlines())
+        psi2, _, _ = s.solve(rho)
+    _, psi1, _, _, _ = oracle_solve(h, rho, p)
+    assert np.array_equal(psi2[:, 1:-1, 1:-1, 1:-1], psi1[:, 1:-1, 1:-1, 1:-1])
