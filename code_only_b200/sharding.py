@@ -1,0 +1,167 @@
+"""Block partition and ghost-cell halo exchange across ranks (one GPU each).
+
+The reference decomposes the hierarchy over MPI ranks block by block: each
+rank owns the blocks of every AMR level that a Peano-Hilbert curve assigns
+to it (refine.F90:662-706), and every ghost fill exchanges packed face
+slabs with the ranks owning the neighbours (fmg_ghostcell.F90:162,168 for
+same-level faces, :353,358 for coarse-fine ones).  This module is the same
+step for GPU ranks:
+
+* ``partition(h, world)`` -- the blocks of each AMR level are already in
+  Morton order (workloads.build_hierarchy); each level is cut into `world`
+  contiguous ranges of nearly equal block counts, so each rank owns a
+  compact region on every level.
+* ``GhostExchange`` -- for every pass (AMR level L, direction d) of the
+  three-pass fill, the cells a rank's own blocks read from blocks another
+  rank owns: the neighbour's boundary plane (whole transverse range, ghosts
+  included) for a same-level face, the coarse block's layer (the octant's
+  half face plus one cell on each side) for a coarse-fine face.  Both ends
+  derive the same lists from the hierarchy, so a pass exchange is one
+  grouped send/receive per peer of the packed values (``torch.distributed``
+  P2P: gloo between CPU ranks, NCCL between GPUs), each into the receiver's
+  own copy of the sender's block -- never a load from another GPU's memory.
+
+Run before each pass, the exchange makes a rank's owned blocks end the fill
+with exactly the values a single rank computes (tests/test_sharding.py,
+world size 2, bit for bit).  Residual maxima are an all-reduce of one value
+(``allreduce_max``); the base grid (at most 32^3 cells) is gathered whole on
+every rank, where the base-grid solve runs redundantly.
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+__all__ = ["partition", "GhostExchange", "allreduce_max"]
+
+
+def partition(h, world: int) -> np.ndarray:
+    """owner[nb]: rank of every block, contiguous Morton ranges per AMR level."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    owner = np.empty(h.nblocks, dtype=np.int32)
+    starts = np.concatenate([[0], np.cumsum(h.level_counts())]).astype(np.int64)
+    for L in range(h.nlev):
+        s, e = int(starts[L]), int(starts[L + 1])
+        cut = s + (np.arange(world + 1, dtype=np.int64) * (e - s)) // world
+        for r in range(world):
+            owner[cut[r]:cut[r + 1]] = r
+    return owner
+
+
+def _faces(h):
+    """(kind[nb,6], src[nb,6]): 0 same-level neighbour, 1 parent-level
+    neighbour (coarse-fine face), 2 physical boundary; the source block."""
+    nb = h.nblocks
+    kind = np.full((nb, 6), 2, dtype=np.int8)
+    src = np.full((nb, 6), -1, dtype=np.int64)
+    same = h.nbr >= 0
+    kind[same] = 0
+    src[same] = h.nbr[same]
+    for b in np.nonzero(h.level > 0)[0]:
+        p = h.parent[b]
+        for f in range(6):
+            if kind[b, f] == 0 or h.touch[b, f]:
+                continue
+            q = h.nbr[p, f]
+            if q >= 0:
+                kind[b, f] = 1
+                src[b, f] = q
+    return kind, src
+
+
+def _put3(d, x, a, b):
+    return (x, a, b) if d == 0 else ((a, x, b) if d == 1 else (a, b, x))
+
+
+class GhostExchange:
+    """Send and receive lists of every ghost pass for one rank.
+
+    Cell indices are flat offsets into a field of shape [nb, G, G, G]
+    (G = n + 2, i fastest), the layout of one fmg level; every rank holds a
+    full-size field and owns the blocks ``owner == rank``.
+    """
+
+    def __init__(self, h, owner: np.ndarray, rank: int, n: int):
+        self.h, self.owner, self.rank, self.n = h, np.asarray(owner), rank, n
+        self.world = int(self.owner.max()) + 1
+        G = n + 2
+        self.G, self.V = G, G ** 3
+        kind, src = _faces(h)
+        lev = np.asarray(h.level)
+        nb2 = n // 2
+        # needs[(L, d)][(reader, holder)] -> sorted unique flat cells the
+        # reader's blocks read from blocks the holder owns
+        self.needs: Dict[Tuple[int, int], Dict[Tuple[int, int], np.ndarray]] = {}
+        rng = np.arange(-1, n + 1)
+        for L in range(h.nlev):
+            blocks = np.nonzero(lev == L)[0]
+            for d in range(3):
+                acc: Dict[Tuple[int, int], List[np.ndarray]] = {}
+                for b in blocks:
+                    reader = int(self.owner[b])
+                    for lr in range(2):
+                        f = lr + 2 * d
+                        k = kind[b, f]
+                        if k == 2:
+                            continue
+                        s = int(src[b, f])
+                        holder = int(self.owner[s])
+                        if holder == reader:
+                            continue
+                        if k == 0:   # the neighbour's boundary plane, whole transverse range
+                            xs = n - 1 if lr == 0 else 0
+                            pa, qa = np.meshgrid(rng, rng, indexing="xy")
+                        else:        # the coarse layer: octant half face +- 1 cell
+                            if L == 0:
+                                continue
+                            xs = n - 1 if lr == 0 else 0
+                            ta = 1 if d == 0 else 0
+                            tb = 1 if d == 2 else 2
+                            oa, ob = int(h.ijk[b, ta] & 1) * nb2, int(h.ijk[b, tb] & 1) * nb2
+                            cr = np.arange(-1, nb2 + 1)
+                            pa, qa = np.meshgrid(cr + oa, cr + ob, indexing="xy")
+                        i, j, kk = _put3(d, xs, pa.ravel(), qa.ravel())
+                        cells = s * self.V + ((kk + 1) * G + (j + 1)) * G + (i + 1)
+                        acc.setdefault((reader, holder), []).append(np.asarray(cells, dtype=np.int64))
+                self.needs[(L, d)] = {key: np.unique(np.concatenate(v)) for key, v in acc.items()}
+
+    def pass_exchange(self, field, L: int, d: int):
+        """Exchange for pass (L, d): send the values of this rank's blocks that
+        other ranks read, receive the values this rank reads from theirs,
+        each into this rank's copy of the sender's block.  `field` is a flat
+        contiguous torch tensor of the level's field (CPU with gloo, CUDA with
+        NCCL); every rank calls this for every pass in the same order."""
+        import torch
+        import torch.distributed as dist
+        ops, recvs = [], []
+        for (reader, holder), cells in self.needs.get((L, d), {}).items():
+            idx = torch.from_numpy(cells).to(field.device)
+            if holder == self.rank:
+                ops.append(dist.P2POp(dist.isend, field[idx].contiguous(), reader))
+            elif reader == self.rank:
+                buf = torch.empty(cells.size, dtype=field.dtype, device=field.device)
+                ops.append(dist.P2POp(dist.irecv, buf, holder))
+                recvs.append((idx, buf))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for idx, buf in recvs:
+            field[idx] = buf
+
+    def bytes_per_pass(self) -> Dict[Tuple[int, int], int]:
+        """Values this rank receives per pass x 8 bytes (FP64)."""
+        out = {}
+        for key, m in self.needs.items():
+            out[key] = 8 * sum(int(c.size) for (reader, _), c in m.items() if reader == self.rank)
+        return out
+
+
+def allreduce_max(value: float, device=None) -> float:
+    """Max over ranks of one value (the residual maxima of fmg_poisson.F90:212)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())

@@ -2017,6 +2017,27 @@ int oracle_apply_LT(const sfm_hier_desc *h, const sfm_params *p, const double *y
     return SFM_OK;
 }
 
+// One ghost pass of fmg_ghostcell_fix -- parentlev then samelev of AMR
+// level L, direction dir (fmg_ghostcell.F90:49-54) -- at fmg level f on
+// `field` ([nblocks][G][G][G], G = (ni >> f) + 2), in place.  L < 0 runs the
+// whole fill (every level ascending, x then y then z).
+int oracle_ghost_pass(const sfm_hier_desc *h, const sfm_params *p, int f, int L, int dir, int cubic, double *field) {
+    Oracle o;
+    int rc = o.setup(h, p);
+    if (rc) return rc;
+    if (f < 0 || f > o.FMax || L >= o.nlev || dir < 0 || dir > 2) return SFM_EINVAL;
+    Arr &A = o.F(IU, f);
+    std::copy(field, field + A.d.size(), A.d.begin());
+    if (L < 0) {
+        o.ghostcell_fix(f, IU, cubic != 0);
+    } else {
+        o.parentlev(L, f, dir, IU, cubic != 0);
+        o.samelev(L, f, dir, IU);
+    }
+    std::copy(A.d.begin(), A.d.end(), field);
+    return SFM_OK;
+}
+
 int oracle_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

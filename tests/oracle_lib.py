@@ -38,6 +38,9 @@ def load_oracle():
     lib.oracle_adjoint.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p,
                                    C.POINTER(abi.SfmStats)]
     lib.oracle_adjoint.restype = C.c_int
+    lib.oracle_ghost_pass.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.c_void_p]
+    lib.oracle_ghost_pass.restype = C.c_int
     _lib = lib
     return lib
 
@@ -78,3 +81,13 @@ def leaf_mask(h, n_ghost):
 
 def make_rho(h, fn, ngh):
     return workloads.block_field(h, ngh, fn)
+
+
+def oracle_ghost_pass(h, field, f, L=-1, d=0, cubic=False):
+    """One ghost pass (AMR level L, direction d) at fmg level f on `field`
+    ([nb, G, G, G], G = (ni >> f) + 2) in place, or the whole fill when L < 0."""
+    lib = load_oracle()
+    assert field.dtype == np.float64 and field.flags.c_contiguous
+    rc = lib.oracle_ghost_pass(abi.HierDesc(h).ref(), C.byref(abi.default_params(abi.SFM_BC_PERIODIC)), f, L, d,
+                               1 if cubic else 0, field.ctypes.data)
+    assert rc == 0, rc
