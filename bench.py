@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint leg (one adjoint solve of W = 1/2 sum rho phi dV, mixed precision)")
+    ap.add_argument("--tune-table", default=None,
+                    help="with --single: load this tuning table if the file exists, else tune and write it "
+                         "(a profiler run then launches only the solve)")
     ap.add_argument("--single", choices=["mixed", "fp64"], default=None,
                     help="autotune, then run exactly one solve of that precision and exit (for profiler launch lists)")
     return ap.parse_args()
@@ -216,7 +219,13 @@ def run_single(args):
     g_d = torch.zeros((h.nblocks, 3, G, G, G), dtype=torch.float64, device="cuda")
     prec = abi.SFM_PREC_MIXED if args.single == "mixed" else abi.SFM_PREC_FP64
     with FMGPoisson(h, params=params_for(bc, prec)) as s:
-        s.autotune(3, rho_d.data_ptr())   # the launch shapes and schedule the timed bench uses
+        if args.tune_table and os.path.exists(args.tune_table):
+            s.load_tune_table(open(args.tune_table).read())
+        else:
+            s.autotune(3, rho_d.data_ptr())   # the launch shapes and schedule the timed bench uses
+            if args.tune_table:
+                with open(args.tune_table, "w") as fh:
+                    fh.write(s.tune_table())
         torch.cuda.synchronize()
         st = s.solve_device(rho_d.data_ptr(), psi_d.data_ptr(), g_d.data_ptr())
         torch.cuda.synchronize()
