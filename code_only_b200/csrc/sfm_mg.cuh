@@ -1,14 +1,15 @@
 // sfm_mg.cuh -- the uniform base-grid multigrid (mg.F90, mg_poisson.F90,
-// mg_interpol_cubic.F90) as one persistent CTA.
+// mg_interpol_cubic.F90) as one persistent CTA or one thread-block cluster.
 //
 // The reference gathers the base level to rank 0 and runs mg_cycle there
 // serially (vmg.F90:407-428, mg_data.F90:179-330).  Here the whole cycle
 // (<= 10 defect corrections of an FMG with Ncycle 2, 2/2 smoothing) runs in
-// one CTA of 512 threads on a base grid of at most 64^3 cells: the coarse
-// levels' working arrays in shared memory, level 0 and the data exchanged
-// with the AMR levels in global memory (L2), every operation separated by
-// __syncthreads; nothing returns to the host.  FP64 throughout (the
-// coarsest-level solve stays in FP64 in the mixed-precision path).
+// one launch of 512-thread CTAs on a base grid of at most 64^3 cells: the
+// coarse levels' working arrays in shared memory, the large levels and the
+// data exchanged with the AMR levels in global memory (L2), every operation
+// separated by a CTA or cluster barrier; nothing returns to the host.  FP64
+// throughout (the coarsest-level solve stays in FP64 in the mixed-precision
+// path).
 #pragma once
 #include "sfm_device.cuh"
 
@@ -37,6 +38,69 @@ __device__ __forceinline__ void mg_ijk(int c, int n, int ln, int &i, int &j, int
 }
 __device__ __forceinline__ double mgH(const MgData &d, int m) { return d.hbase * (double)(1 << m); }
 
+// ---------------------------------------------------------------------------
+// One CTA or a thread-block cluster.  With a cluster, the steps on the large
+// levels (at least wide_min cells per edge; their arrays in global memory,
+// L2-resident) are spread over every thread of every CTA and end with a
+// cluster barrier; the steps on the small levels run on CTA 0 alone, their
+// arrays in its shared memory, separated by __syncthreads, while the other
+// CTAs skip them and wait at the next large-level step.  Each cell is still
+// computed by one thread with the same expression, and the maxima are exact,
+// so the result does not depend on the CTA count.  Distributed shared memory
+// is read twice: the cluster-wide maximum (one value per CTA), and the copy
+// of a small level into every CTA before it is interpolated onto a large one.
+// ---------------------------------------------------------------------------
+struct MgRun {
+    int rank, nct;     // this CTA's rank in the cluster, CTAs in the cluster (1: one CTA)
+    int wide_min;      // levels with at least this many cells per edge use the whole cluster
+    int smem_from;     // first level whose U / RES / RHS live in CTA 0's shared memory
+    bool pending;      // a step ran on CTA 0 alone since the last cluster barrier
+    double *mirror;    // this CTA's copy of a small level (interpolation onto a large level)
+    double *slot;      // this CTA's contribution to a cluster-wide maximum
+};
+struct MgStep {
+    int start, stride; // this thread's first cell index and the step between its cells
+    bool on;           // this CTA works on the step
+    bool wide;         // the step uses the whole cluster
+};
+__device__ __forceinline__ void mg_cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// generic address of the same shared-memory variable in CTA `rank` of the cluster
+__device__ __forceinline__ double *mg_map_rank(double *p, int rank) {
+    uint64_t out;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(p), "r"(rank));
+    return reinterpret_cast<double *>(out);
+}
+__device__ __forceinline__ bool mg_wide(const MgRun &r, const MgData &d, int m) {
+    return r.nct > 1 && (d.N >> m) >= r.wide_min;
+}
+// start of a step on level m: a large-level step first waits (cluster
+// barrier) for whatever CTA 0 did alone before it
+__device__ __forceinline__ MgStep mg_begin(MgRun &r, const MgData &d, int m) {
+    MgStep s;
+    s.wide = mg_wide(r, d, m);
+    if (s.wide) {
+        if (r.pending) {
+            mg_cluster_sync();
+            r.pending = false;
+        }
+        s.start = r.rank * (int)blockDim.x + (int)threadIdx.x;
+        s.stride = r.nct * (int)blockDim.x;
+        s.on = true;
+    } else {
+        r.pending = r.nct > 1;
+        s.start = (int)threadIdx.x;
+        s.stride = (int)blockDim.x;
+        s.on = r.rank == 0;
+    }
+    return s;
+}
+__device__ __forceinline__ void mg_end(const MgStep &s) {
+    if (s.wide) mg_cluster_sync();
+    else if (s.on) __syncthreads();
+}
+
 __device__ double mg_block_max(double v, double *sh) {
     for (int o = 16; o > 0; o >>= 1) {
         double t = __shfl_xor_sync(0xffffffffu, v, o);
@@ -49,6 +113,23 @@ __device__ double mg_block_max(double v, double *sh) {
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = sh[w] > m ? sh[w] : m;
     __syncthreads();
     return m;
+}
+
+// maximum over the CTA, and over the cluster when the step is a large-level
+// one (every CTA's value through distributed shared memory); all threads of
+// every working CTA get the result
+__device__ double mg_max(MgRun &r, double v, double *sh, bool wide) {
+    const double m = mg_block_max(v, sh);
+    if (!wide) return m;
+    if (threadIdx.x == 0) *r.slot = m;
+    mg_cluster_sync();
+    double g = 0.0;
+    for (int q = 0; q < r.nct; q++) {
+        const double t = *mg_map_rank(r.slot, q);
+        g = t > g ? t : g;
+    }
+    mg_cluster_sync();   // no CTA overwrites its slot while another may still read it
+    return g;
 }
 
 // (p, q) = (t mod G, t div G) for t < G^2 <= 130^2 without an integer
@@ -64,51 +145,57 @@ __device__ __forceinline__ void mg_pq(int t, int G, float rG, int &p, int &q) {
 // cell holds the interior cell at its periodic image (wrap each coordinate
 // -1 -> n-1, n -> 0).  That final state is written here in one pass:
 // cells on several faces are written with the same value more than once.
-__device__ void mg_boundary_u(const MgData &d, int m, double *a) {
+__device__ void mg_boundary_u(MgRun &r, const MgData &d, int m, double *a) {
     if (!d.periodic) return;
     const int n = mgN(d, m), G = n + 2;
     const float rG = 1.0f / (float)G;
     auto wrap = [n](int x) { return x < 0 ? n - 1 : (x >= n ? 0 : x); };
-    for (int t = threadIdx.x; t < 3 * G * G; t += blockDim.x) {
-        const int dir = t >= 2 * G * G ? 2 : (t >= G * G ? 1 : 0);
-        int p, q, i, j, k;
-        mg_pq(t - dir * G * G, G, rG, p, q);
-        put3(dir, -1, p - 1, q - 1, i, j, k);
-        a[cidx(G, i, j, k)] = a[cidx(G, wrap(i), wrap(j), wrap(k))];
-        put3(dir, n, p - 1, q - 1, i, j, k);
-        a[cidx(G, i, j, k)] = a[cidx(G, wrap(i), wrap(j), wrap(k))];
-    }
-    __syncthreads();
+    const MgStep s = mg_begin(r, d, m);
+    if (s.on)
+        for (int t = s.start; t < 3 * G * G; t += s.stride) {
+            const int dir = t >= 2 * G * G ? 2 : (t >= G * G ? 1 : 0);
+            int p, q, i, j, k;
+            mg_pq(t - dir * G * G, G, rG, p, q);
+            put3(dir, -1, p - 1, q - 1, i, j, k);
+            a[cidx(G, i, j, k)] = a[cidx(G, wrap(i), wrap(j), wrap(k))];
+            put3(dir, n, p - 1, q - 1, i, j, k);
+            a[cidx(G, i, j, k)] = a[cidx(G, wrap(i), wrap(j), wrap(k))];
+        }
+    mg_end(s);
 }
-__device__ void mg_boundary_fill0(const MgData &d, int m, double *a) {   // mg.F90:735-750
+__device__ void mg_boundary_fill0(MgRun &r, const MgData &d, int m, double *a) {   // mg.F90:735-750
     const int n = mgN(d, m), G = n + 2;
     const float rG = 1.0f / (float)G;
-    for (int f = 0; f < 6; f++) {
-        if (!d.touch[f]) continue;
-        for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
-            int i, j, k, p, q;
-            mg_pq(t, G, rG, p, q);
-            put3(f >> 1, (f & 1) ? n : -1, p - 1, q - 1, i, j, k);
-            a[cidx(G, i, j, k)] = 0.0;
+    const MgStep s = mg_begin(r, d, m);
+    if (s.on)
+        for (int f = 0; f < 6; f++) {
+            if (!d.touch[f]) continue;
+            for (int t = s.start; t < G * G; t += s.stride) {
+                int i, j, k, p, q;
+                mg_pq(t, G, rG, p, q);
+                put3(f >> 1, (f & 1) ? n : -1, p - 1, q - 1, i, j, k);
+                a[cidx(G, i, j, k)] = 0.0;
+            }
         }
-    }
-    __syncthreads();
+    mg_end(s);
 }
-__device__ void mg_boundary_extrap(const MgData &d, int m, double *a) {  // mg.F90:754-771
+__device__ void mg_boundary_extrap(MgRun &r, const MgData &d, int m, double *a) {  // mg.F90:754-771
     const int n = mgN(d, m), G = n + 2;
     const float rG = 1.0f / (float)G;
     for (int dir = 0; dir < 3; dir++) {
-        for (int lr = 0; lr < 2; lr++) {
-            if (!d.touch[lr + 2 * dir]) continue;
-            for (int t = threadIdx.x; t < G * G; t += blockDim.x) {
-                int i, j, k, ii, jj, kk, p, q;
-                mg_pq(t, G, rG, p, q);
-                put3(dir, lr ? n : -1, p - 1, q - 1, i, j, k);
-                put3(dir, lr ? n - 1 : 0, p - 1, q - 1, ii, jj, kk);
-                a[cidx(G, i, j, k)] = -a[cidx(G, ii, jj, kk)];
+        const MgStep s = mg_begin(r, d, m);
+        if (s.on)
+            for (int lr = 0; lr < 2; lr++) {
+                if (!d.touch[lr + 2 * dir]) continue;
+                for (int t = s.start; t < G * G; t += s.stride) {
+                    int i, j, k, ii, jj, kk, p, q;
+                    mg_pq(t, G, rG, p, q);
+                    put3(dir, lr ? n : -1, p - 1, q - 1, i, j, k);
+                    put3(dir, lr ? n - 1 : 0, p - 1, q - 1, ii, jj, kk);
+                    a[cidx(G, i, j, k)] = -a[cidx(G, ii, jj, kk)];
+                }
             }
-        }
-        __syncthreads();
+        mg_end(s);
     }
 }
 __device__ __forceinline__ double mg_lap_sum(const double *u, int G, int i, int j, int k) {
@@ -120,123 +207,150 @@ __device__ __forceinline__ double mg_lap_sum(const double *u, int G, int i, int 
     s = s - 6.0 * u[cidx(G, i, j, k)];
     return s;
 }
-__device__ void mg_resid(const MgData &d, int m, double *res, double *u, const double *rhs) {   // mg_poisson.F90:5-28
+__device__ void mg_resid(MgRun &r, const MgData &d, int m, double *res, double *u, const double *rhs) {   // mg_poisson.F90:5-28
     const int n = mgN(d, m), G = n + 2, ln = __ffs(n) - 1;
     double hh = mgH(d, m);
     double h2i = 1.0 / (hh * hh);
-    mg_boundary_u(d, m, u);
-    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-        int i, j, k;
-        mg_ijk(c, n, ln, i, j, k);
-        res[cidx(G, i, j, k)] = -h2i * mg_lap_sum(u, G, i, j, k) + rhs[cidx(G, i, j, k)];
-    }
-    __syncthreads();
+    mg_boundary_u(r, d, m, u);
+    const MgStep s = mg_begin(r, d, m);
+    if (s.on)
+        for (int c = s.start; c < n * n * n; c += s.stride) {
+            int i, j, k;
+            mg_ijk(c, n, ln, i, j, k);
+            res[cidx(G, i, j, k)] = -h2i * mg_lap_sum(u, G, i, j, k) + rhs[cidx(G, i, j, k)];
+        }
+    mg_end(s);
 }
 // both colours (mg_poisson.F90:32-79); returns this thread's max|resh2|:
-// Resmaxg = (max over the CTA) / h^2 is formed by the caller where it is
-// used (the max is exact, so where it is reduced does not change it)
-__device__ double mg_relax(const MgData &d, int m, double *u, const double *rhs) {
+// Resmaxg = (max over the CTA or cluster) / h^2 is formed by the caller where
+// it is used (the max is exact, so where it is reduced does not change it)
+__device__ double mg_relax(MgRun &r, const MgData &d, int m, double *u, const double *rhs) {
     const int n = mgN(d, m), G = n + 2;
     double hh = mgH(d, m), h2 = hh * hh, rm = 0.0;
     const int half = (n * n * n + 1) / 2;
-    (void)G;
     for (int ipass = 1; ipass <= 2; ipass++) {
-        mg_boundary_u(d, m, u);
-        for (int c = threadIdx.x; c < half; c += blockDim.x) {
-            int i2, j, k, i;
-            if (n == 1) { if (((ipass) & 1) != 0) continue; i = 0; j = 0; k = 0; }
-            else {
-                int hn = n / 2;
-                const int lhn = __ffs(hn) - 1;
-                i2 = c & (hn - 1); j = (c >> lhn) & (n - 1); k = c >> (lhn + __ffs(n) - 1);
-                i = 2 * i2 + ((j + k + ipass) & 1);
+        mg_boundary_u(r, d, m, u);
+        const MgStep s = mg_begin(r, d, m);
+        if (s.on)
+            for (int c = s.start; c < half; c += s.stride) {
+                int i2, j, k, i;
+                if (n == 1) { if (((ipass) & 1) != 0) continue; i = 0; j = 0; k = 0; }
+                else {
+                    int hn = n / 2;
+                    const int lhn = __ffs(hn) - 1;
+                    i2 = c & (hn - 1); j = (c >> lhn) & (n - 1); k = c >> (lhn + __ffs(n) - 1);
+                    i = 2 * i2 + ((j + k + ipass) & 1);
+                }
+                double resh2 = mg_lap_sum(u, G, i, j, k) - h2 * rhs[cidx(G, i, j, k)];
+                u[cidx(G, i, j, k)] = u[cidx(G, i, j, k)] + (1.0 / 6.0) * resh2;
+                double a = fabs(resh2);
+                rm = a > rm ? a : rm;
             }
-            double resh2 = mg_lap_sum(u, G, i, j, k) - h2 * rhs[cidx(G, i, j, k)];
-            u[cidx(G, i, j, k)] = u[cidx(G, i, j, k)] + (1.0 / 6.0) * resh2;
-            double a = fabs(resh2);
-            rm = a > rm ? a : rm;
-        }
-        __syncthreads();
+        mg_end(s);
     }
     return rm;
 }
-__device__ void mg_rstrct(const MgData &d, int m, double *uc, const double *uf) {   // linear (mg.F90:581-602)
+__device__ void mg_rstrct(MgRun &r, const MgData &d, int m, double *uc, const double *uf) {   // linear (mg.F90:581-602)
     const int n = mgN(d, m), G = n + 2, Gf = 2 * n + 2, ln = __ffs(n) - 1;
-    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-        int i, j, k;
-        mg_ijk(c, n, ln, i, j, k);
-        uc[cidx(G, i, j, k)] = rstrct_linear(uf, Gf, 2 * i, 2 * j, 2 * k);
-    }
-    __syncthreads();
+    const MgStep s = mg_begin(r, d, m);
+    if (s.on)
+        for (int c = s.start; c < n * n * n; c += s.stride) {
+            int i, j, k;
+            mg_ijk(c, n, ln, i, j, k);
+            uc[cidx(G, i, j, k)] = rstrct_linear(uf, Gf, 2 * i, 2 * j, 2 * k);
+        }
+    mg_end(s);
 }
-__device__ void mg_interp(const MgData &d, int m, double *uf, double *uc, bool cubic) {   // mg.F90:608-633
+__device__ void mg_interp(MgRun &r, const MgData &d, int m, double *uf, double *uc, bool cubic) {   // mg.F90:608-633
     const int lc = m + 1, n = mgN(d, m), G = n + 2, nc = mgN(d, lc), Gc = nc + 2, ln = __ffs(n) - 1;
     // Lagrange nodes and weights per fine index, evaluated once per call
     __shared__ int tcw[MG_NMAX][4];
     __shared__ double tww[MG_NMAX][4];
     const bool tri = cubic && nc + 2 >= 4;
-    if (tri && (int)threadIdx.x < n) cubic_weights((int)threadIdx.x, -1, nc, tcw[threadIdx.x], tww[threadIdx.x]);
-    mg_boundary_extrap(d, lc, uc);   // ends with __syncthreads
-    mg_boundary_u(d, lc, uc);
-    for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-        int i, j, k;
-        mg_ijk(c, n, ln, i, j, k);
-        uf[cidx(G, i, j, k)] = tri ? tricubic_cell_w(uc, Gc, tcw[i], tww[i], tcw[j], tww[j], tcw[k], tww[k])
-                                   : trilinear_cell(uc, Gc, i, j, k, 0, 0, 0);
+    mg_boundary_extrap(r, d, lc, uc);
+    mg_boundary_u(r, d, lc, uc);
+    {
+        const MgStep s = mg_begin(r, d, m);
+        if (s.on) {
+            if (tri && (int)threadIdx.x < n) cubic_weights((int)threadIdx.x, -1, nc, tcw[threadIdx.x], tww[threadIdx.x]);
+            // a small coarse level kept in CTA 0's shared memory, read by every
+            // CTA of a large-level step: each CTA copies it first
+            const double *src = uc;
+            if (s.wide && !mg_wide(r, d, lc) && lc >= r.smem_from) {
+                const double *c0 = mg_map_rank(uc, 0);
+                for (int t = threadIdx.x; t < Gc * Gc * Gc; t += blockDim.x) r.mirror[t] = c0[t];
+                src = r.mirror;
+            }
+            __syncthreads();
+            for (int c = s.start; c < n * n * n; c += s.stride) {
+                int i, j, k;
+                mg_ijk(c, n, ln, i, j, k);
+                uf[cidx(G, i, j, k)] = tri ? tricubic_cell_w(src, Gc, tcw[i], tww[i], tcw[j], tww[j], tcw[k], tww[k])
+                                           : trilinear_cell(src, Gc, i, j, k, 0, 0, 0);
+            }
+        }
+        mg_end(s);
     }
-    __syncthreads();
-    mg_boundary_fill0(d, m, uf);
-    mg_boundary_fill0(d, lc, uc);
-    mg_boundary_u(d, m, uf);
-    mg_boundary_u(d, lc, uc);
+    mg_boundary_fill0(r, d, m, uf);
+    mg_boundary_fill0(r, d, lc, uc);
+    mg_boundary_u(r, d, m, uf);
+    mg_boundary_u(r, d, lc, uc);
 }
-__device__ void mg_fill0(const MgData &d, int m, double *a) {
+__device__ void mg_fill0(MgRun &r, const MgData &d, int m, double *a) {
     const int G = mgN(d, m) + 2;
-    for (int c = threadIdx.x; c < G * G * G; c += blockDim.x) a[c] = 0.0;
-    __syncthreads();
+    const MgStep s = mg_begin(r, d, m);
+    if (s.on)
+        for (int c = s.start; c < G * G * G; c += s.stride) a[c] = 0.0;
+    mg_end(s);
 }
-__device__ void mg_copy(const MgData &d, int m, double *o, const double *a) {
+__device__ void mg_copy(MgRun &r, const MgData &d, int m, double *o, const double *a) {
     const int G = mgN(d, m) + 2;
-    for (int c = threadIdx.x; c < G * G * G; c += blockDim.x) o[c] = a[c];
-    __syncthreads();
+    const MgStep s = mg_begin(r, d, m);
+    if (s.on)
+        for (int c = s.start; c < G * G * G; c += s.stride) o[c] = a[c];
+    mg_end(s);
 }
-__device__ void mg_addw(const MgData &d, int m, double *a, const double *da) {
+__device__ void mg_addw(MgRun &r, const MgData &d, int m, double *a, const double *da) {
     const int G = mgN(d, m) + 2;
-    for (int c = threadIdx.x; c < G * G * G; c += blockDim.x) a[c] = a[c] + da[c];
-    __syncthreads();
+    const MgStep s = mg_begin(r, d, m);
+    if (s.on)
+        for (int c = s.start; c < G * G * G; c += s.stride) a[c] = a[c] + da[c];
+    mg_end(s);
 }
 
 // mg_lin (mg.F90:106-218); returns the last Resmaxg (the Resmaxg of every
 // earlier mg_relax is overwritten unread, so only the last one is reduced)
-__device__ double mg_lin(const MgData &d, double *sh) {
+__device__ double mg_lin(MgRun &r, const MgData &d, double *sh) {
     double rm = 0.0;   // this thread's max|resh2| of the last mg_relax
     int mr = d.MMax;   // its level
-    for (int m = 1; m <= d.MMax; m++) mg_rstrct(d, m, d.RHO[m], d.RHO[m - 1]);
-    mg_fill0(d, d.MMax, d.U[d.MMax]);
-    for (int q = 0; q < 2; q++) rm = mg_relax(d, d.MMax, d.U[d.MMax], d.RHO[d.MMax]);
+    for (int m = 1; m <= d.MMax; m++) mg_rstrct(r, d, m, d.RHO[m], d.RHO[m - 1]);
+    mg_fill0(r, d, d.MMax, d.U[d.MMax]);
+    for (int q = 0; q < 2; q++) rm = mg_relax(r, d, d.MMax, d.U[d.MMax], d.RHO[d.MMax]);
     for (int m = d.MMax - 1; m >= 0; m--) {
-        mg_interp(d, m, d.U[m], d.U[m + 1], true);
-        mg_copy(d, m, d.RHS[m], d.RHO[m]);
+        mg_interp(r, d, m, d.U[m], d.U[m + 1], true);
+        mg_copy(r, d, m, d.RHS[m], d.RHO[m]);
         for (int jc = 1; jc <= 2; jc++) {
             for (int v = m; v <= d.MMax - 1; v++) {
-                for (int q = 0; q < 2; q++) rm = mg_relax(d, v, d.U[v], d.RHS[v]);
+                for (int q = 0; q < 2; q++) rm = mg_relax(r, d, v, d.U[v], d.RHS[v]);
                 mr = v;
-                mg_resid(d, v, d.RES[v], d.U[v], d.RHS[v]);
-                mg_rstrct(d, v + 1, d.RHS[v + 1], d.RES[v]);
-                mg_fill0(d, v + 1, d.U[v + 1]);
+                mg_resid(r, d, v, d.RES[v], d.U[v], d.RHS[v]);
+                mg_rstrct(r, d, v + 1, d.RHS[v + 1], d.RES[v]);
+                mg_fill0(r, d, v + 1, d.U[v + 1]);
             }
-            for (int q = 0; q < 2; q++) rm = mg_relax(d, d.MMax, d.U[d.MMax], d.RHS[d.MMax]);
+            for (int q = 0; q < 2; q++) rm = mg_relax(r, d, d.MMax, d.U[d.MMax], d.RHS[d.MMax]);
             mr = d.MMax;
             for (int v = d.MMax - 1; v >= m; v--) {
-                mg_interp(d, v, d.RES[v], d.U[v + 1], false);
-                mg_addw(d, v, d.U[v], d.RES[v]);
-                for (int q = 0; q < 2; q++) rm = mg_relax(d, v, d.U[v], d.RHS[v]);
+                mg_interp(r, d, v, d.RES[v], d.U[v + 1], false);
+                mg_addw(r, d, v, d.U[v], d.RES[v]);
+                for (int q = 0; q < 2; q++) rm = mg_relax(r, d, v, d.U[v], d.RHS[v]);
                 mr = v;
             }
         }
     }
     const double hh = mgH(d, mr);
-    return mg_block_max(rm, sh) / (hh * hh);
+    // the last relaxation is on level 0 (m = 0 ends the FMG), a large level
+    // in cluster mode: every CTA takes part and gets the cluster's maximum
+    return mg_max(r, rm, sh, mg_wide(r, d, mr)) / (hh * hh);
 }
 
 // dynamic shared memory of the base-grid CTA
@@ -265,12 +379,41 @@ __host__ __device__ inline int mg_smem_from(int N, int MMax, size_t budget_doubl
     return from;
 }
 
-// mg_cycle (mg.F90:42-94) with ju = PSI, jrho = SRC; one CTA
-// (nmax: cap on the defect corrections, 10 in the reference)
-__global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, int *iters_out, int nmax) {
+// cluster special registers (an ordinary launch is a cluster of one CTA)
+__device__ __forceinline__ int mg_cluster_rank() {
+    int v;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(v));
+    return v;
+}
+__device__ __forceinline__ int mg_cluster_size() {
+    int v;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(v));
+    return v;
+}
+
+// mg_cycle (mg.F90:42-94) with ju = PSI, jrho = SRC, on one CTA or on a
+// cluster (launched with a cluster dimension; smem_from must then be above
+// every level of at least wide_min cells per edge).  nmax: cap on the
+// defect corrections, 10 in the reference.  Dynamic shared memory: the
+// U / RES / RHS of levels >= smem_from, then `mirror_doubles` for the copy of
+// a small level onto a large one (cluster mode only).
+__global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, int *iters_out, int nmax, int wide_min,
+                                                     int mirror_doubles) {
     pdl_enter();
     __shared__ double sh[32];
+    __shared__ double slot;
     MgData d = dg;
+    MgRun r;
+    r.rank = mg_cluster_rank();
+    r.nct = mg_cluster_size();
+    r.wide_min = wide_min;
+    r.smem_from = smem_from;
+    r.pending = false;
+    r.slot = &slot;
+    if (r.nct > 1 && d.N < wide_min) {   // no large level: CTA 0 alone, before any cluster barrier
+        if (r.rank != 0) return;
+        r.nct = 1;
+    }
     {
         double *p = mg_dyn_smem();
         for (int m = d.MMax; m >= smem_from; m--) {
@@ -279,34 +422,40 @@ __global__ void __launch_bounds__(512, 1) k_mg_cycle(MgData dg, int smem_from, i
             d.RES[m] = p; p += V;
             d.RHS[m] = p; p += V;
         }
+        r.mirror = p;
+        p += mirror_doubles;
         const int64_t tot = p - mg_dyn_smem();
         double *z = mg_dyn_smem();
         for (int64_t t = threadIdx.x; t < tot; t += blockDim.x) z[t] = 0.0;
         __syncthreads();
     }
+    if (r.nct > 1) mg_cluster_sync();   // every CTA has started before any reads another's shared memory
     const double errmax = (double)1.e-2f;   // default-real literal (mg.F90:50)
-    mg_boundary_fill0(d, 0, d.PSI);
-    mg_boundary_u(d, 0, d.PSI);
+    mg_boundary_fill0(r, d, 0, d.PSI);
+    mg_boundary_u(r, d, 0, d.PSI);
     double rhomax = 0.0;
     int it;
     for (it = 1; it <= nmax; it++) {
-        mg_resid(d, 0, d.RHO[0], d.PSI, d.SRC);
+        mg_resid(r, d, 0, d.RHO[0], d.PSI, d.SRC);
         if (it == 1) {
             const int n = d.N, G = n + 2;
+            const MgStep s = mg_begin(r, d, 0);
             double v = 0.0;
-            for (int c = threadIdx.x; c < n * n * n; c += blockDim.x) {
-                int i, j, k;
-                mg_ijk(c, n, __ffs(n) - 1, i, j, k);
-                double a = fabs(d.RHO[0][cidx(G, i, j, k)]);
-                v = a > v ? a : v;
-            }
-            rhomax = mg_block_max(v, sh);
+            if (s.on)
+                for (int c = s.start; c < n * n * n; c += s.stride) {
+                    int i, j, k;
+                    mg_ijk(c, n, __ffs(n) - 1, i, j, k);
+                    double a = fabs(d.RHO[0][cidx(G, i, j, k)]);
+                    v = a > v ? a : v;
+                }
+            rhomax = mg_max(r, v, sh, s.wide);
         }
-        double res = mg_lin(d, sh);
-        mg_addw(d, 0, d.PSI, d.U[0]);
+        double res = mg_lin(r, d, sh);
+        mg_addw(r, d, 0, d.PSI, d.U[0]);
         if (res / rhomax < errmax) break;
     }
-    if (threadIdx.x == 0 && iters_out) *iters_out = it > nmax ? nmax : it;
+    if (r.nct > 1) mg_cluster_sync();   // no CTA leaves while another may still read its shared memory
+    if (threadIdx.x == 0 && r.rank == 0 && iters_out) *iters_out = it > nmax ? nmax : it;
 }
 
 }  // namespace sfm

@@ -84,6 +84,15 @@ __global__ void __launch_bounds__(1024) k_mg_uniform_noalloc(MgData d, const dou
     __shared__ double sh[32];
     __shared__ double wsum[32];
     const int n = d.N, G = n + 2, n3 = n * n * n;
+    // one CTA, every level in the scratch array (global memory)
+    MgRun r;
+    r.rank = 0;
+    r.nct = 1;
+    r.wide_min = 1 << 30;
+    r.smem_from = d.MMax + 1;
+    r.pending = false;
+    r.mirror = nullptr;
+    r.slot = nullptr;
     // every array read below starts at zero (U, RES, RHS, RHO of all levels, SRC, PSI)
     for (int64_t t = threadIdx.x; t < clear_doubles; t += blockDim.x) d.U[0][t] = 0.0;
     // A NaN or Inf density would make the mean and every source value NaN;
@@ -121,7 +130,7 @@ __global__ void __launch_bounds__(1024) k_mg_uniform_noalloc(MgData d, const dou
     int it = 0;
     double rrel = 0.0;
     for (;;) {
-        mg_resid(d, 0, d.RHO[0], d.PSI, d.SRC);
+        mg_resid(r, d, 0, d.RHO[0], d.PSI, d.SRC);
         double v = 0.0;
         for (int c = threadIdx.x; c < n3; c += blockDim.x) {
             const double a = fabs(d.RHO[0][cidx(G, c % n, (c / n) % n, c / (n * n))]);
@@ -130,8 +139,8 @@ __global__ void __launch_bounds__(1024) k_mg_uniform_noalloc(MgData d, const dou
         const double rmax = mg_block_max(v, sh);
         rrel = smax > 0.0 ? rmax / smax : 0.0;
         if (rrel <= rel_tol || it >= max_cycles) break;
-        mg_lin(d, sh);
-        mg_addw(d, 0, d.PSI, d.U[0]);
+        mg_lin(r, d, sh);
+        mg_addw(r, d, 0, d.PSI, d.U[0]);
         it++;
     }
     for (int c = threadIdx.x; c < n3; c += blockDim.x) psi[c] = d.PSI[cidx(G, c % n, (c / n) % n, c / (n * n))];

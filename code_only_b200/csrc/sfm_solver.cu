@@ -291,6 +291,94 @@ public:
     MgData mg;
     int mgSmemFrom = 0;
     size_t mgSmemBytes = 0;
+    bool mgSmemOk = true;   // the opt-in to large dynamic shared memory succeeded
+    bool mgFits[5][3] = {}; // a cluster of 2 << a CTAs with wide threshold 16 << b can be resident
+    bool mg_fits(int nct, int wide) const {
+        int a = -1, b = -1;
+        for (int q = 0; q < 5; q++) if ((2 << q) == nct) a = q;
+        for (int q = 0; q < 3; q++) if ((16 << q) == wide) b = q;
+        return a >= 0 && b >= 0 && mgFits[a][b];
+    }
+    // Shared-memory plan of the base-grid launch.  wide = 0: one CTA, the
+    // coarse levels that fit 200 KB in shared memory (never level 0).  wide > 0:
+    // a cluster whose levels of at least `wide` cells per edge stay in global
+    // memory, the smaller ones in CTA 0's shared memory as far as they fit,
+    // plus every CTA's copy of the first small level when it is in shared
+    // memory (it is interpolated onto a large level).
+    struct MgPlan { int from; size_t bytes; int mirror; };
+    MgPlan mg_plan(int wide) const {
+        MgPlan pl{mg.MMax + 1, 0, 0};
+        if (!mgSmemOk) return pl;
+        size_t used = 0;
+        int from = mg_smem_from(mg.N, mg.MMax, (size_t)200 * 1024 / sizeof(double), &used);
+        int firstSmall = 0;
+        if (wide > 0) {
+            while (firstSmall <= mg.MMax && (mg.N >> firstSmall) >= wide) firstSmall++;
+            if (from < firstSmall) {   // large levels stay in global memory
+                from = firstSmall;
+                used = 0;
+                for (int m = from; m <= mg.MMax; m++) {
+                    const size_t G = (size_t)(mg.N >> m) + 2;
+                    used += 3 * G * G * G;
+                }
+            }
+            if (firstSmall <= mg.MMax && firstSmall >= from) {
+                const size_t G = (size_t)(mg.N >> firstSmall) + 2;
+                pl.mirror = (int)(G * G * G);
+            }
+        }
+        pl.from = from;
+        pl.bytes = (used + (size_t)pl.mirror) * sizeof(double);
+        return pl;
+    }
+    // the base-grid launch: one CTA, or a cluster of nct CTAs whose levels
+    // of at least `wide` cells per edge use every CTA (level 0 must be one)
+    void mg_launch(int nct, int wide) {
+        const int nmax = sched(kKnobBaseCorr, 10);
+        if (nct <= 1 || mg.N < wide || !mg_fits(nct, wide)) {
+            launch_pdl(k_mg_cycle, 1, 512, mgSmemBytes, mg, mgSmemFrom, d_mgit, nmax, 1 << 30, 0);
+            ++launches;
+            return;
+        }
+        const MgPlan pl = mg_plan(wide);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nct);
+        cfg.blockDim = dim3(512);
+        cfg.dynamicSmemBytes = pl.bytes;
+        cfg.stream = st_;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = nct;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 2;
+        cudaLaunchKernelEx(&cfg, k_mg_cycle, mg, pl.from, d_mgit, nmax, wide, pl.mirror);
+        ++launches;
+    }
+    // whether a cluster of nct CTAs with this plan can be resident
+    bool mg_cluster_fits(int nct, int wide) {
+        const MgPlan pl = mg_plan(wide);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nct);
+        cfg.blockDim = dim3(512);
+        cfg.dynamicSmemBytes = pl.bytes;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = nct;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void *)k_mg_cycle, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return n >= 1;
+    }
     bool useSerialMg = false;
     int NBc = 0;
     std::vector<std::pair<void *, size_t>> zeroList;   // re-zeroed at every solve
@@ -516,6 +604,30 @@ public:
                 }
                 tune.set(kKnobResidBpc, 8, 8, -1, -1, pick);
             }
+        }
+        // base-grid launch: one CTA or a cluster (same cells, same expressions)
+        if (useSerialMg) {
+            struct Cand { int nct, wide; };
+            std::vector<Cand> cands = {{1, 16}};
+            for (int nct : {2, 4, 8, 16})
+                for (int w : {16, 32, 64})
+                    if (NBc >= w && mg_fits(nct, w)) cands.push_back({nct, w});
+            float best = std::numeric_limits<float>::max();
+            Cand pick = {1, 16};
+            for (const Cand &c : cands) {
+                mg_launch(c.nct, c.wide);   // a launch the driver refuses is skipped
+                if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st_) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                const float t = time_min([&] { mg_launch(c.nct, c.wide); }, reps);
+                if (t < best) {
+                    best = t;
+                    pick = c;
+                }
+            }
+            tune.set(kKnobBaseCtas, (int)sizeof(T), NBc, -1, -1, pick.nct);
+            tune.set(kKnobBaseWide, (int)sizeof(T), NBc, -1, -1, pick.wide);
         }
         FmgLevel_fill0 = Undef;
         if (iterExec) {   // the graph holds the old launch shapes
@@ -790,16 +902,24 @@ public:
                 mg.RHS[m] = mem.alloc<double>(V); mg.RHO[m] = mem.alloc<double>(V);
                 for (double *q : {mg.U[m], mg.RES[m], mg.RHS[m], mg.RHO[m]}) zeroList.push_back({q, V * sizeof(double)});
             }
-            size_t used = 0;
-            mgSmemFrom = mg_smem_from(NBc, MMax, (size_t)200 * 1024 / sizeof(double), &used);
-            mgSmemBytes = used * sizeof(double);
-            if (mgSmemBytes > 0 &&   // opt in whatever the size: static + dynamic may pass 48 KB
-                cudaFuncSetAttribute(k_mg_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mgSmemBytes) !=
-                    cudaSuccess) {
+            // shared-memory plans of the one-CTA launch and of the cluster
+            // launches (one per wide threshold); opt in to the largest,
+            // whatever the size: static and dynamic together may pass 48 KB
+            size_t most = 0;
+            for (int w : {0, 16, 32, 64}) most = std::max(most, mg_plan(w).bytes);
+            bool optin = cudaFuncSetAttribute(k_mg_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most) ==
+                         cudaSuccess;
+            if (!optin) cudaGetLastError();
+            mgSmemOk = optin;
+            if (cudaFuncSetAttribute(k_mg_cycle, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
                 cudaGetLastError();
-                mgSmemFrom = MMax + 1;   // no opt-in: all levels in global memory
-                mgSmemBytes = 0;
-            }
+            const MgPlan one = mg_plan(0);
+            mgSmemFrom = one.from;
+            mgSmemBytes = one.bytes;
+            // which cluster shapes can be resident, asked once here (outside
+            // any stream capture); a table may only pick among these
+            for (int a = 0; a < 5; a++)
+                for (int b = 0; b < 3; b++) mgFits[a][b] = mg_cluster_fits(2 << a, 16 << b);
             size_t G0 = (size_t)NBc + 2, V0 = G0 * G0 * G0;
             mg.SRC = mem.alloc<double>(V0); mg.PSI = mem.alloc<double>(V0);
             zeroList.push_back({mg.SRC, V0 * sizeof(double)});
@@ -1285,8 +1405,8 @@ public:
         const int F = H.FMax;
         int64_t N3 = (int64_t)NBc * NBc * NBc;
         run(OpMgGather<T>{mg.SRC, mg.PSI, rhs, u, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
-        launch_pdl(k_mg_cycle, 1, 512, mgSmemBytes, mg, mgSmemFrom, d_mgit, sched(kKnobBaseCorr, 10));
-        ++launches;
+        mg_launch(tune.get(kKnobBaseCtas, (int)sizeof(T), NBc, -1, -1, 1),
+                  tune.get(kKnobBaseWide, (int)sizeof(T), NBc, -1, -1, 16));
         run(OpMgScatter<T>{u, mg.PSI, d_baseIdx, H.ngb[0], H.ngb[1], nf[F], Gf[F], NBc, Vf[F]}, N3);
     }
     // vmg_fas (vmg.F90:116-243); jrho = IRHS when copy_rhs (second and later calls)

@@ -14,6 +14,11 @@
 //                 key: element size, block edge n
 //   resid_bpc     blocks per CTA of the tiled residual (1, 2 or 4);
 //                 key: element size, block edge n
+//   base_ctas     CTAs of the base-grid multigrid launch: 1, or a cluster
+//                 of 2, 4, 8 or 16 (sfm_mg.cuh); key: element size, base
+//                 grid cells per edge
+//   base_wide     with a cluster, the smallest level (cells per edge: 16,
+//                 32 or 64) whose steps use every CTA; same key
 // and, for the mixed-precision path only (element size 4), the schedule of
 // the FP32 inner solve, which is a preconditioner inside the FP64 defect
 // correction: the outer loop converges to the same potential whatever the
@@ -43,7 +48,8 @@ namespace sfm {
 
 enum TuneKnob {
     kKnobGhostFill = 0, kKnobRelaxThreads = 1, kKnobResidBpc = 2,
-    kKnobFmgCycles = 3, kKnobFmgSweeps = 4, kKnobVmgSweeps = 5, kKnobBaseCorr = 6, kKnobCount = 7
+    kKnobFmgCycles = 3, kKnobFmgSweeps = 4, kKnobVmgSweeps = 5, kKnobBaseCorr = 6,
+    kKnobBaseCtas = 7, kKnobBaseWide = 8, kKnobCount = 9
 };
 inline const char *tune_knob_name(int k) {
     switch (k) {
@@ -54,6 +60,8 @@ inline const char *tune_knob_name(int k) {
         case kKnobFmgSweeps: return "fmg_sweeps";
         case kKnobVmgSweeps: return "vmg_sweeps";
         case kKnobBaseCorr: return "base_corrections";
+        case kKnobBaseCtas: return "base_ctas";
+        case kKnobBaseWide: return "base_wide";
         default: return nullptr;
     }
 }
@@ -66,6 +74,8 @@ inline bool tune_choice_ok(int knob, int v) {
         case kKnobFmgSweeps: return v >= 1 && v <= 3;
         case kKnobVmgSweeps: return v >= 1 && v <= 3;
         case kKnobBaseCorr: return v >= 1 && v <= 10;
+        case kKnobBaseCtas: return v == 1 || v == 2 || v == 4 || v == 8 || v == 16;
+        case kKnobBaseWide: return v == 16 || v == 32 || v == 64;
         default: return false;
     }
 }

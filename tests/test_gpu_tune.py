@@ -95,3 +95,45 @@ def test_fp64_context_keeps_the_reference_schedule():
         psi2, _, _ = s.solve(rho)
     _, psi1, _, _, _ = oracle_solve(h, rho, p)
     assert np.array_equal(psi2[:, 1:-1, 1:-1, 1:-1], psi1[:, 1:-1, 1:-1, 1:-1])
+
+
+BASE_CASES = {
+    "uniform128": (lambda: w.uniform_periodic(16, 8), 32),   # 32^3 base grid
+    "amr_base16": (lambda: w.small_periodic(16, 8, 2, 3), 32),
+    "uniform64": (lambda: w.uniform_periodic(8, 8), 16),     # 16^3 base grid
+}
+
+
+@pytest.mark.parametrize("nct,wide", [(2, 16), (4, 16), (8, 16), (8, 32), (16, 16), (4, 32)])
+@pytest.mark.parametrize("name", list(BASE_CASES))
+def test_base_grid_cluster_is_bitwise(name, nct, wide):
+    """The base-grid multigrid as a cluster of CTAs (the large levels spread
+    over every CTA, the small ones on CTA 0, the maxima over the cluster)
+    computes every cell with the same expression: the FP64 solve stays
+    bit-identical to the oracle whatever the shape.  A shape the GPU cannot
+    hold resident falls back to one CTA, which must match as well."""
+    mk, nbase = BASE_CASES[name]
+    h = mk()
+    p = abi.default_params(abi.SFM_BC_PERIODIC, rel_tol=1e-10, max_outer=30)
+    rho = w.block_field(h, p.ngh_io, w.gaussian_peak)
+    _, psi_o, g_o, st_o, _ = oracle_solve(h, rho, p)
+    with FMGPoisson(h, params=p) as s:
+        s.load_tune_table(f"base_ctas 8 {nbase} -1 -1 {nct}\nbase_wide 8 {nbase} -1 -1 {wide}\n")
+        psi, g, st = s.solve(rho)
+        psi2, g2, _ = s.solve(rho)                       # the graph replayed
+    assert st.outer_iters == st_o.outer_iters
+    assert np.array_equal(psi[:, 1:-1, 1:-1, 1:-1], psi_o[:, 1:-1, 1:-1, 1:-1])
+    n = h.ni
+    assert np.array_equal(g[:, :, 2:2 + n, 2:2 + n, 2:2 + n], g_o[:, :, 2:2 + n, 2:2 + n, 2:2 + n])
+    assert np.array_equal(psi, psi2) and np.array_equal(g, g2)
+
+
+def test_autotuned_base_grid_choice_is_recorded():
+    mk, nbase = BASE_CASES["uniform128"]
+    h = mk()
+    p = abi.default_params(abi.SFM_BC_PERIODIC, rel_tol=1e-10, max_outer=30)
+    with FMGPoisson(h, params=p) as s:
+        s.autotune(2)
+        lines = s.tune_table().splitlines()
+    assert any(ln.startswith(f"base_ctas 8 {nbase} ") for ln in lines)
+    assert any(ln.startswith(f"base_wide 8 {nbase} ") for ln in lines)

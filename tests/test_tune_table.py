@@ -53,6 +53,8 @@ def test_later_entry_wins_and_empty_table(lib):
     "ghost_fill 4 8 2 -1",            # missing field
     "ghost_fill 4 8 2 -1 1 7",        # extra field
     "ghost_fill four 8 2 -1 1",
+    "base_ctas 8 32 -1 -1 3",          # not a cluster size offered
+    "base_wide 8 32 -1 -1 8",
 ])
 def test_malformed_entries_are_rejected(lib, bad):
     assert check(lib, "ghost_fill 4 8 0 -1 1\n" + bad + "\n")[0] == abi.SFM_EINVAL
@@ -61,3 +63,8 @@ def test_malformed_entries_are_rejected(lib, bad):
 def test_small_output_buffer(lib):
     rc, _ = check(lib, "ghost_fill 4 8 0 -1 1\n", cap=8)
     assert rc == abi.SFM_ESIZE
+
+
+def test_base_grid_knobs_parse(lib):
+    rc, out = check(lib, "base_ctas 8 32 -1 -1 8\nbase_wide 8 32 -1 -1 16\nbase_ctas 4 16 -1 -1 1\n")
+    assert rc == 3 and "base_ctas 8 32 -1 -1 8" in out and "base_wide 8 32 -1 -1 16" in out
