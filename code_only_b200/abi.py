@@ -66,7 +66,7 @@ class SfmStats(C.Structure):
         ("ratio", C.c_double * SFM_MAX_HISTORY), ("true_rel_residual", C.c_double),
         ("rho_mean", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64),
         ("smoother_ms", C.c_double), ("smoother_launches", C.c_int64), ("smoother_cells", C.c_int64),
-        ("elem_bytes", C.c_int32),
+        ("elem_bytes", C.c_int32), ("smoother_colours", C.c_int32),
     ]
 
     def history(self):

@@ -778,7 +778,18 @@ __host__ __device__ constexpr int relax_bulk_min_ctas() {
 // (the default; the autotuner may choose the other count per block edge)
 template <int N>
 __host__ __device__ constexpr int relax_bulk_threads() { return N >= 16 ? 512 : 256; }
-template <class T, int N, int NT = relax_bulk_threads<N>()>
+//
+// FUSED (a choice of the mixed path's schedule, never of the FP64 path):
+// both colours of every staged block in one pass -- the first colour's new
+// values go to u and back into the stage, the consumer warps meet at a named
+// barrier, and the second colour reads them there, with the block's ghost
+// cells and reflux fluxes as they were before the sweep (the reference
+// refreshes them between the colours, fmg_poisson.F90:160-165).  u and rhs
+// are read once and u written once per full sweep.  A consumer's failed
+// stage wait is recorded before the first barrier of the tile and every
+// consumer warp leaves after it, so none waits at the barrier for one that
+// has gone.
+template <class T, int N, int NT = relax_bulk_threads<N>(), bool FUSED = false>
 __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
     k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
                                                     const int32_t *__restrict__ blocks, int nblk,
@@ -887,32 +898,54 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
         const int ct = tid - 32;   // consumer thread 0..NCT-1
         T mt = (T)0;               // max |resh2| (exact in T; widened once)
         int it = 0;
+        auto consumers_sync = [] { asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory"); };
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
-            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), cpolls))) {
-                if (lane == 0) atomicExch(&cab, 1);
-                break;
+            const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), cpolls));
+            if constexpr (FUSED) {
+                if (!got && lane == 0) atomicExch(&cab, 1);
+                consumers_sync();
+                if (*(volatile int *)&cab) break;   // the same decision in every consumer warp
+            } else {
+                if (!got) {
+                    if (lane == 0) atomicExch(&cab, 1);
+                    break;
+                }
             }
             const int first = tile * BPC;
             const int slot = it % (2 * R);
-            const T *ut = ust + s * BPC * V;
+            T *ut = ust + s * BPC * V;
             const T *rt = rst + s * BPC * V;
-            for (int t = ct; t < BPC * HALF; t += NCT) {
-                const int q = t / HALF, r = t - q * HALF;
-                if (first + q >= nblk) continue;
-                constexpr int HN = N / 2;
-                const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
-                const int i = 2 * i2 + ((j + k + ipass) & 1);
-                const T hh = shh[slot][q], hi = shi[slot][q];
-                const T *ub = ut + q * V;
-                // blocks without a reflux face (a warp's cells share a block)
-                // skip the per-face slot tests: same fluxes, fewer instructions
-                TileFlux<T, N> F{ub, hi, hasr[slot][q] ? ssl[slot][q] : nullptr, rbuf};
-                const int c = cidx(G, i, j, k);
-                const T resh2 = (F.div(i, j, k) - rt[q * V + c] * hh) * hh;
-                u[(int64_t)bid[slot][q] * V + c] = ub[c] + (T)(1.0 / 6.0) * resh2;
-                const T a = resh2 < (T)0 ? -resh2 : resh2;
-                mt = a > mt ? a : mt;
+            auto colour = [&](int pass) {
+                for (int t = ct; t < BPC * HALF; t += NCT) {
+                    const int q = t / HALF, r = t - q * HALF;
+                    if (first + q >= nblk) continue;
+                    constexpr int HN = N / 2;
+                    const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
+                    const int i = 2 * i2 + ((j + k + pass) & 1);
+                    const T hh = shh[slot][q], hi = shi[slot][q];
+                    T *ub = ut + q * V;
+                    // blocks without a reflux face (a warp's cells share a block)
+                    // skip the per-face slot tests: same fluxes, fewer instructions
+                    TileFlux<T, N> F{ub, hi, hasr[slot][q] ? ssl[slot][q] : nullptr, rbuf};
+                    const int c = cidx(G, i, j, k);
+                    const T resh2 = (F.div(i, j, k) - rt[q * V + c] * hh) * hh;
+                    const T v = ub[c] + (T)(1.0 / 6.0) * resh2;
+                    u[(int64_t)bid[slot][q] * V + c] = v;
+                    if (FUSED && pass == 1) ub[c] = v;   // read by the second colour
+                    const T a = resh2 < (T)0 ? -resh2 : resh2;
+                    mt = a > mt ? a : mt;
+                }
+            };
+            if constexpr (FUSED) {
+                colour(1);
+                consumers_sync();
+                colour(2);
+                // the stage held ordinary stores; the next bulk copy into it
+                // goes through the async proxy
+                fence_async_shared();
+            } else {
+                colour(ipass);
             }
             __syncwarp();
             if (lane == 0) {

@@ -284,7 +284,7 @@ public:
     int *d_err = nullptr;                  // set by a device wait that gave up
     uint32_t waitPolls = kWaitPolls;       // poll limit of the smoother's stage waits (tests lower it)
     int nSM = 148;
-    int bulkGrid[5][2] = {};               // persistent CTAs of k_relax_bulk<T, N, NT>, by log2(N) and NT / 512
+    int bulkGrid[5][2][2] = {};            // persistent CTAs of k_relax_bulk<T, N, NT, FUSED>, by log2(N), NT / 512, FUSED
     double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
     int *d_mgit = nullptr;
     // base grid
@@ -520,7 +520,8 @@ public:
             return best;
         };
         struct Knob { int knob; int ref; std::vector<int> vals; };
-        const Knob ks[] = {{kKnobBaseCorr, 10, {10, 4, 2, 1}},
+        const Knob ks[] = {{kKnobFusedSweep, 0, {0, 1}},
+                           {kKnobBaseCorr, 10, {10, 4, 2, 1}},
                            {kKnobFmgCycles, 2, {2, 1}},
                            {kKnobFmgSweeps, 2, {2, 1, 3}},
                            {kKnobVmgSweeps, 2, {2, 1}}};
@@ -873,7 +874,7 @@ public:
         d_bad = mem.alloc<int>(1);
         d_err = mem.alloc<int>(1);
         zeroList.push_back({d_err, sizeof(int)});
-        for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], ((void)bulk_grid<N, 256>(), (void)bulk_grid<N, 512>()), (void)0);
+        for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], bulk_grids<N>(), (void)0);
         d_mom = mem.alloc<double>(32);
         if (P.bc == SFM_BC_SPHERE)   // per-cell moment terms of the base level, summed in order
             d_part = mem.alloc<double>((size_t)H.lstart[1] * H.NI * H.NI * H.NI * kMomentTerms);
@@ -1118,14 +1119,24 @@ public:
     // fmg level operations on the inner fields
     void relax(int f, T *u, T *rhs, bool bf0, int slot) {   // fmg_poisson_relax
         cudaMemsetAsync(d_max + slot, 0, sizeof(unsigned long long), st_);
-        const int n = nf[f];
-        for (int ipass = 1; ipass <= 2; ipass++) {
+        // the mixed schedule may sweep both colours in one launch (one ghost
+        // refresh per sweep instead of one per colour)
+        const bool fused = fused_at(f);
+        for (int ipass = 1; ipass <= (fused ? 1 : 2); ipass++) {
             poisson_flux(f, u, bf0);
             const bool prof = f == 0 && profNext < (int)profEv.size() / 2;
             if (prof) prof_mark(2 * profNext);
-            relax_launch(u, rhs, d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max + slot);
+            relax_launch(u, rhs, d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max + slot, fused);
             if (prof) prof_mark(2 * profNext++ + 1);
         }
+    }
+    // both colours per launch at fmg level f: a mixed-path schedule choice,
+    // on blocks the bulk-copy smoother serves
+    bool fused_at(int f) const {
+        if (sizeof(T) != 4 || serialRelax || sched(kKnobFusedSweep, 0) != 1) return false;
+        bool ok = false;
+        SFM_WITH_N(nf[f], ok = bulk_ok<N>(), ok = false)
+        return ok;
     }
     // persistent grid of k_relax_bulk<T, N> (N >= 4): every SM filled to the
     // kernel's occupancy; computed once, at set-up, outside stream capture
@@ -1133,34 +1144,54 @@ public:
     // (on 2^3 blocks it measured slower than k_relax_tiled)
     template <int N>
     static constexpr bool bulk_ok() { return N >= 4 && BulkPlan<T, N>::SMEM <= 220 * 1024; }
-    template <int N, int NT>
+    template <int N, int NT, bool FUSED>
     int bulk_grid() {
         if (!bulk_ok<N>()) return 0;
         constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : (N >= 4 ? 2 : 1));   // log2(N), capped
         constexpr int ti = NT == 512 ? 1 : 0;
-        if (!bulkGrid[li][ti]) {
+        if (!bulkGrid[li][ti][FUSED]) {
             const int smem = BulkPlan<T, N>::SMEM;
             // opt in whatever the size: static and dynamic shared memory together may pass 48 KB
-            cudaFuncSetAttribute(k_relax_bulk<T, N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaFuncSetAttribute(k_relax_bulk<T, N, NT, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             int per = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N, NT>, NT, smem) != cudaSuccess ||
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N, NT, FUSED>, NT, smem) !=
+                    cudaSuccess ||
                 per < 1) {
                 cudaGetLastError();
                 per = 1;
             }
-            bulkGrid[li][ti] = nSM * per;
+            bulkGrid[li][ti][FUSED] = nSM * per;
         }
-        return bulkGrid[li][ti];
+        return bulkGrid[li][ti][FUSED];
     }
-    template <int N, int NT>
+    template <int N>
+    void bulk_grids() {   // every variant a solve may launch
+        (void)bulk_grid<N, 256, false>();
+        (void)bulk_grid<N, 512, false>();
+        if constexpr (sizeof(T) == 4) {
+            (void)bulk_grid<N, 256, true>();
+            (void)bulk_grid<N, 512, true>();
+        }
+    }
+    template <int N, int NT, bool FUSED>
     void relax_bulk_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
                            int f, int ipass, unsigned long long *out) {
-        launch_pdl(k_relax_bulk<T, N, NT>,
-                   (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N, NT>()), NT,
+        launch_pdl(k_relax_bulk<T, N, NT, FUSED>,
+                   (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N, NT, FUSED>()), NT,
                    BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out, d_err, waitPolls);
     }
+    template <int N, int NT>
+    void relax_bulk_any(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
+                        int f, int ipass, unsigned long long *out, bool fused) {
+        if constexpr (sizeof(T) == 4) {   // the FP64 path always runs the reference's two colour launches
+            if (fused) return relax_bulk_launch<N, NT, true>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+        }
+        relax_bulk_launch<N, NT, false>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+    }
+    // one colour (ipass 1 or 2) over the listed blocks, or both colours with
+    // `fused` (bulk-copy smoother only; fused_at decides)
     void relax_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
-                      int f, int ipass, unsigned long long *out) {
+                      int f, int ipass, unsigned long long *out, bool fused = false) {
         const int n = nf[f];
         if (nblk <= 0) return;
         if (serialRelax) {   // race check: the same cells in a single-threaded sweep's order
@@ -1172,8 +1203,8 @@ public:
         }
         const int nt = tune.get(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, n >= 16 ? 512 : 256);
         SFM_WITH_N(n,
-                   (bulk_ok<N>() ? (nt == 512 ? relax_bulk_launch<N, 512>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out)
-                                              : relax_bulk_launch<N, 256>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out))
+                   (bulk_ok<N>() ? (nt == 512 ? relax_bulk_any<N, 512>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, fused)
+                                              : relax_bulk_any<N, 256>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, fused))
                                  : launch_pdl(k_relax_tiled<T, N>,
                                               (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
                                               256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
@@ -1241,6 +1272,7 @@ public:
             stats->smoother_ms = profMs;
             stats->smoother_launches = profN;
             stats->smoother_cells = profN * nLeaves * H.NI * H.NI * H.NI;
+            stats->smoother_colours = fused_at(0) ? 2 : 1;
         }
         profMs = 0.0;
         profN = 0;

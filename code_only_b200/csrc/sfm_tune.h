@@ -28,6 +28,12 @@
 //   fmg_sweeps      pre- and post-smoothing sweeps in fmg_lin (reference 2)
 //   vmg_sweeps      pre- and post-smoothing sweeps in vmg_fas (reference 2, vmg.F90:125-135)
 //   base_corrections  cap on mg_cycle's defect corrections (reference 10, mg.F90:50-52)
+//   fused_sweeps    1: each smoothing sweep at a fmg level with blocks of 4^3
+//                   and up does both colours in one launch, the second colour
+//                   with the block's ghost cells and reflux fluxes as they
+//                   were before the sweep (k_relax_bulk FUSED); 0: the
+//                   reference's two colour launches with a ghost refresh
+//                   between them (fmg_poisson.F90:160-165)
 //   key: element size 4, block edge NI, level -1, kind -1
 // Text form, one entry per line (blank lines and lines starting with '#'
 // are skipped):
@@ -49,7 +55,7 @@ namespace sfm {
 enum TuneKnob {
     kKnobGhostFill = 0, kKnobRelaxThreads = 1, kKnobResidBpc = 2,
     kKnobFmgCycles = 3, kKnobFmgSweeps = 4, kKnobVmgSweeps = 5, kKnobBaseCorr = 6,
-    kKnobBaseCtas = 7, kKnobBaseWide = 8, kKnobCount = 9
+    kKnobBaseCtas = 7, kKnobBaseWide = 8, kKnobFusedSweep = 9, kKnobCount = 10
 };
 inline const char *tune_knob_name(int k) {
     switch (k) {
@@ -62,6 +68,7 @@ inline const char *tune_knob_name(int k) {
         case kKnobBaseCorr: return "base_corrections";
         case kKnobBaseCtas: return "base_ctas";
         case kKnobBaseWide: return "base_wide";
+        case kKnobFusedSweep: return "fused_sweeps";
         default: return nullptr;
     }
 }
@@ -76,6 +83,7 @@ inline bool tune_choice_ok(int knob, int v) {
         case kKnobBaseCorr: return v >= 1 && v <= 10;
         case kKnobBaseCtas: return v == 1 || v == 2 || v == 4 || v == 8 || v == 16;
         case kKnobBaseWide: return v == 16 || v == 32 || v == 64;
+        case kKnobFusedSweep: return v == 0 || v == 1;
         default: return false;
     }
 }

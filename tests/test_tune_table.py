@@ -55,6 +55,7 @@ def test_later_entry_wins_and_empty_table(lib):
     "ghost_fill four 8 2 -1 1",
     "base_ctas 8 32 -1 -1 3",          # not a cluster size offered
     "base_wide 8 32 -1 -1 8",
+    "fused_sweeps 4 8 -1 -1 2",
 ])
 def test_malformed_entries_are_rejected(lib, bad):
     assert check(lib, "ghost_fill 4 8 0 -1 1\n" + bad + "\n")[0] == abi.SFM_EINVAL
@@ -68,3 +69,8 @@ def test_small_output_buffer(lib):
 def test_base_grid_knobs_parse(lib):
     rc, out = check(lib, "base_ctas 8 32 -1 -1 8\nbase_wide 8 32 -1 -1 16\nbase_ctas 4 16 -1 -1 1\n")
     assert rc == 3 and "base_ctas 8 32 -1 -1 8" in out and "base_wide 8 32 -1 -1 16" in out
+
+
+def test_fused_sweep_knob_parses(lib):
+    rc, out = check(lib, "fused_sweeps 4 8 -1 -1 1\nfused_sweeps 4 16 -1 -1 0\n")
+    assert rc == 2 and "fused_sweeps 4 8 -1 -1 1" in out and "fused_sweeps 4 16 -1 -1 0" in out
