@@ -599,9 +599,10 @@ struct RelaxTileSmem {
     T shh[Tile<N>::BPC], shi[Tile<N>::BPC];
 };
 
-// one colour over tiles tile0, tile0 + tstride, ... of BPC consecutive listed
-// blocks: each block with its ghost shell staged in shared memory, updated,
-// interior rows written back; |resh2| folded into m.
+// one colour (ipass 1 or 2; 0: both, a mixed-schedule choice) over tiles
+// tile0, tile0 + tstride, ... of BPC consecutive listed blocks: each block
+// with its ghost shell staged in shared memory, updated, interior rows
+// written back; |resh2| folded into m.
 template <class T, int N>
 __device__ __forceinline__ void relax_tiles(RelaxTileSmem<T, N> &sm, T *u, const T *__restrict__ rhs,
                                             const int32_t *__restrict__ blocks, int nblk,
@@ -624,23 +625,27 @@ __device__ __forceinline__ void relax_tiles(RelaxTileSmem<T, N> &sm, T *u, const
             sm.shi[threadIdx.x] = (T)(1.0 / hd);
         }
         __syncthreads();
-        for (int t = threadIdx.x; t < BPC * HALF; t += blockDim.x) {
-            const int q = t / HALF, r = t - q * HALF;
-            if (first + q >= nblk) continue;
-            const int b = blocks[first + q];
-            constexpr int HN = N / 2;
-            const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
-            const int i = 2 * i2 + ((j + k + ipass) & 1);
-            const T hh = sm.shh[q], hi = sm.shi[q];
-            T *ub = sm.sh + q * V;
-            TileFlux<T, N> F{ub, hi, rslot ? sm.ssl[q] : nullptr, rbuf};
-            const int c = (int)cidx(G, i, j, k);
-            const T resh2 = (F.div(i, j, k) - rhs[(int64_t)b * V + c] * hh) * hh;
-            ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
-            const double a = fabs((double)resh2);
-            m = a > m ? a : m;
+        // ipass 0: both colours, the second reading the first's new values
+        // from the stage (ghost cells and reflux fluxes as staged)
+        for (int pass = ipass ? ipass : 1; pass <= (ipass ? ipass : 2); pass++) {
+            for (int t = threadIdx.x; t < BPC * HALF; t += blockDim.x) {
+                const int q = t / HALF, r = t - q * HALF;
+                if (first + q >= nblk) continue;
+                const int b = blocks[first + q];
+                constexpr int HN = N / 2;
+                const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
+                const int i = 2 * i2 + ((j + k + pass) & 1);
+                const T hh = sm.shh[q], hi = sm.shi[q];
+                T *ub = sm.sh + q * V;
+                TileFlux<T, N> F{ub, hi, rslot ? sm.ssl[q] : nullptr, rbuf};
+                const int c = (int)cidx(G, i, j, k);
+                const T resh2 = (F.div(i, j, k) - rhs[(int64_t)b * V + c] * hh) * hh;
+                ub[c] = ub[c] + (T)(1.0 / 6.0) * resh2;   // only this thread reads this cell
+                const double a = fabs((double)resh2);
+                m = a > m ? a : m;
+            }
+            __syncthreads();
         }
-        __syncthreads();
         // write back the interior rows of every staged block
         for (int t = threadIdx.x; t < BPC * Tl::CELLS; t += blockDim.x) {
             const int q = t / Tl::CELLS, r = t - q * Tl::CELLS;

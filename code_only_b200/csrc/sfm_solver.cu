@@ -520,7 +520,7 @@ public:
             return best;
         };
         struct Knob { int knob; int ref; std::vector<int> vals; };
-        const Knob ks[] = {{kKnobFusedSweep, 0, {0, 1}},
+        const Knob ks[] = {{kKnobFusedSweep, 0, {0, 1, 2, 3}},
                            {kKnobBaseCorr, 10, {10, 4, 2, 1}},
                            {kKnobFmgCycles, 2, {2, 1}},
                            {kKnobFmgSweeps, 2, {2, 1, 3}},
@@ -1130,12 +1130,13 @@ public:
             if (prof) prof_mark(2 * profNext++ + 1);
         }
     }
-    // both colours per launch at fmg level f: a mixed-path schedule choice,
-    // on blocks the bulk-copy smoother serves
-    bool fused_at(int f) const {
-        if (sizeof(T) != 4 || serialRelax || sched(kKnobFusedSweep, 0) != 1) return false;
+    // both colours per launch at fmg level f: a mixed-path schedule choice
+    // (fused_sweeps bit 0 for fmg_lin's sweeps, bit 1 for vmg_fas's), on
+    // block edges the tiled and bulk-copy smoothers serve
+    bool fused_at(int f, int bit = 1) const {
+        if (sizeof(T) != 4 || serialRelax || !(sched(kKnobFusedSweep, 0) & bit)) return false;
         bool ok = false;
-        SFM_WITH_N(nf[f], ok = bulk_ok<N>(), ok = false)
+        SFM_WITH_N(nf[f], ok = true, ok = false)
         return ok;
     }
     // persistent grid of k_relax_bulk<T, N> (N >= 4): every SM filled to the
@@ -1189,7 +1190,7 @@ public:
         relax_bulk_launch<N, NT, false>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
     }
     // one colour (ipass 1 or 2) over the listed blocks, or both colours with
-    // `fused` (bulk-copy smoother only; fused_at decides)
+    // `fused` (fused_at decides; never on the per-element path)
     void relax_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
                       int f, int ipass, unsigned long long *out, bool fused = false) {
         const int n = nf[f];
@@ -1207,7 +1208,8 @@ public:
                                               : relax_bulk_any<N, 256>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, fused))
                                  : launch_pdl(k_relax_tiled<T, N>,
                                               (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
-                                              256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out),
+                                              256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f,
+                                              fused ? 0 : ipass, out),
                     ++launches),
                    runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
                           (int64_t)nblk * n * n * n / 2, out))
@@ -1381,12 +1383,12 @@ public:
         ghost_fill_level(L, F, u, false, 1);   // coarse-fine faces, x then y then z
         boundary_fill0_level(L, F, u);
     }
-    void vmg_relax(int L, T *u, const T *rhs) {
-        const int F = H.FMax, n = nf[F];
-        for (int ipass = 1; ipass <= 2; ipass++) {
+    void vmg_relax(int L, T *u, const T *rhs) {   // vmg_poisson_relax (vmg_poisson.F90:98-145)
+        const int F = H.FMax;
+        const bool fused = fused_at(F, 2);
+        for (int ipass = 1; ipass <= (fused ? 1 : 2); ipass++) {
             vmg_ghostcell(L, u);
-            (void)n;
-            relax_launch(u, rhs, d_all + H.lstart[L], cnt(L), nullptr, nullptr, F, ipass, d_max + 1);
+            relax_launch(u, rhs, d_all + H.lstart[L], cnt(L), nullptr, nullptr, F, ipass, d_max + 1, fused);
         }
     }
     void vmg_rstrct(int Lc, T *u, bool cubic) {

@@ -28,12 +28,13 @@
 //   fmg_sweeps      pre- and post-smoothing sweeps in fmg_lin (reference 2)
 //   vmg_sweeps      pre- and post-smoothing sweeps in vmg_fas (reference 2, vmg.F90:125-135)
 //   base_corrections  cap on mg_cycle's defect corrections (reference 10, mg.F90:50-52)
-//   fused_sweeps    1: each smoothing sweep at a fmg level with blocks of 4^3
-//                   and up does both colours in one launch, the second colour
-//                   with the block's ghost cells and reflux fluxes as they
-//                   were before the sweep (k_relax_bulk FUSED); 0: the
+//   fused_sweeps    bit 0: each smoothing sweep of fmg_lin does both colours
+//                   in one launch, the second colour with the block's ghost
+//                   cells and reflux fluxes as they were before the sweep
+//                   (k_relax_bulk FUSED, k_relax_tiled with ipass 0); bit 1:
+//                   the same for the sweeps of vmg_fas; clear: the
 //                   reference's two colour launches with a ghost refresh
-//                   between them (fmg_poisson.F90:160-165)
+//                   between them (fmg_poisson.F90:160-165, vmg_poisson.F90:114-115)
 //   key: element size 4, block edge NI, level -1, kind -1
 // Text form, one entry per line (blank lines and lines starting with '#'
 // are skipped):
@@ -83,7 +84,7 @@ inline bool tune_choice_ok(int knob, int v) {
         case kKnobBaseCorr: return v >= 1 && v <= 10;
         case kKnobBaseCtas: return v == 1 || v == 2 || v == 4 || v == 8 || v == 16;
         case kKnobBaseWide: return v == 16 || v == 32 || v == 64;
-        case kKnobFusedSweep: return v == 0 || v == 1;
+        case kKnobFusedSweep: return v >= 0 && v <= 3;
         default: return false;
     }
 }

@@ -78,12 +78,13 @@ def test_tuned_mixed_schedule_keeps_the_fp64_solution(name):
     assert np.abs(ga - gb).max() / np.abs(gb).max() <= 1e-9
 
 
+@pytest.mark.parametrize("mask", [1, 2, 3])
 @pytest.mark.parametrize("name", list(CASES))
-def test_fused_sweep_keeps_the_fp64_solution(name):
-    """fused_sweeps 1 makes every smoothing sweep of the mixed path's FP32
-    inner solve at fmg levels with 4^3 blocks and up one launch for both
-    colours (the second colour with the ghost cells and reflux fluxes of
-    before the sweep).  The FP64 defect correction must still reach the
+def test_fused_sweep_keeps_the_fp64_solution(name, mask):
+    """fused_sweeps bit 0 makes every smoothing sweep of the mixed path's
+    FP32 fmg_lin one launch for both colours (the second colour with the
+    ghost cells and reflux fluxes of before the sweep), bit 1 the same for
+    the sweeps of vmg_fas.  The FP64 defect correction must still reach the
     FP64 oracle's potential within 1e-9 at relative residual <= 1e-10, the
     profiled launches must report two colours each, and a solve after the
     table is cleared runs the two-launch sweep again (one colour each)."""
@@ -92,13 +93,13 @@ def test_fused_sweep_keeps_the_fp64_solution(name):
     p = abi.default_params(bc, rel_tol=1e-10, max_outer=40, precision=abi.SFM_PREC_MIXED, profile=1, **kw)
     rho = w.block_field(h, p.ngh_io, fn)
     with FMGPoisson(h, params=p) as s:
-        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 1\n")
+        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 {mask}\n")
         psi2, g2, st2 = s.solve(rho)
         psi3, g3, _ = s.solve(rho)                     # the graph replayed
         s.load_tune_table("")
         _, _, st4 = s.solve(rho)
     assert st2.converged and st2.true_rel_residual <= 1e-10
-    assert st2.smoother_colours == 2 and st2.smoother_launches > 0
+    assert st2.smoother_colours == (2 if mask & 1 else 1) and st2.smoother_launches > 0
     assert st4.smoother_colours == 1
     assert np.array_equal(psi2, psi3) and np.array_equal(g2, g3)
     _, psi1, g1, _, _ = oracle_solve(h, rho, abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw))
@@ -119,7 +120,7 @@ def test_fused_sweep_is_ignored_in_fp64():
     p = abi.default_params(bc, rel_tol=1e-10, max_outer=40, profile=1, **kw)
     rho = w.block_field(h, p.ngh_io, fn)
     with FMGPoisson(h, params=p) as s:
-        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 1\nfused_sweeps 8 {h.ni} -1 -1 1\n")
+        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 3\nfused_sweeps 8 {h.ni} -1 -1 3\n")
         psi2, _, st2 = s.solve(rho)
     assert st2.smoother_colours == 1
     _, psi1, _, _, _ = oracle_solve(h, rho, abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw))

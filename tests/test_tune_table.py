@@ -55,7 +55,7 @@ def test_later_entry_wins_and_empty_table(lib):
     "ghost_fill four 8 2 -1 1",
     "base_ctas 8 32 -1 -1 3",          # not a cluster size offered
     "base_wide 8 32 -1 -1 8",
-    "fused_sweeps 4 8 -1 -1 2",
+    "fused_sweeps 4 8 -1 -1 4",
 ])
 def test_malformed_entries_are_rejected(lib, bad):
     assert check(lib, "ghost_fill 4 8 0 -1 1\n" + bad + "\n")[0] == abi.SFM_EINVAL
@@ -72,5 +72,6 @@ def test_base_grid_knobs_parse(lib):
 
 
 def test_fused_sweep_knob_parses(lib):
-    rc, out = check(lib, "fused_sweeps 4 8 -1 -1 1\nfused_sweeps 4 16 -1 -1 0\n")
-    assert rc == 2 and "fused_sweeps 4 8 -1 -1 1" in out and "fused_sweeps 4 16 -1 -1 0" in out
+    rc, out = check(lib, "fused_sweeps 4 8 -1 -1 1\nfused_sweeps 4 16 -1 -1 0\nfused_sweeps 4 4 -1 -1 3\n")
+    assert rc == 3 and "fused_sweeps 4 8 -1 -1 1" in out and "fused_sweeps 4 16 -1 -1 0" in out
+    assert "fused_sweeps 4 4 -1 -1 3" in out
