@@ -284,7 +284,7 @@ public:
     int *d_err = nullptr;                  // set by a device wait that gave up
     uint32_t waitPolls = kWaitPolls;       // poll limit of the smoother's stage waits (tests lower it)
     int nSM = 148;
-    int bulkGrid[5][2][2] = {};            // persistent CTAs of k_relax_bulk<T, N, NT, FUSED>, by log2(N), NT / 512, FUSED
+    int bulkGrid[5][4][2] = {};            // persistent CTAs of k_relax_bulk<T, N, NT, FUSED>, by log2(N), NT, FUSED
     double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
     int *d_mgit = nullptr;
     // base grid
@@ -562,20 +562,28 @@ public:
         tune_ghost<T>(U[FMax], FMax, 0, reps);
         tune_ghost<T>(U[FMax], FMax, 1, reps);
         if (sizeof(T) != sizeof(double)) tune_ghost<double>(PSI0, 0, -1, reps);
-        // smoother CTA size on the bulk-copy levels
+        // smoother CTA size on the bulk-copy levels: the two colour launches
+        // (key kind -1) and, in the mixed path, the fused sweep (kind 1)
         for (int f = 0; f <= FMax; f++) {
             const int n = nf[f];
-            if (n < 4 || nLeaves <= 0) continue;
-            float t[2];
-            const int cand[2] = {256, 512};
-            for (int c = 0; c < 2; c++) {
-                tune.set(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, cand[c]);
-                t[c] = time_min([&] {
-                    for (int ipass = 1; ipass <= 2; ipass++)
-                        relax_launch(U[f], RHS[f], d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max);
-                }, reps);
+            bool bulk = false;
+            SFM_WITH_N(n, bulk = bulk_ok<N>(), bulk = false)
+            if (!bulk || nLeaves <= 0) continue;
+            for (int kind : {-1, 1}) {
+                const bool fused = kind == 1;
+                if (fused && sizeof(T) != 4) continue;
+                float best = std::numeric_limits<float>::max();
+                int pick = n >= 16 ? 512 : 256;
+                for (int nt : kRelaxNT) {
+                    tune.set(kKnobRelaxThreads, (int)sizeof(T), n, -1, kind, nt);
+                    const float t = time_min([&] {
+                        for (int ipass = 1; ipass <= (fused ? 1 : 2); ipass++)
+                            relax_launch(U[f], RHS[f], d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max, fused);
+                    }, reps);
+                    if (t < best) { best = t; pick = nt; }
+                }
+                tune.set(kKnobRelaxThreads, (int)sizeof(T), n, -1, kind, pick);
             }
-            tune.set(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, t[1] < t[0] ? 512 : 256);
         }
         // residual blocks per CTA on 8^3 blocks (inner and outer precision)
         for (int f = 0; f <= FMax; f++) {
@@ -1145,34 +1153,47 @@ public:
     // (on 2^3 blocks it measured slower than k_relax_tiled)
     template <int N>
     static constexpr bool bulk_ok() { return N >= 4 && BulkPlan<T, N>::SMEM <= 220 * 1024; }
+    // CTA sizes of the bulk-copy smoother: warp 0 produces, the rest
+    // consume; 288 and 544 give 8 and 16 consumer warps, which divide a
+    // colour's 256 cells (8^3 blocks, or eight 4^3 blocks) or 2048 cells
+    // (16^3) evenly, where 256 and 512 leave a last partial round
+    static constexpr int kRelaxNT[4] = {256, 288, 512, 544};
+    template <int NT>
+    static constexpr int nt_index() { return NT == 256 ? 0 : (NT == 288 ? 1 : (NT == 512 ? 2 : 3)); }
     template <int N, int NT, bool FUSED>
     int bulk_grid() {
-        if (!bulk_ok<N>()) return 0;
-        constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : (N >= 4 ? 2 : 1));   // log2(N), capped
-        constexpr int ti = NT == 512 ? 1 : 0;
-        if (!bulkGrid[li][ti][FUSED]) {
-            const int smem = BulkPlan<T, N>::SMEM;
-            // opt in whatever the size: static and dynamic shared memory together may pass 48 KB
-            cudaFuncSetAttribute(k_relax_bulk<T, N, NT, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            int per = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N, NT, FUSED>, NT, smem) !=
-                    cudaSuccess ||
-                per < 1) {
-                cudaGetLastError();
-                per = 1;
+        if constexpr (!bulk_ok<N>()) {
+            return 0;
+        } else {
+            constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : 2);   // log2(N), capped
+            constexpr int ti = nt_index<NT>();
+            if (!bulkGrid[li][ti][FUSED]) {
+                const int smem = BulkPlan<T, N>::SMEM;
+                // opt in whatever the size: static and dynamic shared memory together may pass 48 KB
+                cudaFuncSetAttribute(k_relax_bulk<T, N, NT, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                int per = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N, NT, FUSED>, NT, smem) !=
+                        cudaSuccess ||
+                    per < 1) {
+                    cudaGetLastError();
+                    per = 1;
+                }
+                bulkGrid[li][ti][FUSED] = nSM * per;
             }
-            bulkGrid[li][ti][FUSED] = nSM * per;
+            return bulkGrid[li][ti][FUSED];
         }
-        return bulkGrid[li][ti][FUSED];
+    }
+    template <int N, bool FUSED>
+    void bulk_grids_of() {
+        (void)bulk_grid<N, 256, FUSED>();
+        (void)bulk_grid<N, 288, FUSED>();
+        (void)bulk_grid<N, 512, FUSED>();
+        (void)bulk_grid<N, 544, FUSED>();
     }
     template <int N>
     void bulk_grids() {   // every variant a solve may launch
-        (void)bulk_grid<N, 256, false>();
-        (void)bulk_grid<N, 512, false>();
-        if constexpr (sizeof(T) == 4) {
-            (void)bulk_grid<N, 256, true>();
-            (void)bulk_grid<N, 512, true>();
-        }
+        bulk_grids_of<N, false>();
+        if constexpr (sizeof(T) == 4) bulk_grids_of<N, true>();
     }
     template <int N, int NT, bool FUSED>
     void relax_bulk_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
@@ -1181,13 +1202,34 @@ public:
                    (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N, NT, FUSED>()), NT,
                    BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out, d_err, waitPolls);
     }
-    template <int N, int NT>
-    void relax_bulk_any(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
-                        int f, int ipass, unsigned long long *out, bool fused) {
-        if constexpr (sizeof(T) == 4) {   // the FP64 path always runs the reference's two colour launches
-            if (fused) return relax_bulk_launch<N, NT, true>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+    template <int N, bool FUSED>
+    void relax_bulk_nt(int nt, T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot,
+                       const double *rb, int f, int ipass, unsigned long long *out) {
+        switch (nt) {
+            case 288: relax_bulk_launch<N, 288, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
+            case 512: relax_bulk_launch<N, 512, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
+            case 544: relax_bulk_launch<N, 544, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
+            default: relax_bulk_launch<N, 256, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
         }
-        relax_bulk_launch<N, NT, false>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+    }
+    // CTA size of the bulk smoother at block edge n, two-launch sweep (tune
+    // key kind -1) or fused sweep (kind 1)
+    int relax_nt(int n, bool fused) const {
+        return tune.get(kKnobRelaxThreads, (int)sizeof(T), n, -1, fused ? 1 : -1, n >= 16 ? 512 : 256);
+    }
+    template <int N>
+    void relax_dispatch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
+                        int f, int ipass, unsigned long long *out, bool fused) {
+        if constexpr (bulk_ok<N>()) {
+            const int nt = relax_nt(N, fused);
+            if constexpr (sizeof(T) == 4) {   // the FP64 path always runs the reference's two colour launches
+                if (fused) return relax_bulk_nt<N, true>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+            }
+            relax_bulk_nt<N, false>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+        } else {
+            launch_pdl(k_relax_tiled<T, N>, (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
+                       256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, fused ? 0 : ipass, out);
+        }
     }
     // one colour (ipass 1 or 2) over the listed blocks, or both colours with
     // `fused` (fused_at decides; never on the per-element path)
@@ -1202,15 +1244,7 @@ public:
             ++launches;
             return;
         }
-        const int nt = tune.get(kKnobRelaxThreads, (int)sizeof(T), n, -1, -1, n >= 16 ? 512 : 256);
-        SFM_WITH_N(n,
-                   (bulk_ok<N>() ? (nt == 512 ? relax_bulk_any<N, 512>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, fused)
-                                              : relax_bulk_any<N, 256>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, fused))
-                                 : launch_pdl(k_relax_tiled<T, N>,
-                                              (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
-                                              256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f,
-                                              fused ? 0 : ipass, out),
-                    ++launches),
+        SFM_WITH_N(n, (relax_dispatch<N>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, fused), ++launches),
                    runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
                           (int64_t)nblk * n * n * n / 2, out))
     }

@@ -10,8 +10,9 @@
 //   ghost_fill    level fill by the three directional passes (0) or by one
 //                 launch per level (1; only where Solver::ghost_merge_ok);
 //                 key: element size, block edge n, AMR level, fill kind
-//   relax_threads threads of the bulk-copy smoother CTA (256 or 512);
-//                 key: element size, block edge n
+//   relax_threads threads of the bulk-copy smoother CTA (256, 288, 512 or
+//                 544); key: element size, block edge n, kind -1 for the
+//                 two colour launches, 1 for the fused sweep
 //   resid_bpc     blocks per CTA of the tiled residual (1, 2 or 4);
 //                 key: element size, block edge n
 //   base_ctas     CTAs of the base-grid multigrid launch: 1, or a cluster
@@ -76,7 +77,7 @@ inline const char *tune_knob_name(int k) {
 inline bool tune_choice_ok(int knob, int v) {
     switch (knob) {
         case kKnobGhostFill: return v == 0 || v == 1;
-        case kKnobRelaxThreads: return v == 256 || v == 512;
+        case kKnobRelaxThreads: return v == 256 || v == 288 || v == 512 || v == 544;
         case kKnobResidBpc: return v == 1 || v == 2 || v == 4;
         case kKnobFmgCycles: return v >= 1 && v <= 3;
         case kKnobFmgSweeps: return v >= 1 && v <= 3;

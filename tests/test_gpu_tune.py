@@ -112,6 +112,33 @@ def test_fused_sweep_keeps_the_fp64_solution(name, mask):
     assert np.abs(ga - gb).max() / np.abs(gb).max() <= 1e-9
 
 
+@pytest.mark.parametrize("nt", [288, 512, 544])
+@pytest.mark.parametrize("name", ["amr3_periodic", "amr3_periodic_ni16"])
+def test_smoother_cta_sizes_are_bitwise(name, nt):
+    """Every CTA size of the bulk-copy smoother (warp 0 producing, 7, 8, 15
+    or 16 consumer warps) computes each cell with the same expression: the
+    FP64 solve stays bit-identical to the oracle, and the mixed solve with
+    fused sweeps is bit-identical to the one with the default CTA size."""
+    mk, fn, bc, kw = CASES[name]
+    h = mk()
+    edges = [e for e in (4, 8, 16) if e <= h.ni]
+    p64 = abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw)
+    rho = w.block_field(h, p64.ngh_io, fn)
+    with FMGPoisson(h, params=p64) as s:
+        s.load_tune_table("".join(f"relax_threads 8 {e} -1 -1 {nt}\n" for e in edges))
+        psi, _, _ = s.solve(rho)
+    _, psi_o, _, _, _ = oracle_solve(h, rho, p64)
+    assert np.array_equal(psi[:, 1:-1, 1:-1, 1:-1], psi_o[:, 1:-1, 1:-1, 1:-1])
+    pmx = abi.default_params(bc, rel_tol=1e-10, max_outer=40, precision=abi.SFM_PREC_MIXED, **kw)
+    fused = f"fused_sweeps 4 {h.ni} -1 -1 3\n"
+    with FMGPoisson(h, params=pmx) as s:
+        s.load_tune_table(fused)
+        psi_a, g_a, _ = s.solve(rho)
+        s.load_tune_table(fused + "".join(f"relax_threads 4 {e} -1 {k} {nt}\n" for e in edges for k in (-1, 1)))
+        psi_b, g_b, _ = s.solve(rho)
+    assert np.array_equal(psi_a, psi_b) and np.array_equal(g_a, g_b)
+
+
 def test_fused_sweep_is_ignored_in_fp64():
     """An FP64 context given fused_sweeps 1 still runs the reference's two
     colour launches and stays bit-identical to the oracle."""

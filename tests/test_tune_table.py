@@ -75,3 +75,8 @@ def test_fused_sweep_knob_parses(lib):
     rc, out = check(lib, "fused_sweeps 4 8 -1 -1 1\nfused_sweeps 4 16 -1 -1 0\nfused_sweeps 4 4 -1 -1 3\n")
     assert rc == 3 and "fused_sweeps 4 8 -1 -1 1" in out and "fused_sweeps 4 16 -1 -1 0" in out
     assert "fused_sweeps 4 4 -1 -1 3" in out
+
+
+def test_smoother_cta_sizes_parse(lib):
+    rc, out = check(lib, "relax_threads 4 8 -1 -1 288\nrelax_threads 4 8 -1 1 544\nrelax_threads 8 16 -1 -1 512\n")
+    assert rc == 3 and "relax_threads 4 8 -1 1 544" in out and "relax_threads 4 8 -1 -1 288" in out
