@@ -745,6 +745,21 @@ struct BulkPlan {
     static_assert(HI <= V && (V * (int)sizeof(T)) % 16 == 0, "span within the block, blocks 16-byte aligned");
 };
 
+// barrier `id` of `nthreads` threads (a multiple of 32, whole warps) that
+// also ORs a predicate over them: every participant gets the same result
+__device__ __forceinline__ bool consumers_sync_or(int id, int nthreads, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
@@ -790,10 +805,10 @@ __host__ __device__ constexpr int relax_bulk_threads() { return N >= 16 ? 512 : 
 // barrier, and the second colour reads them there, with the block's ghost
 // cells and reflux fluxes as they were before the sweep (the reference
 // refreshes them between the colours, fmg_poisson.F90:160-165).  u and rhs
-// are read once and u written once per full sweep.  A consumer's failed
-// stage wait is recorded before the first barrier of the tile and every
-// consumer warp leaves after it, so none waits at the barrier for one that
-// has gone.
+// are read once and u written once per full sweep.  A consumer warp whose
+// stage wait failed skips the first colour and still reaches the tile's
+// barrier, which ORs the failures: every consumer warp leaves after it, so
+// none waits at the barrier for one that has gone.
 template <class T, int N, int NT = relax_bulk_threads<N>(), bool FUSED = false>
 __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
     k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
@@ -903,15 +918,10 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
         const int ct = tid - 32;   // consumer thread 0..NCT-1
         T mt = (T)0;               // max |resh2| (exact in T; widened once)
         int it = 0;
-        auto consumers_sync = [] { asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory"); };
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
             const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), cpolls));
-            if constexpr (FUSED) {
-                if (!got && lane == 0) atomicExch(&cab, 1);
-                consumers_sync();
-                if (*(volatile int *)&cab) break;   // the same decision in every consumer warp
-            } else {
+            if constexpr (!FUSED) {
                 if (!got) {
                     if (lane == 0) atomicExch(&cab, 1);
                     break;
@@ -943,8 +953,14 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                 }
             };
             if constexpr (FUSED) {
-                colour(1);
-                consumers_sync();
+                if (got) colour(1);
+                // one barrier of the consumer threads per tile: colour 2 reads
+                // colour 1's values from the stage, and the OR over the failed
+                // waits gives every consumer warp the same decision
+                if (consumers_sync_or(1, NCT, !got)) {
+                    if (ct == 0) atomicExch(&cab, 1);
+                    break;
+                }
                 colour(2);
                 // the stage held ordinary stores; the next bulk copy into it
                 // goes through the async proxy

@@ -216,6 +216,31 @@ def test_bounded_smoother_wait_reports_timeout():
     assert rel(psi2, psi1) == 0.0 and rel(interior(h, g2, 2), interior(h, g1, 2)) == 0.0
 
 
+def test_bounded_wait_of_the_fused_sweep_reports_timeout():
+    """The same give-up in the fused sweep of the mixed path (both colours
+    per launch, one barrier of the consumer warps per tile): a warp whose
+    stage wait failed still reaches the tile's barrier, the barrier's OR
+    sends every consumer warp out, and the solve returns SFM_ETIMEOUT; the
+    context then solves normally once the poll limit is restored."""
+    lib = abi.load_library()
+    lib.sfm_debug_set_wait_polls.argtypes = [C.c_void_p, C.c_uint32]
+    lib.sfm_debug_set_wait_polls.restype = C.c_int
+    h = w.small_periodic(2, 8, 2, 0)
+    p = abi.default_params(abi.SFM_BC_PERIODIC, max_outer=1, precision=abi.SFM_PREC_MIXED)
+    rho = w.block_field(h, p.ngh_io, w.gaussian_peak)
+    with FMGPoisson(h, params=p) as s:
+        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 1\n")
+        assert lib.sfm_debug_set_wait_polls(s.ctx, 0) == abi.SFM_OK
+        psi = np.zeros_like(rho)
+        rc = lib.sfm_solve(s.ctx, rho.ctypes.data, psi.ctypes.data, None, None)
+        assert rc == abi.SFM_ETIMEOUT
+    p = abi.default_params(abi.SFM_BC_PERIODIC, rel_tol=1e-10, max_outer=40, precision=abi.SFM_PREC_MIXED)
+    with FMGPoisson(h, params=p) as s:
+        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 1\n")
+        _, _, st = s.solve(rho)
+    assert st.converged and st.true_rel_residual <= 1e-10
+
+
 @pytest.mark.parametrize("name", ["amr3_periodic", "amr3_sphere_l4", "amr3_periodic_ni16"])
 def test_red_black_sweeps_have_no_intra_colour_race(name):
     """Race check of the red-black smoother: with every colour sweep run one
