@@ -329,8 +329,8 @@ def run_ours(args):
     elem = mx["st"].elem_bytes or 4
     colours = mx["st"].smoother_colours or 1
     # one colour: u read, half of rhs read, half of u written (2 values per
-    # cell); both colours in one launch: u and rhs read, u written (3)
-    alg_bytes_per_launch = (sm_cells / max(sm_n, 1)) * (1 + colours) * elem
+    # cell); fused sweeps in one launch: u and rhs read, u written once (3)
+    alg_bytes_per_launch = (sm_cells / max(sm_n, 1)) * (2 if colours == 1 else 3) * elem
     launch_s = (sm_ms / max(sm_n, 1)) * 1e-3
     achieved = alg_bytes_per_launch / launch_s / 1e9 if launch_s > 0 else None
     peaks = {}
@@ -375,8 +375,8 @@ def run_ours(args):
         },
         "phi_rel_err_mixed_vs_fp64": phi_err,
         "roofline": {
-            "kernel": f"k_relax_bulk<float, {h.ni}>: " + ("both red-black colours" if colours == 2 else
-                                                          "one red-black colour") + " over the leaf cells, fmg level 0",
+            "kernel": f"k_relax_bulk<float, {h.ni}>: " + (f"{colours // 2} fused red-black sweep(s)" if colours >= 2
+                                                          else "one red-black colour") + " over the leaf cells, fmg level 0",
             "bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4) if achieved else None,
             "traffic": traffic,

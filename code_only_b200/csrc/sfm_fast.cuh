@@ -599,16 +599,16 @@ struct RelaxTileSmem {
     T shh[Tile<N>::BPC], shi[Tile<N>::BPC];
 };
 
-// one colour (ipass 1 or 2; 0: both, a mixed-schedule choice) over tiles
-// tile0, tile0 + tstride, ... of BPC consecutive listed blocks: each block
-// with its ghost shell staged in shared memory, updated, interior rows
-// written back; |resh2| folded into m.
+// one colour (ipass 1 or 2), or sw > 0 full sweeps (a mixed-schedule
+// choice), over tiles tile0, tile0 + tstride, ... of BPC consecutive listed
+// blocks: each block with its ghost shell staged in shared memory, updated,
+// interior rows written back; |resh2| folded into m.
 template <class T, int N>
 __device__ __forceinline__ void relax_tiles(RelaxTileSmem<T, N> &sm, T *u, const T *__restrict__ rhs,
                                             const int32_t *__restrict__ blocks, int nblk,
                                             const double *__restrict__ h0, const int32_t *__restrict__ level,
                                             const int32_t *__restrict__ rslot, const double *rbuf,
-                                            int f, int ipass, int tile0, int tstride, double &m) {
+                                            int f, int ipass, int sw, int tile0, int tstride, double &m) {
     using Tl = Tile<N>;
     constexpr int G = Tl::G, V = Tl::V, BPC = Tl::BPC, HALF = Tl::CELLS / 2;
     const int ntiles = (nblk + BPC - 1) / BPC;
@@ -625,9 +625,10 @@ __device__ __forceinline__ void relax_tiles(RelaxTileSmem<T, N> &sm, T *u, const
             sm.shi[threadIdx.x] = (T)(1.0 / hd);
         }
         __syncthreads();
-        // ipass 0: both colours, the second reading the first's new values
-        // from the stage (ghost cells and reflux fluxes as staged)
-        for (int pass = ipass ? ipass : 1; pass <= (ipass ? ipass : 2); pass++) {
+        // sw > 0: sw full sweeps, each colour reading the previous one's new
+        // values from the stage (ghost cells and reflux fluxes as staged)
+        for (int q2 = 0; q2 < (sw > 0 ? 2 * sw : 1); q2++) {
+            const int pass = sw > 0 ? 1 + (q2 & 1) : ipass;
             for (int t = threadIdx.x; t < BPC * HALF; t += blockDim.x) {
                 const int q = t / HALF, r = t - q * HALF;
                 if (first + q >= nblk) continue;
@@ -664,11 +665,11 @@ __global__ void __launch_bounds__(256) k_relax_tiled(T *__restrict__ u, const T 
                                                      const int32_t *__restrict__ blocks, int nblk,
                                                      const double *__restrict__ h0, const int32_t *__restrict__ level,
                                                      const int32_t *__restrict__ rslot, const double *__restrict__ rbuf,
-                                                     int f, int ipass, unsigned long long *out) {
+                                                     int f, int ipass, int sw, unsigned long long *out) {
     pdl_enter();
     __shared__ RelaxTileSmem<T, N> sm;
     double m = 0.0;
-    relax_tiles<T, N>(sm, u, rhs, blocks, nblk, h0, level, rslot, rbuf, f, ipass, blockIdx.x, gridDim.x, m);
+    relax_tiles<T, N>(sm, u, rhs, blocks, nblk, h0, level, rslot, rbuf, f, ipass, sw, blockIdx.x, gridDim.x, m);
     cta_max_atomic(m, out);
 }
 
@@ -799,17 +800,18 @@ __host__ __device__ constexpr int relax_bulk_min_ctas() {
 template <int N>
 __host__ __device__ constexpr int relax_bulk_threads() { return N >= 16 ? 512 : 256; }
 //
-// FUSED (a choice of the mixed path's schedule, never of the FP64 path):
-// both colours of every staged block in one pass -- the first colour's new
-// values go to u and back into the stage, the consumer warps meet at a named
-// barrier, and the second colour reads them there, with the block's ghost
-// cells and reflux fluxes as they were before the sweep (the reference
-// refreshes them between the colours, fmg_poisson.F90:160-165).  u and rhs
-// are read once and u written once per full sweep.  A consumer warp whose
-// stage wait failed skips the first colour and still reaches the tile's
-// barrier, which ORs the failures: every consumer warp leaves after it, so
-// none waits at the barrier for one that has gone.
-template <class T, int N, int NT = relax_bulk_threads<N>(), bool FUSED = false>
+// SW > 0 (a choice of the mixed path's schedule, never of the FP64 path):
+// SW full red-black sweeps of every staged block in one pass -- each
+// colour's new values go back into the stage, the consumer warps meet at a
+// named barrier, and the next colour reads them there, with the block's
+// ghost cells and reflux fluxes as they were before the launch (the
+// reference refreshes them between the colours, fmg_poisson.F90:160-165);
+// only the last sweep's values are stored to u.  u and rhs are read once
+// and u written once per launch.  A consumer warp whose stage wait failed
+// skips the first colour and still reaches the tile's first barrier, which
+// ORs the failures: every consumer warp leaves after it, so none waits at a
+// barrier for one that has gone.  SW = 0: the one colour `ipass`.
+template <class T, int N, int NT = relax_bulk_threads<N>(), int SW = 0>
 __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
     k_relax_bulk(T *__restrict__ u, const T *__restrict__ rhs,
                                                     const int32_t *__restrict__ blocks, int nblk,
@@ -921,7 +923,7 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
             const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), cpolls));
-            if constexpr (!FUSED) {
+            if constexpr (SW == 0) {
                 if (!got) {
                     if (lane == 0) atomicExch(&cab, 1);
                     break;
@@ -931,7 +933,9 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
             const int slot = it % (2 * R);
             T *ut = ust + s * BPC * V;
             const T *rt = rst + s * BPC * V;
-            auto colour = [&](int pass) {
+            // keep: the new values go back into the stage for a later colour;
+            // store: they go to u
+            auto colour = [&](int pass, bool keep, bool store) {
                 for (int t = ct; t < BPC * HALF; t += NCT) {
                     const int q = t / HALF, r = t - q * HALF;
                     if (first + q >= nblk) continue;
@@ -946,27 +950,36 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                     const int c = cidx(G, i, j, k);
                     const T resh2 = (F.div(i, j, k) - rt[q * V + c] * hh) * hh;
                     const T v = ub[c] + (T)(1.0 / 6.0) * resh2;
-                    u[(int64_t)bid[slot][q] * V + c] = v;
-                    if (FUSED && pass == 1) ub[c] = v;   // read by the second colour
+                    if (store) u[(int64_t)bid[slot][q] * V + c] = v;
+                    if (keep) ub[c] = v;
                     const T a = resh2 < (T)0 ? -resh2 : resh2;
                     mt = a > mt ? a : mt;
                 }
             };
-            if constexpr (FUSED) {
-                if (got) colour(1);
-                // one barrier of the consumer threads per tile: colour 2 reads
-                // colour 1's values from the stage, and the OR over the failed
-                // waits gives every consumer warp the same decision
+            if constexpr (SW > 0) {
+                if (got) colour(1, true, SW == 1);
+                // the consumer threads' barriers: each colour reads the
+                // previous one's values from the stage; the first also ORs
+                // the failed waits, so every consumer warp decides alike
                 if (consumers_sync_or(1, NCT, !got)) {
                     if (ct == 0) atomicExch(&cab, 1);
                     break;
                 }
-                colour(2);
+#pragma unroll 1
+                for (int r = 0; r < SW; r++) {
+                    const bool last = r == SW - 1;
+                    if (r > 0) {
+                        colour(1, true, last);
+                        asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
+                    }
+                    colour(2, !last, last);
+                    if (!last) asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
+                }
                 // the stage held ordinary stores; the next bulk copy into it
                 // goes through the async proxy
                 fence_async_shared();
             } else {
-                colour(ipass);
+                colour(ipass, false, true);
             }
             __syncwarp();
             if (lane == 0) {

@@ -284,7 +284,7 @@ public:
     int *d_err = nullptr;                  // set by a device wait that gave up
     uint32_t waitPolls = kWaitPolls;       // poll limit of the smoother's stage waits (tests lower it)
     int nSM = 148;
-    int bulkGrid[5][4][2] = {};            // persistent CTAs of k_relax_bulk<T, N, NT, FUSED>, by log2(N), NT, FUSED
+    int bulkGrid[5][4][3] = {};            // persistent CTAs of k_relax_bulk<T, N, NT, SW>, by log2(N), NT, SW
     double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
     int *d_mgit = nullptr;
     // base grid
@@ -521,6 +521,7 @@ public:
         };
         struct Knob { int knob; int ref; std::vector<int> vals; };
         const Knob ks[] = {{kKnobFusedSweep, 0, {0, 1, 2, 3}},
+                           {kKnobLocalSweeps, 1, {1, 2}},
                            {kKnobBaseCorr, 10, {10, 4, 2, 1}},
                            {kKnobFmgCycles, 2, {2, 1}},
                            {kKnobFmgSweeps, 2, {2, 1, 3}},
@@ -578,7 +579,8 @@ public:
                     tune.set(kKnobRelaxThreads, (int)sizeof(T), n, -1, kind, nt);
                     const float t = time_min([&] {
                         for (int ipass = 1; ipass <= (fused ? 1 : 2); ipass++)
-                            relax_launch(U[f], RHS[f], d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max, fused);
+                            relax_launch(U[f], RHS[f], d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max,
+                                         fused ? 1 : 0);
                     }, reps);
                     if (t < best) { best = t; pick = nt; }
                 }
@@ -1134,7 +1136,7 @@ public:
             poisson_flux(f, u, bf0);
             const bool prof = f == 0 && profNext < (int)profEv.size() / 2;
             if (prof) prof_mark(2 * profNext);
-            relax_launch(u, rhs, d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max + slot, fused);
+            relax_launch(u, rhs, d_leaves, nLeaves, d_rslot, rbuf[f], f, ipass, d_max + slot, fused ? local_sweeps() : 0);
             if (prof) prof_mark(2 * profNext++ + 1);
         }
     }
@@ -1147,6 +1149,9 @@ public:
         SFM_WITH_N(nf[f], ok = true, ok = false)
         return ok;
     }
+    // full sweeps per fused launch (local_sweeps: 1, or 2 on the staged
+    // block between ghost refreshes)
+    int local_sweeps() const { return sched(kKnobLocalSweeps, 1); }
     // persistent grid of k_relax_bulk<T, N> (N >= 4): every SM filled to the
     // kernel's occupancy; computed once, at set-up, outside stream capture
     // the bulk pipeline serves blocks of 4^3 and up whose stages fit in 220 KB
@@ -1160,81 +1165,86 @@ public:
     static constexpr int kRelaxNT[4] = {256, 288, 512, 544};
     template <int NT>
     static constexpr int nt_index() { return NT == 256 ? 0 : (NT == 288 ? 1 : (NT == 512 ? 2 : 3)); }
-    template <int N, int NT, bool FUSED>
+    template <int N, int NT, int SW>
     int bulk_grid() {
         if constexpr (!bulk_ok<N>()) {
             return 0;
         } else {
             constexpr int li = N >= 16 ? 4 : (N >= 8 ? 3 : 2);   // log2(N), capped
             constexpr int ti = nt_index<NT>();
-            if (!bulkGrid[li][ti][FUSED]) {
+            if (!bulkGrid[li][ti][SW]) {
                 const int smem = BulkPlan<T, N>::SMEM;
                 // opt in whatever the size: static and dynamic shared memory together may pass 48 KB
-                cudaFuncSetAttribute(k_relax_bulk<T, N, NT, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                cudaFuncSetAttribute(k_relax_bulk<T, N, NT, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
                 int per = 0;
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N, NT, FUSED>, NT, smem) !=
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relax_bulk<T, N, NT, SW>, NT, smem) !=
                         cudaSuccess ||
                     per < 1) {
                     cudaGetLastError();
                     per = 1;
                 }
-                bulkGrid[li][ti][FUSED] = nSM * per;
+                bulkGrid[li][ti][SW] = nSM * per;
             }
-            return bulkGrid[li][ti][FUSED];
+            return bulkGrid[li][ti][SW];
         }
     }
-    template <int N, bool FUSED>
+    template <int N, int SW>
     void bulk_grids_of() {
-        (void)bulk_grid<N, 256, FUSED>();
-        (void)bulk_grid<N, 288, FUSED>();
-        (void)bulk_grid<N, 512, FUSED>();
-        (void)bulk_grid<N, 544, FUSED>();
+        (void)bulk_grid<N, 256, SW>();
+        (void)bulk_grid<N, 288, SW>();
+        (void)bulk_grid<N, 512, SW>();
+        (void)bulk_grid<N, 544, SW>();
     }
     template <int N>
     void bulk_grids() {   // every variant a solve may launch
-        bulk_grids_of<N, false>();
-        if constexpr (sizeof(T) == 4) bulk_grids_of<N, true>();
+        bulk_grids_of<N, 0>();
+        if constexpr (sizeof(T) == 4) {
+            bulk_grids_of<N, 1>();
+            bulk_grids_of<N, 2>();
+        }
     }
-    template <int N, int NT, bool FUSED>
+    template <int N, int NT, int SW>
     void relax_bulk_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
                            int f, int ipass, unsigned long long *out) {
-        launch_pdl(k_relax_bulk<T, N, NT, FUSED>,
-                   (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N, NT, FUSED>()), NT,
+        launch_pdl(k_relax_bulk<T, N, NT, SW>,
+                   (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, bulk_grid<N, NT, SW>()), NT,
                    BulkPlan<T, N>::SMEM, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, out, d_err, waitPolls);
     }
-    template <int N, bool FUSED>
+    template <int N, int SW>
     void relax_bulk_nt(int nt, T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot,
                        const double *rb, int f, int ipass, unsigned long long *out) {
         switch (nt) {
-            case 288: relax_bulk_launch<N, 288, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
-            case 512: relax_bulk_launch<N, 512, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
-            case 544: relax_bulk_launch<N, 544, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
-            default: relax_bulk_launch<N, 256, FUSED>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
+            case 288: relax_bulk_launch<N, 288, SW>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
+            case 512: relax_bulk_launch<N, 512, SW>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
+            case 544: relax_bulk_launch<N, 544, SW>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
+            default: relax_bulk_launch<N, 256, SW>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out); break;
         }
     }
     // CTA size of the bulk smoother at block edge n, two-launch sweep (tune
-    // key kind -1) or fused sweep (kind 1)
+    // key kind -1) or fused sweeps (kind 1)
     int relax_nt(int n, bool fused) const {
         return tune.get(kKnobRelaxThreads, (int)sizeof(T), n, -1, fused ? 1 : -1, n >= 16 ? 512 : 256);
     }
     template <int N>
     void relax_dispatch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
-                        int f, int ipass, unsigned long long *out, bool fused) {
+                        int f, int ipass, unsigned long long *out, int sw) {
         if constexpr (bulk_ok<N>()) {
-            const int nt = relax_nt(N, fused);
+            const int nt = relax_nt(N, sw > 0);
             if constexpr (sizeof(T) == 4) {   // the FP64 path always runs the reference's two colour launches
-                if (fused) return relax_bulk_nt<N, true>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+                if (sw == 1) return relax_bulk_nt<N, 1>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+                if (sw == 2) return relax_bulk_nt<N, 2>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
             }
-            relax_bulk_nt<N, false>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+            relax_bulk_nt<N, 0>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
         } else {
             launch_pdl(k_relax_tiled<T, N>, (unsigned)std::min((nblk + Tile<N>::BPC - 1) / Tile<N>::BPC, persistGrid),
-                       256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, fused ? 0 : ipass, out);
+                       256, 0, u, rhs, blocks, nblk, d_h0, d_level, rslot, rb, f, ipass, sizeof(T) == 4 ? sw : 0,
+                       out);
         }
     }
-    // one colour (ipass 1 or 2) over the listed blocks, or both colours with
-    // `fused` (fused_at decides; never on the per-element path)
+    // one colour (ipass 1 or 2) over the listed blocks, or sw > 0 full
+    // sweeps in one launch (fused_at decides; never on the per-element path)
     void relax_launch(T *u, const T *rhs, const int32_t *blocks, int nblk, const int32_t *rslot, const double *rb,
-                      int f, int ipass, unsigned long long *out, bool fused = false) {
+                      int f, int ipass, unsigned long long *out, int sw = 0) {
         const int n = nf[f];
         if (nblk <= 0) return;
         if (serialRelax) {   // race check: the same cells in a single-threaded sweep's order
@@ -1244,7 +1254,7 @@ public:
             ++launches;
             return;
         }
-        SFM_WITH_N(n, (relax_dispatch<N>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, fused), ++launches),
+        SFM_WITH_N(n, (relax_dispatch<N>(u, rhs, blocks, nblk, rslot, rb, f, ipass, out, sw), ++launches),
                    runMax(OpRelax<T, T>{u, rhs, blocks, d_h0, d_level, rslot, rb, f, n, Gf[f], Vf[f], ipass},
                           (int64_t)nblk * n * n * n / 2, out))
     }
@@ -1308,7 +1318,7 @@ public:
             stats->smoother_ms = profMs;
             stats->smoother_launches = profN;
             stats->smoother_cells = profN * nLeaves * H.NI * H.NI * H.NI;
-            stats->smoother_colours = fused_at(0) ? 2 : 1;
+            stats->smoother_colours = fused_at(0) ? 2 * local_sweeps() : 1;
         }
         profMs = 0.0;
         profN = 0;
@@ -1422,7 +1432,8 @@ public:
         const bool fused = fused_at(F, 2);
         for (int ipass = 1; ipass <= (fused ? 1 : 2); ipass++) {
             vmg_ghostcell(L, u);
-            relax_launch(u, rhs, d_all + H.lstart[L], cnt(L), nullptr, nullptr, F, ipass, d_max + 1, fused);
+            relax_launch(u, rhs, d_all + H.lstart[L], cnt(L), nullptr, nullptr, F, ipass, d_max + 1,
+                         fused ? local_sweeps() : 0);
         }
     }
     void vmg_rstrct(int Lc, T *u, bool cubic) {

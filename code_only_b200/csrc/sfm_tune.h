@@ -36,6 +36,8 @@
 //                   the same for the sweeps of vmg_fas; clear: the
 //                   reference's two colour launches with a ghost refresh
 //                   between them (fmg_poisson.F90:160-165, vmg_poisson.F90:114-115)
+//   local_sweeps    full sweeps of each fused launch on the staged block
+//                   (1 or 2; the ghost cells stay as staged between them)
 //   key: element size 4, block edge NI, level -1, kind -1
 // Text form, one entry per line (blank lines and lines starting with '#'
 // are skipped):
@@ -57,7 +59,7 @@ namespace sfm {
 enum TuneKnob {
     kKnobGhostFill = 0, kKnobRelaxThreads = 1, kKnobResidBpc = 2,
     kKnobFmgCycles = 3, kKnobFmgSweeps = 4, kKnobVmgSweeps = 5, kKnobBaseCorr = 6,
-    kKnobBaseCtas = 7, kKnobBaseWide = 8, kKnobFusedSweep = 9, kKnobCount = 10
+    kKnobBaseCtas = 7, kKnobBaseWide = 8, kKnobFusedSweep = 9, kKnobLocalSweeps = 10, kKnobCount = 11
 };
 inline const char *tune_knob_name(int k) {
     switch (k) {
@@ -71,6 +73,7 @@ inline const char *tune_knob_name(int k) {
         case kKnobBaseCtas: return "base_ctas";
         case kKnobBaseWide: return "base_wide";
         case kKnobFusedSweep: return "fused_sweeps";
+        case kKnobLocalSweeps: return "local_sweeps";
         default: return nullptr;
     }
 }
@@ -86,6 +89,7 @@ inline bool tune_choice_ok(int knob, int v) {
         case kKnobBaseCtas: return v == 1 || v == 2 || v == 4 || v == 8 || v == 16;
         case kKnobBaseWide: return v == 16 || v == 32 || v == 64;
         case kKnobFusedSweep: return v >= 0 && v <= 3;
+        case kKnobLocalSweeps: return v == 1 || v == 2;
         default: return false;
     }
 }

@@ -120,8 +120,9 @@ typedef struct sfm_stats {
     int64_t smoother_launches;   /* number of those launches                  */
     int64_t smoother_cells;      /* leaf cells swept per launch x launches    */
     int32_t elem_bytes;          /* bytes per value of the inner solve (8 or 4) */
-    int32_t smoother_colours;    /* red-black colours per timed launch: 1, or 2
-                                    when the mixed schedule fuses the sweep   */
+    int32_t smoother_colours;    /* red-black colours per timed launch: 1, or
+                                    2 x the local sweeps when the mixed
+                                    schedule fuses them                       */
 } sfm_stats;
 
 typedef struct sfm_ctx sfm_ctx;

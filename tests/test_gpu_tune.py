@@ -64,7 +64,7 @@ def test_tuned_mixed_schedule_keeps_the_fp64_solution(name):
     with FMGPoisson(h, params=p) as s:
         s.autotune(2, rho_d.data_ptr())
         table = s.tune_table()
-        for knob in ("fmg_ncycle", "fmg_sweeps", "vmg_sweeps", "base_corrections", "fused_sweeps"):
+        for knob in ("fmg_ncycle", "fmg_sweeps", "vmg_sweeps", "base_corrections", "fused_sweeps", "local_sweeps"):
             assert any(ln.startswith(knob + " 4 ") for ln in table.splitlines()), knob
         psi2, g2, st2 = s.solve(rho)
     assert st2.converged and st2.true_rel_residual <= 1e-10
@@ -78,13 +78,14 @@ def test_tuned_mixed_schedule_keeps_the_fp64_solution(name):
     assert np.abs(ga - gb).max() / np.abs(gb).max() <= 1e-9
 
 
-@pytest.mark.parametrize("mask", [1, 2, 3])
+@pytest.mark.parametrize("mask,local", [(1, 1), (2, 1), (3, 1), (1, 2), (3, 2)])
 @pytest.mark.parametrize("name", list(CASES))
-def test_fused_sweep_keeps_the_fp64_solution(name, mask):
+def test_fused_sweep_keeps_the_fp64_solution(name, mask, local):
     """fused_sweeps bit 0 makes every smoothing sweep of the mixed path's
     FP32 fmg_lin one launch for both colours (the second colour with the
     ghost cells and reflux fluxes of before the sweep), bit 1 the same for
-    the sweeps of vmg_fas.  The FP64 defect correction must still reach the
+    the sweeps of vmg_fas; local_sweeps 2 runs two full sweeps on the staged
+    block per launch.  The FP64 defect correction must still reach the
     FP64 oracle's potential within 1e-9 at relative residual <= 1e-10, the
     profiled launches must report two colours each, and a solve after the
     table is cleared runs the two-launch sweep again (one colour each)."""
@@ -93,13 +94,13 @@ def test_fused_sweep_keeps_the_fp64_solution(name, mask):
     p = abi.default_params(bc, rel_tol=1e-10, max_outer=40, precision=abi.SFM_PREC_MIXED, profile=1, **kw)
     rho = w.block_field(h, p.ngh_io, fn)
     with FMGPoisson(h, params=p) as s:
-        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 {mask}\n")
+        s.load_tune_table(f"fused_sweeps 4 {h.ni} -1 -1 {mask}\nlocal_sweeps 4 {h.ni} -1 -1 {local}\n")
         psi2, g2, st2 = s.solve(rho)
         psi3, g3, _ = s.solve(rho)                     # the graph replayed
         s.load_tune_table("")
         _, _, st4 = s.solve(rho)
     assert st2.converged and st2.true_rel_residual <= 1e-10
-    assert st2.smoother_colours == (2 if mask & 1 else 1) and st2.smoother_launches > 0
+    assert st2.smoother_colours == (2 * local if mask & 1 else 1) and st2.smoother_launches > 0
     assert st4.smoother_colours == 1
     assert np.array_equal(psi2, psi3) and np.array_equal(g2, g3)
     _, psi1, g1, _, _ = oracle_solve(h, rho, abi.default_params(bc, rel_tol=1e-10, max_outer=40, **kw))
@@ -166,7 +167,8 @@ def test_fp64_context_keeps_the_reference_schedule():
     rho_d = torch.from_numpy(rho).cuda()
     with FMGPoisson(h, params=p) as s:
         s.autotune(2, rho_d.data_ptr())
-        assert not any(ln.startswith(("fmg_ncycle", "fmg_sweeps", "vmg_sweeps", "base_corrections", "fused_sweeps"))
+        assert not any(ln.startswith(("fmg_ncycle", "fmg_sweeps", "vmg_sweeps", "base_corrections", "fused_sweeps",
+                                      "local_sweeps"))
                        for ln in s.tune_table().splitlines())
         psi2, _, _ = s.solve(rho)
     _, psi1, _, _, _ = oracle_solve(h, rho, p)

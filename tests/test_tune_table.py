@@ -56,6 +56,7 @@ def test_later_entry_wins_and_empty_table(lib):
     "base_ctas 8 32 -1 -1 3",          # not a cluster size offered
     "base_wide 8 32 -1 -1 8",
     "fused_sweeps 4 8 -1 -1 4",
+    "local_sweeps 4 8 -1 -1 3",
 ])
 def test_malformed_entries_are_rejected(lib, bad):
     assert check(lib, "ghost_fill 4 8 0 -1 1\n" + bad + "\n")[0] == abi.SFM_EINVAL
@@ -80,3 +81,8 @@ def test_fused_sweep_knob_parses(lib):
 def test_smoother_cta_sizes_parse(lib):
     rc, out = check(lib, "relax_threads 4 8 -1 -1 288\nrelax_threads 4 8 -1 1 544\nrelax_threads 8 16 -1 -1 512\n")
     assert rc == 3 and "relax_threads 4 8 -1 1 544" in out and "relax_threads 4 8 -1 -1 288" in out
+
+
+def test_local_sweeps_parse(lib):
+    rc, out = check(lib, "local_sweeps 4 8 -1 -1 2\nfused_sweeps 4 8 -1 -1 1\n")
+    assert rc == 2 and "local_sweeps 4 8 -1 -1 2" in out
