@@ -957,7 +957,77 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                 }
             };
             if constexpr (SW > 0) {
-                if (got) colour(1, true, SW == 1);
+                // A thread's cell t has the same place in both colours: its
+                // colour-1 cell and colour-2 cell are x neighbours.  Outside
+                // reflux blocks their current values stay in registers
+                // (own1, own2), so each colour loads only the other x
+                // neighbour and the four y and z neighbours; the per-block
+                // data is read once per tile.  The expressions are those of
+                // TileFlux::div without reflux slots, term for term.
+                constexpr int ITER = (BPC * HALF + NCT - 1) / NCT;
+                T own1[ITER], own2[ITER], th[ITER], ti[ITER];
+                bool flux[ITER], live[ITER];
+                int64_t gb[ITER];
+#pragma unroll
+                for (int x = 0; x < ITER; x++) {
+                    const int t = ct + x * NCT, q = t / HALF;
+                    live[x] = t < BPC * HALF && first + q < nblk;
+                    if (live[x]) {
+                        th[x] = shh[slot][q];
+                        ti[x] = shi[slot][q];
+                        flux[x] = hasr[slot][q] != 0;
+                        gb[x] = (int64_t)bid[slot][q] * V;
+                    }
+                }
+                auto fused_colour = [&](int pass, bool first_colour, bool keep, bool store) {
+#pragma unroll
+                    for (int x = 0; x < ITER; x++) {
+                        if (!live[x]) continue;
+                        const int t = ct + x * NCT, q = t / HALF, r = t - q * HALF;
+                        constexpr int HN = N / 2;
+                        const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
+                        const int p1 = (j + k + 1) & 1;
+                        const int i = 2 * i2 + (pass == 1 ? p1 : 1 - p1);
+                        const int dp = pass == 1 ? 1 - 2 * p1 : 2 * p1 - 1;   // to this thread's other cell
+                        const T hh = th[x], hi = ti[x];
+                        T *ub = ut + q * V;
+                        const int c = cidx(G, i, j, k);
+                        const T rr = rt[q * V + c];
+                        T uc, resh2;
+                        if (flux[x]) {
+                            TileFlux<T, N> F{ub, hi, ssl[slot][q], rbuf};
+                            uc = ub[c];
+                            resh2 = (F.div(i, j, k) - rr * hh) * hh;
+                        } else {
+                            T partner;
+                            if (first_colour) {   // both cells still hold the values staged
+                                uc = ub[c];
+                                partner = ub[c + dp];
+                                own2[x] = partner;
+                            } else {
+                                uc = pass == 1 ? own1[x] : own2[x];
+                                partner = pass == 1 ? own2[x] : own1[x];
+                            }
+                            const T other = ub[c - dp];
+                            const T xp = dp > 0 ? partner : other, xm = dp > 0 ? other : partner;
+                            const T ym = ub[c - G], yp = ub[c + G], zm = ub[c - G * G], zp = ub[c + G * G];
+                            T tt = (xp - uc) * hi - (uc - xm) * hi;
+                            tt = tt + (yp - uc) * hi;
+                            tt = tt - (uc - ym) * hi;
+                            tt = tt + (zp - uc) * hi;
+                            tt = tt - (uc - zm) * hi;
+                            resh2 = (tt - rr * hh) * hh;
+                        }
+                        const T v = uc + (T)(1.0 / 6.0) * resh2;
+                        if (pass == 1) own1[x] = v;
+                        else own2[x] = v;
+                        if (store) u[gb[x] + c] = v;
+                        if (keep) ub[c] = v;
+                        const T a = resh2 < (T)0 ? -resh2 : resh2;
+                        mt = a > mt ? a : mt;
+                    }
+                };
+                if (got) fused_colour(1, true, true, SW == 1);
                 // the consumer threads' barriers: each colour reads the
                 // previous one's values from the stage; the first also ORs
                 // the failed waits, so every consumer warp decides alike
@@ -969,10 +1039,10 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                 for (int r = 0; r < SW; r++) {
                     const bool last = r == SW - 1;
                     if (r > 0) {
-                        colour(1, true, last);
+                        fused_colour(1, false, true, last);
                         asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
                     }
-                    colour(2, !last, last);
+                    fused_colour(2, false, !last, last);
                     if (!last) asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
                 }
                 // the stage held ordinary stores; the next bulk copy into it
