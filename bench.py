@@ -328,9 +328,13 @@ def run_ours(args):
     sm_ms, sm_n, sm_cells = mx["smo"]
     elem = mx["st"].elem_bytes or 4
     colours = mx["st"].smoother_colours or 1
-    # one colour: u read, half of rhs read, half of u written (2 values per
-    # cell); fused sweeps in one launch: u and rhs read, u written once (3)
-    alg_bytes_per_launch = (sm_cells / max(sm_n, 1)) * (2 if colours == 1 else 3) * elem
+    # algorithmic bytes of one launch: one colour reads u, half of rhs and
+    # writes half of u (2 values per leaf cell, the floor of the reference's
+    # schedule, which refreshes ghosts between the colours); a fused launch
+    # does colours / 2 full sweeps, each 3 values per leaf cell (u and rhs
+    # read, u written) -- the per-sweep unit counted once per sweep done
+    cells_per_launch = sm_cells / max(sm_n, 1)
+    alg_bytes_per_launch = cells_per_launch * (2 if colours == 1 else 3 * (colours // 2)) * elem
     launch_s = (sm_ms / max(sm_n, 1)) * 1e-3
     achieved = alg_bytes_per_launch / launch_s / 1e9 if launch_s > 0 else None
     peaks = {}
@@ -342,7 +346,7 @@ def run_ours(args):
     traffic = None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        traffic = prof.get(args.workload, {}).get("bytes_per_launch")
+        traffic = prof.get(args.workload, {}).get("one_colour" if colours == 1 else "fused")
     except Exception:
         pass
     cells_updates = leaf_cells * 1.0
@@ -381,6 +385,8 @@ def run_ours(args):
             "frac": round(achieved / peak, 4) if achieved else None,
             "traffic": traffic,
             "alg_bytes_per_launch": alg_bytes_per_launch,
+            "alg_bytes_rule": ("2 values per leaf cell (one colour)" if colours == 1 else
+                               f"3 values per leaf cell per full sweep x {colours // 2} sweep(s) per launch"),
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
         },
         "gpu_launches": int(mx["launches"]),
