@@ -920,6 +920,24 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
         const int ct = tid - 32;   // consumer thread 0..NCT-1
         T mt = (T)0;               // max |resh2| (exact in T; widened once)
         int it = 0;
+        // fused sweeps: cell t = ct + x NCT of each tile's colour-1 cells
+        // (and its x neighbour, the colour-2 cell of t) for x < ITER
+        constexpr int ITER = SW > 0 ? (BPC * HALF + NCT - 1) / NCT : 1;
+        // block, in-block offset of the colour-1 cell and the step to its
+        // x neighbour, recomputed where used (held across the tile loop
+        // they cost registers the 7-CTA occupancy does not have)
+        auto cell_of = [&](int x, int &q, int &i1, int &j, int &k, int &d1) {
+            const int t = ct + x * NCT;
+            q = t / HALF;
+            const int r = t - q * HALF;
+            constexpr int HN = N / 2;
+            const int i2 = r % HN;
+            j = (r / HN) % N;
+            k = r / (HN * N);
+            const int p1 = (j + k + 1) & 1;
+            i1 = 2 * i2 + p1;
+            d1 = 1 - 2 * p1;
+        };
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
             const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), cpolls));
@@ -962,9 +980,11 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                 // reflux blocks their current values stay in registers
                 // (own1, own2), so each colour loads only the other x
                 // neighbour and the four y and z neighbours; the per-block
-                // data is read once per tile.  The expressions are those of
-                // TileFlux::div without reflux slots, term for term.
-                constexpr int ITER = (BPC * HALF + NCT - 1) / NCT;
+                // data is read once per tile.  This path only serves the mixed schedule's FP32
+                // preconditioner, so it takes the cheaper form
+                //   resh2 = (sum over faces of (u_nb - u_c)) (hi hh) - rhs hh^2
+                // with explicit fused multiply-adds (hi hh = 1 up to
+                // rounding); reflux blocks keep the reference's flux form.
                 T own1[ITER], own2[ITER], th[ITER], ti[ITER];
                 bool flux[ITER], live[ITER];
                 int64_t gb[ITER];
@@ -983,21 +1003,18 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
 #pragma unroll
                     for (int x = 0; x < ITER; x++) {
                         if (!live[x]) continue;
-                        const int t = ct + x * NCT, q = t / HALF, r = t - q * HALF;
-                        constexpr int HN = N / 2;
-                        const int i2 = r % HN, j = (r / HN) % N, k = r / (HN * N);
-                        const int p1 = (j + k + 1) & 1;
-                        const int i = 2 * i2 + (pass == 1 ? p1 : 1 - p1);
-                        const int dp = pass == 1 ? 1 - 2 * p1 : 2 * p1 - 1;   // to this thread's other cell
-                        const T hh = th[x], hi = ti[x];
-                        T *ub = ut + q * V;
+                        int q, i1, j, k, d1;
+                        cell_of(x, q, i1, j, k, d1);
+                        const int dp = pass == 1 ? d1 : -d1;   // to this thread's other cell
+                        const int i = pass == 1 ? i1 : i1 + d1;
                         const int c = cidx(G, i, j, k);
+                        T *ub = ut + q * V;
                         const T rr = rt[q * V + c];
                         T uc, resh2;
                         if (flux[x]) {
-                            TileFlux<T, N> F{ub, hi, ssl[slot][q], rbuf};
+                            TileFlux<T, N> F{ub, ti[x], ssl[slot][q], rbuf};
                             uc = ub[c];
-                            resh2 = (F.div(i, j, k) - rr * hh) * hh;
+                            resh2 = (F.div(i, j, k) - rr * th[x]) * th[x];
                         } else {
                             T partner;
                             if (first_colour) {   // both cells still hold the values staged
@@ -1009,16 +1026,13 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                                 partner = pass == 1 ? own2[x] : own1[x];
                             }
                             const T other = ub[c - dp];
-                            const T xp = dp > 0 ? partner : other, xm = dp > 0 ? other : partner;
                             const T ym = ub[c - G], yp = ub[c + G], zm = ub[c - G * G], zp = ub[c + G * G];
-                            T tt = (xp - uc) * hi - (uc - xm) * hi;
-                            tt = tt + (yp - uc) * hi;
-                            tt = tt - (uc - ym) * hi;
-                            tt = tt + (zp - uc) * hi;
-                            tt = tt - (uc - zm) * hi;
-                            resh2 = (tt - rr * hh) * hh;
+                            const T sx = (partner - uc) + (other - uc);
+                            const T sy = (yp - uc) + (ym - uc);
+                            const T sz = (zp - uc) + (zm - uc);
+                            resh2 = fma((sx + sy) + sz, ti[x] * th[x], -(rr * (th[x] * th[x])));
                         }
-                        const T v = uc + (T)(1.0 / 6.0) * resh2;
+                        const T v = fma((T)(1.0 / 6.0), resh2, uc);
                         if (pass == 1) own1[x] = v;
                         else own2[x] = v;
                         if (store) u[gb[x] + c] = v;
