@@ -163,7 +163,16 @@ __device__ void mg_boundary_u(MgRun &r, const MgData &d, int m, double *a) {
         }
     mg_end(s);
 }
+// A step with nothing to do (no face of the box on the physical boundary:
+// a periodic box) is skipped with its barrier: the previous step's barrier
+// already orders what came before it against what follows.
+__device__ __forceinline__ bool mg_touches(const MgData &d, int f0, int f1) {
+    bool t = false;
+    for (int f = f0; f < f1; f++) t = t || d.touch[f];
+    return t;
+}
 __device__ void mg_boundary_fill0(MgRun &r, const MgData &d, int m, double *a) {   // mg.F90:735-750
+    if (!mg_touches(d, 0, 6)) return;
     const int n = mgN(d, m), G = n + 2;
     const float rG = 1.0f / (float)G;
     const MgStep s = mg_begin(r, d, m);
@@ -183,6 +192,7 @@ __device__ void mg_boundary_extrap(MgRun &r, const MgData &d, int m, double *a) 
     const int n = mgN(d, m), G = n + 2;
     const float rG = 1.0f / (float)G;
     for (int dir = 0; dir < 3; dir++) {
+        if (!mg_touches(d, 2 * dir, 2 * dir + 2)) continue;
         const MgStep s = mg_begin(r, d, m);
         if (s.on)
             for (int lr = 0; lr < 2; lr++) {
@@ -207,17 +217,37 @@ __device__ __forceinline__ double mg_lap_sum(const double *u, int G, int i, int 
     s = s - 6.0 * u[cidx(G, i, j, k)];
     return s;
 }
+// The same sum on a periodic box, each neighbour read at its periodic image
+// instead of from the ghost layer: the values a wrap of the ghost layer
+// (mg_boundary_u) would have put there, so the sum is the same to the bit.
+// The relaxation and the residual read only these six face neighbours, so
+// on periodic boxes they skip the wrap step (and its barrier) the reference
+// does before each of them; their u ghost layers are then left as they
+// were, and every reader of ghost cells (the prolongation, which also reads
+// edges and corners) wraps its level itself first.
+__device__ __forceinline__ double mg_lap_sum_wrap(const double *u, int G, int n, int i, int j, int k) {
+    const int ip = i + 1 == n ? 0 : i + 1, im = i == 0 ? n - 1 : i - 1;
+    const int jp = j + 1 == n ? 0 : j + 1, jm = j == 0 ? n - 1 : j - 1;
+    const int kp = k + 1 == n ? 0 : k + 1, km = k == 0 ? n - 1 : k - 1;
+    double s = u[cidx(G, ip, j, k)] + u[cidx(G, im, j, k)];
+    s = s + u[cidx(G, i, jp, k)];
+    s = s + u[cidx(G, i, jm, k)];
+    s = s + u[cidx(G, i, j, kp)];
+    s = s + u[cidx(G, i, j, km)];
+    s = s - 6.0 * u[cidx(G, i, j, k)];
+    return s;
+}
 __device__ void mg_resid(MgRun &r, const MgData &d, int m, double *res, double *u, const double *rhs) {   // mg_poisson.F90:5-28
     const int n = mgN(d, m), G = n + 2, ln = __ffs(n) - 1;
     double hh = mgH(d, m);
     double h2i = 1.0 / (hh * hh);
-    mg_boundary_u(r, d, m, u);
     const MgStep s = mg_begin(r, d, m);
     if (s.on)
         for (int c = s.start; c < n * n * n; c += s.stride) {
             int i, j, k;
             mg_ijk(c, n, ln, i, j, k);
-            res[cidx(G, i, j, k)] = -h2i * mg_lap_sum(u, G, i, j, k) + rhs[cidx(G, i, j, k)];
+            const double lap = d.periodic ? mg_lap_sum_wrap(u, G, n, i, j, k) : mg_lap_sum(u, G, i, j, k);
+            res[cidx(G, i, j, k)] = -h2i * lap + rhs[cidx(G, i, j, k)];
         }
     mg_end(s);
 }
@@ -229,7 +259,6 @@ __device__ double mg_relax(MgRun &r, const MgData &d, int m, double *u, const do
     double hh = mgH(d, m), h2 = hh * hh, rm = 0.0;
     const int half = (n * n * n + 1) / 2;
     for (int ipass = 1; ipass <= 2; ipass++) {
-        mg_boundary_u(r, d, m, u);
         const MgStep s = mg_begin(r, d, m);
         if (s.on)
             for (int c = s.start; c < half; c += s.stride) {
@@ -241,7 +270,8 @@ __device__ double mg_relax(MgRun &r, const MgData &d, int m, double *u, const do
                     i2 = c & (hn - 1); j = (c >> lhn) & (n - 1); k = c >> (lhn + __ffs(n) - 1);
                     i = 2 * i2 + ((j + k + ipass) & 1);
                 }
-                double resh2 = mg_lap_sum(u, G, i, j, k) - h2 * rhs[cidx(G, i, j, k)];
+                const double lap = d.periodic ? mg_lap_sum_wrap(u, G, n, i, j, k) : mg_lap_sum(u, G, i, j, k);
+                double resh2 = lap - h2 * rhs[cidx(G, i, j, k)];
                 u[cidx(G, i, j, k)] = u[cidx(G, i, j, k)] + (1.0 / 6.0) * resh2;
                 double a = fabs(resh2);
                 rm = a > rm ? a : rm;
@@ -293,8 +323,10 @@ __device__ void mg_interp(MgRun &r, const MgData &d, int m, double *uf, double *
     }
     mg_boundary_fill0(r, d, m, uf);
     mg_boundary_fill0(r, d, lc, uc);
-    mg_boundary_u(r, d, m, uf);
-    mg_boundary_u(r, d, lc, uc);
+    // the reference wraps uf and uc again here (mg.F90:631-632); uc was
+    // wrapped above and is unchanged, and no later step reads the ghost
+    // layer of uf before wrapping it (relaxation and residual read periodic
+    // images, the next prolongation wraps its coarse level first)
 }
 __device__ void mg_fill0(MgRun &r, const MgData &d, int m, double *a) {
     const int G = mgN(d, m) + 2;
