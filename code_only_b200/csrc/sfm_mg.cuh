@@ -291,7 +291,13 @@ __device__ void mg_rstrct(MgRun &r, const MgData &d, int m, double *uc, const do
         }
     mg_end(s);
 }
-__device__ void mg_interp(MgRun &r, const MgData &d, int m, double *uf, double *uc, bool cubic) {   // mg.F90:608-633
+// add: uf += the prolongation of uc on uf's interior (the reference's
+// mg_interp into a scratch level followed by mg_add: mg_addint, mg.F90:727-731, in one
+// step: each sum is the one mg_add forms; uf's ghost layer is left alone,
+// which is what adding the scratch level's zero-filled (isolated box) or
+// never-read (periodic box) ghost layer does to it)
+__device__ void mg_interp(MgRun &r, const MgData &d, int m, double *uf, double *uc, bool cubic,
+                          bool add = false) {   // mg.F90:608-633
     const int lc = m + 1, n = mgN(d, m), G = n + 2, nc = mgN(d, lc), Gc = nc + 2, ln = __ffs(n) - 1;
     // Lagrange nodes and weights per fine index, evaluated once per call
     __shared__ int tcw[MG_NMAX][4];
@@ -315,18 +321,50 @@ __device__ void mg_interp(MgRun &r, const MgData &d, int m, double *uf, double *
             for (int c = s.start; c < n * n * n; c += s.stride) {
                 int i, j, k;
                 mg_ijk(c, n, ln, i, j, k);
-                uf[cidx(G, i, j, k)] = tri ? tricubic_cell_w(src, Gc, tcw[i], tww[i], tcw[j], tww[j], tcw[k], tww[k])
-                                           : trilinear_cell(src, Gc, i, j, k, 0, 0, 0);
+                const double v = tri ? tricubic_cell_w(src, Gc, tcw[i], tww[i], tcw[j], tww[j], tcw[k], tww[k])
+                                     : trilinear_cell(src, Gc, i, j, k, 0, 0, 0);
+                const int cf = cidx(G, i, j, k);
+                uf[cf] = add ? uf[cf] + v : v;
             }
         }
         mg_end(s);
     }
-    mg_boundary_fill0(r, d, m, uf);
+    if (!add) mg_boundary_fill0(r, d, m, uf);
     mg_boundary_fill0(r, d, lc, uc);
     // the reference wraps uf and uc again here (mg.F90:631-632); uc was
     // wrapped above and is unchanged, and no later step reads the ghost
     // layer of uf before wrapping it (relaxation and residual read periodic
     // images, the next prolongation wraps its coarse level first)
+}
+// The descent step of mg_lin (mg.F90:185-187) in one step on level v + 1: the
+// residual of level v at the eight children of each level-(v+1) cell (the
+// expression of mg_resid), their linear restriction (rstrct_linear's sum and
+// order) into rhsc, and level v + 1's correction uc zeroed.  The fine
+// residual array is not written: nothing reads it before the ascent
+// overwrites it.
+__device__ void mg_resid_rstrct_fill0(MgRun &r, const MgData &d, int v, double *rhsc, const double *u,
+                                      const double *rhs, double *uc) {
+    const int n = mgN(d, v), G = n + 2, nc = mgN(d, v + 1), Gc = nc + 2, lnc = __ffs(nc) - 1;
+    const double hh = mgH(d, v);
+    const double h2i = 1.0 / (hh * hh);
+    auto res = [&](int i, int j, int k) {
+        const double lap = d.periodic ? mg_lap_sum_wrap(u, G, n, i, j, k) : mg_lap_sum(u, G, i, j, k);
+        return -h2i * lap + rhs[cidx(G, i, j, k)];
+    };
+    const MgStep s = mg_begin(r, d, v + 1);
+    if (s.on) {
+        for (int c = s.start; c < nc * nc * nc; c += s.stride) {
+            int i, j, k;
+            mg_ijk(c, nc, lnc, i, j, k);
+            const int i0 = 2 * i, j0 = 2 * j, k0 = 2 * k;
+            rhsc[cidx(Gc, i, j, k)] = (res(i0, j0, k0) + res(i0 + 1, j0, k0) + res(i0, j0 + 1, k0) +
+                                       res(i0, j0, k0 + 1) + res(i0 + 1, j0 + 1, k0) + res(i0 + 1, j0, k0 + 1) +
+                                       res(i0, j0 + 1, k0 + 1) + res(i0 + 1, j0 + 1, k0 + 1)) *
+                                      (1.0 / 8.0);
+        }
+        for (int c = s.start; c < Gc * Gc * Gc; c += s.stride) uc[c] = 0.0;
+    }
+    mg_end(s);
 }
 __device__ void mg_fill0(MgRun &r, const MgData &d, int m, double *a) {
     const int G = mgN(d, m) + 2;
@@ -365,15 +403,12 @@ __device__ double mg_lin(MgRun &r, const MgData &d, double *sh) {
             for (int v = m; v <= d.MMax - 1; v++) {
                 for (int q = 0; q < 2; q++) rm = mg_relax(r, d, v, d.U[v], d.RHS[v]);
                 mr = v;
-                mg_resid(r, d, v, d.RES[v], d.U[v], d.RHS[v]);
-                mg_rstrct(r, d, v + 1, d.RHS[v + 1], d.RES[v]);
-                mg_fill0(r, d, v + 1, d.U[v + 1]);
+                mg_resid_rstrct_fill0(r, d, v, d.RHS[v + 1], d.U[v], d.RHS[v], d.U[v + 1]);
             }
             for (int q = 0; q < 2; q++) rm = mg_relax(r, d, d.MMax, d.U[d.MMax], d.RHS[d.MMax]);
             mr = d.MMax;
             for (int v = d.MMax - 1; v >= m; v--) {
-                mg_interp(r, d, v, d.RES[v], d.U[v + 1], false);
-                mg_addw(r, d, v, d.U[v], d.RES[v]);
+                mg_interp(r, d, v, d.U[v], d.U[v + 1], false, true);   // mg_interp + mg_add
                 for (int q = 0; q < 2; q++) rm = mg_relax(r, d, v, d.U[v], d.RHS[v]);
                 mr = v;
             }

@@ -1146,7 +1146,7 @@ public:
     bool fused_at(int f, int bit = 1) const {
         if (sizeof(T) != 4 || serialRelax || !(sched(kKnobFusedSweep, 0) & bit)) return false;
         bool ok = false;
-        SFM_WITH_N(nf[f], ok = true, ok = false)
+        SFM_WITH_N(nf[f], ok = N > 0, ok = false)
         return ok;
     }
     // full sweeps per fused launch (local_sweeps: 1, or 2 on the staged
