@@ -160,24 +160,90 @@ __device__ __forceinline__ void ghost_copy(T *u, const FaceItem *items, int ncel
         if (src[t] >= 0) u[dst[t]] = val[t];
 }
 
-// One ghost pass of (level, direction): the n0 same-level items0 by flat
-// copy in the first CTAs, the n1 coarse-fine items1
-// (fmg_ghfix_parentlev) by ghost_face in the rest.  The two sets write
-// disjoint ghost cells and read none of the pass direction, so they run
-// side by side.
-template <int N>
-__host__ __device__ constexpr int ghost_copy_ctas(int n0) {
-    return (int)(((int64_t)n0 * (N + 2) * (N + 2) + 256 * ghost_k<N>() - 1) / (256 * ghost_k<N>()));
-}
+// Elements per copy unit of a same-level face in pass `dir`: the y pass
+// copies rows of G contiguous values, the z pass planes of G^2 contiguous
+// values, so both move whole 8- or 16-byte vectors -- the largest power of
+// two up to 16 bytes that divides the row (y) or the plane (z).  Every
+// block starts at a multiple of V = G^3 values and every row or plane at a
+// multiple of G or G^2 values from it, so with a 16-byte aligned field (the
+// host checks) each unit is aligned to its own size.  The x pass (one value
+// per row) stays scalar.
 template <class T, int N>
+__host__ __device__ constexpr int ghost_vec(int dir) {
+    constexpr int G = N + 2, CAP = 16 / (int)sizeof(T);
+    const int len = dir == 1 ? G : (dir == 2 ? G * G : 1);
+    int w = 1;
+    while (2 * w <= CAP && len % (2 * w) == 0) w *= 2;
+    return w;
+}
+template <class T, int W>
+struct GhostVec;
+template <class T>
+struct GhostVec<T, 1> { using type = T; };
+template <>
+struct GhostVec<float, 2> { using type = float2; };
+template <>
+struct GhostVec<float, 4> { using type = float4; };
+template <>
+struct GhostVec<double, 2> { using type = double2; };
+// the flat copy of ghost_copy in units of W values (W > 1: dir 1 or 2)
+template <class T, int N, int W>
+__device__ __forceinline__ void ghost_copy_vec(T *u, const FaceItem *items, int nunit, int dir, int g0, int stride) {
+    using VT = typename GhostVec<T, W>::type;
+    constexpr int G = N + 2, NU = G * G / W, K = ghost_k<N>();
+    constexpr int64_t V = (int64_t)G * G * G;
+    static_assert((G * G) % W == 0 && V % W == 0, "units stay inside a face and blocks stay aligned");
+    const int sd = dir == 1 ? G : G * G;
+    const int sb = dir == 2 ? G : G * G;
+    int64_t src[K], dst[K];
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+        const int g = g0 + t * stride;
+        src[t] = -1;
+        dst[t] = 0;
+        if (g < nunit) {
+            const int fidx = g / NU, c = (g - fidx * NU) * W;
+            const FaceItem fi = items[fidx];
+            const int base = c % G + (c / G) * sb;
+            const bool lo = fi.lr == 0;
+            dst[t] = (int64_t)fi.dst * V + base + (lo ? 0 : N + 1) * sd;
+            src[t] = (int64_t)fi.src * V + base + (lo ? N : 1) * sd;
+        }
+    }
+    VT val[K];
+#pragma unroll
+    for (int t = 0; t < K; t++)
+        if (src[t] >= 0) val[t] = *reinterpret_cast<const VT *>(u + src[t]);
+#pragma unroll
+    for (int t = 0; t < K; t++)
+        if (src[t] >= 0) *reinterpret_cast<VT *>(u + dst[t]) = val[t];
+}
+
+// One ghost pass of (level, direction): the n0 same-level items0 by flat
+// copy in the first CTAs (vectors of `vec` values: ghost_vec, or 1), the n1
+// coarse-fine items1 (fmg_ghfix_parentlev) by ghost_face in the rest.  The
+// two sets write disjoint ghost cells and read none of the pass direction,
+// so they run side by side.
+template <int N>
+__host__ __device__ constexpr int ghost_copy_ctas(int n0, int vec = 1) {
+    return (int)(((int64_t)n0 * ((N + 2) * (N + 2) / vec) + 256 * ghost_k<N>() - 1) / (256 * ghost_k<N>()));
+}
+// W: values per same-level copy unit (1, or ghost_vec<T, N>(dir) for a
+// y or z pass on a 16-byte aligned field); one instantiation per width keeps
+// the scalar x pass at its own register count
+template <class T, int N, int W = 1>
 __global__ void __launch_bounds__(256) k_ghost_faces(T *u, const FaceItem *__restrict__ items0, int n0,
                                                      const FaceItem *__restrict__ items1, int n1, int dir,
                                                      int cubic) {
     pdl_enter();
     constexpr int G = N + 2, NB2 = N / 2, LN = ghost_lanes<N>();
-    const int nb0 = ghost_copy_ctas<N>(n0);
+    const int nb0 = ghost_copy_ctas<N>(n0, W);
     if ((int)blockIdx.x < nb0) {
-        ghost_copy<T, N>(u, items0, n0 * G * G, dir, (int)blockIdx.x * 256 * ghost_k<N>() + (int)threadIdx.x, 256);
+        const int g0 = (int)blockIdx.x * 256 * ghost_k<N>() + (int)threadIdx.x;
+        if constexpr (W > 1)
+            ghost_copy_vec<T, N, W>(u, items0, n0 * (G * G / W), dir, g0, 256);
+        else
+            ghost_copy<T, N>(u, items0, n0 * G * G, dir, g0, 256);
         return;
     }
     __shared__ GhostCubicTable<N> tab;

@@ -1046,6 +1046,20 @@ public:
     void ghostcell_fix(int f, TT *u, bool cubic) {
         for (int L = 0; L < H.nlev; L++) ghost_fill_level(L, f, u, cubic, -1);
     }
+    template <class TT, int N, int W>
+    void ghost_pass_launch_w(TT *u, int64_t o, int64_t n0, int64_t sp, int64_t n1, int dir, bool cubic) {
+        launch_pdl(k_ghost_faces<TT, N, W>,
+                   (unsigned)(ghost_copy_ctas<N>((int)n0, W) +
+                              (n1 + 256 / ghost_lanes<N>() - 1) / (256 / ghost_lanes<N>())),
+                   256, 0, u, d_faces + o, (int)n0, d_faces + sp, (int)n1, dir, cubic ? 1 : 0);
+    }
+    template <class TT, int N>
+    void ghost_pass_launch(TT *u, int64_t o, int64_t n0, int64_t sp, int64_t n1, int dir, bool cubic, bool aligned) {
+        constexpr int WY = ghost_vec<TT, N>(1), WZ = ghost_vec<TT, N>(2);
+        if (aligned && dir == 1) return ghost_pass_launch_w<TT, N, WY>(u, o, n0, sp, n1, dir, cubic);
+        if (aligned && dir == 2) return ghost_pass_launch_w<TT, N, WZ>(u, o, n0, sp, n1, dir, cubic);
+        ghost_pass_launch_w<TT, N, 1>(u, o, n0, sp, n1, dir, cubic);
+    }
     template <class TT>
     void ghost_pass(int L, int f, int dir, TT *u, bool cubic, int sel = -1) {   // parentlev/samelev of (L, dir)
         const int k = L * 3 + dir;
@@ -1055,13 +1069,9 @@ public:
         int GT = nf[f] + 2;
         const int n = nf[f];
         if ((n == 2 || n == 4 || n == 8 || n == 16) && n0 * GT * GT <= INT32_MAX) {
-            SFM_WITH_N(n,
-                       (launch_pdl(k_ghost_faces<TT, N>,
-                                   (unsigned)(ghost_copy_ctas<N>((int)n0) +
-                                              (n1 + 256 / ghost_lanes<N>() - 1) / (256 / ghost_lanes<N>())),
-                                   256, 0, u, d_faces + o, (int)n0, d_faces + sp, (int)n1, dir, cubic ? 1 : 0),
-                        ++launches),
-                       (void)0)
+            // whole-vector copies of y rows and z planes need a 16-byte aligned field
+            const bool aligned = ((uintptr_t)u & 15) == 0;
+            SFM_WITH_N(n, (ghost_pass_launch<TT, N>(u, o, n0, sp, n1, dir, cubic, aligned), ++launches), (void)0)
             return;
         }
         run(OpGhostPass<TT>{u, d_faces + o, nf[f], Gf[f], Vf[f], dir, cubic ? 1 : 0, sel}, c * GT * GT);
