@@ -119,6 +119,19 @@ __global__ void __launch_bounds__(256) k_blocks(Op op, int nblk, int bpc) {
         }
 }
 
+// k_blocks in units of W values (V a multiple of W, arrays 16-byte aligned):
+// one vector access per array and unit instead of W scalar ones
+template <class Op, int W>
+__global__ void __launch_bounds__(256) k_blocks_vec(Op op, int nblk, int bpc) {
+    pdl_enter();
+    const int VU = (int)op.V / W;
+    for (int b0 = blockIdx.x * bpc; b0 < nblk; b0 += gridDim.x * bpc)
+        for (int e = threadIdx.x; e < bpc * VU; e += blockDim.x) {
+            const int q = e / VU, c = e - q * VU;
+            if (b0 + q < nblk) op.template cells<W>((int64_t)op.blocks[b0 + q] * op.V + (int64_t)c * W);
+        }
+}
+
 // Serial reference order for race checks: one thread per listed block
 // applies op to the block's items per_block*q .. per_block*(q+1)-1 in order
 // (the cell order of a single-threaded sweep), max of the results folded
@@ -507,29 +520,103 @@ struct OpH2Abs {
 // block-wise BLAS-1 over listed blocks, whole (G^3) arrays (fmg.F90:847-946,
 // vmg.F90:509-563,682-706)
 // ---------------------------------------------------------------------------
+// W consecutive values as one 8- or 16-byte access (p aligned to W values)
+template <class T, int W>
+struct VecOf;
+template <class T>
+struct VecOf<T, 1> { using type = T; };
+template <>
+struct VecOf<float, 2> { using type = float2; };
+template <>
+struct VecOf<float, 4> { using type = float4; };
+template <>
+struct VecOf<double, 2> { using type = double2; };
+template <class T, int W>
+__device__ __forceinline__ void vec_load(const T *p, T (&v)[W]) {
+    const typename VecOf<T, W>::type x = *reinterpret_cast<const typename VecOf<T, W>::type *>(p);
+    const T *e = reinterpret_cast<const T *>(&x);
+#pragma unroll
+    for (int i = 0; i < W; i++) v[i] = e[i];
+}
+template <class T, int W>
+__device__ __forceinline__ void vec_store(T *p, const T (&v)[W]) {
+    typename VecOf<T, W>::type x;
+    T *e = reinterpret_cast<T *>(&x);
+#pragma unroll
+    for (int i = 0; i < W; i++) e[i] = v[i];
+    *reinterpret_cast<typename VecOf<T, W>::type *>(p) = x;
+}
+__host__ __device__ constexpr int vec_width(int bytes) { return 16 / bytes; }
+inline bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+// Each op also offers cells<W>(c): values c .. c+W-1 (one vector access per
+// array, the same per-value expression), VW its widest W (16 bytes of its
+// largest element type), aligned() whether its arrays allow vectors.
 template <class TO, class TI>
 struct OpCopy {
     TO *o; const TI *a; const int32_t *blocks; int64_t V;
+    static constexpr int VW = vec_width(sizeof(TO) > sizeof(TI) ? sizeof(TO) : sizeof(TI));
     __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
     __device__ void cell(int64_t c) const { o[c] = (TO)a[c]; }
+    template <int W>
+    __device__ void cells(int64_t c) const {
+        TI x[W];
+        TO y[W];
+        vec_load<TI, W>(a + c, x);
+#pragma unroll
+        for (int i = 0; i < W; i++) y[i] = (TO)x[i];
+        vec_store<TO, W>(o + c, y);
+    }
+    bool aligned() const { return aligned16(o) && aligned16(a); }
 };
 template <class TA, class TD>
 struct OpAdd {
     TA *a; const TD *d; const int32_t *blocks; int64_t V;
+    static constexpr int VW = vec_width(sizeof(TA) > sizeof(TD) ? sizeof(TA) : sizeof(TD));
     __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
     __device__ void cell(int64_t c) const { a[c] = a[c] + (TA)d[c]; }
+    template <int W>
+    __device__ void cells(int64_t c) const {
+        TA x[W];
+        TD y[W];
+        vec_load<TA, W>(a + c, x);
+        vec_load<TD, W>(d + c, y);
+#pragma unroll
+        for (int i = 0; i < W; i++) x[i] = x[i] + (TA)y[i];
+        vec_store<TA, W>(a + c, x);
+    }
+    bool aligned() const { return aligned16(a) && aligned16(d); }
 };
 template <class T>
 struct OpSub {
     T *o; const T *a; const T *b_; const int32_t *blocks; int64_t V;
+    static constexpr int VW = vec_width(sizeof(T));
     __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
     __device__ void cell(int64_t c) const { o[c] = a[c] - b_[c]; }
+    template <int W>
+    __device__ void cells(int64_t c) const {
+        T x[W], y[W];
+        vec_load<T, W>(a + c, x);
+        vec_load<T, W>(b_ + c, y);
+#pragma unroll
+        for (int i = 0; i < W; i++) x[i] = x[i] - y[i];
+        vec_store<T, W>(o + c, x);
+    }
+    bool aligned() const { return aligned16(o) && aligned16(a) && aligned16(b_); }
 };
 template <class T>
 struct OpZero {
     T *o; const int32_t *blocks; int64_t V;
+    static constexpr int VW = vec_width(sizeof(T));
     __device__ void operator()(int64_t idx) const { cell((int64_t)blocks[idx / V] * V + idx % V); }
     __device__ void cell(int64_t c) const { o[c] = (T)0; }
+    template <int W>
+    __device__ void cells(int64_t c) const {
+        T x[W];
+#pragma unroll
+        for (int i = 0; i < W; i++) x[i] = (T)0;
+        vec_store<T, W>(o + c, x);
+    }
+    bool aligned() const { return aligned16(o); }
 };
 
 }  // namespace sfm

@@ -1364,9 +1364,16 @@ public:
     template <class Op>
     void runB(const Op &op, int64_t nblk) {
         if (nblk <= 0) return;
-        const int bpc = std::max(1, 256 / (int)op.V);
-        const int64_t g = std::min<int64_t>((nblk + bpc - 1) / bpc, (int64_t)nSM * 16);
-        launch_pdl(k_blocks<Op>, (unsigned)g, 256, 0, op, (int)nblk, bpc);
+        constexpr int W = Op::VW;
+        if (op.V % W == 0 && op.aligned()) {   // whole vectors
+            const int bpc = std::max(1, 256 / (int)(op.V / W));
+            const int64_t g = std::min<int64_t>((nblk + bpc - 1) / bpc, (int64_t)nSM * 16);
+            launch_pdl(k_blocks_vec<Op, W>, (unsigned)g, 256, 0, op, (int)nblk, bpc);
+        } else {
+            const int bpc = std::max(1, 256 / (int)op.V);
+            const int64_t g = std::min<int64_t>((nblk + bpc - 1) / bpc, (int64_t)nSM * 16);
+            launch_pdl(k_blocks<Op>, (unsigned)g, 256, 0, op, (int)nblk, bpc);
+        }
         ++launches;
     }
     void fill0(int f, T *u) { runB(OpZero<T>{u, d_leaves, Vf[f]}, nLeaves); }
