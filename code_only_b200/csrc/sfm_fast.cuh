@@ -989,9 +989,8 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
         // fused sweeps: cell t = ct + x NCT of each tile's colour-1 cells
         // (and its x neighbour, the colour-2 cell of t) for x < ITER
         constexpr int ITER = SW > 0 ? (BPC * HALF + NCT - 1) / NCT : 1;
-        // block, in-block offset of the colour-1 cell and the step to its
-        // x neighbour, recomputed where used (held across the tile loop
-        // they cost registers the 7-CTA occupancy does not have)
+        // block, in-block coordinates of the colour-1 cell and the step to
+        // its x neighbour
         auto cell_of = [&](int x, int &q, int &i1, int &j, int &k, int &d1) {
             const int t = ct + x * NCT;
             q = t / HALF;
@@ -1004,6 +1003,8 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
             i1 = 2 * i2 + p1;
             d1 = 1 - 2 * p1;
         };
+        // (recomputed where used: held across the tile loop they cost
+        // registers the 7-CTA occupancy does not have)
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
             const int s = it % S;
             const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)((it / S) & 1), cpolls));
@@ -1103,8 +1104,7 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                         else own2[x] = v;
                         if (store) u[gb[x] + c] = v;
                         if (keep) ub[c] = v;
-                        const T a = resh2 < (T)0 ? -resh2 : resh2;
-                        mt = a > mt ? a : mt;
+                        mt = fmax(mt, fabs(resh2));
                     }
                 };
                 if (got) fused_colour(1, true, true, SW == 1);
