@@ -25,6 +25,7 @@ GPU results' error against the oracle (phi_rel_err_vs_oracle).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -303,20 +304,22 @@ def run_ours(args):
                 s.solve(rho_h, psi_h)
             barrier(info)
             t_sum = 0.0
+            st_e = abi.SfmStats()
             for _ in range(args.steps):
                 psi_h[...] = 0.0   # the caller's cold start, outside the call
                 t0 = time.perf_counter()
-                out = s.lib.sfm_solve(s.ctx, rho_h.ctypes.data, psi_h.ctypes.data, g_h.ctypes.data, None)
+                out = s.lib.sfm_solve(s.ctx, rho_h.ctypes.data, psi_h.ctypes.data, g_h.ctypes.data,
+                                      ctypes.byref(st_e))
                 t_sum += time.perf_counter() - t0
                 if out not in (abi.SFM_OK, abi.SFM_ENOTCONVERGED):
                     raise RuntimeError(f"sfm_solve failed {out}")
             barrier(info)
             ms_e2e = max_over_ranks(t_sum * 1e3 / args.steps, info)
-            nbytes = rho.nbytes
-            g_int = h.nblocks * 3 * h.ni ** 3 * 8   # g leaves the device as block interiors
+            # bytes the call moved, as it reports them: the (-1:ni)^3 region of
+            # rho and psi in, of psi out, and g's block interiors out
             e2e = {"value": world * 1e3 / ms_e2e, "unit": "solves/s",
-                   "h2d_bytes_per_step": 2 * nbytes,          # rho, psi (warm start)
-                   "d2h_bytes_per_step": nbytes + g_int,      # psi, g interiors
+                   "h2d_bytes_per_step": int(st_e.h2d_bytes),
+                   "d2h_bytes_per_step": int(st_e.d2h_bytes),
                    "timing": "host wall clock around each blocking sfm_solve call (pinned host arrays)"}
     if rank != 0:
         from code_only_b200 import replicas

@@ -67,6 +67,7 @@ class SfmStats(C.Structure):
         ("rho_mean", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64),
         ("smoother_ms", C.c_double), ("smoother_launches", C.c_int64), ("smoother_cells", C.c_int64),
         ("elem_bytes", C.c_int32), ("smoother_colours", C.c_int32),
+        ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
     ]
 
     def history(self):

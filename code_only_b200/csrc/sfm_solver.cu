@@ -19,6 +19,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -229,6 +230,10 @@ public:
     // layers) instead of the caller's layout: the host-array entry point
     // stages g this way
     bool gCompact = false;
+    // io ghost width of rho and psi for this call (0: params.ngh_io); the
+    // host-array entry point stages only the (-1:ni)^3 region the solve
+    // reads and writes, a width of 1
+    int ioGw = 0;
 };
 
 template <class T>
@@ -1590,7 +1595,7 @@ public:
         st_ = s ? s : own_;   // all work of this call is ordered on the caller's stream
         launches = 0;
         prof_init();
-        const int nb = H.nb, gw = P.ngh_io;
+        const int nb = H.nb, gw = ioGw > 0 ? ioGw : P.ngh_io;
         cudaEventRecord(ev0, st_);
         // fresh, zero-filled arrays as fmg_alloc_arr gives (fmg_data.F90:393)
         for (auto &z : zeroList) cudaMemsetAsync(z.first, 0, z.second, st_);
@@ -1941,11 +1946,17 @@ struct sfm_ctx {
     sfm::SolverBase *s = nullptr;
     sfm_params p;
     int device = 0, nb = 0, ni = 0, ngh = 0;
-    double *d_rho = nullptr, *d_psi = nullptr;   // staging for host calls
+    // host calls: rho and psi staged as the (-1:ni)^3 region of every block
+    // ((ni+2)^3 values), on the device and in host buffers (pinned when the
+    // driver grants it)
+    double *d_rho = nullptr, *d_psi = nullptr;
+    double *h_rho = nullptr, *h_psi = nullptr;
+    bool h_pinned = false;
     double *d_gc = nullptr, *h_gc = nullptr;     // g interiors, device and pinned host staging
-    cudaStream_t cs = nullptr;                   // device-to-host copies of the outputs
-    static constexpr int kGChunks = 8;           // g leaves in chunks, each scattered as it lands
-    cudaEvent_t gev[kGChunks] = {};
+    cudaStream_t cs = nullptr;                   // the host call's copies and solve
+    static constexpr int kGChunks = 8;           // arrays move in chunks, each gathered or scattered
+    cudaEvent_t gev[kGChunks] = {};              // while the others are in flight
+    cudaEvent_t pev[kGChunks] = {};
     std::string err;
 };
 
@@ -2063,8 +2074,10 @@ int sfm_create(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **out) {
     return sfm_guard([&] { return create_impl(h, p, out); });
 }
 
-static int64_t io_elems(const sfm_ctx *c) {
-    int64_t G = c->ni + 2 * c->ngh;
+// values of the (-1:ni)^3 region of every block: what the host-array entry
+// point moves for rho and psi
+static int64_t stage_elems(const sfm_ctx *c) {
+    int64_t G = c->ni + 2;
     return (int64_t)c->nb * G * G * G;
 }
 
@@ -2077,83 +2090,167 @@ int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g
     return sfm_guard([&] { return c->s->solve(d_rho, d_psi, d_g, st, (cudaStream_t)stream, 0, nullptr); });
 }
 
-// rows [row0, row1) of the g interiors [nblocks][3][ni^3] (a row = ni
-// values) into the caller's [nblocks][3][(ni+2g)^3], on up to 16 host
-// threads; the io ghost layers of the caller's array are not touched
-static void scatter_g_interiors(const double *src, double *g, int64_t row0, int64_t row1, int n, int gw) {
-    const int Gi = n + 2 * gw;
-    const int64_t Vi = (int64_t)Gi * Gi * Gi, rows = row1 - row0;
-    auto work = [=](int64_t r0, int64_t r1) {
-        r0 += row0;
-        r1 += row0;
-        for (int64_t r = r0; r < r1; r++) {
-            const int64_t bc = r / ((int64_t)n * n);
-            const int kj = (int)(r - bc * n * n), k = kj / n, j = kj - k * n;
-            std::memcpy(g + bc * Vi + ((int64_t)(k + gw) * Gi + (j + gw)) * Gi + gw, src + r * n,
-                        (size_t)n * sizeof(double));
-        }
-    };
-    const int64_t per = (int64_t)1 << 16;   // rows per thread at least
+}  // extern "C"
+
+// fn(r0, r1) over rows [0, rows) on up to 16 host threads (at least 2^16
+// rows each); whatever no thread can be had for runs on this one
+template <class F>
+static void host_rows(int64_t rows, const F &fn) {
+    const int64_t per = (int64_t)1 << 16;
     const int nt = (int)std::max<int64_t>(1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(),
                                                                   rows / per}));
     std::vector<std::thread> th;
     int t = 1;
     try {
-        for (; t < nt; t++) th.emplace_back(work, rows * t / nt, rows * (t + 1) / nt);
+        for (; t < nt; t++) th.emplace_back(fn, rows * t / nt, rows * (t + 1) / nt);
     } catch (...) {   // no thread to be had: the rest on this one (nothing may leave the C ABI)
-        work(rows * t / nt, rows);
+        fn(rows * t / nt, rows);
     }
-    work(0, rows / nt);
+    fn(0, rows / nt);
     for (auto &x : th) x.join();
 }
 
-static int solve_impl(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
-    if (!c || !c->s || !rho) return SFM_EINVAL;
-    DeviceGuard dg(c->device);
-    int64_t n = io_elems(c);
-    size_t bytes = (size_t)n * sizeof(double);
-    const size_t gbytes = (size_t)c->nb * 3 * c->ni * c->ni * c->ni * sizeof(double);
+extern "C" {
+
+// rows [row0, row1) of the g interiors [nblocks][3][ni^3] (a row = ni
+// values) into the caller's [nblocks][3][(ni+2g)^3]; the io ghost layers of
+// the caller's array are not touched
+static void scatter_g_interiors(const double *src, double *g, int64_t row0, int64_t row1, int n, int gw) {
+    const int Gi = n + 2 * gw;
+    const int64_t Vi = (int64_t)Gi * Gi * Gi;
+    host_rows(row1 - row0, [=](int64_t r0, int64_t r1) {
+        for (int64_t r = row0 + r0; r < row0 + r1; r++) {
+            const int64_t bc = r / ((int64_t)n * n);
+            const int kj = (int)(r - bc * n * n), k = kj / n, j = kj - k * n;
+            std::memcpy(g + bc * Vi + ((int64_t)(k + gw) * Gi + (j + gw)) * Gi + gw, src + r * n,
+                        (size_t)n * sizeof(double));
+        }
+    });
+}
+
+// rows [row0, row1) of the (-1:ni)^3 regions [nblocks][(ni+2)^3] (a row =
+// ni+2 values) between the staging buffer and the caller's
+// [nblocks][(ni+2g)^3]: gather (to_stage) or scatter; the caller's outer
+// ghost layers (g >= 2) are never touched
+static void stage_rows(double *stage, double *io, int64_t row0, int64_t row1, int n, int gw, bool to_stage) {
+    const int Gc = n + 2, Gi = n + 2 * gw;
+    const int64_t Vi = (int64_t)Gi * Gi * Gi;
+    host_rows(row1 - row0, [=](int64_t r0, int64_t r1) {
+        for (int64_t r = row0 + r0; r < row0 + r1; r++) {
+            const int64_t b = r / ((int64_t)Gc * Gc);
+            const int kj = (int)(r - b * Gc * Gc), k = kj / Gc, j = kj - k * Gc;
+            double *o = io + b * Vi + ((int64_t)(k + gw - 1) * Gi + (j + gw - 1)) * Gi + (gw - 1);
+            if (to_stage) std::memcpy(stage + r * Gc, o, (size_t)Gc * sizeof(double));
+            else std::memcpy(o, stage + r * Gc, (size_t)Gc * sizeof(double));
+        }
+    });
+}
+
+static int stage_alloc(sfm_ctx *c, bool with_g) {
+    const size_t bytes = (size_t)stage_elems(c) * sizeof(double);
     if (!c->d_rho) {
         if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess)
             return SFM_ENOMEM;
+        c->h_pinned = cudaMallocHost(&c->h_rho, bytes) == cudaSuccess &&
+                      cudaMallocHost(&c->h_psi, bytes) == cudaSuccess;
+        if (!c->h_pinned) {   // ordinary host memory: the copies still work, without overlap
+            cudaGetLastError();
+            if (c->h_rho) cudaFreeHost(c->h_rho);
+            c->h_rho = static_cast<double *>(std::malloc(bytes));
+            c->h_psi = static_cast<double *>(std::malloc(bytes));
+            if (!c->h_rho || !c->h_psi) return SFM_ENOMEM;
+        }
     }
-    if (g && !c->d_gc) {
+    if (!c->cs) {
+        if (cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking) != cudaSuccess) return SFM_ECUDA;
+        for (auto *ev : {c->gev, c->pev})
+            for (int q = 0; q < sfm_ctx::kGChunks; q++)
+                if (cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming) != cudaSuccess) return SFM_ECUDA;
+    }
+    if (with_g && !c->d_gc) {
+        const size_t gbytes = (size_t)c->nb * 3 * c->ni * c->ni * c->ni * sizeof(double);
         if (cudaMalloc(&c->d_gc, gbytes) != cudaSuccess) return SFM_ENOMEM;
         if (cudaMallocHost(&c->h_gc, gbytes) != cudaSuccess) {
             c->h_gc = nullptr;
             return SFM_ENOMEM;
         }
     }
-    if (cudaMemcpy(c->d_rho, rho, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA;
-    if (psi) { if (cudaMemcpy(c->d_psi, psi, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA; }
+    return SFM_OK;
+}
+
+// The host-array call moves only what the solve uses: the (-1:ni)^3 region
+// of rho and psi in ((ni+2)^3 of the (ni+2g)^3 values per block), that
+// region of psi out, and g's interiors out.  Each array goes in chunks: the
+// host threads gather chunk q+1 while chunk q is on the link, and scatter
+// an output chunk as soon as it has landed.  Copies and solve are ordered
+// on the context's copy stream.
+static int solve_impl(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st) {
+    if (!c || !c->s || !rho) return SFM_EINVAL;
+    DeviceGuard dg(c->device);
+    int rc = stage_alloc(c, g != nullptr);
+    if (rc) return rc;
+    const int Gc = c->ni + 2, K = sfm_ctx::kGChunks;
+    const int64_t rows = (int64_t)c->nb * Gc * Gc;
+    auto chunk = [&](int64_t total, int q, int64_t &r0, int64_t &r1) {
+        r0 = total * q / K;
+        r1 = total * (q + 1) / K;
+    };
+    for (int q = 0; q < K; q++) {
+        int64_t r0, r1;
+        chunk(rows, q, r0, r1);
+        const size_t off = (size_t)r0 * Gc, len = (size_t)(r1 - r0) * Gc * sizeof(double);
+        stage_rows(c->h_rho, const_cast<double *>(rho), r0, r1, c->ni, c->ngh, true);
+        if (cudaMemcpyAsync(c->d_rho + off, c->h_rho + off, len, cudaMemcpyHostToDevice, c->cs) != cudaSuccess)
+            return SFM_ECUDA;
+        if (psi) {
+            stage_rows(c->h_psi, psi, r0, r1, c->ni, c->ngh, true);
+            if (cudaMemcpyAsync(c->d_psi + off, c->h_psi + off, len, cudaMemcpyHostToDevice, c->cs) != cudaSuccess)
+                return SFM_ECUDA;
+        }
+    }
     // g: the solve writes block interiors only, staged compact on the device
     // and scattered into the caller's array on the host -- its io ghost
     // layers keep the caller's values without a copy in
     c->s->gCompact = true;
-    int rc = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, g ? c->d_gc : nullptr, st, nullptr, 0, nullptr);
+    c->s->ioGw = 1;
+    rc = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, g ? c->d_gc : nullptr, st, c->cs, 0, nullptr);
     c->s->gCompact = false;
+    c->s->ioGw = 0;
     if (rc != SFM_OK && rc != SFM_ENOTCONVERGED) return rc;
-    if (psi && cudaMemcpy(psi, c->d_psi, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return SFM_ECUDA;
-    if (g) {
-        // chunk q is scattered on the host while chunks q+1.. are in flight
-        if (!c->cs) {
-            if (cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking) != cudaSuccess) return SFM_ECUDA;
-            for (auto &e : c->gev)
-                if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return SFM_ECUDA;
-        }
-        const int64_t rows = (int64_t)c->nb * 3 * c->ni * c->ni;
-        for (int q = 0; q < sfm_ctx::kGChunks; q++) {
-            const int64_t r0 = rows * q / sfm_ctx::kGChunks, r1 = rows * (q + 1) / sfm_ctx::kGChunks;
-            if (cudaMemcpyAsync(c->h_gc + r0 * c->ni, c->d_gc + r0 * c->ni, (size_t)(r1 - r0) * c->ni * sizeof(double),
-                                cudaMemcpyDeviceToHost, c->cs) != cudaSuccess ||
-                cudaEventRecord(c->gev[q], c->cs) != cudaSuccess)
-                return SFM_ECUDA;
-        }
-        for (int q = 0; q < sfm_ctx::kGChunks; q++) {
-            const int64_t r0 = rows * q / sfm_ctx::kGChunks, r1 = rows * (q + 1) / sfm_ctx::kGChunks;
-            if (cudaEventSynchronize(c->gev[q]) != cudaSuccess) return SFM_ECUDA;
-            scatter_g_interiors(c->h_gc, g, r0, r1, c->ni, c->ngh);
-        }
+    const int64_t grows = (int64_t)c->nb * 3 * c->ni * c->ni;
+    // every output chunk is queued before the first is scattered
+    for (int q = 0; q < K && psi; q++) {
+        int64_t r0, r1;
+        chunk(rows, q, r0, r1);
+        const size_t off = (size_t)r0 * Gc, len = (size_t)(r1 - r0) * Gc * sizeof(double);
+        if (cudaMemcpyAsync(c->h_psi + off, c->d_psi + off, len, cudaMemcpyDeviceToHost, c->cs) != cudaSuccess ||
+            cudaEventRecord(c->pev[q], c->cs) != cudaSuccess)
+            return SFM_ECUDA;
+    }
+    for (int q = 0; q < K && g; q++) {
+        int64_t r0, r1;
+        chunk(grows, q, r0, r1);
+        if (cudaMemcpyAsync(c->h_gc + r0 * c->ni, c->d_gc + r0 * c->ni, (size_t)(r1 - r0) * c->ni * sizeof(double),
+                            cudaMemcpyDeviceToHost, c->cs) != cudaSuccess ||
+            cudaEventRecord(c->gev[q], c->cs) != cudaSuccess)
+            return SFM_ECUDA;
+    }
+    for (int q = 0; q < K && psi; q++) {
+        int64_t r0, r1;
+        chunk(rows, q, r0, r1);
+        if (cudaEventSynchronize(c->pev[q]) != cudaSuccess) return SFM_ECUDA;
+        stage_rows(c->h_psi, psi, r0, r1, c->ni, c->ngh, false);
+    }
+    for (int q = 0; q < K && g; q++) {
+        int64_t r0, r1;
+        chunk(grows, q, r0, r1);
+        if (cudaEventSynchronize(c->gev[q]) != cudaSuccess) return SFM_ECUDA;
+        scatter_g_interiors(c->h_gc, g, r0, r1, c->ni, c->ngh);
+    }
+    if (st) {
+        const int64_t sb = stage_elems(c) * (int64_t)sizeof(double);
+        st->h2d_bytes = sb * (psi ? 2 : 1);
+        st->d2h_bytes = (psi ? sb : 0) + (g ? grows * c->ni * (int64_t)sizeof(double) : 0);
     }
     return rc;
 }
@@ -2173,10 +2270,18 @@ void sfm_destroy(sfm_ctx *c) {
     DeviceGuard dg(c->device);
     if (c->d_rho) cudaFree(c->d_rho);
     if (c->d_psi) cudaFree(c->d_psi);
+    if (c->h_pinned) {
+        cudaFreeHost(c->h_rho);
+        cudaFreeHost(c->h_psi);
+    } else {
+        std::free(c->h_rho);
+        std::free(c->h_psi);
+    }
     if (c->d_gc) cudaFree(c->d_gc);
     if (c->h_gc) cudaFreeHost(c->h_gc);
-    for (auto e : c->gev)
-        if (e) cudaEventDestroy(e);
+    for (auto *ev : {c->gev, c->pev})
+        for (int q = 0; q < sfm_ctx::kGChunks; q++)
+            if (ev[q]) cudaEventDestroy(ev[q]);
     if (c->cs) cudaStreamDestroy(c->cs);
     delete c->s;
     delete c;
@@ -2282,19 +2387,25 @@ int sfm_debug_set_ghost_merge(sfm_ctx *c, int on) {
 int sfm_debug_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *st, int stop_stage,
                     double *dump) {
     if (!c || !c->s || !rho) return SFM_EINVAL;
-    DeviceGuard dg(c->device);
-    int64_t n = io_elems(c);
-    size_t bytes = (size_t)n * sizeof(double);
     if (stop_stage == 0) return sfm_solve(c, rho, psi, g, st);
-    if (!c->d_rho) {
-        if (cudaMalloc(&c->d_rho, bytes) != cudaSuccess || cudaMalloc(&c->d_psi, bytes) != cudaSuccess)
-            return SFM_ENOMEM;
+    DeviceGuard dg(c->device);
+    int rc = stage_alloc(c, false);
+    if (rc) return rc;
+    const int64_t rows = (int64_t)c->nb * (c->ni + 2) * (c->ni + 2);
+    const size_t bytes = (size_t)stage_elems(c) * sizeof(double);
+    stage_rows(c->h_rho, const_cast<double *>(rho), 0, rows, c->ni, c->ngh, true);
+    if (cudaMemcpy(c->d_rho, c->h_rho, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA;
+    if (psi) {
+        stage_rows(c->h_psi, psi, 0, rows, c->ni, c->ngh, true);
+        if (cudaMemcpy(c->d_psi, c->h_psi, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return SFM_ECUDA;
     }
-    cudaMemcpy(c->d_rho, rho, bytes, cudaMemcpyHostToDevice);
-    if (psi) cudaMemcpy(c->d_psi, psi, bytes, cudaMemcpyHostToDevice);
     (void)g;   // an early stop writes no g
-    return sfm_guard(
-        [&] { return c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, nullptr, st, nullptr, stop_stage, dump); });
+    return sfm_guard([&] {
+        c->s->ioGw = 1;
+        const int r = c->s->solve(c->d_rho, psi ? c->d_psi : nullptr, nullptr, st, nullptr, stop_stage, dump);
+        c->s->ioGw = 0;
+        return r;
+    });
 }
 
 }  // extern "C"

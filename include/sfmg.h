@@ -123,6 +123,9 @@ typedef struct sfm_stats {
     int32_t smoother_colours;    /* red-black colours per timed launch: 1, or
                                     2 x the local sweeps when the mixed
                                     schedule fuses them                       */
+    int64_t h2d_bytes;           /* sfm_solve: bytes copied host to device    */
+    int64_t d2h_bytes;           /* sfm_solve: bytes copied device to host
+                                    (0 for the device-array call)             */
 } sfm_stats;
 
 typedef struct sfm_ctx sfm_ctx;

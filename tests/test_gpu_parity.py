@@ -167,6 +167,39 @@ def test_host_g_writes_interiors_only():
     assert np.array_equal(psi, psi_d.cpu().numpy())
 
 
+def test_host_arrays_move_only_the_solved_region():
+    """sfm_solve reads rho and psi on (-1:ni)^3 and writes psi there: the
+    outer io ghost layer of rho may hold anything (NaN here) and psi's keeps
+    the caller's values; the result equals the device-array call's, and the
+    call reports the bytes it moved ((ni+2)^3 values per block for rho and
+    psi each way, g's interiors out)."""
+    import torch
+    h = w.small_periodic(2, 8, 3, 1)
+    p = abi.default_params(abi.SFM_BC_PERIODIC)
+    assert p.ngh_io == 2
+    rho = w.block_field(h, p.ngh_io, w.gaussian_peak)
+    G, n = rho.shape[1], h.ni
+    inner = np.zeros((G, G, G), dtype=bool)
+    inner[1:G - 1, 1:G - 1, 1:G - 1] = True          # (-1:ni)^3
+    rho_h = rho.copy()
+    rho_h[:, ~inner] = np.nan
+    psi_h = np.zeros_like(rho)
+    psi_h[:, ~inner] = 777.0
+    with FMGPoisson(h, params=p) as s:
+        st = abi.SfmStats()
+        rc = s.lib.sfm_solve(s.ctx, rho_h.ctypes.data, psi_h.ctypes.data, None, C.byref(st))
+        assert rc == abi.SFM_OK
+        rho_d = torch.from_numpy(rho).cuda()
+        psi_d = torch.zeros_like(rho_d)
+        s.solve_device(rho_d.data_ptr(), psi_d.data_ptr(), None)
+        torch.cuda.synchronize()
+        psi_dev = psi_d.cpu().numpy()
+    assert np.all(psi_h[:, ~inner] == 777.0)
+    assert np.array_equal(psi_h[:, inner], psi_dev[:, inner])
+    staged = h.nblocks * (n + 2) ** 3 * 8
+    assert st.h2d_bytes == 2 * staged and st.d2h_bytes == staged
+
+
 def test_solve_device_rejects_host_pointers():
     """sfm_solve_device checks that every array is device memory of the
     context's device before it launches anything, and leaves the caller's
