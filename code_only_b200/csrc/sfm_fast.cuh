@@ -1052,7 +1052,11 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                 //   resh2 = (sum over faces of (u_nb - u_c)) (hi hh) - rhs hh^2
                 // with explicit fused multiply-adds (hi hh = 1 up to
                 // rounding); reflux blocks keep the reference's flux form.
-                T own1[ITER], own2[ITER], th[ITER], ti[ITER];
+                // rhs of this thread's two cells, read from the stage once per
+                // launch when the launch does more than one sweep (with one
+                // cell per colour: more would cost registers the occupancy
+                // does not have)
+                T own1[ITER], own2[ITER], th[ITER], ti[ITER], rr1[ITER], rr2[ITER];
                 bool flux[ITER], live[ITER];
                 int64_t gb[ITER];
 #pragma unroll
@@ -1066,6 +1070,7 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                         gb[x] = (int64_t)bid[slot][q] * V;
                     }
                 }
+                bool have_rr2 = false;   // rr2 holds the colour-2 rhs (after the first colour-2 pass)
                 auto fused_colour = [&](int pass, bool first_colour, bool keep, bool store) {
 #pragma unroll
                     for (int x = 0; x < ITER; x++) {
@@ -1076,7 +1081,18 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                         const int i = pass == 1 ? i1 : i1 + d1;
                         const int c = cidx(G, i, j, k);
                         T *ub = ut + q * V;
-                        const T rr = rt[q * V + c];
+                        T rr;
+                        if constexpr (SW > 1 && ITER == 1) {
+                            if (first_colour || (pass == 2 && !have_rr2)) {
+                                rr = rt[q * V + c];
+                                if (pass == 1) rr1[x] = rr;
+                                else rr2[x] = rr;
+                            } else {
+                                rr = pass == 1 ? rr1[x] : rr2[x];
+                            }
+                        } else {
+                            rr = rt[q * V + c];
+                        }
                         T uc, resh2;
                         if (flux[x]) {
                             TileFlux<T, N> F{ub, ti[x], ssl[slot][q], rbuf};
@@ -1123,6 +1139,7 @@ __global__ void __launch_bounds__(NT, relax_bulk_min_ctas<T, N, NT>())
                         asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
                     }
                     fused_colour(2, false, !last, last);
+                    have_rr2 = true;
                     if (!last) asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
                 }
                 // the stage held ordinary stores; the next bulk copy into it
