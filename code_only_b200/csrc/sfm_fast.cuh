@@ -1237,10 +1237,14 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
     // cubic_weights evaluated once per CTA instead of once per staged value
     __shared__ int cwc[N][4];
     __shared__ double cww[N][4];
+    __shared__ T cwt[N][4];   // the weights rounded to T once (each use rounds them the same way)
     const int q0 = blockIdx.x * IB;
     const int nq = nblk - q0 < IB ? nblk - q0 : IB;
     if ((int)threadIdx.x < nq) sb[threadIdx.x] = blocks[q0 + threadIdx.x];
-    if (threadIdx.x < N) cubic_weights((int)threadIdx.x, -1, NC, cwc[threadIdx.x], cww[threadIdx.x]);
+    if (threadIdx.x < N) {
+        cubic_weights((int)threadIdx.x, -1, NC, cwc[threadIdx.x], cww[threadIdx.x]);
+        for (int e = 0; e < 4; e++) cwt[threadIdx.x][e] = (T)cww[threadIdx.x][e];
+    }
     __syncthreads();
     for (int t = threadIdx.x; t < nq * VC; t += blockDim.x) {
         const int q = t / VC;
@@ -1260,9 +1264,9 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
         const int q = t / BX, r = t - q * BX;
         const int i = r % N, jc = (r / N) % W - 1, kc = r / (N * W) - 1;
         const int *c = cwc[i];
-        const double *w = cww[i];
+        const T *w = cwt[i];
         const T *row = sc + q * VC + cidx(GC, 0, jc, kc);
-        bx[t] = (T)w[0] * row[c[0]] + (T)w[1] * row[c[1]] + (T)w[2] * row[c[2]] + (T)w[3] * row[c[3]];
+        bx[t] = w[0] * row[c[0]] + w[1] * row[c[1]] + w[2] * row[c[2]] + w[3] * row[c[3]];
     }
     __syncthreads();
     // y: bxy(i, j, kc)
@@ -1270,10 +1274,10 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
         const int q = t / BXY, r = t - q * BXY;
         const int i = r % N, j = (r / N) % N, kc = r / (N * N) - 1;
         const int *c = cwc[j];
-        const double *w = cww[j];
+        const T *w = cwt[j];
         const T *bq = bx + q * BX;
         auto X = [&](int jc) { return bq[((kc + 1) * W + (jc + 1)) * N + i]; };
-        bxy[t] = (T)w[0] * X(c[0]) + (T)w[1] * X(c[1]) + (T)w[2] * X(c[2]) + (T)w[3] * X(c[3]);
+        bxy[t] = w[0] * X(c[0]) + w[1] * X(c[1]) + w[2] * X(c[2]) + w[3] * X(c[3]);
     }
     __syncthreads();
     // z
@@ -1281,11 +1285,10 @@ __global__ void __launch_bounds__(256) k_interp_tiled(T *__restrict__ uf, const 
         const int q = t / NF, r = t - q * NF;
         const int i = r % N, j = (r / N) % N, k = r / (N * N);
         const int *c = cwc[k];
-        const double *w = cww[k];
+        const T *w = cwt[k];
         const T *bq = bxy + q * BXY;
         auto Y = [&](int kc) { return bq[((kc + 1) * N + j) * N + i]; };
-        uf[(int64_t)sb[q] * VF + cidx(GF, i, j, k)] =
-            (T)w[0] * Y(c[0]) + (T)w[1] * Y(c[1]) + (T)w[2] * Y(c[2]) + (T)w[3] * Y(c[3]);
+        uf[(int64_t)sb[q] * VF + cidx(GF, i, j, k)] = w[0] * Y(c[0]) + w[1] * Y(c[1]) + w[2] * Y(c[2]) + w[3] * Y(c[3]);
     }
 }
 
