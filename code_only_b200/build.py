@@ -24,6 +24,7 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-std=c++17", "--fmad=false", "-lineinfo",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+    "-Xcompiler", "-fopenmp", "-lgomp",   # host threads of the host-array call's staging
     "-shared",
 ]
 

@@ -14,6 +14,7 @@
 // accumulation into phi, the reflux flux sums and the base-grid solve in FP64.
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <array>
@@ -289,7 +290,7 @@ public:
     int *d_err = nullptr;                  // set by a device wait that gave up
     uint32_t waitPolls = kWaitPolls;       // poll limit of the smoother's stage waits (tests lower it)
     int nSM = 148;
-    int bulkGrid[5][4][3] = {};            // persistent CTAs of k_relax_bulk<T, N, NT, SW>, by log2(N), NT, SW
+    int bulkGrid[5][4][4] = {};            // persistent CTAs of k_relax_bulk<T, N, NT, SW>, by log2(N), NT, SW
     double *d_mom = nullptr, *d_part = nullptr, *d_psum = nullptr;
     int *d_mgit = nullptr;
     // base grid
@@ -526,7 +527,7 @@ public:
         };
         struct Knob { int knob; int ref; std::vector<int> vals; };
         const Knob ks[] = {{kKnobFusedSweep, 0, {0, 1, 2, 3}},
-                           {kKnobLocalSweeps, 1, {1, 2}},
+                           {kKnobLocalSweeps, 1, {1, 2, 3}},
                            {kKnobBaseCorr, 10, {10, 4, 2, 1}},
                            {kKnobFmgCycles, 2, {2, 1}},
                            {kKnobFmgSweeps, 2, {2, 1, 3}},
@@ -1164,7 +1165,7 @@ public:
         SFM_WITH_N(nf[f], ok = N > 0, ok = false)
         return ok;
     }
-    // full sweeps per fused launch (local_sweeps: 1, or 2 on the staged
+    // full sweeps per fused launch (local_sweeps: 1, or 2 or 3 on the staged
     // block between ghost refreshes)
     int local_sweeps() const { return sched(kKnobLocalSweeps, 1); }
     // persistent grid of k_relax_bulk<T, N> (N >= 4): every SM filled to the
@@ -1216,6 +1217,7 @@ public:
         if constexpr (sizeof(T) == 4) {
             bulk_grids_of<N, 1>();
             bulk_grids_of<N, 2>();
+            bulk_grids_of<N, 3>();
         }
     }
     template <int N, int NT, int SW>
@@ -1248,6 +1250,7 @@ public:
             if constexpr (sizeof(T) == 4) {   // the FP64 path always runs the reference's two colour launches
                 if (sw == 1) return relax_bulk_nt<N, 1>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
                 if (sw == 2) return relax_bulk_nt<N, 2>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
+                if (sw == 3) return relax_bulk_nt<N, 3>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
             }
             relax_bulk_nt<N, 0>(nt, u, rhs, blocks, nblk, rslot, rb, f, ipass, out);
         } else {
@@ -2093,21 +2096,35 @@ int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g
 }  // extern "C"
 
 // fn(r0, r1) over rows [0, rows) on up to 16 host threads (at least 2^16
-// rows each); whatever no thread can be had for runs on this one
+// rows each), an OpenMP team that stays alive between calls
 template <class F>
 static void host_rows(int64_t rows, const F &fn) {
     const int64_t per = (int64_t)1 << 16;
-    const int nt = (int)std::max<int64_t>(1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(),
-                                                                  rows / per}));
-    std::vector<std::thread> th;
-    int t = 1;
-    try {
-        for (; t < nt; t++) th.emplace_back(fn, rows * t / nt, rows * (t + 1) / nt);
-    } catch (...) {   // no thread to be had: the rest on this one (nothing may leave the C ABI)
-        fn(rows * t / nt, rows);
+    const int nt = (int)std::max<int64_t>(1, std::min<int64_t>({16, (int64_t)omp_get_num_procs(), rows / per}));
+#pragma omp parallel num_threads(nt)
+    {
+        const int t = omp_get_thread_num(), n = omp_get_num_threads();
+        fn(rows * t / n, rows * (t + 1) / n);
     }
-    fn(0, rows / nt);
-    for (auto &x : th) x.join();
+}
+// a row of L doubles; a compile-time length makes the copy a few vector
+// moves instead of a library call per row
+template <int L>
+static inline void copy_row_n(double *d, const double *s) {
+    std::memcpy(d, s, L * sizeof(double));
+}
+static inline void copy_row(double *d, const double *s, int len) {
+    switch (len) {
+        case 4: copy_row_n<4>(d, s); break;
+        case 6: copy_row_n<6>(d, s); break;
+        case 8: copy_row_n<8>(d, s); break;
+        case 10: copy_row_n<10>(d, s); break;
+        case 16: copy_row_n<16>(d, s); break;
+        case 18: copy_row_n<18>(d, s); break;
+        case 32: copy_row_n<32>(d, s); break;
+        case 34: copy_row_n<34>(d, s); break;
+        default: std::memcpy(d, s, (size_t)len * sizeof(double)); break;
+    }
 }
 
 extern "C" {
@@ -2122,8 +2139,7 @@ static void scatter_g_interiors(const double *src, double *g, int64_t row0, int6
         for (int64_t r = row0 + r0; r < row0 + r1; r++) {
             const int64_t bc = r / ((int64_t)n * n);
             const int kj = (int)(r - bc * n * n), k = kj / n, j = kj - k * n;
-            std::memcpy(g + bc * Vi + ((int64_t)(k + gw) * Gi + (j + gw)) * Gi + gw, src + r * n,
-                        (size_t)n * sizeof(double));
+            copy_row(g + bc * Vi + ((int64_t)(k + gw) * Gi + (j + gw)) * Gi + gw, src + r * n, n);
         }
     });
 }
@@ -2140,8 +2156,8 @@ static void stage_rows(double *stage, double *io, int64_t row0, int64_t row1, in
             const int64_t b = r / ((int64_t)Gc * Gc);
             const int kj = (int)(r - b * Gc * Gc), k = kj / Gc, j = kj - k * Gc;
             double *o = io + b * Vi + ((int64_t)(k + gw - 1) * Gi + (j + gw - 1)) * Gi + (gw - 1);
-            if (to_stage) std::memcpy(stage + r * Gc, o, (size_t)Gc * sizeof(double));
-            else std::memcpy(o, stage + r * Gc, (size_t)Gc * sizeof(double));
+            if (to_stage) copy_row(stage + r * Gc, o, Gc);
+            else copy_row(o, stage + r * Gc, Gc);
         }
     });
 }

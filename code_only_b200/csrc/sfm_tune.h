@@ -37,7 +37,7 @@
 //                   reference's two colour launches with a ghost refresh
 //                   between them (fmg_poisson.F90:160-165, vmg_poisson.F90:114-115)
 //   local_sweeps    full sweeps of each fused launch on the staged block
-//                   (1 or 2; the ghost cells stay as staged between them)
+//                   (1 to 3; the ghost cells stay as staged between them)
 //   key: element size 4, block edge NI, level -1, kind -1
 // Text form, one entry per line (blank lines and lines starting with '#'
 // are skipped):
@@ -89,7 +89,7 @@ inline bool tune_choice_ok(int knob, int v) {
         case kKnobBaseCtas: return v == 1 || v == 2 || v == 4 || v == 8 || v == 16;
         case kKnobBaseWide: return v == 16 || v == 32 || v == 64;
         case kKnobFusedSweep: return v >= 0 && v <= 3;
-        case kKnobLocalSweeps: return v == 1 || v == 2;
+        case kKnobLocalSweeps: return v >= 1 && v <= 3;
         default: return false;
     }
 }

@@ -78,7 +78,7 @@ def test_tuned_mixed_schedule_keeps_the_fp64_solution(name):
     assert np.abs(ga - gb).max() / np.abs(gb).max() <= 1e-9
 
 
-@pytest.mark.parametrize("mask,local", [(1, 1), (2, 1), (3, 1), (1, 2), (3, 2)])
+@pytest.mark.parametrize("mask,local", [(1, 1), (2, 1), (3, 1), (1, 2), (3, 2), (3, 3)])
 @pytest.mark.parametrize("name", list(CASES))
 def test_fused_sweep_keeps_the_fp64_solution(name, mask, local):
     """fused_sweeps bit 0 makes every smoothing sweep of the mixed path's

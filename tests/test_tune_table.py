@@ -56,7 +56,7 @@ def test_later_entry_wins_and_empty_table(lib):
     "base_ctas 8 32 -1 -1 3",          # not a cluster size offered
     "base_wide 8 32 -1 -1 8",
     "fused_sweeps 4 8 -1 -1 4",
-    "local_sweeps 4 8 -1 -1 3",
+    "local_sweeps 4 8 -1 -1 4",
 ])
 def test_malformed_entries_are_rejected(lib, bad):
     assert check(lib, "ghost_fill 4 8 0 -1 1\n" + bad + "\n")[0] == abi.SFM_EINVAL
