@@ -535,26 +535,22 @@ public:
         for (const Knob &k : ks) tune.set(k.knob, 4, H.NI, -1, -1, k.ref);
         float best = candidate();
         if (best == std::numeric_limits<float>::max()) return SFM_ENOTCONVERGED;   // not even the reference
-        // coordinate descent; a second round revisits every knob with the
-        // others at their new values (stops early when a round changes none)
-        for (int round = 0; round < 2; round++) {
-            bool changed = false;
-            for (const Knob &k : ks) {
-                const int cur = tune.get(k.knob, 4, H.NI, -1, -1, k.ref);
-                int pick = cur;
-                for (int v : k.vals) {
-                    if (v == cur) continue;
-                    tune.set(k.knob, 4, H.NI, -1, -1, v);
-                    const float t = candidate();
-                    if (t < 0.98f * best) {
-                        best = t;
-                        pick = v;
-                    }
+        // one round of coordinate descent (a second round, revisiting every
+        // knob with the others at their new values, changed nothing on the
+        // benchmark hierarchies and doubled the tuning time)
+        for (const Knob &k : ks) {
+            const int cur = tune.get(k.knob, 4, H.NI, -1, -1, k.ref);
+            int pick = cur;
+            for (int v : k.vals) {
+                if (v == cur) continue;
+                tune.set(k.knob, 4, H.NI, -1, -1, v);
+                const float t = candidate();
+                if (t < 0.98f * best) {
+                    best = t;
+                    pick = v;
                 }
-                tune.set(k.knob, 4, H.NI, -1, -1, pick);
-                changed = changed || pick != cur;
             }
-            if (!changed) break;
+            tune.set(k.knob, 4, H.NI, -1, -1, pick);
         }
         if (iterExec) {
             cudaGraphExecDestroy(iterExec);
