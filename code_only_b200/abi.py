@@ -28,6 +28,7 @@ SFM_ESIZE = -9
 
 SFM_BC_PERIODIC = 0
 SFM_BC_SPHERE = 1
+SFM_BC_ZMIRROR = 2
 SFM_PREC_FP64 = 0
 SFM_PREC_MIXED = 1
 SFM_MAX_HISTORY = 64

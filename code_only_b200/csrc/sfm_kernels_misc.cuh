@@ -84,6 +84,19 @@ struct OpSubScalarInterior { // a := a - *s on the interior of consecutive block
 // ---------------------------------------------------------------------------
 // isolated boundary (fmg_boundary_phys_sphere.F90:81-354)
 // ---------------------------------------------------------------------------
+// z-mirror plane: u(:,:,-1) = u(:,:,0) over the whole transverse range of
+// the listed blocks (those touching the box's z-min face;
+// fmg_boundary_phys_zmirror.F90:66-80): the first G^2 values of a block get
+// the next G^2
+template <class T>
+struct OpMirrorZ {
+    T *u; const int32_t *blocks; int G; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        const int64_t per = (int64_t)G * G;
+        const int64_t b = blocks[idx / per], t = idx % per;
+        u[b * V + t] = u[b * V + t + per];
+    }
+};
 struct OpSphereMask {        // rho := 0 where x^2+y^2+z^2 >= rad2, all cells of all blocks
     double *R; const double *x0; const double *h0; const int32_t *level; int n, G; int64_t V; double rad2;
     __device__ void operator()(int64_t idx) const {
@@ -193,8 +206,18 @@ __device__ __forceinline__ double moment_norm(int m, double a) {
     }
 }
 
+// factor of moment term m on a z-mirror box: the mirror image doubles the
+// terms even in z (l + m even) and cancels the odd ones
+// (fmg_boundary_phys_zmirror.F90:243-258; l = 4 by the same rule)
+__device__ __forceinline__ double zmirror_factor(int m) {
+    // (l + m) parity of the terms a00, a10, a11r, a11i, a20, ..., a33i, l = 4
+    constexpr unsigned kOdd = (1u << 1) | (1u << 5) | (1u << 6) | (1u << 9) | (1u << 12) | (1u << 13) | (1u << 17) |
+                              (1u << 18) | (1u << 21) | (1u << 22);
+    return ((kOdd >> m) & 1u) ? 0.0 : 2.0;
+}
 // one warp; lane m < 25 sums term m over the cells in order
-__global__ void __launch_bounds__(32) k_moments_ordered(const double *__restrict__ T, int64_t ncell, double *mom) {
+__global__ void __launch_bounds__(32) k_moments_ordered(const double *__restrict__ T, int64_t ncell, double *mom,
+                                                         int zmirror) {
     pdl_enter();
     const int m = threadIdx.x;
     if (m >= kMomentTerms) return;
@@ -209,7 +232,7 @@ __global__ void __launch_bounds__(32) k_moments_ordered(const double *__restrict
         for (int u = 0; u < U; u++) a = a + t[u];
     }
     for (; c < ncell; c++) a = a + T[c * kMomentTerms + m];
-    mom[m] = moment_norm(m, a);
+    mom[m] = zmirror ? moment_norm(m, a) * zmirror_factor(m) : moment_norm(m, a);
 }
 
 // U00..U33 (sphere.F90:267-293) and the l = 4 terms

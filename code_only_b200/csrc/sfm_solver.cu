@@ -273,6 +273,8 @@ public:
     RefluxItem *d_reflux = nullptr;
     BFace *d_tfL = nullptr, *d_tfDL = nullptr, *d_crop = nullptr;
     std::vector<int64_t> faceOff, faceSplit, tfLOff, tfDLOff, cropOff, wcOff;
+    int32_t *d_zmin = nullptr;             // z-mirror: blocks touching the z-min face, level by level
+    std::vector<int64_t> zminOff;
     int nLeaves = 0, nReflux = 0, nSlots = 0;
     std::vector<int> leafList;
 
@@ -874,6 +876,18 @@ public:
         for (int q = 0; q < 3; q++) d_kind26[q] = mem.upload(kind26[q]);
         d_reflux = mem.upload(refl);
         d_tfL = mem.upload(tfL);
+        {   // z-mirror plane (TouchBoundary(Left, MZ)), per AMR level
+            std::vector<int32_t> zm;
+            zminOff.assign(nlev + 1, 0);
+            for (int L = 0; L < nlev; L++) {
+                zminOff[L] = (int64_t)zm.size();
+                if (P.bc == SFM_BC_ZMIRROR)
+                    for (int b = H.lstart[L]; b < H.lstart[L + 1]; b++)
+                        if (H.touch[6 * b + 4]) zm.push_back(b);
+            }
+            zminOff[nlev] = (int64_t)zm.size();
+            d_zmin = mem.upload(zm);
+        }
         d_tfDL = mem.upload(tfDL);
         d_crop = mem.upload(crop);
         d_baseIdx = mem.upload(std::vector<int32_t>(H.baseIdx.begin(), H.baseIdx.end()));
@@ -895,7 +909,7 @@ public:
         zeroList.push_back({d_err, sizeof(int)});
         for (int f = 0; f <= FMax; f++) SFM_WITH_N(nf[f], bulk_grids<N>(), (void)0);
         d_mom = mem.alloc<double>(32);
-        if (P.bc == SFM_BC_SPHERE)   // per-cell moment terms of the base level, summed in order
+        if (P.bc != SFM_BC_PERIODIC)   // per-cell moment terms of the base level, summed in order
             d_part = mem.alloc<double>((size_t)H.lstart[1] * H.NI * H.NI * H.NI * kMomentTerms);
         d_psum = mem.alloc<double>((size_t)nb);
         d_mgit = mem.alloc<int>(1);
@@ -912,6 +926,7 @@ public:
             mg.N = NBc; mg.MMax = MMax;
             mg.hbase = hlev(H.h0.data(), 0, FMax);
             mg.periodic = P.bc == SFM_BC_PERIODIC ? 1 : 0;
+            mg.zmirror = P.bc == SFM_BC_ZMIRROR ? 1 : 0;
             for (int f = 0; f < 6; f++) {
                 mg.touch[f] = 0;
                 for (int b = H.lstart[0]; b < H.lstart[1]; b++) mg.touch[f] |= H.touch[6 * b + f];
@@ -1132,13 +1147,31 @@ public:
         int h = nf[f] / 2;
         run(OpReflux<TT>{u, d_reflux, rbuf[f], d_h0, d_level, f, nf[f], Gf[f], Vf[f]}, (int64_t)nReflux * h * h);
     }
+    // fmg_boundary_u / vmg_boundary_u: the z-mirror plane of the blocks of
+    // AMR level L (or of all levels) touching the box's z-min face
+    // (fmg_boundary_phys_zmirror.F90:55-80); the periodic and sphere
+    // modules' hooks are no-ops
+    template <class TT>
+    void vmg_boundary_u(int L, int f, TT *u) {
+        if (P.bc != SFM_BC_ZMIRROR || L < 0) return;
+        const int64_t o = zminOff[L], c = zminOff[L + 1] - o;
+        if (c > 0) run(OpMirrorZ<TT>{u, d_zmin + o, Gf[f], Vf[f]}, c * Gf[f] * Gf[f]);
+    }
+    template <class TT>
+    void fmg_boundary_u(int f, TT *u) {   // every level in one launch (the blocks are independent)
+        if (P.bc != SFM_BC_ZMIRROR) return;
+        const int64_t c = zminOff[H.nlev];
+        if (c > 0) run(OpMirrorZ<TT>{u, d_zmin, Gf[f], Vf[f]}, c * Gf[f] * Gf[f]);
+    }
     // fmg_poisson_flux (fmg_poisson.F90:53-124)
     template <class TT>
     void poisson_flux(int f, TT *u, bool bf0) {
         if (FmgLevel_fill0 != f) {
             converge_c2p(f, u);
+            fmg_boundary_u(f, u);
             ghostcell_fix(f, u, false);
             if (bf0) boundary_fill0(f, u);
+            fmg_boundary_u(f, u);
         }
         FmgLevel_fill0 = Undef;
         reflux(f, u);
@@ -1399,8 +1432,10 @@ public:
     void fmg_interp(int f, T *uf, T *uc, bool cubic) {
         int lc = f + 1;
         converge_c2p(lc, uc, cubic);
+        fmg_boundary_u(lc, uc);
         ghostcell_fix(lc, uc, cubic);
         boundary_extrap(lc, uc);
+        fmg_boundary_u(lc, uc);
         const int n = nf[f];
         SFM_WITH_N(n,
                    (launch_pdl(k_interp_tiled<T, N>, (unsigned)((nLeaves + interp_bpc<N>() - 1) / interp_bpc<N>()), 256, 0, uf,
@@ -1410,6 +1445,8 @@ public:
                        (int64_t)nLeaves * n * n * n))
         boundary_fill0(lc, uc);
         boundary_fill0(f, uf);
+        fmg_boundary_u(lc, uc);
+        fmg_boundary_u(f, uf);
     }
 
     // fmg_lin (fmg.F90:270-377)
@@ -1445,15 +1482,22 @@ public:
 
     // -----------------------------------------------------------------
     // vmg (vmg.F90) at fmg level FMax
-    void vmg_ghostcell(int L, T *u) {
+    // (vmg_poisson_flux mirrors once more after vmg_ghostcell,
+    // vmg_poisson.F90:73-74: the plane it copies is unchanged since the
+    // mirror at the end of vmg_ghostcell, so that copy is left out)
+    void vmg_ghostcell(int L, T *u) {   // vmg.F90:729-743
         const int F = H.FMax;
+        vmg_boundary_u(L, F, u);
         ghost_fill_level(L, F, u, false, 0);   // same-level faces, x then y then z
         boundary_fill0_level(L, F, u);
+        vmg_boundary_u(L, F, u);
     }
-    void vmg_gridboundary(int L, T *u) {
+    void vmg_gridboundary(int L, T *u) {   // vmg.F90:710-725
         const int F = H.FMax;
+        vmg_boundary_u(L - 1, F, u);
         ghost_fill_level(L, F, u, false, 1);   // coarse-fine faces, x then y then z
         boundary_fill0_level(L, F, u);
+        vmg_boundary_u(L, F, u);
     }
     void vmg_relax(int L, T *u, const T *rhs) {   // vmg_poisson_relax (vmg_poisson.F90:98-145)
         const int F = H.FMax;
@@ -1494,8 +1538,10 @@ public:
         int Lc = Lf - 1;
         vmg_ghostcell(Lc, uc);
         boundary_extrap_level(Lc, F, uc);
+        vmg_boundary_u(Lc, F, uc);
         run(OpP2C<T>{uf, uc, d_parent, d_oct, H.lstart[Lf], n, Gf[F], Vf[F]}, (int64_t)cnt(Lf) * n * n * n);
         boundary_fill0_level(Lc, F, uc);
+        vmg_boundary_u(Lc, F, uc);
     }
     void vmg_zeroAverage(T *a) {
         const int F = H.FMax, n = nf[F];
@@ -1526,6 +1572,7 @@ public:
         converge_c2p(F, U[F]);
         converge_c2p(F, RHO[F]);
         boundary_fill0(F, U[F]);
+        fmg_boundary_u(F, U[F]);
         runB(OpCopy<T, T>{RHS[F], RHO[F], d_all, Vf[F]}, H.nb);
         const int nvs = sched(kKnobVmgSweeps, 2);
         for (int v = nlev - 1; v >= 1; v--) {
@@ -1552,20 +1599,25 @@ public:
 
     // -----------------------------------------------------------------
     // outer FP64 stages
-    void boundary_physical_grid() {   // sphere: mask SRC0, moments, multipole ghosts of PSI0
-        if (P.bc != SFM_BC_SPHERE) return;
+    // sphere and z-mirror: mask SRC0, moments, multipole ghosts of PSI0
+    // (fmg_boundary_phys_sphere.F90:81-354, fmg_boundary_phys_zmirror.F90:100-382)
+    void boundary_physical_grid() {
+        if (P.bc != SFM_BC_SPHERE && P.bc != SFM_BC_ZMIRROR) return;
+        const bool zm = P.bc == SFM_BC_ZMIRROR;
         const int n = H.NI;
         int bmin = H.baseIdx.front(), bmax = H.baseIdx.back();
         auto X = [&](int b, int d, int i) { return H.x0[3 * b + d] + (double)i * H.h0[H.level[b]]; };
         double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
         double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
-        double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        // the z-mirror box's z-min face is the mirror plane, not an edge of the sphere
+        double rr = zm ? std::min(std::min(std::min(xmax, ymax), zmax), std::min(-xmin, -ymin))
+                       : std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
         double rad2 = rr * rr;
         run(OpSphereMask{SRC0, d_x0, d_h0, d_level, n, Gf[0], Vf[0], rad2}, (int64_t)H.nb * Vf[0]);
         const int64_t ncell = (int64_t)cnt(0) * n * n * n;
         launch_pdl(k_moment_terms, (unsigned)std::min<int64_t>((ncell + 255) / 256, (int64_t)nSM * 8), 256, 0, SRC0,
                    d_x0, d_h0, n, Gf[0], Vf[0], cnt(0), P.lmax, d_part);
-        launch_pdl(k_moments_ordered, 1, 32, 0, d_part, ncell, d_mom);
+        launch_pdl(k_moments_ordered, 1, 32, 0, d_part, ncell, d_mom, zm ? 1 : 0);
         launches += 2;
         int GT = n + 2;
         run(OpSphereGhost{PSI0, d_tfL, d_mom, d_x0, d_h0, d_level, n, Gf[0], Vf[0], P.lmax}, tfLOff[H.nlev] * GT * GT);
@@ -1624,6 +1676,7 @@ public:
         converge_c2p(0, SRC0);
         converge_c2p(0, PSI0);
         boundary_physical_grid();
+        fmg_boundary_u(0, PSI0);
         h2absmax(SRC0, 2);
         int rc = check("setup");
         if (rc) return rc;
@@ -1663,6 +1716,7 @@ public:
         if (stop_stage == 4) return dumpd(PSI0, dump);
         copy(0, PHI0, PSI0, true);
         converge_c2p(0, PHI0);
+        fmg_boundary_u(0, PHI0);
         poisson_flux(0, PHI0, false);
         if (g)
             run(OpPsi2g{g, PHI0, d_skip, d_level, d_h0, d_rslot, rbuf[0], H.NI, Gf[0], gCompact ? 0 : gw, Vf[0]},
@@ -1806,6 +1860,10 @@ public:
     }
 
     int adjoint(const double *dJdphi, double *dJdrho, sfm_stats *stats, cudaStream_t s) override {
+        if (P.bc == SFM_BC_ZMIRROR) {   // the transpose of the mirror plane is not built
+            last_error = "sfm_adjoint: not available on a z-mirror box";
+            return SFM_EINVAL;
+        }
         st_ = s ? s : own_;
         launches = 0;
         int rc = adj_init();
@@ -2046,7 +2104,8 @@ static int create_impl(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **ou
     if (!h || !p || !out) return SFM_EINVAL;
     *out = nullptr;
     if (p->ngh_io < 1 || p->max_outer < 0 || p->max_outer > 1000 || !(p->rel_tol >= 0) ||
-        (p->bc != SFM_BC_PERIODIC && p->bc != SFM_BC_SPHERE) || (p->lmax != 3 && p->lmax != 4) ||
+        (p->bc != SFM_BC_PERIODIC && p->bc != SFM_BC_SPHERE && p->bc != SFM_BC_ZMIRROR) ||
+        (p->lmax != 3 && p->lmax != 4) ||
         (p->precision != SFM_PREC_FP64 && p->precision != SFM_PREC_MIXED))
         return SFM_EINVAL;
     {   // the hierarchy is validated on the host before any device work

@@ -314,6 +314,39 @@ def small_sphere(nbase: int = 2, ni: int = 8, nlev: int = 2, seed: int = 0) -> H
     return build_hierarchy((nbase,) * 3, ni, nlev, ref, False, box_lo=(-0.5, -0.5, -0.5), box_size=1.0)
 
 
+def _near_origin(levels_radius):
+    """Refines a block when the point of its box nearest the origin lies
+    within levels_radius[L] (a predicate symmetric under z -> -z)."""
+    def ref(L, q, g):
+        cw = g.box_size / (g.ngb[0] * g.ni * (1 << L))
+        lo = g.box_lo[None, :] + q * g.ni * cw
+        hi = lo + g.ni * cw
+        near = np.clip(0.0, lo, hi)
+        return np.sqrt((near * near).sum(axis=1)) < levels_radius[min(L, len(levels_radius) - 1)]
+    return ref
+
+
+def mirror_sphere(nbase: int = 3, ni: int = 8, nlev: int = 3, full: bool = False) -> Hierarchy:
+    """An isolated box for the z-mirror boundary: [-1/2, 1/2]^2 x [0, 1] with
+    nbase^3 base blocks (the mirror plane z = 0 is the box's z-min face),
+    refined around the origin.  full=True gives the box's mirror-symmetric
+    double [-1/2, 1/2]^2 x [-1, 1] (nbase x nbase x 2 nbase base blocks) for
+    the ordinary isolated boundary: its upper half holds the same blocks."""
+    radii = (0.3, 0.15, 0.08, 0.04)
+    if full:
+        return build_hierarchy((nbase, nbase, 2 * nbase), ni, nlev, _near_origin(radii), False,
+                               box_lo=(-0.5, -0.5, -1.0), box_size=1.0)
+    return build_hierarchy((nbase,) * 3, ni, nlev, _near_origin(radii), False,
+                           box_lo=(-0.5, -0.5, 0.0), box_size=1.0)
+
+
+def wide_sphere(x, y, z):
+    """rho = 1/(1+(r/0.08)^2) for r < 0.45, else 1e-3 (centred at the origin;
+    even in z)."""
+    r = np.sqrt(x * x + y * y + z * z)
+    return np.where(r < 0.45, 1.0 / (1.0 + (r / 0.08) ** 2), 1e-3)
+
+
 def gaussian_random_field(n: int, seed: int, kmin: float = 2.0, kmax: float = 64.0,
                           slope: float = -4.0, sigma: float = 1.5) -> np.ndarray:
     """ln(rho) on an n^3 periodic grid: P(k) ~ k^slope for kmin <= |k| <= kmax

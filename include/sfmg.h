@@ -79,12 +79,15 @@ typedef struct sfm_hier_desc {
  * The reference hard-codes these (fmg.F90:146,179; config.h:194). */
 #define SFM_BC_PERIODIC 0   /* fmg_boundary_phys_periodic.F90                  */
 #define SFM_BC_SPHERE   1   /* fmg_boundary_phys_sphere.F90 (multipole ghosts)  */
+#define SFM_BC_ZMIRROR  2   /* fmg_boundary_phys_zmirror.F90: multipole ghosts,
+                               a mirror plane on the box's z-min face          */
 #define SFM_PREC_FP64   0   /* every operation in FP64, as the reference       */
 #define SFM_PREC_MIXED  1   /* FP32 inner fmg_lin/vmg, FP64 outer loop and base solve */
 
 typedef struct sfm_params {
     int32_t bc;              /* SFM_BC_*                                        */
-    int32_t lmax;            /* multipole order for SFM_BC_SPHERE: 3 (reference) or 4 */
+    int32_t lmax;            /* multipole order for SFM_BC_SPHERE / _ZMIRROR: 3
+                                (reference) or 4                                */
     int32_t precision;       /* SFM_PREC_*                                      */
     int32_t max_outer;       /* nfmgmax (reference: 10)                         */
     double  rel_tol;         /* errormax (reference: 1e-3)                      */
@@ -177,6 +180,7 @@ int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g
  *   - The first call allocates the Krylov vectors (as many as fit, up to 30
  *     restarts' worth, in 80% of the free device memory).
  *   - Results are reproducible to roundoff, not bitwise (FP64 atomics).
+ *   - Periodic and sphere boxes only: a z-mirror box returns SFM_EINVAL.
  * st: outer_iters = Krylov iterations, ratio[] = their residual history,
  * true_rel_residual = the final true relative residual. */
 int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st);

@@ -597,10 +597,31 @@ struct Oracle {
         for (int b = 0; b < nb; b++) extrap_block(A, b, n);
     }
 
-    // fmg_boundary_physical_grid (fmg_boundary_phys_sphere.F90:81-354);
-    // a no-op for periodic (fmg_boundary_phys_periodic.F90:109-112)
+    // z-mirror hooks (fmg_boundary_phys_zmirror.F90:55-80): every block of
+    // AMR level L touching the box's z-min face gets u(:,:,-1) = u(:,:,0)
+    // over the whole transverse range; no-ops for the other modules (the
+    // periodic and sphere modules' fmg/vmg_boundary_u do nothing)
+    void vmg_boundary_u(int L, int f, int code) {
+        if (bc != SFM_BC_ZMIRROR) return;
+        Arr &A = F(code, f);
+        const int n = nF(f);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+            if (!touch[6 * b + Left + 2 * MZ]) continue;
+            for (int j = -1; j <= n; j++)
+                for (int i = -1; i <= n; i++) A.at(b, i, j, -1) = A.at(b, i, j, 0);
+        }
+    }
+    void fmg_boundary_u(int f, int code) {   // zmirror.F90:55-62
+        if (bc != SFM_BC_ZMIRROR) return;
+        for (int L = 0; L < nlev; L++) vmg_boundary_u(L, f, code);
+    }
+
+    // fmg_boundary_physical_grid (fmg_boundary_phys_sphere.F90:81-354, and
+    // fmg_boundary_phys_zmirror.F90:100-382: the mask radius leaves out
+    // -zmin, the moments carry the mirror's factor 2 or 0); a no-op for
+    // periodic (fmg_boundary_phys_periodic.F90:109-112)
     void boundary_physical_grid(int ju, int jrho) {
-        if (bc != SFM_BC_SPHERE) return;
+        if (bc != SFM_BC_SPHERE && bc != SFM_BC_ZMIRROR) return;
         const int f = 0, n = NI;
         Arr &R = F(jrho, f), &U = F(ju, f);
         auto X = [&](int b, int d, int i) { return x0[3 * b + d] + (double)i * h0[level[b]]; };
@@ -608,7 +629,9 @@ struct Oracle {
         int bmin = baseIdx[0], bmax = baseIdx.back();
         double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
         double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
-        double rr = std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        double rr = bc == SFM_BC_ZMIRROR
+                        ? std::min(std::min(std::min(xmax, ymax), zmax), std::min(-xmin, -ymin))
+                        : std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
         double rad2 = rr * rr;
         for (int b = 0; b < nb; b++)
             for (int k = -1; k <= n; k++)
@@ -633,6 +656,15 @@ struct Oracle {
                 }
     }
 
+    // factor of moment term t on a z-mirror box: 2 for terms even in z
+    // (l + m even), 0 for odd ones; terms in the order a00, a10, a11r, a11i,
+    // a20, a21r, a21i, a22r, a22i, a30 .. a33i, then l = 4, m = 0 .. 4
+    static double zmirror_factor(int t) {
+        static const int lm[25][2] = {{0, 0}, {1, 0}, {1, 1}, {1, 1}, {2, 0}, {2, 1}, {2, 1}, {2, 2}, {2, 2},
+                                      {3, 0}, {3, 1}, {3, 1}, {3, 2}, {3, 2}, {3, 3}, {3, 3}, {4, 0}, {4, 1},
+                                      {4, 1}, {4, 2}, {4, 2}, {4, 3}, {4, 3}, {4, 4}, {4, 4}};
+        return ((lm[t][0] + lm[t][1]) & 1) ? 0.0 : 2.0;
+    }
     // moments a_lm over base-level interior cells (sphere.F90:132-242);
     // l = 4 terms extend the reference (which stops at l = 3).
     void multipole_moments(Arr &R, double *out) {
@@ -717,6 +749,10 @@ struct Oracle {
         out[22] = -a[22] / (4.0 * pi) * (35.0 / 8.0);
         out[23] = -a[23] / (4.0 * pi) * (35.0 / 64.0);
         out[24] = -a[24] / (4.0 * pi) * (35.0 / 64.0);
+        // z-mirror: the mirror image doubles the terms even in z (l + m even)
+        // and cancels the odd ones (zmirror.F90:243-258; l = 4 by the same rule)
+        if (bc == SFM_BC_ZMIRROR)
+            for (int t = 0; t < 25; t++) out[t] = out[t] * zmirror_factor(t);
     }
 
     // U00..U33 (sphere.F90:267-293), plus the l = 4 extension
@@ -763,8 +799,10 @@ struct Oracle {
     void poisson_flux(int f, int ju, bool bf0) {
         if (FmgLevel_fill0 != f) {
             converge_c2p(f, ju);
+            fmg_boundary_u(f, ju);
             ghostcell_fix(f, ju);
             if (bf0) boundary_fill0(f, ju);
+            fmg_boundary_u(f, ju);
         }
         FmgLevel_fill0 = Undef;
         Arr &U = F(ju, f);
@@ -943,8 +981,10 @@ struct Oracle {
     void fmg_interp(int f, int iuf, int iuc, bool cubic) {
         int lc = f + 1;
         converge_c2p(lc, iuc, cubic);
+        fmg_boundary_u(lc, iuc);
         ghostcell_fix(lc, iuc, cubic);
         boundary_extrap(lc, iuc);
+        fmg_boundary_u(lc, iuc);
         Arr &Fo = F(iuf, f), &C = F(iuc, lc);
         const int n = nF(f), nc = nF(lc);
         OMP_FOR
@@ -958,6 +998,8 @@ struct Oracle {
         }
         boundary_fill0(lc, iuc);
         boundary_fill0(f, iuf);
+        fmg_boundary_u(lc, iuc);
+        fmg_boundary_u(f, iuf);
     }
     void fmg_addint(int f, int juf, int juc, int jres) {   // fmg.F90:942-946
         fmg_interp(f, jres, juc, false);
@@ -1021,15 +1063,20 @@ struct Oracle {
         for (int b = lstart[L]; b < lstart[L + 1]; b++) extrap_block(A, b, nF(FMax));
     }
     void vmg_ghostcell(int L, int code) {   // vmg.F90:729-743
+        vmg_boundary_u(L, FMax, code);
         for (int dir = 0; dir < 3; dir++) samelev(L, FMax, dir, code);
         vmg_boundary_fill0(L, code);
+        vmg_boundary_u(L, FMax, code);
     }
     void vmg_gridboundary(int L, int code) {   // vmg.F90:710-725 (CubicInterp = .FALSE. for Ngh = 1)
+        vmg_boundary_u(L - 1, FMax, code);
         for (int dir = 0; dir < 3; dir++) parentlev(L, FMax, dir, code, false);
         vmg_boundary_fill0(L, code);
+        vmg_boundary_u(L, FMax, code);
     }
     void vmg_poisson_flux(int L, int ju) {   // vmg_poisson.F90:63-94
         vmg_ghostcell(L, ju);
+        vmg_boundary_u(L, FMax, ju);
         Arr &U = F(ju, FMax);
         const int n = nF(FMax);
         double hi = 1.0 / h(L, FMax);
@@ -1116,6 +1163,7 @@ struct Oracle {
         int Lc = Lf - 1;
         vmg_ghostcell(Lc, juc);
         vmg_boundary_extrap(Lc, juc);
+        vmg_boundary_u(Lc, FMax, juc);
         Arr &Fo = F(juf, FMax), &C = F(juc, FMax);
         const int n = nF(FMax), h2n = n / 2;
         for (int p = lstart[Lc]; p < lstart[Lc + 1]; p++)
@@ -1128,6 +1176,7 @@ struct Oracle {
                         for (int i = 0; i < n; i++) Fo.at(cb, i, j, k) = trilinear_cell(C, p, i, j, k, oi, oj, ok);
             }
         vmg_boundary_fill0(Lc, juc);
+        vmg_boundary_u(Lc, FMax, juc);
     }
     // vmg_zeroAverage (vmg.F90:900-916) through fmg_ave (fmg_data.F90:730-769)
     void vmg_zeroAverage(int L, int code) {
@@ -1166,6 +1215,7 @@ struct Oracle {
         converge_c2p(FMax, IU);
         converge_c2p(FMax, IRHO);
         boundary_fill0(FMax, IU);
+        fmg_boundary_u(FMax, IU);
         for (int L = 0; L < nlev; L++) vmg_copy(L, IRHS, IRHO);
         for (int v = nlev - 1; v >= 1; v--) {
             vmg_gridboundary(v, IU);
@@ -1220,8 +1270,19 @@ struct Oracle {
                 }
     }
     // periodic wrap of one ghost layer (fmg_boundary_phys_periodic.F90:71-104);
-    // the sphere module's mg_boundary_u is a no-op
+    // the z-mirror plane on the base grid's z-min face, u(:,:,k) =
+    // u(:,:,2 kmin - 1 - k) for k = kmingh .. kmin (zmirror.F90:84-96; the
+    // second of the two copies writes u(:,:,0) onto itself); the sphere
+    // module's mg_boundary_u is a no-op
     void mg_boundary_u(int m, int code) {
+        if (bc == SFM_BC_ZMIRROR) {
+            Arr &A = MG(code, m);
+            const int n = A.n;
+            for (int k = -1; k <= 0; k++)
+                for (int j = -1; j <= n; j++)
+                    for (int i = -1; i <= n; i++) A.at(0, i, j, k) = A.at(0, i, j, -1 - k);
+            return;
+        }
         if (bc != SFM_BC_PERIODIC) return;
         Arr &A = MG(code, m);
         const int n = A.n;
@@ -1436,6 +1497,7 @@ struct Oracle {
         converge_c2p(f, ISRC);
         converge_c2p(f, IPSI);
         boundary_physical_grid(IPSI, ISRC);
+        fmg_boundary_u(f, IPSI);
         double resh2max = h2absmax(0, ISRC);
         if (stop_stage == 1) { dumpf(ISRC, dump); return SFM_OK; }
         double ratio_prev = std::numeric_limits<double>::max();
@@ -1463,6 +1525,7 @@ struct Oracle {
         if (stop_stage == 4) { dumpf(IPSI, dump); return SFM_OK; }
         copy(f, IU, IPSI, true);
         converge_c2p(f, IU);
+        fmg_boundary_u(f, IU);
         if (g) psi2g(IU, g, gw);
         else poisson_flux(0, IU, false);
         // fmg_restore_u: U (with its ghost layer) back into the caller's array
@@ -1731,6 +1794,7 @@ struct Oracle {
 
     // dJdphi, dJdrho: [nb][(NI+2gw)^3]; interiors used / written
     int adjoint(const double *dJdphi, double *dJdrho, int gw, sfm_stats *st) {
+        if (bc == SFM_BC_ZMIRROR) return SFM_EINVAL;   // the mirror's transpose is not built
         const int n = NI, Gi = NI + 2 * gw;
         for (auto &a : fld) std::fill(a.d.begin(), a.d.end(), 0.0);
         for (auto &a : flx) std::fill(a.d.begin(), a.d.end(), 0.0);
