@@ -29,6 +29,8 @@ SFM_ESIZE = -9
 SFM_BC_PERIODIC = 0
 SFM_BC_SPHERE = 1
 SFM_BC_ZMIRROR = 2
+SFM_BC_CYL_ZPERIODIC = 3
+SFM_BC_MASK_ZPERIODIC = 4
 SFM_PREC_FP64 = 0
 SFM_PREC_MIXED = 1
 SFM_MAX_HISTORY = 64
@@ -57,7 +59,7 @@ class SfmParams(C.Structure):
         ("bc", C.c_int32), ("lmax", C.c_int32), ("precision", C.c_int32),
         ("max_outer", C.c_int32), ("rel_tol", C.c_double), ("four_pi_G", C.c_double),
         ("zero_mean", C.c_int32), ("ngh_io", C.c_int32), ("report_residual", C.c_int32),
-        ("stagnation_exit", C.c_int32), ("profile", C.c_int32),
+        ("stagnation_exit", C.c_int32), ("profile", C.c_int32), ("rho_mask", C.c_double),
     ]
 
 
@@ -120,6 +122,7 @@ def default_params(bc: int = SFM_BC_PERIODIC, **kw) -> SfmParams:
     p.report_residual = 1
     p.stagnation_exit = 1
     p.profile = 0
+    p.rho_mask = 0.0
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -97,6 +97,38 @@ struct OpMirrorZ {
         u[b * V + t] = u[b * V + t + per];
     }
 };
+// the z-periodic cylinders' masks and ghosts
+// (fmg_boundary_phys_cyl_zperiodic.F90:120-232, ..._mask_zperiodic.F90:129)
+struct OpCylMask {           // rho := 0 where x^2+y^2 >= rad2, all cells of all blocks
+    double *R; const double *x0; const double *h0; const int32_t *level; int n, G; int64_t V; double rad2;
+    __device__ void operator()(int64_t idx) const {
+        int64_t b = idx / V;
+        int r = (int)(idx % V);
+        int i = r % G - 1, j = (r / G) % G - 1;
+        double h = h0[level[b]];
+        double x = x0[3 * b] + (double)i * h, y = x0[3 * b + 1] + (double)j * h;
+        if (x * x + y * y >= rad2) R[idx] = 0.0;
+    }
+};
+struct OpRhoMask {           // rho := 0 where rho < MP_rhomask, all cells of all blocks
+    double *R; double thresh;
+    __device__ void operator()(int64_t idx) const {
+        if (R[idx] < thresh) R[idx] = 0.0;
+    }
+};
+struct OpCylGhost {          // a00 ln(r) on the first ghost layer of the x and y boundary faces
+    double *U; const BFace *faces; const double *lnr; const double *mom; int n, G; int64_t V;
+    __device__ void operator()(int64_t idx) const {
+        const int GT = n + 2;
+        int64_t it = idx / (GT * GT);
+        int r = (int)(idx - it * GT * GT);
+        BFace bf = faces[it];
+        int dir = bf.face >> 1, lr = bf.face & 1, i, j, k;
+        if (dir == 2) return;   // z is periodic
+        put3(dir, lr == 0 ? -1 : n, r % GT - 1, r / GT - 1, i, j, k);
+        U[(int64_t)bf.b * V + cidx(G, i, j, k)] = lnr[idx] * mom[0];
+    }
+};
 struct OpSphereMask {        // rho := 0 where x^2+y^2+z^2 >= rad2, all cells of all blocks
     double *R; const double *x0; const double *h0; const int32_t *level; int n, G; int64_t V; double rad2;
     __device__ void operator()(int64_t idx) const {
@@ -216,8 +248,11 @@ __device__ __forceinline__ double zmirror_factor(int m) {
     return ((kOdd >> m) & 1u) ? 0.0 : 2.0;
 }
 // one warp; lane m < 25 sums term m over the cells in order
+// mode 0: the sphere's normalisations; 1: the same times the z-mirror
+// factors; 2: the z-periodic cylinders' a00 = (sum of term 0) / zlen / pi2
+// (cyl_zperiodic.F90:197) in mom[0]
 __global__ void __launch_bounds__(32) k_moments_ordered(const double *__restrict__ T, int64_t ncell, double *mom,
-                                                         int zmirror) {
+                                                         int mode, double zlen, double pi2) {
     pdl_enter();
     const int m = threadIdx.x;
     if (m >= kMomentTerms) return;
@@ -232,7 +267,11 @@ __global__ void __launch_bounds__(32) k_moments_ordered(const double *__restrict
         for (int u = 0; u < U; u++) a = a + t[u];
     }
     for (; c < ncell; c++) a = a + T[c * kMomentTerms + m];
-    mom[m] = zmirror ? moment_norm(m, a) * zmirror_factor(m) : moment_norm(m, a);
+    if (mode == 2) {
+        if (m == 0) mom[0] = a / zlen / pi2;
+        return;
+    }
+    mom[m] = mode == 1 ? moment_norm(m, a) * zmirror_factor(m) : moment_norm(m, a);
 }
 
 // U00..U33 (sphere.F90:267-293) and the l = 4 terms

@@ -25,7 +25,8 @@ struct MgData {
     int MMax;            // coarsest level (1 cell)
     double hbase;        // cell width on level 0 (fmg_get_h(Lmin, FMG_LevelMax))
     int periodic;        // mg_boundary_u wraps (periodic module) or is a no-op (sphere)
-    int zmirror;         // mg_boundary_u mirrors the z-min face (zmirror module)
+    int zbc;             // mg_boundary_u on the z faces: 1 mirrors the z-min face
+                         // (zmirror module), 2 wraps z (the z-periodic cylinders)
     int touch[6];        // TouchBoundary of the base grid (mg_data.F90:77-83)
 };
 
@@ -147,11 +148,24 @@ __device__ __forceinline__ void mg_pq(int t, int G, float rG, int &p, int &q) {
 // -1 -> n-1, n -> 0).  That final state is written here in one pass:
 // cells on several faces are written with the same value more than once.
 __device__ void mg_boundary_u(MgRun &r, const MgData &d, int m, double *a) {
-    if (d.zmirror) {   // u(:,:,-1) = u(:,:,0) (fmg_boundary_phys_zmirror.F90:84-96)
+    if (d.zbc == 1) {   // u(:,:,-1) = u(:,:,0) (fmg_boundary_phys_zmirror.F90:84-96)
         const int n = mgN(d, m), G = n + 2;
         const MgStep s = mg_begin(r, d, m);
         if (s.on)
             for (int t = s.start; t < G * G; t += s.stride) a[(int64_t)t] = a[(int64_t)t + G * G];
+        mg_end(s);
+        return;
+    }
+    if (d.zbc == 2) {   // u(:,:,-1) = u(:,:,n-1), then u(:,:,n) = u(:,:,0) (cyl_zperiodic.F90:60-72)
+        const int n = mgN(d, m), G = n + 2;
+        const int64_t P = (int64_t)G * G;
+        MgStep s = mg_begin(r, d, m);
+        if (s.on)
+            for (int t = s.start; t < G * G; t += s.stride) a[t] = a[t + n * P];
+        mg_end(s);
+        s = mg_begin(r, d, m);
+        if (s.on)
+            for (int t = s.start; t < G * G; t += s.stride) a[t + (n + 1) * P] = a[t + P];
         mg_end(s);
         return;
     }
@@ -250,7 +264,7 @@ __device__ void mg_resid(MgRun &r, const MgData &d, int m, double *res, double *
     const int n = mgN(d, m), G = n + 2, ln = __ffs(n) - 1;
     double hh = mgH(d, m);
     double h2i = 1.0 / (hh * hh);
-    if (d.zmirror) mg_boundary_u(r, d, m, u);   // mg_poisson.F90:16
+    if (d.zbc) mg_boundary_u(r, d, m, u);   // mg_poisson.F90:16
     const MgStep s = mg_begin(r, d, m);
     if (s.on)
         for (int c = s.start; c < n * n * n; c += s.stride) {
@@ -269,7 +283,7 @@ __device__ double mg_relax(MgRun &r, const MgData &d, int m, double *u, const do
     double hh = mgH(d, m), h2 = hh * hh, rm = 0.0;
     const int half = (n * n * n + 1) / 2;
     for (int ipass = 1; ipass <= 2; ipass++) {
-        if (d.zmirror) mg_boundary_u(r, d, m, u);   // mg_poisson.F90:56 (a wrap on periodic boxes is not needed)
+        if (d.zbc) mg_boundary_u(r, d, m, u);   // mg_poisson.F90:56 (a wrap on periodic boxes is not needed)
         const MgStep s = mg_begin(r, d, m);
         if (s.on)
             for (int c = s.start; c < half; c += s.stride) {
@@ -356,7 +370,7 @@ __device__ void mg_interp(MgRun &r, const MgData &d, int m, double *uf, double *
 __device__ void mg_resid_rstrct_fill0(MgRun &r, const MgData &d, int v, double *rhsc, double *u,
                                       const double *rhs, double *uc) {
     const int n = mgN(d, v), G = n + 2, nc = mgN(d, v + 1), Gc = nc + 2, lnc = __ffs(nc) - 1;
-    if (d.zmirror) mg_boundary_u(r, d, v, u);   // mg_poisson_resid's mirror (mg_poisson.F90:16)
+    if (d.zbc) mg_boundary_u(r, d, v, u);   // mg_poisson_resid's boundary (mg_poisson.F90:16)
     const double hh = mgH(d, v);
     const double h2i = 1.0 / (hh * hh);
     auto res = [&](int i, int j, int k) {

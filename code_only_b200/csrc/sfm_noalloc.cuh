@@ -68,7 +68,7 @@ __host__ __device__ inline MgData noalloc_layout(double *s, int n, double h) {
     d.MMax = MMax;
     d.hbase = h;
     d.periodic = 1;
-    d.zmirror = 0;
+    d.zbc = 0;
     for (int f = 0; f < 6; f++) d.touch[f] = 0;   // periodic: no face touches a physical boundary
     return d;
 }

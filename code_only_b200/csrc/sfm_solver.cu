@@ -275,6 +275,9 @@ public:
     std::vector<int64_t> faceOff, faceSplit, tfLOff, tfDLOff, cropOff, wcOff;
     int32_t *d_zmin = nullptr;             // z-mirror: blocks touching the z-min face, level by level
     std::vector<int64_t> zminOff;
+    double *d_cyllog = nullptr;            // z-periodic cylinders: ln(sqrt(x^2 + y^2)) at every ghost
+                                           // cell of the boundary faces (d_tfL order), from the host's libm
+    bool zperiodic() const { return P.bc == SFM_BC_CYL_ZPERIODIC || P.bc == SFM_BC_MASK_ZPERIODIC; }
     int nLeaves = 0, nReflux = 0, nSlots = 0;
     std::vector<int> leafList;
 
@@ -876,6 +879,22 @@ public:
         for (int q = 0; q < 3; q++) d_kind26[q] = mem.upload(kind26[q]);
         d_reflux = mem.upload(refl);
         d_tfL = mem.upload(tfL);
+        if (zperiodic()) {   // the cylinders' ghost values are a00 times these (x and y faces only)
+            const int n = H.NI, GT = n + 2;
+            std::vector<double> lg((size_t)tfL.size() * GT * GT, 0.0);
+            for (size_t it = 0; it < tfL.size(); it++) {
+                const int b = tfL[it].b, dir = tfL[it].face >> 1, lr = tfL[it].face & 1;
+                if (dir == 2) continue;
+                const double hb = H.h0[H.level[b]];
+                for (int r = 0; r < GT * GT; r++) {
+                    int i, j, k;
+                    put3(dir, lr == 0 ? -1 : n, r % GT - 1, r / GT - 1, i, j, k);
+                    const double x = H.x0[3 * b] + (double)i * hb, y = H.x0[3 * b + 1] + (double)j * hb;
+                    lg[it * GT * GT + r] = std::log(std::sqrt(x * x + y * y));
+                }
+            }
+            d_cyllog = mem.upload(lg);
+        }
         {   // z-mirror plane (TouchBoundary(Left, MZ)), per AMR level
             std::vector<int32_t> zm;
             zminOff.assign(nlev + 1, 0);
@@ -926,7 +945,7 @@ public:
             mg.N = NBc; mg.MMax = MMax;
             mg.hbase = hlev(H.h0.data(), 0, FMax);
             mg.periodic = P.bc == SFM_BC_PERIODIC ? 1 : 0;
-            mg.zmirror = P.bc == SFM_BC_ZMIRROR ? 1 : 0;
+            mg.zbc = P.bc == SFM_BC_ZMIRROR ? 1 : (zperiodic() ? 2 : 0);
             for (int f = 0; f < 6; f++) {
                 mg.touch[f] = 0;
                 for (int b = H.lstart[0]; b < H.lstart[1]; b++) mg.touch[f] |= H.touch[6 * b + f];
@@ -1602,6 +1621,7 @@ public:
     // sphere and z-mirror: mask SRC0, moments, multipole ghosts of PSI0
     // (fmg_boundary_phys_sphere.F90:81-354, fmg_boundary_phys_zmirror.F90:100-382)
     void boundary_physical_grid() {
+        if (zperiodic()) return boundary_physical_grid_cyl();
         if (P.bc != SFM_BC_SPHERE && P.bc != SFM_BC_ZMIRROR) return;
         const bool zm = P.bc == SFM_BC_ZMIRROR;
         const int n = H.NI;
@@ -1617,10 +1637,37 @@ public:
         const int64_t ncell = (int64_t)cnt(0) * n * n * n;
         launch_pdl(k_moment_terms, (unsigned)std::min<int64_t>((ncell + 255) / 256, (int64_t)nSM * 8), 256, 0, SRC0,
                    d_x0, d_h0, n, Gf[0], Vf[0], cnt(0), P.lmax, d_part);
-        launch_pdl(k_moments_ordered, 1, 32, 0, d_part, ncell, d_mom, zm ? 1 : 0);
+        launch_pdl(k_moments_ordered, 1, 32, 0, d_part, ncell, d_mom, zm ? 1 : 0, 1.0, 1.0);
         launches += 2;
         int GT = n + 2;
         run(OpSphereGhost{PSI0, d_tfL, d_mom, d_x0, d_h0, d_level, n, Gf[0], Vf[0], P.lmax}, tfLOff[H.nlev] * GT * GT);
+    }
+
+    // z-periodic cylinder and its density-masked variant
+    // (fmg_boundary_phys_cyl_zperiodic.F90:97-232, ..._mask_zperiodic.F90):
+    // mask SRC0, a00 = (sum of rho dv over the base-level cells, in the
+    // reference's order) / zlen / (2 pi), ghost = a00 ln(r) on the x and y faces
+    void boundary_physical_grid_cyl() {
+        const int n = H.NI;
+        int bmin = H.baseIdx.front(), bmax = H.baseIdx.back();
+        auto X = [&](int b, int d, int i) { return H.x0[3 * b + d] + (double)i * H.h0[H.level[b]]; };
+        double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
+        double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
+        const double zlen = zmax - zmin + H.h0[0];
+        if (P.bc == SFM_BC_CYL_ZPERIODIC) {
+            double rr = std::min(std::min(xmax, ymax), std::min(-xmin, -ymin));
+            run(OpCylMask{SRC0, d_x0, d_h0, d_level, n, Gf[0], Vf[0], rr * rr}, (int64_t)H.nb * Vf[0]);
+        } else {
+            run(OpRhoMask{SRC0, P.rho_mask}, (int64_t)H.nb * Vf[0]);
+        }
+        const int64_t ncell = (int64_t)cnt(0) * n * n * n;
+        launch_pdl(k_moment_terms, (unsigned)std::min<int64_t>((ncell + 255) / 256, (int64_t)nSM * 8), 256, 0, SRC0,
+                   d_x0, d_h0, n, Gf[0], Vf[0], cnt(0), P.lmax, d_part);
+        const double pi2 = 2.0 * (4.0 * std::atan(1.0));   // Pi2 (parameter.F90:14-15)
+        launch_pdl(k_moments_ordered, 1, 32, 0, d_part, ncell, d_mom, 2, zlen, pi2);
+        launches += 2;
+        int GT = n + 2;
+        run(OpCylGhost{PSI0, d_tfL, d_cyllog, d_mom, n, Gf[0], Vf[0]}, tfLOff[H.nlev] * GT * GT);
     }
 
     double read_max(int slot) {
@@ -1860,8 +1907,8 @@ public:
     }
 
     int adjoint(const double *dJdphi, double *dJdrho, sfm_stats *stats, cudaStream_t s) override {
-        if (P.bc == SFM_BC_ZMIRROR) {   // the transpose of the mirror plane is not built
-            last_error = "sfm_adjoint: not available on a z-mirror box";
+        if (P.bc == SFM_BC_ZMIRROR || zperiodic()) {   // these boundaries' transposes are not built
+            last_error = "sfm_adjoint: not available on z-mirror and z-periodic cylinder boxes";
             return SFM_EINVAL;
         }
         st_ = s ? s : own_;
@@ -2082,6 +2129,7 @@ void sfm_default_params(sfm_params *p) {
     p->report_residual = 1;
     p->stagnation_exit = 1;
     p->profile = 0;
+    p->rho_mask = 0.0;
 }
 
 // No C++ exception may cross the C ABI: every entry point below runs its
@@ -2104,7 +2152,7 @@ static int create_impl(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **ou
     if (!h || !p || !out) return SFM_EINVAL;
     *out = nullptr;
     if (p->ngh_io < 1 || p->max_outer < 0 || p->max_outer > 1000 || !(p->rel_tol >= 0) ||
-        (p->bc != SFM_BC_PERIODIC && p->bc != SFM_BC_SPHERE && p->bc != SFM_BC_ZMIRROR) ||
+        p->bc < SFM_BC_PERIODIC || p->bc > SFM_BC_MASK_ZPERIODIC || !std::isfinite(p->rho_mask) ||
         (p->lmax != 3 && p->lmax != 4) ||
         (p->precision != SFM_PREC_FP64 && p->precision != SFM_PREC_MIXED))
         return SFM_EINVAL;

@@ -95,9 +95,13 @@ _NEIGH26 = np.array([(a, b, c) for c in (-1, 0, 1) for b in (-1, 0, 1) for a in 
 
 def build_hierarchy(ngb: Sequence[int], ni: int, nlev: int,
                     refine: Callable[[int, np.ndarray, "Hierarchy"], np.ndarray],
-                    periodic: bool, box_lo=(0.0, 0.0, 0.0), box_size: float = 1.0,
+                    periodic, box_lo=(0.0, 0.0, 0.0), box_size: float = 1.0,
                     max_iter: int = 50) -> Hierarchy:
     """Builds a properly nested octree.
+
+    ``periodic``: one bool for all three directions, or three (x, y, z);
+    a periodic direction wraps its links, the others touch the physical
+    boundary.
 
     ``refine(level, ijk, geom)`` returns a bool mask over the blocks ``ijk``
     (int array [m,3]) of ``level``: True refines the block into 8 children.
@@ -105,6 +109,8 @@ def build_hierarchy(ngb: Sequence[int], ni: int, nlev: int,
     predicate to compute cell coordinates.
     """
     ngb = tuple(int(v) for v in ngb)
+    per = (bool(periodic),) * 3 if np.isscalar(periodic) else tuple(bool(v) for v in periodic)
+    periodic = all(per)
     box_lo = np.asarray(box_lo, dtype=np.float64)
     geom = Hierarchy(ni=ni, ngb=ngb, nlev=nlev, periodic=periodic, box_lo=box_lo,
                      box_size=float(box_size), level=None, ijk=None, parent=None,
@@ -141,11 +147,11 @@ def build_hierarchy(ngb: Sequence[int], ni: int, nlev: int,
             keyset = np.sort(_pack(blk))
             ref = blk[flags[L]]
             nb_ = (ref[:, None, :] + _NEIGH26[None, :, :]).reshape(-1, 3)
-            if periodic:
-                nb_ = np.mod(nb_, ext)
-            else:
-                ok = np.all((nb_ >= 0) & (nb_ < ext), axis=1)
-                nb_ = nb_[ok]
+            for d in range(3):
+                if per[d]:
+                    nb_[:, d] = np.mod(nb_[:, d], ext[d])
+            ok = np.all((nb_ >= 0) & (nb_ < ext), axis=1)
+            nb_ = nb_[ok]
             k = _pack(nb_)
             pos = np.searchsorted(keyset, k)
             pos = np.minimum(pos, keyset.size - 1)
@@ -208,7 +214,7 @@ def build_hierarchy(ngb: Sequence[int], ni: int, nlev: int,
                 off[d] = -1 if lr == 0 else 1
                 qq = q + off
                 edge = (qq[:, d] < 0) | (qq[:, d] >= ext[d])
-                if periodic:
+                if per[d]:
                     qq = np.mod(qq, ext)
                     nbr[s:e, lr + 2 * d] = lookup(L, qq)
                 else:
@@ -338,6 +344,39 @@ def mirror_sphere(nbase: int = 3, ni: int = 8, nlev: int = 3, full: bool = False
                                box_lo=(-0.5, -0.5, -1.0), box_size=1.0)
     return build_hierarchy((nbase,) * 3, ni, nlev, _near_origin(radii), False,
                            box_lo=(-0.5, -0.5, 0.0), box_size=1.0)
+
+
+def _near_axis(levels_radius):
+    """Refines a block when the point of its box nearest the z axis lies
+    within levels_radius[L] (independent of z)."""
+    def ref(L, q, g):
+        cw = g.box_size / (g.ngb[0] * g.ni * (1 << L))
+        lo = g.box_lo[None, :2] + q[:, :2] * g.ni * cw
+        hi = lo + g.ni * cw
+        near = np.clip(0.0, lo, hi)
+        return np.sqrt((near * near).sum(axis=1)) < levels_radius[min(L, len(levels_radius) - 1)]
+    return ref
+
+
+def zperiodic_cylinder(nbase: int = 2, ni: int = 8, nlev: int = 3) -> Hierarchy:
+    """[-1/2, 1/2]^3 periodic in z, isolated in x and y (the box of
+    fmg_boundary_phys_cyl_zperiodic.F90 and ..._mask_zperiodic.F90), with
+    nbase^3 base blocks refined around the z axis."""
+    return build_hierarchy((nbase,) * 3, ni, nlev, _near_axis((0.3, 0.15, 0.08, 0.04)), (False, False, True),
+                           box_lo=(-0.5, -0.5, -0.5), box_size=1.0)
+
+
+def line_mass(x, y, z):
+    """rho = 1/(1+(R/0.08)^2) for R < 0.45, else 1e-3, R = sqrt(x^2+y^2):
+    independent of z."""
+    R = np.sqrt(x * x + y * y) + 0.0 * z
+    return np.where(R < 0.45, 1.0 / (1.0 + (R / 0.08) ** 2), 1e-3)
+
+
+def beaded_line(x, y, z):
+    """line_mass modulated along z (period 1/2): a z-periodic source that
+    depends on z."""
+    return line_mass(x, y, z) * (1.0 + 0.5 * np.cos(4.0 * np.pi * z))
 
 
 def wide_sphere(x, y, z):

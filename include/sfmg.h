@@ -81,6 +81,11 @@ typedef struct sfm_hier_desc {
 #define SFM_BC_SPHERE   1   /* fmg_boundary_phys_sphere.F90 (multipole ghosts)  */
 #define SFM_BC_ZMIRROR  2   /* fmg_boundary_phys_zmirror.F90: multipole ghosts,
                                a mirror plane on the box's z-min face          */
+#define SFM_BC_CYL_ZPERIODIC  3  /* fmg_boundary_phys_cyl_zperiodic.F90: periodic
+                               in z, the 2D potential a00 ln(r) on the x and y
+                               faces, the source masked outside a cylinder  */
+#define SFM_BC_MASK_ZPERIODIC 4  /* fmg_boundary_phys_mask_zperiodic.F90: as 3,
+                               the source masked below params.rho_mask      */
 #define SFM_PREC_FP64   0   /* every operation in FP64, as the reference       */
 #define SFM_PREC_MIXED  1   /* FP32 inner fmg_lin/vmg, FP64 outer loop and base solve */
 
@@ -102,6 +107,9 @@ typedef struct sfm_params {
                                 fmg.F90:193 does; 0: run until rel_tol/max_outer */
     int32_t profile;         /* 1: time every smoother launch on fmg level 0
                                 with CUDA events (sfm_stats.smoother_*)        */
+    double  rho_mask;        /* SFM_BC_MASK_ZPERIODIC: the source (4 pi G rho)
+                                is set to 0 where it is below this value
+                                (MP_rhomask, fmg_boundary_phys_mask_zperiodic.F90:129) */
 } sfm_params;
 
 /* Fills *p with the reference's defaults (periodic, FP64, 10 outer

@@ -108,6 +108,8 @@ struct Oracle {
 
     // ---------------- parameters ----------------
     int bc = SFM_BC_PERIODIC, lmax = 3, zero_mean = 1, nfmgmax = 10, stagnation_exit = 1;
+    double rho_mask = 0.0;   // MP_rhomask (SFM_BC_MASK_ZPERIODIC)
+    bool zperiodic() const { return bc == SFM_BC_CYL_ZPERIODIC || bc == SFM_BC_MASK_ZPERIODIC; }
     double four_pi_G = 4.0 * M_PI, errormax = 1e-3;
 
     // ---------------- fmg fields ----------------
@@ -157,7 +159,7 @@ struct Oracle {
             lstart[level[b] + 1]++;
         }
         for (int L = 0; L < nlev; L++) lstart[L + 1] += lstart[L];
-        bc = p->bc; lmax = p->lmax; zero_mean = p->zero_mean;
+        bc = p->bc; lmax = p->lmax; zero_mean = p->zero_mean; rho_mask = p->rho_mask;
         nfmgmax = p->max_outer; errormax = p->rel_tol; four_pi_G = p->four_pi_G;
         stagnation_exit = p->stagnation_exit;
         int rc = build_links();
@@ -621,6 +623,7 @@ struct Oracle {
     // -zmin, the moments carry the mirror's factor 2 or 0); a no-op for
     // periodic (fmg_boundary_phys_periodic.F90:109-112)
     void boundary_physical_grid(int ju, int jrho) {
+        if (zperiodic()) return boundary_physical_grid_cyl(ju, jrho);
         if (bc != SFM_BC_SPHERE && bc != SFM_BC_ZMIRROR) return;
         const int f = 0, n = NI;
         Arr &R = F(jrho, f), &U = F(ju, f);
@@ -652,6 +655,59 @@ struct Oracle {
                         for (int p = -1; p <= n; p++) {
                             int i, j, k; put3(dir, xg, p, q, i, j, k);
                             U.at(b, i, j, k) = multipole_eval(mom, X(b, 0, i), X(b, 1, j), X(b, 2, k));
+                        }
+                }
+    }
+
+    // z-periodic cylinder (fmg_boundary_phys_cyl_zperiodic.F90:97-232) and
+    // its density-masked variant (fmg_boundary_phys_mask_zperiodic.F90:97-232):
+    // mask the source -- outside the cylinder x^2 + y^2 >= min(xmax, ymax,
+    // -xmin, -ymin)^2, or where it is below MP_rhomask -- then a00 = (sum of
+    // rho dv over the base-level cells) / zlen / (2 pi) and the first ghost
+    // layer of every x and y boundary face gets a00 ln(sqrt(x^2 + y^2))
+    void boundary_physical_grid_cyl(int ju, int jrho) {
+        const int f = 0, n = NI;
+        Arr &R = F(jrho, f), &U = F(ju, f);
+        auto X = [&](int b, int d, int i) { return x0[3 * b + d] + (double)i * h0[level[b]]; };
+        int bmin = baseIdx[0], bmax = baseIdx.back();
+        double xmin = X(bmin, 0, 0), ymin = X(bmin, 1, 0), zmin = X(bmin, 2, 0);
+        double xmax = X(bmax, 0, n - 1), ymax = X(bmax, 1, n - 1), zmax = X(bmax, 2, n - 1);
+        double zlen = zmax - zmin + h0[0];   // fmg_bndp_xyzminmax
+        if (bc == SFM_BC_CYL_ZPERIODIC) {
+            double rr = std::min(std::min(xmax, ymax), std::min(-xmin, -ymin));
+            double rad2 = rr * rr;
+            for (int b = 0; b < nb; b++)
+                for (int k = -1; k <= n; k++)
+                    for (int j = -1; j <= n; j++)
+                        for (int i = -1; i <= n; i++) {
+                            double x = X(b, 0, i), y = X(b, 1, j);
+                            if (x * x + y * y >= rad2) R.at(b, i, j, k) = 0.0;
+                        }
+        } else {
+            for (int b = 0; b < nb; b++)
+                for (int k = -1; k <= n; k++)
+                    for (int j = -1; j <= n; j++)
+                        for (int i = -1; i <= n; i++)
+                            if (R.at(b, i, j, k) < rho_mask) R.at(b, i, j, k) = 0.0;
+        }
+        const double dv = h0[0] * h0[0] * h0[0];
+        double a00 = 0.0;
+        for (int b = lstart[0]; b < lstart[1]; b++)
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) a00 = a00 + R.at(b, i, j, k) * dv;
+        const double pi2 = 2.0 * (4.0 * std::atan(1.0));   // Pi2 (parameter.F90:14-15)
+        a00 = a00 / zlen / pi2;
+        for (int b = 0; b < nb; b++)
+            for (int dir = 0; dir < 2; dir++)
+                for (int lr = 0; lr < 2; lr++) {
+                    if (!touch[6 * b + lr + 2 * dir]) continue;
+                    int xg = (lr == Left) ? -1 : n;
+                    for (int q = -1; q <= n; q++)
+                        for (int p = -1; p <= n; p++) {
+                            int i, j, k; put3(dir, xg, p, q, i, j, k);
+                            double x = X(b, 0, i), y = X(b, 1, j);
+                            U.at(b, i, j, k) = std::log(std::sqrt(x * x + y * y)) * a00;
                         }
                 }
     }
@@ -1275,6 +1331,15 @@ struct Oracle {
     // second of the two copies writes u(:,:,0) onto itself); the sphere
     // module's mg_boundary_u is a no-op
     void mg_boundary_u(int m, int code) {
+        if (zperiodic()) {   // z wrap only (cyl_zperiodic.F90:60-72)
+            Arr &A = MG(code, m);
+            const int n = A.n;
+            for (int j = -1; j <= n; j++)
+                for (int i = -1; i <= n; i++) A.at(0, i, j, -1) = A.at(0, i, j, n - 1);
+            for (int j = -1; j <= n; j++)
+                for (int i = -1; i <= n; i++) A.at(0, i, j, n) = A.at(0, i, j, 0);
+            return;
+        }
         if (bc == SFM_BC_ZMIRROR) {
             Arr &A = MG(code, m);
             const int n = A.n;
@@ -1794,7 +1859,7 @@ struct Oracle {
 
     // dJdphi, dJdrho: [nb][(NI+2gw)^3]; interiors used / written
     int adjoint(const double *dJdphi, double *dJdrho, int gw, sfm_stats *st) {
-        if (bc == SFM_BC_ZMIRROR) return SFM_EINVAL;   // the mirror's transpose is not built
+        if (bc == SFM_BC_ZMIRROR || zperiodic()) return SFM_EINVAL;   // these boundaries' transposes are not built
         const int n = NI, Gi = NI + 2 * gw;
         for (auto &a : fld) std::fill(a.d.begin(), a.d.end(), 0.0);
         for (auto &a : flx) std::fill(a.d.begin(), a.d.end(), 0.0);
