@@ -31,6 +31,7 @@ SFM_BC_SPHERE = 1
 SFM_BC_ZMIRROR = 2
 SFM_BC_CYL_ZPERIODIC = 3
 SFM_BC_MASK_ZPERIODIC = 4
+SFM_BC_SPHERE_MHD_BE = 5
 SFM_PREC_FP64 = 0
 SFM_PREC_MIXED = 1
 SFM_MAX_HISTORY = 64
@@ -60,6 +61,7 @@ class SfmParams(C.Structure):
         ("max_outer", C.c_int32), ("rel_tol", C.c_double), ("four_pi_G", C.c_double),
         ("zero_mean", C.c_int32), ("ngh_io", C.c_int32), ("report_residual", C.c_int32),
         ("stagnation_exit", C.c_int32), ("profile", C.c_int32), ("rho_mask", C.c_double),
+        ("r_cloud", C.c_double),
     ]
 
 
@@ -123,6 +125,7 @@ def default_params(bc: int = SFM_BC_PERIODIC, **kw) -> SfmParams:
     p.stagnation_exit = 1
     p.profile = 0
     p.rho_mask = 0.0
+    p.r_cloud = 0.0
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -1622,7 +1622,7 @@ public:
     // (fmg_boundary_phys_sphere.F90:81-354, fmg_boundary_phys_zmirror.F90:100-382)
     void boundary_physical_grid() {
         if (zperiodic()) return boundary_physical_grid_cyl();
-        if (P.bc != SFM_BC_SPHERE && P.bc != SFM_BC_ZMIRROR) return;
+        if (P.bc != SFM_BC_SPHERE && P.bc != SFM_BC_ZMIRROR && P.bc != SFM_BC_SPHERE_MHD_BE) return;
         const bool zm = P.bc == SFM_BC_ZMIRROR;
         const int n = H.NI;
         int bmin = H.baseIdx.front(), bmax = H.baseIdx.back();
@@ -1632,6 +1632,7 @@ public:
         // the z-mirror box's z-min face is the mirror plane, not an edge of the sphere
         double rr = zm ? std::min(std::min(std::min(xmax, ymax), zmax), std::min(-xmin, -ymin))
                        : std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        if (P.bc == SFM_BC_SPHERE_MHD_BE) rr = P.r_cloud;   // the cloud's radius (sphere_MHD_BE.F90:72)
         double rad2 = rr * rr;
         run(OpSphereMask{SRC0, d_x0, d_h0, d_level, n, Gf[0], Vf[0], rad2}, (int64_t)H.nb * Vf[0]);
         const int64_t ncell = (int64_t)cnt(0) * n * n * n;
@@ -1907,8 +1908,9 @@ public:
     }
 
     int adjoint(const double *dJdphi, double *dJdrho, sfm_stats *stats, cudaStream_t s) override {
-        if (P.bc == SFM_BC_ZMIRROR || zperiodic()) {   // these boundaries' transposes are not built
-            last_error = "sfm_adjoint: not available on z-mirror and z-periodic cylinder boxes";
+        if (P.bc == SFM_BC_ZMIRROR || zperiodic() || P.bc == SFM_BC_SPHERE_MHD_BE) {
+            // these boundaries' transposes are not built
+            last_error = "sfm_adjoint: periodic and sphere boxes only";
             return SFM_EINVAL;
         }
         st_ = s ? s : own_;
@@ -2130,6 +2132,7 @@ void sfm_default_params(sfm_params *p) {
     p->stagnation_exit = 1;
     p->profile = 0;
     p->rho_mask = 0.0;
+    p->r_cloud = 0.0;
 }
 
 // No C++ exception may cross the C ABI: every entry point below runs its
@@ -2152,7 +2155,8 @@ static int create_impl(const sfm_hier_desc *h, const sfm_params *p, sfm_ctx **ou
     if (!h || !p || !out) return SFM_EINVAL;
     *out = nullptr;
     if (p->ngh_io < 1 || p->max_outer < 0 || p->max_outer > 1000 || !(p->rel_tol >= 0) ||
-        p->bc < SFM_BC_PERIODIC || p->bc > SFM_BC_MASK_ZPERIODIC || !std::isfinite(p->rho_mask) ||
+        p->bc < SFM_BC_PERIODIC || p->bc > SFM_BC_SPHERE_MHD_BE || !std::isfinite(p->rho_mask) ||
+        !std::isfinite(p->r_cloud) ||
         (p->lmax != 3 && p->lmax != 4) ||
         (p->precision != SFM_PREC_FP64 && p->precision != SFM_PREC_MIXED))
         return SFM_EINVAL;

@@ -86,6 +86,8 @@ typedef struct sfm_hier_desc {
                                faces, the source masked outside a cylinder  */
 #define SFM_BC_MASK_ZPERIODIC 4  /* fmg_boundary_phys_mask_zperiodic.F90: as 3,
                                the source masked below params.rho_mask      */
+#define SFM_BC_SPHERE_MHD_BE  5  /* fmg_boundary_phys_sphere_MHD_BE.F90: as 1,
+                               the source masked outside params.r_cloud     */
 #define SFM_PREC_FP64   0   /* every operation in FP64, as the reference       */
 #define SFM_PREC_MIXED  1   /* FP32 inner fmg_lin/vmg, FP64 outer loop and base solve */
 
@@ -110,6 +112,9 @@ typedef struct sfm_params {
     double  rho_mask;        /* SFM_BC_MASK_ZPERIODIC: the source (4 pi G rho)
                                 is set to 0 where it is below this value
                                 (MP_rhomask, fmg_boundary_phys_mask_zperiodic.F90:129) */
+    double  r_cloud;         /* SFM_BC_SPHERE_MHD_BE: the source is set to 0 at
+                                x^2+y^2+z^2 >= r_cloud^2 (Rcloud,
+                                fmg_boundary_phys_sphere_MHD_BE.F90:72)       */
 } sfm_params;
 
 /* Fills *p with the reference's defaults (periodic, FP64, 10 outer
@@ -188,7 +193,7 @@ int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g
  *   - The first call allocates the Krylov vectors (as many as fit, up to 30
  *     restarts' worth, in 80% of the free device memory).
  *   - Results are reproducible to roundoff, not bitwise (FP64 atomics).
- *   - Periodic and sphere boxes only: a z-mirror box returns SFM_EINVAL.
+ *   - Periodic and sphere boxes only: the other boundaries return SFM_EINVAL.
  * st: outer_iters = Krylov iterations, ratio[] = their residual history,
  * true_rel_residual = the final true relative residual. */
 int sfm_adjoint(sfm_ctx *c, const double *dJ_dphi, double *dJ_drho, sfm_stats *st);

@@ -109,6 +109,7 @@ struct Oracle {
     // ---------------- parameters ----------------
     int bc = SFM_BC_PERIODIC, lmax = 3, zero_mean = 1, nfmgmax = 10, stagnation_exit = 1;
     double rho_mask = 0.0;   // MP_rhomask (SFM_BC_MASK_ZPERIODIC)
+    double r_cloud = 0.0;    // Rcloud (SFM_BC_SPHERE_MHD_BE)
     bool zperiodic() const { return bc == SFM_BC_CYL_ZPERIODIC || bc == SFM_BC_MASK_ZPERIODIC; }
     double four_pi_G = 4.0 * M_PI, errormax = 1e-3;
 
@@ -160,6 +161,7 @@ struct Oracle {
         }
         for (int L = 0; L < nlev; L++) lstart[L + 1] += lstart[L];
         bc = p->bc; lmax = p->lmax; zero_mean = p->zero_mean; rho_mask = p->rho_mask;
+        r_cloud = p->r_cloud;
         nfmgmax = p->max_outer; errormax = p->rel_tol; four_pi_G = p->four_pi_G;
         stagnation_exit = p->stagnation_exit;
         int rc = build_links();
@@ -624,7 +626,7 @@ struct Oracle {
     // periodic (fmg_boundary_phys_periodic.F90:109-112)
     void boundary_physical_grid(int ju, int jrho) {
         if (zperiodic()) return boundary_physical_grid_cyl(ju, jrho);
-        if (bc != SFM_BC_SPHERE && bc != SFM_BC_ZMIRROR) return;
+        if (bc != SFM_BC_SPHERE && bc != SFM_BC_ZMIRROR && bc != SFM_BC_SPHERE_MHD_BE) return;
         const int f = 0, n = NI;
         Arr &R = F(jrho, f), &U = F(ju, f);
         auto X = [&](int b, int d, int i) { return x0[3 * b + d] + (double)i * h0[level[b]]; };
@@ -635,6 +637,7 @@ struct Oracle {
         double rr = bc == SFM_BC_ZMIRROR
                         ? std::min(std::min(std::min(xmax, ymax), zmax), std::min(-xmin, -ymin))
                         : std::min(std::min(std::min(xmax, ymax), std::min(zmax, -xmin)), std::min(-ymin, -zmin));
+        if (bc == SFM_BC_SPHERE_MHD_BE) rr = r_cloud;   // Rcloud (sphere_MHD_BE.F90:72)
         double rad2 = rr * rr;
         for (int b = 0; b < nb; b++)
             for (int k = -1; k <= n; k++)
@@ -1859,7 +1862,8 @@ struct Oracle {
 
     // dJdphi, dJdrho: [nb][(NI+2gw)^3]; interiors used / written
     int adjoint(const double *dJdphi, double *dJdrho, int gw, sfm_stats *st) {
-        if (bc == SFM_BC_ZMIRROR || zperiodic()) return SFM_EINVAL;   // these boundaries' transposes are not built
+        if (bc == SFM_BC_ZMIRROR || zperiodic() || bc == SFM_BC_SPHERE_MHD_BE)
+            return SFM_EINVAL;   // these boundaries' transposes are not built
         const int n = NI, Gi = NI + 2 * gw;
         for (auto &a : fld) std::fill(a.d.begin(), a.d.end(), 0.0);
         for (auto &a : flx) std::fill(a.d.begin(), a.d.end(), 0.0);

@@ -111,3 +111,23 @@ def test_zmirror_adjoint_is_refused():
         s.solve(rho)
         with pytest.raises(SFMError):
             s.adjoint(np.ones_like(rho))
+
+
+@pytest.mark.parametrize("prec", [abi.SFM_PREC_FP64, abi.SFM_PREC_MIXED], ids=["fp64", "mixed"])
+def test_mhd_be_sphere_matches_oracle(prec):
+    """fmg_boundary_phys_sphere_MHD_BE.F90: the sphere boundary with the
+    source masked outside the cloud radius Rcloud (params.r_cloud)."""
+    h = w.small_sphere(2, 8, 3, 2)
+    kw = dict(rel_tol=1e-10, max_outer=30, zero_mean=0, r_cloud=0.2)
+    rho = w.block_field(h, 2, w.softened_sphere)
+    _, psi1, g1, st1, _ = oracle_solve(h, rho, abi.default_params(abi.SFM_BC_SPHERE_MHD_BE, **kw))
+    with FMGPoisson(h, params=abi.default_params(abi.SFM_BC_SPHERE_MHD_BE, precision=prec, **kw)) as s:
+        psi2, g2, st2 = s.solve(rho)
+    n = h.ni
+    if prec == abi.SFM_PREC_FP64:
+        assert st2.outer_iters == st1.outer_iters
+        assert np.array_equal(psi2[:, 1:-1, 1:-1, 1:-1], psi1[:, 1:-1, 1:-1, 1:-1])
+        assert np.array_equal(g2[:, :, 2:2 + n, 2:2 + n, 2:2 + n], g1[:, :, 2:2 + n, 2:2 + n, 2:2 + n])
+    else:
+        assert st2.converged and st2.true_rel_residual <= 1e-10
+        assert rel(psi2[:, 2:2 + n, 2:2 + n, 2:2 + n], psi1[:, 2:2 + n, 2:2 + n, 2:2 + n]) <= 1e-9

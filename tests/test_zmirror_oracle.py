@@ -57,3 +57,24 @@ def test_mirror_ghost_layer_mirrors_the_first_plane():
     assert on.size > 0
     # (k, j, i) axes with 2 io ghost layers: plane k = -1 is index 1, k = 0 index 2
     assert np.array_equal(psi[on, 1, 1:-1, 1:-1], psi[on, 2, 1:-1, 1:-1])
+
+
+def test_mhd_be_sphere_masks_at_the_cloud_radius():
+    """fmg_boundary_phys_sphere_MHD_BE.F90 is the sphere module with the mask
+    radius Rcloud: with r_cloud equal to the sphere module's own radius
+    min(xmax, ymax, zmax, -xmin, -ymin, -zmin) the solve is the sphere's to
+    the bit; a smaller cloud masks more of the source."""
+    h = w.small_sphere(2, 8, 3, 2)
+    n = h.ni
+    base = h.x0[h.level == 0]
+    cw = h.cellwidth[0]
+    rr = min(base[:, 0].max() + (n - 1) * cw, base[:, 1].max() + (n - 1) * cw, base[:, 2].max() + (n - 1) * cw,
+             -base[:, 0].min(), -base[:, 1].min(), -base[:, 2].min())
+    kw = dict(rel_tol=1e-10, max_outer=30, zero_mean=0)
+    rho = w.block_field(h, 2, w.softened_sphere)
+    _, psi_s, _, _, _ = oracle_solve(h, rho, abi.default_params(abi.SFM_BC_SPHERE, **kw))
+    _, psi_b, _, _, _ = oracle_solve(h, rho, abi.default_params(abi.SFM_BC_SPHERE_MHD_BE, r_cloud=rr, **kw))
+    assert np.array_equal(psi_s, psi_b)
+    rc, psi_c, _, st, _ = oracle_solve(h, rho, abi.default_params(abi.SFM_BC_SPHERE_MHD_BE, r_cloud=0.2, **kw))
+    assert rc == abi.SFM_OK and st.converged
+    assert not np.array_equal(psi_c, psi_s)
