@@ -5,13 +5,20 @@
 // operation of fmg_cycle / fmg_lin / vmg_fas (fmg.F90:134-377, vmg.F90:116-243):
 // every block of a level (or of all levels) is updated by one launch driven
 // from device-resident block, face and reflux tables; the base-grid solve
-// (mg.F90:42-218) is one persistent CTA.  All fields of all levels stay in
-// HBM for the whole solve and across calls.
+// (mg.F90:42-218) is one persistent CTA or a thread-block cluster.  All
+// fields of all levels stay in HBM for the whole solve and across calls.
 //
 // Precision: Solver<double> is the plain FP64 path (bit-identical
 // expressions to the reference's); Solver<float> runs fmg_lin and vmg_fas in
 // FP32 inside the FP64 defect-correction loop, with the outer residual, the
-// accumulation into phi, the reflux flux sums and the base-grid solve in FP64.
+// accumulation into phi, the reflux flux sums and the base-grid solve in FP64;
+// its inner solve may follow a cheaper schedule than the reference's (the
+// tuner's fused multi-sweep smoothing, fewer V-cycles), since it only
+// preconditions the FP64 correction.
+//
+// Physical boundaries: periodic, isolated sphere, z-mirror sphere, MHD
+// Bonnor-Ebert sphere and the z-periodic cylinders (fmg_boundary_phys_*.F90),
+// each with its hooks at the reference's call sites.
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <omp.h>
