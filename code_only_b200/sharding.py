@@ -11,21 +11,33 @@ step for GPU ranks:
   Morton order (workloads.build_hierarchy); each level is cut into `world`
   contiguous ranges of nearly equal block counts, so each rank owns a
   compact region on every level.
-* ``GhostExchange`` -- for every pass (AMR level L, direction d) of the
-  three-pass fill, the cells a rank's own blocks read from blocks another
-  rank owns: the neighbour's boundary plane (whole transverse range, ghosts
-  included) for a same-level face, the coarse block's layer (the octant's
-  half face plus one cell on each side) for a coarse-fine face.  Both ends
-  derive the same lists from the hierarchy, so a pass exchange is one
-  grouped send/receive per peer of the packed values (``torch.distributed``
-  P2P: gloo between CPU ranks, NCCL between GPUs), each into the receiver's
-  own copy of the sender's block -- never a load from another GPU's memory.
+* ``HaloExchange`` -- for every step of the composite operator that reads
+  across blocks, the cells a rank's own blocks read from blocks another
+  rank owns:
+  - each pass (AMR level L, direction d) of the three-pass ghost fill: the
+    neighbour's boundary plane (whole transverse range, ghosts included) for
+    a same-level face, the coarse block's layer (the octant's half face plus
+    one cell on each side) for a coarse-fine face (fmg_ghostcell.F90:162,168,
+    353,358);
+  - each level of fmg_converge_c2p (children at L + 1 restricted onto their
+    parent at L): the child's interior for the linear restriction, the whole
+    block with its ghost layer for the cubic one (fmg_converge.F90:139,144);
+  - the flux correction: the face fluxes of a fine block whose face borders
+    the parent level, read by the owner of the coarse neighbour
+    (fmg_reflux.F90:158,166).
+  Both ends derive the same lists from the hierarchy, so a step's exchange
+  is one grouped send/receive per peer of the packed values
+  (``torch.distributed`` P2P: gloo between CPU ranks, NCCL between GPUs),
+  each into the receiver's own copy of the sender's block -- never a load
+  from another GPU's memory.
 
-Run before each pass, the exchange makes a rank's owned blocks end the fill
-with exactly the values a single rank computes (tests/test_sharding.py,
-world size 2, bit for bit).  Residual maxima are an all-reduce of one value
-(``allreduce_max``); the base grid (at most 32^3 cells) is gathered whole on
-every rank, where the base-grid solve runs redundantly.
+Run before each such step, the exchanges make a rank's owned blocks hold
+exactly the values a single rank computes: after the ghost fill, and after
+whole red-black sweeps and residuals of the composite operator
+(tests/test_sharding.py, world size 2, bit for bit).  Residual maxima are an
+all-reduce of one value (``allreduce_max``); the base grid (at most 32^3
+cells) is gathered whole on every rank, where the base-grid solve runs
+redundantly.
 """
 from __future__ import annotations
 
@@ -33,7 +45,7 @@ from typing import Dict, List, Tuple
 
 import numpy as np
 
-__all__ = ["partition", "GhostExchange", "allreduce_max"]
+__all__ = ["partition", "HaloExchange", "allreduce_max"]
 
 
 def partition(h, world: int) -> np.ndarray:
@@ -75,12 +87,14 @@ def _put3(d, x, a, b):
     return (x, a, b) if d == 0 else ((a, x, b) if d == 1 else (a, b, x))
 
 
-class GhostExchange:
-    """Send and receive lists of every ghost pass for one rank.
+class HaloExchange:
+    """Send and receive lists of every cross-block step for one rank.
 
-    Cell indices are flat offsets into a field of shape [nb, G, G, G]
-    (G = n + 2, i fastest), the layout of one fmg level; every rank holds a
-    full-size field and owns the blocks ``owner == rank``.
+    Cell indices are flat offsets into a field (or face-flux array) of shape
+    [nb, G, G, G] (G = n + 2, i fastest), the layout of one fmg level; every
+    rank holds full-size arrays and owns the blocks ``owner == rank``.
+    Steps are keyed ("ghost", L, d), ("converge", L, cubic) and
+    ("reflux", d).
     """
 
     def __init__(self, h, owner: np.ndarray, rank: int, n: int):
@@ -91,9 +105,9 @@ class GhostExchange:
         kind, src = _faces(h)
         lev = np.asarray(h.level)
         nb2 = n // 2
-        # needs[(L, d)][(reader, holder)] -> sorted unique flat cells the
+        # needs[step][(reader, holder)] -> sorted unique flat cells the
         # reader's blocks read from blocks the holder owns
-        self.needs: Dict[Tuple[int, int], Dict[Tuple[int, int], np.ndarray]] = {}
+        self.needs: Dict[tuple, Dict[Tuple[int, int], np.ndarray]] = {}
         rng = np.arange(-1, n + 1)
         for L in range(h.nlev):
             blocks = np.nonzero(lev == L)[0]
@@ -125,18 +139,63 @@ class GhostExchange:
                         i, j, kk = _put3(d, xs, pa.ravel(), qa.ravel())
                         cells = s * self.V + ((kk + 1) * G + (j + 1)) * G + (i + 1)
                         acc.setdefault((reader, holder), []).append(np.asarray(cells, dtype=np.int64))
-                self.needs[(L, d)] = {key: np.unique(np.concatenate(v)) for key, v in acc.items()}
+                self.needs[("ghost", L, d)] = {key: np.unique(np.concatenate(v)) for key, v in acc.items()}
+        # converge_c2p of level Lc: the parent's owner reads its children
+        inner = np.arange(0, n)
+        whole = np.arange(-1, n + 1)
+        for Lc in range(h.nlev - 1):
+            for cubic in (False, True):
+                r = whole if cubic else inner
+                kk, jj, ii = np.meshgrid(r, r, r, indexing="ij")
+                off = (((kk + 1) * G + (jj + 1)) * G + (ii + 1)).ravel()
+                acc = {}
+                for b in np.nonzero(lev == Lc + 1)[0]:
+                    reader, holder = int(self.owner[h.parent[b]]), int(self.owner[b])
+                    if reader != holder:
+                        acc.setdefault((reader, holder), []).append(int(b) * self.V + off)
+                self.needs[("converge", Lc, cubic)] = {k: np.unique(np.concatenate(v)) for k, v in acc.items()}
+        # flux correction: a fine face next to the parent level is read by the
+        # coarse neighbour's owner (the n x n fluxes on that face)
+        pq = np.arange(0, n)
+        pa, qa = np.meshgrid(pq, pq, indexing="xy")
+        for d in range(3):
+            acc = {}
+            for b in np.nonzero(lev > 0)[0]:
+                for lr in range(2):
+                    f = lr + 2 * d
+                    if kind[b, f] != 1:
+                        continue
+                    reader, holder = int(self.owner[src[b, f]]), int(self.owner[b])
+                    if reader == holder:
+                        continue
+                    xf = -1 if lr == 0 else n - 1
+                    i, j, kk = _put3(d, xf, pa.ravel(), qa.ravel())
+                    acc.setdefault((reader, holder), []).append(
+                        int(b) * self.V + ((kk + 1) * G + (j + 1)) * G + (i + 1))
+            self.needs[("reflux", d)] = {k: np.unique(np.concatenate(v)) for k, v in acc.items()}
 
-    def pass_exchange(self, field, L: int, d: int):
-        """Exchange for pass (L, d): send the values of this rank's blocks that
-        other ranks read, receive the values this rank reads from theirs,
-        each into this rank's copy of the sender's block.  `field` is a flat
-        contiguous torch tensor of the level's field (CPU with gloo, CUDA with
-        NCCL); every rank calls this for every pass in the same order."""
+    def ghost(self, field, L: int, d: int):
+        """Exchange before ghost pass (L, d) of `field`."""
+        self.exchange(field, ("ghost", L, d))
+
+    def converge(self, field, Lc: int, cubic: bool = False):
+        """Exchange before converge_c2p of level Lc (children at Lc + 1)."""
+        self.exchange(field, ("converge", Lc, bool(cubic)))
+
+    def reflux(self, flux_d, d: int):
+        """Exchange of direction d's face fluxes before the flux correction."""
+        self.exchange(flux_d, ("reflux", d))
+
+    def exchange(self, field, step: tuple):
+        """Send the values of this rank's blocks that other ranks read in
+        `step`, receive the values this rank reads from theirs, each into
+        this rank's copy of the sender's block.  `field` is a flat contiguous
+        torch tensor (CPU with gloo, CUDA with NCCL); every rank calls this
+        for every step in the same order."""
         import torch
         import torch.distributed as dist
         ops, recvs = [], []
-        for (reader, holder), cells in self.needs.get((L, d), {}).items():
+        for (reader, holder), cells in self.needs.get(step, {}).items():
             idx = torch.from_numpy(cells).to(field.device)
             if holder == self.rank:
                 ops.append(dist.P2POp(dist.isend, field[idx].contiguous(), reader))
@@ -150,8 +209,8 @@ class GhostExchange:
         for idx, buf in recvs:
             field[idx] = buf
 
-    def bytes_per_pass(self) -> Dict[Tuple[int, int], int]:
-        """Values this rank receives per pass x 8 bytes (FP64)."""
+    def bytes_per_step(self) -> Dict[tuple, int]:
+        """Values this rank receives per step x 8 bytes (FP64)."""
         out = {}
         for key, m in self.needs.items():
             out[key] = 8 * sum(int(c.size) for (reader, _), c in m.items() if reader == self.rank)

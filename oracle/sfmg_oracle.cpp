@@ -117,6 +117,11 @@ struct Oracle {
     std::vector<Arr> fld;   // [code*(FMax+1) + f]
     std::vector<Arr> flx;   // [dir*(FMax+1) + f]
     int FmgLevel_fill0 = Undef;
+    // blocks this process computes when the hierarchy is split over ranks
+    // (oracle_step); nullptr: every block, as one MPI rank of the reference
+    // with NPE = 1
+    const int8_t *own = nullptr;
+    bool mine(int b) const { return !own || own[b]; }
     double Resh2maxg = 0.0;
     std::vector<double> vmgResmaxg;
 
@@ -417,6 +422,7 @@ struct Oracle {
         OMP_FOR
         for (int b = lstart[Lf]; b < lstart[Lf + 1]; b++) {
             int p = parent[b];
+            if (!mine(p)) continue;
             int oi = octant[3 * b] * h2n, oj = octant[3 * b + 1] * h2n, ok = octant[3 * b + 2] * h2n;
             for (int kc = 0; kc < h2n; kc++)
                 for (int jc = 0; jc < h2n; jc++)
@@ -443,7 +449,7 @@ struct Oracle {
         for (int b = lstart[L]; b < lstart[L + 1]; b++)
             for (int lr = 0; lr < 2; lr++) {
                 int fc = lr + 2 * dir;
-                if (!sameLev[6 * b + fc]) continue;
+                if (!sameLev[6 * b + fc] || !mine(b)) continue;
                 int s = nbrGid[6 * b + fc];
                 int xr = (lr == Left) ? -1 : n;       // Recv
                 int xs = (lr == Left) ? n - 1 : 0;    // Send
@@ -488,7 +494,7 @@ struct Oracle {
         for (int b = lstart[L]; b < lstart[L + 1]; b++)
             for (int lr = 0; lr < 2; lr++) {
                 int fc = lr + 2 * dir;
-                if (!parLev[6 * b + fc]) continue;
+                if (!parLev[6 * b + fc] || !mine(b)) continue;
                 int cb = nbrGid[6 * b + fc];
                 // buffer = coarse layer adjacent to the face, octant half +-1
                 int xc = (lr == Left) ? n - 1 : 0;
@@ -610,7 +616,7 @@ struct Oracle {
         Arr &A = F(code, f);
         const int n = nF(f);
         for (int b = lstart[L]; b < lstart[L + 1]; b++) {
-            if (!touch[6 * b + Left + 2 * MZ]) continue;
+            if (!touch[6 * b + Left + 2 * MZ] || !mine(b)) continue;
             for (int j = -1; j <= n; j++)
                 for (int i = -1; i <= n; i++) A.at(b, i, j, -1) = A.at(b, i, j, 0);
         }
@@ -864,11 +870,17 @@ struct Oracle {
             fmg_boundary_u(f, ju);
         }
         FmgLevel_fill0 = Undef;
+        face_flux(f, ju);
+        fluxcorrection(f);
+    }
+    // the face fluxes of every non-skip block from its cells and ghost layer
+    // (fmg_poisson.F90:93-119)
+    void face_flux(int f, int ju) {
         Arr &U = F(ju, f);
         const int n = nF(f);
         OMP_FOR
         for (int b = 0; b < nb; b++) {
-            if (skip(b)) continue;
+            if (skip(b) || !mine(b)) continue;
             double hi = 1.0 / h(level[b], f);
             for (int k = -1; k <= n - 1; k++)
                 for (int j = -1; j <= n - 1; j++)
@@ -879,7 +891,6 @@ struct Oracle {
                         FL(MZ, f).at(b, i, j, k) = (U.at(b, i, j, k + 1) - u) * hi;
                     }
         }
-        fluxcorrection(f);
     }
 
     // fmg_fluxcorrection (fmg_reflux.F90:28-258): for every fine face whose
@@ -895,7 +906,7 @@ struct Oracle {
                 for (int dir = 0; dir < 3; dir++)
                     for (int lr = 0; lr < 2; lr++) {
                         int fc = lr + 2 * dir;
-                        if (!parLev[6 * b + fc]) continue;
+                        if (!parLev[6 * b + fc] || !mine(nbrGid[6 * b + fc])) continue;
                         Arr &Ff = FL(dir, f);
                         int xf = (lr == Left) ? -1 : n - 1;       // Ifs(lr,ndir)
                         Item it;
@@ -938,40 +949,48 @@ struct Oracle {
 
     // fmg_poisson_relax (:130-213)
     void relax(int f, int ju, int jrhs, bool bf0) {
-        const double sixth = 1.0 / 6.0;
-        const int n = nF(f);
         double resmax = 0.0;
         for (int ipass = 1; ipass <= 2; ipass++) {
             poisson_flux(f, ju, bf0);
-            Arr &U = F(ju, f), &R = F(jrhs, f);
-            double pm = 0.0;
+            resmax = std::max(resmax, relax_colour(f, ju, jrhs, ipass));
+        }
+        Resh2maxg = resmax;
+    }
+    // one colour (ipass) of the sweep from the current face fluxes; returns
+    // the maximum of |resh2| over the blocks it updates
+    double relax_colour(int f, int ju, int jrhs, int ipass) {
+        const double sixth = 1.0 / 6.0;
+        const int n = nF(f);
+        Arr &U = F(ju, f), &R = F(jrhs, f);
+        double pm = 0.0;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static) reduction(max : pm)
 #endif
-            for (int b = 0; b < nb; b++) {
-                if (skip(b)) continue;
-                double hh = h(level[b], f);
-                for (int k = 0; k < n; k++)
-                    for (int j = 0; j < n; j++)
-                        for (int i = (j + k + ipass) % 2; i < n; i += 2) {
-                            double resh2 = (divF(b, f, i, j, k) - R.at(b, i, j, k) * hh) * hh;
-                            U.at(b, i, j, k) = U.at(b, i, j, k) + sixth * resh2;
-                            pm = std::max(pm, std::fabs(resh2));
-                        }
-            }
-            resmax = std::max(resmax, pm);
+        for (int b = 0; b < nb; b++) {
+            if (skip(b) || !mine(b)) continue;
+            double hh = h(level[b], f);
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++)
+                    for (int i = (j + k + ipass) % 2; i < n; i += 2) {
+                        double resh2 = (divF(b, f, i, j, k) - R.at(b, i, j, k) * hh) * hh;
+                        U.at(b, i, j, k) = U.at(b, i, j, k) + sixth * resh2;
+                        pm = std::max(pm, std::fabs(resh2));
+                    }
         }
-        Resh2maxg = resmax;
+        return pm;
     }
 
     // fmg_poisson_resid (:217-265)
     void resid(int f, int jres, int ju, int jrhs, bool bf0) {
-        const int n = nF(f);
         poisson_flux(f, ju, bf0);
+        resid_from_flux(f, jres, jrhs);
+    }
+    void resid_from_flux(int f, int jres, int jrhs) {
+        const int n = nF(f);
         Arr &Rs = F(jres, f), &R = F(jrhs, f);
         OMP_FOR
         for (int b = 0; b < nb; b++) {
-            if (skip(b)) continue;
+            if (skip(b) || !mine(b)) continue;
             double hi = 1.0 / h(level[b], f);
             for (int k = 0; k < n; k++)
                 for (int j = 0; j < n; j++)
@@ -2168,6 +2187,92 @@ int oracle_ghost_pass(const sfm_hier_desc *h, const sfm_params *p, int f, int L,
         o.samelev(L, f, dir, IU);
     }
     std::copy(A.d.begin(), A.d.end(), field);
+    return SFM_OK;
+}
+
+// One piece of the composite operator at fmg level f, run only for the
+// blocks with own[b] != 0 (own NULL: every block) -- what one rank computes
+// between two exchanges when the blocks are split over ranks.  Arrays are
+// [nblocks][G][G][G] (G = (ni >> f) + 2); fx, fy, fz hold the face fluxes
+// (flux at i+1/2 stored at i, as GridLevel()%Block()%F).
+//   step 0  converge_c2p of AMR level L (children at L + 1), u in place; flag: cubic
+//   step 1  fmg_boundary_u, u in place
+//   step 2  ghost pass (L, dir): parentlev then samelev, u in place; flag: cubic
+//   step 3  face fluxes of u -> fx, fy, fz
+//   step 4  fluxcorrection on fx, fy, fz in place
+//   step 5  residual out = rhs - div F / h from fx, fy, fz
+//   step 6  one colour (flag = ipass 1 or 2) of the red-black sweep of u from
+//           fx, fy, fz and rhs; out[0] = max |resh2| over the blocks updated
+int oracle_step(const sfm_hier_desc *h, const sfm_params *p, int step, int f, int L, int dir, int flag,
+                const int8_t *own, double *u, double *fx, double *fy, double *fz, const double *rhs, double *out) {
+    Oracle o;
+    int rc = o.setup(h, p);
+    if (rc) return rc;
+    if (f < 0 || f > o.FMax || step < 0 || step > 6) return SFM_EINVAL;
+    o.own = own;
+    Arr &U = o.F(IU, f);
+    const size_t nv = U.d.size();
+    auto load = [&](Arr &A, const double *src) { if (src) std::copy(src, src + nv, A.d.begin()); };
+    auto store = [&](Arr &A, double *dst) { if (dst) std::copy(A.d.begin(), A.d.end(), dst); };
+    Arr *fl[3] = {&o.FL(MX, f), &o.FL(MY, f), &o.FL(MZ, f)};
+    double *fp[3] = {fx, fy, fz};
+    load(U, u);
+    for (int d = 0; d < 3; d++) load(*fl[d], fp[d]);
+    switch (step) {
+        case 0:
+            if (L < 0 || L > o.nlev - 2) return SFM_EINVAL;
+            o.converge_c2p_lev(L, f, IU, flag != 0);
+            store(U, u);
+            break;
+        case 1:
+            o.fmg_boundary_u(f, IU);
+            store(U, u);
+            break;
+        case 2:
+            if (L < 0 || L >= o.nlev || dir < 0 || dir > 2) return SFM_EINVAL;
+            o.parentlev(L, f, dir, IU, flag != 0);
+            o.samelev(L, f, dir, IU);
+            store(U, u);
+            break;
+        case 3:
+            o.face_flux(f, IU);
+            for (int d = 0; d < 3; d++) store(*fl[d], fp[d]);
+            break;
+        case 4:
+            o.fluxcorrection(f);
+            for (int d = 0; d < 3; d++) store(*fl[d], fp[d]);
+            break;
+        case 5:
+            if (!rhs || !out) return SFM_EINVAL;
+            load(o.F(IRHS, f), rhs);
+            o.resid_from_flux(f, IRES, IRHS);
+            store(o.F(IRES, f), out);
+            break;
+        case 6:
+            if (!rhs || !out || (flag != 1 && flag != 2)) return SFM_EINVAL;
+            load(o.F(IRHS, f), rhs);
+            out[0] = o.relax_colour(f, IU, IRHS, flag);
+            store(U, u);
+            break;
+    }
+    return SFM_OK;
+}
+
+// `sweeps` red-black sweeps of fmg_poisson_relax at fmg level f on u
+// (rhs fixed); returns Resh2maxg of the last sweep in *resmax
+int oracle_relax(const sfm_hier_desc *h, const sfm_params *p, int f, int sweeps, double *u, const double *rhs,
+                 double *resmax) {
+    Oracle o;
+    int rc = o.setup(h, p);
+    if (rc) return rc;
+    if (f < 0 || f > o.FMax || sweeps < 0) return SFM_EINVAL;
+    Arr &U = o.F(IU, f), &R = o.F(IRHS, f);
+    std::copy(u, u + U.d.size(), U.d.begin());
+    std::copy(rhs, rhs + R.d.size(), R.d.begin());
+    o.FmgLevel_fill0 = Undef;
+    for (int s = 0; s < sweeps; s++) o.relax(f, IU, IRHS, false);
+    std::copy(U.d.begin(), U.d.end(), u);
+    if (resmax) *resmax = o.Resh2maxg;
     return SFM_OK;
 }
 

@@ -41,6 +41,13 @@ def load_oracle():
     lib.oracle_ghost_pass.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.c_void_p]
     lib.oracle_ghost_pass.restype = C.c_int
+    lib.oracle_step.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_int, C.c_int, C.c_int,
+                                C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p]
+    lib.oracle_step.restype = C.c_int
+    lib.oracle_relax.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_int, C.c_int,
+                                 C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.oracle_relax.restype = C.c_int
     _lib = lib
     return lib
 
@@ -91,3 +98,41 @@ def oracle_ghost_pass(h, field, f, L=-1, d=0, cubic=False):
     rc = lib.oracle_ghost_pass(abi.HierDesc(h).ref(), C.byref(abi.default_params(abi.SFM_BC_PERIODIC)), f, L, d,
                                1 if cubic else 0, field.ctypes.data)
     assert rc == 0, rc
+
+
+# pieces of the composite operator (oracle_step)
+STEP_CONVERGE, STEP_BOUNDARY_U, STEP_GHOST, STEP_FLUX, STEP_FLUXCORR, STEP_RESID, STEP_RELAX = range(7)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    assert a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def oracle_step(h, step, f, u=None, flux=None, rhs=None, out=None, L=0, d=0, flag=0, own=None):
+    """One piece of the composite operator at fmg level f, for the blocks with
+    own[b] (all blocks when own is None); arrays [nb, G, G, G] updated in
+    place, flux a list of the three face-flux arrays."""
+    lib = load_oracle()
+    G = (h.ni >> f) + 2
+    for a in [u, rhs, None if step == STEP_RELAX else out] + list(flux or []):   # relax: out[0] = max
+        assert a is None or (a.dtype == np.float64 and a.size == h.nblocks * G ** 3), "array of the wrong size"
+    own8 = None if own is None else np.ascontiguousarray(own, dtype=np.int8)
+    fx, fy, fz = flux if flux is not None else (None, None, None)
+    rc = lib.oracle_step(abi.HierDesc(h).ref(), C.byref(abi.default_params(abi.SFM_BC_PERIODIC)), step, f, L, d,
+                         flag, _ptr(own8), _ptr(u), _ptr(fx), _ptr(fy), _ptr(fz), _ptr(rhs), _ptr(out))
+    assert rc == 0, rc
+
+
+def oracle_relax(h, u, rhs, f, sweeps):
+    """`sweeps` red-black sweeps of fmg_poisson_relax on u in place; returns Resh2maxg."""
+    lib = load_oracle()
+    G = (h.ni >> f) + 2
+    assert u.size == rhs.size == h.nblocks * G ** 3, "array of the wrong size"
+    m = C.c_double(0.0)
+    rc = lib.oracle_relax(abi.HierDesc(h).ref(), C.byref(abi.default_params(abi.SFM_BC_PERIODIC)), f, sweeps,
+                          _ptr(u), _ptr(np.ascontiguousarray(rhs)), C.byref(m))
+    assert rc == 0, rc
+    return m.value

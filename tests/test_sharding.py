@@ -1,17 +1,25 @@
-"""Block partition and ghost-cell halo exchange across two ranks (gloo on CPU).
+"""Block partition and halo exchange across two ranks (gloo on CPU).
 
 Each rank owns contiguous Morton ranges of blocks on every AMR level
-(sharding.partition).  Starting from a field whose blocks are all set on
-rank 0's view but whose non-owned blocks are NaN on each rank, every pass of
-the three-pass ghost fill (AMR level ascending, x then y then z;
-fmg_ghostcell.F90:43-55) is preceded by that pass's exchange
-(GhostExchange.pass_exchange) and then computed by the oracle's pass on the
-rank's field.  A rank's owned blocks must then hold, bit for bit, what one
-rank computes for the whole hierarchy -- no value read from a block another
-rank owns may be missing or stale, or a NaN (or a wrong value) appears.
-Hierarchies: periodic with 3 AMR levels (same-level and coarse-fine faces),
-isolated with physical-boundary faces; fmg levels n = 8 and n = 2, bilinear
-and bicubic coarse-fine ghosts.
+(sharding.partition) and holds NaN in the blocks it does not own.
+
+Ghost fill: every pass of the three-pass fill (AMR level ascending, x then
+y then z; fmg_ghostcell.F90:43-55) is preceded by that pass's exchange
+(HaloExchange.ghost) and then computed by the oracle's pass on the rank's
+field.
+
+Composite operator: red-black sweeps (fmg_poisson_relax) and residuals
+(fmg_poisson_resid) run as the oracle's pieces restricted to the rank's own
+blocks (oracle_step), with the converge, ghost-pass and flux-correction
+exchanges before the pieces that read other blocks, and the residual maximum
+all-reduced.
+
+A rank's owned blocks must then hold, bit for bit, what one rank computes
+for the whole hierarchy -- no value read from a block another rank owns may
+be missing or stale, or a NaN (or a wrong value) appears.  Hierarchies:
+periodic with 3 AMR levels (same-level and coarse-fine faces), isolated
+with physical-boundary faces; fmg levels n = 8, 4 and 2, bilinear and
+bicubic coarse-fine ghosts.
 """
 import os
 import socket
@@ -23,6 +31,9 @@ import torch.multiprocessing as mp
 
 CASES = [("periodic", 0, False), ("periodic", 2, False), ("periodic", 0, True), ("sphere", 0, True),
          ("sphere", 1, False)]
+# composite-operator cases: (hierarchy, fmg level)
+OP_CASES = [("periodic", 0), ("periodic", 1), ("periodic", 2), ("sphere", 0)]
+SWEEPS = 2
 
 
 def _free_port():
@@ -38,10 +49,10 @@ def _hier(kind):
     return w.small_periodic(2, 8, 3, 1) if kind == "periodic" else w.small_sphere(2, 8, 3, 2)
 
 
-def _field(h, f):
+def _field(h, f, seed=0):
     n = h.ni >> f
     G = n + 2
-    return np.random.default_rng(123 + f).standard_normal((h.nblocks, G, G, G))
+    return np.random.default_rng(123 + f + 1000 * seed).standard_normal((h.nblocks, G, G, G))
 
 
 def _worker(rank, world, port, q):
@@ -59,20 +70,72 @@ def _worker(rank, world, port, q):
             h = _hier(kind)
             n = h.ni >> f
             owner = sharding.partition(h, world)
-            ex = sharding.GhostExchange(h, owner, rank, n)
+            ex = sharding.HaloExchange(h, owner, rank, n)
             a = _field(h, f)
             a[owner != rank] = np.nan          # another rank's blocks are unknown here
             t = torch.from_numpy(a.reshape(-1))   # shares memory with a
             for L in range(h.nlev):
                 for d in range(3):
-                    ex.pass_exchange(t, L, d)
+                    ex.ghost(t, L, d)
                     oracle_ghost_pass(h, a, f, L, d, cubic)
             mine = owner == rank
             q.put((rank, kind, f, cubic, a[mine].copy(), int(mine.sum()),
-                   sum(ex.bytes_per_pass().values())))
+                   sum(ex.bytes_per_step().values())))
+        for kind, f in OP_CASES:
+            h = _hier(kind)
+            owner = sharding.partition(h, world)
+            u, res, maxima = _split_operator(h, f, owner, rank)
+            q.put((rank, "op", kind, f, u[owner == rank].copy(), res[owner == rank].copy(), maxima))
         q.put((rank, "max", sharding.allreduce_max(float(rank + 1))))
     finally:
         dist.destroy_process_group()
+
+
+def _split_operator(h, f, owner, rank):
+    """SWEEPS red-black sweeps and then one residual of the composite
+    operator on this rank's blocks, exchanges before the pieces that read
+    other ranks' blocks; returns (u, residual, per-sweep maxima)."""
+    import torch
+    from code_only_b200 import sharding
+    from tests import oracle_lib as ol
+    n = h.ni >> f
+    ex = sharding.HaloExchange(h, owner, rank, n)
+    own = owner == rank
+    u = _field(h, f)
+    rhs = _field(h, f, seed=1)
+    u[~own] = np.nan
+    flux = [np.full_like(u, np.nan) for _ in range(3)]
+    ut = torch.from_numpy(u.reshape(-1))
+    ft = [torch.from_numpy(a.reshape(-1)) for a in flux]
+
+    def poisson_flux():   # fmg_poisson_flux (fmg_poisson.F90:53-124)
+        for Lc in range(h.nlev - 2, -1, -1):
+            ex.converge(ut, Lc)
+            ol.oracle_step(h, ol.STEP_CONVERGE, f, u=u, L=Lc, own=own)
+        ol.oracle_step(h, ol.STEP_BOUNDARY_U, f, u=u, own=own)
+        for L in range(h.nlev):
+            for d in range(3):
+                ex.ghost(ut, L, d)
+                ol.oracle_step(h, ol.STEP_GHOST, f, u=u, L=L, d=d, own=own)
+        ol.oracle_step(h, ol.STEP_BOUNDARY_U, f, u=u, own=own)
+        ol.oracle_step(h, ol.STEP_FLUX, f, u=u, flux=flux, own=own)
+        for d in range(3):
+            ex.reflux(ft[d], d)
+        ol.oracle_step(h, ol.STEP_FLUXCORR, f, flux=flux, own=own)
+
+    maxima = []
+    for _ in range(SWEEPS):
+        m = 0.0
+        for ipass in (1, 2):
+            poisson_flux()
+            out = np.zeros(1)
+            ol.oracle_step(h, ol.STEP_RELAX, f, u=u, flux=flux, rhs=rhs, out=out, flag=ipass, own=own)
+            m = max(m, float(out[0]))
+        maxima.append(sharding.allreduce_max(m))
+    poisson_flux()
+    res = np.full_like(u, np.nan)
+    ol.oracle_step(h, ol.STEP_RESID, f, flux=flux, rhs=rhs, out=res, own=own)
+    return u, res, maxima
 
 
 def _run(world=2, timeout=240):
@@ -84,7 +147,7 @@ def _run(world=2, timeout=240):
         p.start()
     out = []
     t0 = time.time()
-    while len(out) < world * (len(CASES) + 1) and time.time() - t0 < timeout:
+    while len(out) < world * (len(CASES) + len(OP_CASES) + 1) and time.time() - t0 < timeout:
         try:
             out.append(q.get(timeout=5))
         except Exception:
@@ -124,7 +187,7 @@ def test_two_rank_ghost_fill_is_bitwise(two_ranks, case):
     oracle_ghost_pass(h, ref, f, -1, 0, cubic)         # the whole fill on one rank
     owner = sharding.partition(h, 2)
     got = {r: v for (r, k, ff, c, v, cnt, nbytes) in
-           [x for x in two_ranks if x[1] != "max"] if (k, ff, c) == case}
+           [x for x in two_ranks if x[1] not in ("max", "op")] if (k, ff, c) == case}
     assert set(got) == {0, 1}, "a rank did not report"
     for r in (0, 1):
         assert np.isfinite(got[r]).all()
@@ -134,3 +197,113 @@ def test_two_rank_ghost_fill_is_bitwise(two_ranks, case):
 def test_allreduce_max(two_ranks):
     vals = [x[2] for x in two_ranks if x[1] == "max"]
     assert vals == [2.0, 2.0]
+
+
+def _single_rank_operator(h, f):
+    """The same sweeps by the oracle's integrated fmg_poisson_relax, then the
+    residual of the result (one rank, every block)."""
+    from tests import oracle_lib as ol
+    u = _field(h, f)
+    rhs = _field(h, f, seed=1)
+    maxima = [ol.oracle_relax(h, u, rhs, f, 1) for _ in range(SWEEPS)]
+    flux = [np.zeros_like(u) for _ in range(3)]
+    v = u   # the residual's fill updates u's ghost layers and covered cells, as in the split run
+    # residual pieces without an ownership mask: fill, fluxes, correction
+    for Lc in range(h.nlev - 2, -1, -1):
+        ol.oracle_step(h, ol.STEP_CONVERGE, f, u=v, L=Lc)
+    ol.oracle_step(h, ol.STEP_BOUNDARY_U, f, u=v)
+    ol.oracle_ghost_pass(h, v, f, -1, 0, False)
+    ol.oracle_step(h, ol.STEP_BOUNDARY_U, f, u=v)
+    ol.oracle_step(h, ol.STEP_FLUX, f, u=v, flux=flux)
+    ol.oracle_step(h, ol.STEP_FLUXCORR, f, flux=flux)
+    res = np.zeros_like(u)
+    ol.oracle_step(h, ol.STEP_RESID, f, flux=flux, rhs=rhs, out=res)
+    return u, res, maxima
+
+
+@pytest.mark.parametrize("case", OP_CASES, ids=[f"{k}-f{f}" for k, f in OP_CASES])
+def test_two_rank_relax_and_residual_are_bitwise(two_ranks, case):
+    """Sweeps and residual of the composite operator split over two ranks
+    (converge, ghost-pass and flux-correction exchanges) equal one rank's."""
+    from code_only_b200 import sharding
+    kind, f = case
+    h = _hier(kind)
+    u_ref, res_ref, max_ref = _single_rank_operator(h, f)
+    owner = sharding.partition(h, 2)
+    got = {x[0]: x[4:] for x in two_ranks if x[1] == "op" and (x[2], x[3]) == case}
+    assert set(got) == {0, 1}, "a rank did not report"
+    for r in (0, 1):
+        u, res, maxima = got[r]
+        mine = owner == r
+        assert np.isfinite(u).all()
+        assert np.array_equal(u, u_ref[mine])
+        skip = (h.level != h.nlev - 1) & (h.child[:, 0] >= 0)
+        assert np.array_equal(res[~skip[mine]], res_ref[mine & ~skip])
+        assert maxima == max_ref
+
+
+def test_residual_pieces_match_the_composite_operator():
+    """The pieces of oracle_step, run on one rank, give the oracle's own
+    composite operator L u (oracle_apply_L: residual of rhs = 0)."""
+    import ctypes as C
+    from code_only_b200 import abi
+    from tests import oracle_lib as ol
+    h = _hier("periodic")
+    u = _field(h, 0)
+    v = u.copy()
+    flux = [np.zeros_like(u) for _ in range(3)]
+    for Lc in range(h.nlev - 2, -1, -1):
+        ol.oracle_step(h, ol.STEP_CONVERGE, 0, u=v, L=Lc)
+    ol.oracle_step(h, ol.STEP_BOUNDARY_U, 0, u=v)
+    ol.oracle_ghost_pass(h, v, 0, -1, 0, False)
+    ol.oracle_step(h, ol.STEP_BOUNDARY_U, 0, u=v)
+    ol.oracle_step(h, ol.STEP_FLUX, 0, u=v, flux=flux)
+    ol.oracle_step(h, ol.STEP_FLUXCORR, 0, flux=flux)
+    res = np.zeros_like(u)
+    ol.oracle_step(h, ol.STEP_RESID, 0, flux=flux, rhs=np.zeros_like(u), out=res)
+    lu = np.zeros_like(u)
+    lib = ol.load_oracle()
+    rc = lib.oracle_apply_L(abi.HierDesc(h).ref(), C.byref(abi.default_params(abi.SFM_BC_PERIODIC)),
+                            u.ctypes.data, lu.ctypes.data)
+    assert rc == 0
+    skip = (h.level != h.nlev - 1) & (h.child[:, 0] >= 0)
+    assert np.array_equal(-res[~skip], lu[~skip])
+
+
+def _drop_worker(rank, world, port, drop, q):
+    """_split_operator on the periodic hierarchy with one kind of exchange
+    turned into a no-op; reports whether the owned blocks stayed finite."""
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch.distributed as dist
+    from code_only_b200 import sharding
+    setattr(sharding.HaloExchange, drop, lambda *a, **k: None)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        h = _hier("periodic")
+        owner = sharding.partition(h, world)
+        u, res, _ = _split_operator(h, 0, owner, rank)
+        q.put((rank, bool(np.isfinite(u[owner == rank]).all() and np.isfinite(res[owner == rank]).all())))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("drop", ["ghost", "converge", "reflux"])
+def test_dropping_an_exchange_leaves_unknown_values(drop):
+    """Each kind of exchange is needed: without it a rank reads another rank's
+    block that it never received (NaN here)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_drop_worker, args=(r, 2, port, drop, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    try:
+        out = sorted(q.get(timeout=180) for _ in procs)
+    finally:
+        for p in procs:
+            p.join(timeout=30)
+            if p.is_alive():
+                p.kill()
+    assert [finite for _, finite in out] == [False, False]
