@@ -22,6 +22,9 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <omp.h>
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 #include <algorithm>
 #include <array>
@@ -2234,6 +2237,20 @@ template <int L>
 static inline void copy_row_n(double *d, const double *s) {
     std::memcpy(d, s, L * sizeof(double));
 }
+// a row into the staging buffer: the staging rows are written once and
+// then read by the copy engine only, so on x86-64 they go out as
+// non-temporal 16-byte stores (no read of the destination lines into the
+// cache before they are overwritten); d is 16-byte aligned (the staging
+// buffer is, and every row holds an even number of values)
+static inline void stream_row(double *d, const double *s, int len) {
+#if defined(__x86_64__)
+    if ((len & 1) == 0 && ((uintptr_t)d & 15) == 0) {
+        for (int q = 0; q < len; q += 2) _mm_stream_pd(d + q, _mm_loadu_pd(s + q));
+        return;
+    }
+#endif
+    std::memcpy(d, s, (size_t)len * sizeof(double));
+}
 static inline void copy_row(double *d, const double *s, int len) {
     switch (len) {
         case 4: copy_row_n<4>(d, s); break;
@@ -2277,9 +2294,12 @@ static void stage_rows(double *stage, double *io, int64_t row0, int64_t row1, in
             const int64_t b = r / ((int64_t)Gc * Gc);
             const int kj = (int)(r - b * Gc * Gc), k = kj / Gc, j = kj - k * Gc;
             double *o = io + b * Vi + ((int64_t)(k + gw - 1) * Gi + (j + gw - 1)) * Gi + (gw - 1);
-            if (to_stage) copy_row(stage + r * Gc, o, Gc);
+            if (to_stage) stream_row(stage + r * Gc, o, Gc);
             else copy_row(o, stage + r * Gc, Gc);
         }
+#if defined(__x86_64__)
+        if (to_stage) _mm_sfence();   // the streamed rows are visible before the copy is queued
+#endif
     });
 }
 
