@@ -24,7 +24,13 @@ step for GPU ranks:
     block with its ghost layer for the cubic one (fmg_converge.F90:139,144);
   - the flux correction: the face fluxes of a fine block whose face borders
     the parent level, read by the owner of the coarse neighbour
-    (fmg_reflux.F90:158,166).
+    (fmg_reflux.F90:158,166);
+  - the prolongation of the AMR-level V-cycle (vmg_interp_p2c_lev,
+    vmg_interpol.F90:82-164): the whole parent block, read by the child's
+    owner (the V-cycle's restriction is the converge step);
+  - the base-grid solve (mg_dataPrepare, mg_data.F90:179-253): the interior
+    of every base block, read by every rank, each of which then solves the
+    base grid itself and keeps its own base blocks.
   Both ends derive the same lists from the hierarchy, so a step's exchange
   is one grouped send/receive per peer of the packed values
   (``torch.distributed`` P2P: gloo between CPU ranks, NCCL between GPUs),
@@ -32,9 +38,10 @@ step for GPU ranks:
   from another GPU's memory.
 
 Run before each such step, the exchanges make a rank's owned blocks hold
-exactly the values a single rank computes: after the ghost fill, and after
-whole red-black sweeps and residuals of the composite operator
-(tests/test_sharding.py, world size 2, bit for bit).  Residual maxima are an
+exactly the values a single rank computes: after the ghost fill, after
+whole red-black sweeps and residuals of the composite operator, and after
+the V-cycle's prolongation and base-grid solve (tests/test_sharding.py,
+world size 2, bit for bit, for Morton-range and alternating owners).  Residual maxima are an
 all-reduce of one value (``allreduce_max``); the base grid (at most 32^3
 cells) is gathered whole on every rank, where the base-grid solve runs
 redundantly.
@@ -93,8 +100,8 @@ class HaloExchange:
     Cell indices are flat offsets into a field (or face-flux array) of shape
     [nb, G, G, G] (G = n + 2, i fastest), the layout of one fmg level; every
     rank holds full-size arrays and owns the blocks ``owner == rank``.
-    Steps are keyed ("ghost", L, d), ("converge", L, cubic) and
-    ("reflux", d).
+    Steps are keyed ("ghost", L, d), ("converge", L, cubic), ("reflux", d),
+    ("p2c", L) and ("base",).
     """
 
     def __init__(self, h, owner: np.ndarray, rank: int, n: int):
@@ -173,6 +180,30 @@ class HaloExchange:
                     acc.setdefault((reader, holder), []).append(
                         int(b) * self.V + ((kk + 1) * G + (j + 1)) * G + (i + 1))
             self.needs[("reflux", d)] = {k: np.unique(np.concatenate(v)) for k, v in acc.items()}
+        # prolongation of the AMR-level V-cycle (vmg_interp, parent onto its
+        # children at Lc + 1): the child's owner reads the whole parent block,
+        # ghost layer included (the trilinear stencil reaches it)
+        kk, jj, ii = np.meshgrid(whole, whole, whole, indexing="ij")
+        whole_off = (((kk + 1) * G + (jj + 1)) * G + (ii + 1)).ravel()
+        for Lc in range(h.nlev - 1):
+            acc = {}
+            for b in np.nonzero(lev == Lc + 1)[0]:
+                p = int(h.parent[b])
+                reader, holder = int(self.owner[b]), int(self.owner[p])
+                if reader != holder:
+                    acc.setdefault((reader, holder), []).append(p * self.V + whole_off)
+            self.needs[("p2c", Lc)] = {k: np.unique(np.concatenate(v)) for k, v in acc.items()}
+        # base-grid solve (vmg_slvsml -> mg_dataPrepare): every rank gathers
+        # the interiors of all base blocks and solves the base grid itself
+        kk, jj, ii = np.meshgrid(inner, inner, inner, indexing="ij")
+        inner_off = (((kk + 1) * G + (jj + 1)) * G + (ii + 1)).ravel()
+        acc = {}
+        for b in np.nonzero(lev == 0)[0]:
+            holder = int(self.owner[b])
+            for reader in range(self.world):
+                if reader != holder:
+                    acc.setdefault((reader, holder), []).append(int(b) * self.V + inner_off)
+        self.needs[("base",)] = {k: np.unique(np.concatenate(v)) for k, v in acc.items()}
 
     def ghost(self, field, L: int, d: int):
         """Exchange before ghost pass (L, d) of `field`."""
@@ -185,6 +216,14 @@ class HaloExchange:
     def reflux(self, flux_d, d: int):
         """Exchange of direction d's face fluxes before the flux correction."""
         self.exchange(flux_d, ("reflux", d))
+
+    def p2c(self, field, Lc: int):
+        """Exchange before the prolongation of level Lc onto Lc + 1."""
+        self.exchange(field, ("p2c", Lc))
+
+    def base(self, field):
+        """Exchange before the base-grid solve: every base block to every rank."""
+        self.exchange(field, ("base",))
 
     def exchange(self, field, step: tuple):
         """Send the values of this rank's blocks that other ranks read in

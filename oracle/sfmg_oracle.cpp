@@ -1242,19 +1242,24 @@ struct Oracle {
         vmg_ghostcell(Lc, juc);
         vmg_boundary_extrap(Lc, juc);
         vmg_boundary_u(Lc, FMax, juc);
+        vmg_p2c(Lf, juf, juc);
+        vmg_boundary_fill0(Lc, juc);
+        vmg_boundary_u(Lc, FMax, juc);
+    }
+    // the prolongation loop of vmg_interp: every child at Lf from its parent
+    void vmg_p2c(int Lf, int juf, int juc) {
+        const int Lc = Lf - 1;
         Arr &Fo = F(juf, FMax), &C = F(juc, FMax);
         const int n = nF(FMax), h2n = n / 2;
         for (int p = lstart[Lc]; p < lstart[Lc + 1]; p++)
             for (int c = 0; c < 8; c++) {
                 int cb = child[8 * p + c];
-                if (cb == Undef) continue;
+                if (cb == Undef || !mine(cb)) continue;
                 int oi = (c & 1) * h2n, oj = ((c >> 1) & 1) * h2n, ok = ((c >> 2) & 1) * h2n;
                 for (int k = 0; k < n; k++)
                     for (int j = 0; j < n; j++)
                         for (int i = 0; i < n; i++) Fo.at(cb, i, j, k) = trilinear_cell(C, p, i, j, k, oi, oj, ok);
             }
-        vmg_boundary_fill0(Lc, juc);
-        vmg_boundary_u(Lc, FMax, juc);
     }
     // vmg_zeroAverage (vmg.F90:900-916) through fmg_ave (fmg_data.F90:730-769)
     void vmg_zeroAverage(int L, int code) {
@@ -1342,6 +1347,7 @@ struct Oracle {
             for (int jb = 0; jb < ngb[1]; jb++)
                 for (int ib = 0; ib < ngb[0]; ib++) {
                     int b = baseIdx[((size_t)kb * ngb[1] + jb) * ngb[0] + ib];
+                    if (!mine(b)) continue;
                     for (int k = 0; k < n; k++)
                         for (int j = 0; j < n; j++)
                             for (int i = 0; i < n; i++) U.at(b, i, j, k) = P.at(0, ib * n + i, jb * n + j, kb * n + k);
@@ -2203,12 +2209,18 @@ int oracle_ghost_pass(const sfm_hier_desc *h, const sfm_params *p, int f, int L,
 //   step 5  residual out = rhs - div F / h from fx, fy, fz
 //   step 6  one colour (flag = ipass 1 or 2) of the red-black sweep of u from
 //           fx, fy, fz and rhs; out[0] = max |resh2| over the blocks updated
+//   step 7  (f = FMax) the base-grid solve of vmg_slvsml: the base blocks of
+//           u and rhs gathered into the base grid, one mg_cycle, u of the
+//           base blocks restored
+//   step 8  (f = FMax) the prolongation loop of vmg_interp onto AMR level L:
+//           out (every child at L) from u (its parent)
 int oracle_step(const sfm_hier_desc *h, const sfm_params *p, int step, int f, int L, int dir, int flag,
                 const int8_t *own, double *u, double *fx, double *fy, double *fz, const double *rhs, double *out) {
     Oracle o;
     int rc = o.setup(h, p);
     if (rc) return rc;
-    if (f < 0 || f > o.FMax || step < 0 || step > 6) return SFM_EINVAL;
+    if (f < 0 || f > o.FMax || step < 0 || step > 8) return SFM_EINVAL;
+    if (step >= 7 && f != o.FMax) return SFM_EINVAL;
     o.own = own;
     Arr &U = o.F(IU, f);
     const size_t nv = U.d.size();
@@ -2253,6 +2265,20 @@ int oracle_step(const sfm_hier_desc *h, const sfm_params *p, int step, int f, in
             load(o.F(IRHS, f), rhs);
             out[0] = o.relax_colour(f, IU, IRHS, flag);
             store(U, u);
+            break;
+        case 7:
+            if (!rhs || !o.useSerialMg) return SFM_EINVAL;
+            load(o.F(IRHS, f), rhs);
+            o.mg_dataPrepare(IRHS, IU);
+            o.mg_cycle();
+            o.mg_dataRestore(IU);
+            store(U, u);
+            break;
+        case 8:
+            if (!out || L < 1 || L >= o.nlev) return SFM_EINVAL;
+            load(o.F(IRES, f), out);
+            o.vmg_p2c(L, IRES, IU);
+            store(o.F(IRES, f), out);
             break;
     }
     return SFM_OK;

@@ -101,7 +101,8 @@ def oracle_ghost_pass(h, field, f, L=-1, d=0, cubic=False):
 
 
 # pieces of the composite operator (oracle_step)
-STEP_CONVERGE, STEP_BOUNDARY_U, STEP_GHOST, STEP_FLUX, STEP_FLUXCORR, STEP_RESID, STEP_RELAX = range(7)
+(STEP_CONVERGE, STEP_BOUNDARY_U, STEP_GHOST, STEP_FLUX, STEP_FLUXCORR, STEP_RESID, STEP_RELAX, STEP_BASE_SOLVE,
+ STEP_P2C) = range(9)
 
 
 def _ptr(a):
@@ -111,7 +112,8 @@ def _ptr(a):
     return a.ctypes.data
 
 
-def oracle_step(h, step, f, u=None, flux=None, rhs=None, out=None, L=0, d=0, flag=0, own=None):
+def oracle_step(h, step, f, u=None, flux=None, rhs=None, out=None, L=0, d=0, flag=0, own=None,
+                bc=abi.SFM_BC_PERIODIC):
     """One piece of the composite operator at fmg level f, for the blocks with
     own[b] (all blocks when own is None); arrays [nb, G, G, G] updated in
     place, flux a list of the three face-flux arrays."""
@@ -121,7 +123,7 @@ def oracle_step(h, step, f, u=None, flux=None, rhs=None, out=None, L=0, d=0, fla
         assert a is None or (a.dtype == np.float64 and a.size == h.nblocks * G ** 3), "array of the wrong size"
     own8 = None if own is None else np.ascontiguousarray(own, dtype=np.int8)
     fx, fy, fz = flux if flux is not None else (None, None, None)
-    rc = lib.oracle_step(abi.HierDesc(h).ref(), C.byref(abi.default_params(abi.SFM_BC_PERIODIC)), step, f, L, d,
+    rc = lib.oracle_step(abi.HierDesc(h).ref(), C.byref(abi.default_params(bc)), step, f, L, d,
                          flag, _ptr(own8), _ptr(u), _ptr(fx), _ptr(fy), _ptr(fz), _ptr(rhs), _ptr(out))
     assert rc == 0, rc
 

@@ -14,6 +14,15 @@ blocks (oracle_step), with the converge, ghost-pass and flux-correction
 exchanges before the pieces that read other blocks, and the residual maximum
 all-reduced.
 
+AMR-level V-cycle: the prolongation onto every level (parent blocks to the
+children's owners) and the base-grid solve (every base block to every
+rank), likewise.
+
+Owners are contiguous Morton ranges per level (sharding.partition) and,
+to put most neighbours, parents and children on the other rank, alternating
+blocks; with alternating owners, turning any one kind of exchange into a
+no-op must leave NaN in the owned blocks.
+
 A rank's owned blocks must then hold, bit for bit, what one rank computes
 for the whole hierarchy -- no value read from a block another rank owns may
 be missing or stale, or a NaN (or a wrong value) appears.  Hierarchies:
@@ -34,6 +43,20 @@ CASES = [("periodic", 0, False), ("periodic", 2, False), ("periodic", 0, True), 
 # composite-operator cases: (hierarchy, fmg level)
 OP_CASES = [("periodic", 0), ("periodic", 1), ("periodic", 2), ("sphere", 0)]
 SWEEPS = 2
+# AMR-level V-cycle transfers (prolongation, base-grid solve) at the vmg
+# blocks' fmg level
+VMG_CASES = ["periodic", "sphere"]
+# owners: contiguous Morton ranges per level (sharding.partition), and
+# alternating blocks, which puts most neighbours, parents and children of a
+# block on the other rank
+PARTS = ["morton", "alternating"]
+
+
+def _owner(h, part, world=2):
+    from code_only_b200 import sharding
+    if part == "morton":
+        return sharding.partition(h, world)
+    return (np.arange(h.nblocks) % world).astype(np.int32)
 
 
 def _free_port():
@@ -81,11 +104,17 @@ def _worker(rank, world, port, q):
             mine = owner == rank
             q.put((rank, kind, f, cubic, a[mine].copy(), int(mine.sum()),
                    sum(ex.bytes_per_step().values())))
-        for kind, f in OP_CASES:
-            h = _hier(kind)
-            owner = sharding.partition(h, world)
-            u, res, maxima = _split_operator(h, f, owner, rank)
-            q.put((rank, "op", kind, f, u[owner == rank].copy(), res[owner == rank].copy(), maxima))
+        for part in PARTS:
+            for kind, f in OP_CASES:
+                h = _hier(kind)
+                owner = _owner(h, part, world)
+                u, res, maxima = _split_operator(h, f, owner, rank)
+                q.put((rank, "op", (kind, f, part), u[owner == rank].copy(), res[owner == rank].copy(), maxima))
+            for kind in VMG_CASES:
+                h = _hier(kind)
+                owner = _owner(h, part, world)
+                fine, base = _split_vmg(h, owner, rank)
+                q.put((rank, "vmg", (kind, part), fine[owner == rank].copy(), base[owner == rank].copy()))
         q.put((rank, "max", sharding.allreduce_max(float(rank + 1))))
     finally:
         dist.destroy_process_group()
@@ -138,6 +167,43 @@ def _split_operator(h, f, owner, rank):
     return u, res, maxima
 
 
+def _fmax(h):
+    f = 0
+    while (2 << f) < h.ni:
+        f += 1
+    return f
+
+
+def _bc(kind):
+    from code_only_b200 import abi
+    return abi.SFM_BC_PERIODIC if kind == "periodic" else abi.SFM_BC_SPHERE
+
+
+def _split_vmg(h, owner, rank):
+    """The V-cycle's prolongation onto every AMR level and the base-grid
+    solve on this rank's blocks, exchanges first; returns (prolonged field,
+    field after the base solve)."""
+    import torch
+    from code_only_b200 import sharding
+    from tests import oracle_lib as ol
+    f = _fmax(h)
+    ex = sharding.HaloExchange(h, owner, rank, h.ni >> f)
+    own = owner == rank
+    c, fine = _field(h, f, seed=2), _field(h, f, seed=3)
+    u, r = _field(h, f, seed=4), _field(h, f, seed=5)
+    for a in (c, fine, u, r):
+        a[~own] = np.nan
+    ct, ut, rt = (torch.from_numpy(a.reshape(-1)) for a in (c, u, r))
+    for Lf in range(1, h.nlev):
+        ex.p2c(ct, Lf - 1)
+        ol.oracle_step(h, ol.STEP_P2C, f, u=c, out=fine, L=Lf, own=own)
+    ex.base(ut)
+    ex.base(rt)
+    bc = _bc("periodic" if (h.touch == 0).all() else "sphere")
+    ol.oracle_step(h, ol.STEP_BASE_SOLVE, f, u=u, rhs=r, own=own, bc=bc)
+    return fine, u
+
+
 def _run(world=2, timeout=240):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -147,7 +213,8 @@ def _run(world=2, timeout=240):
         p.start()
     out = []
     t0 = time.time()
-    while len(out) < world * (len(CASES) + len(OP_CASES) + 1) and time.time() - t0 < timeout:
+    n_msgs = len(CASES) + len(PARTS) * (len(OP_CASES) + len(VMG_CASES)) + 1
+    while len(out) < world * n_msgs and time.time() - t0 < timeout:
         try:
             out.append(q.get(timeout=5))
         except Exception:
@@ -187,7 +254,7 @@ def test_two_rank_ghost_fill_is_bitwise(two_ranks, case):
     oracle_ghost_pass(h, ref, f, -1, 0, cubic)         # the whole fill on one rank
     owner = sharding.partition(h, 2)
     got = {r: v for (r, k, ff, c, v, cnt, nbytes) in
-           [x for x in two_ranks if x[1] not in ("max", "op")] if (k, ff, c) == case}
+           [x for x in two_ranks if x[1] not in ("max", "op", "vmg")] if (k, ff, c) == case}
     assert set(got) == {0, 1}, "a rank did not report"
     for r in (0, 1):
         assert np.isfinite(got[r]).all()
@@ -221,16 +288,16 @@ def _single_rank_operator(h, f):
     return u, res, maxima
 
 
+@pytest.mark.parametrize("part", PARTS)
 @pytest.mark.parametrize("case", OP_CASES, ids=[f"{k}-f{f}" for k, f in OP_CASES])
-def test_two_rank_relax_and_residual_are_bitwise(two_ranks, case):
+def test_two_rank_relax_and_residual_are_bitwise(two_ranks, case, part):
     """Sweeps and residual of the composite operator split over two ranks
     (converge, ghost-pass and flux-correction exchanges) equal one rank's."""
-    from code_only_b200 import sharding
     kind, f = case
     h = _hier(kind)
     u_ref, res_ref, max_ref = _single_rank_operator(h, f)
-    owner = sharding.partition(h, 2)
-    got = {x[0]: x[4:] for x in two_ranks if x[1] == "op" and (x[2], x[3]) == case}
+    owner = _owner(h, part)
+    got = {x[0]: x[3:] for x in two_ranks if x[1] == "op" and x[2] == (kind, f, part)}
     assert set(got) == {0, 1}, "a rank did not report"
     for r in (0, 1):
         u, res, maxima = got[r]
@@ -282,14 +349,17 @@ def _drop_worker(rank, world, port, drop, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         h = _hier("periodic")
-        owner = sharding.partition(h, world)
-        u, res, _ = _split_operator(h, 0, owner, rank)
-        q.put((rank, bool(np.isfinite(u[owner == rank]).all() and np.isfinite(res[owner == rank]).all())))
+        owner = _owner(h, "alternating", world)
+        if drop in ("p2c", "base"):
+            a, b = _split_vmg(h, owner, rank)
+        else:
+            a, b = _split_operator(h, 0, owner, rank)[:2]
+        q.put((rank, bool(np.isfinite(a[owner == rank]).all() and np.isfinite(b[owner == rank]).all())))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("drop", ["ghost", "converge", "reflux"])
+@pytest.mark.parametrize("drop", ["ghost", "converge", "reflux", "p2c", "base"])
 def test_dropping_an_exchange_leaves_unknown_values(drop):
     """Each kind of exchange is needed: without it a rank reads another rank's
     block that it never received (NaN here)."""
@@ -306,4 +376,30 @@ def test_dropping_an_exchange_leaves_unknown_values(drop):
             p.join(timeout=30)
             if p.is_alive():
                 p.kill()
-    assert [finite for _, finite in out] == [False, False]
+    assert len(out) == 2 and not any(finite for _, finite in out)
+
+
+@pytest.mark.parametrize("part", PARTS)
+@pytest.mark.parametrize("kind", VMG_CASES)
+def test_two_rank_vcycle_transfers_are_bitwise(two_ranks, kind, part):
+    """The AMR-level V-cycle's prolongation (parent block to the child's
+    owner) and base-grid solve (every base block to every rank) split over
+    two ranks equal one rank's, block for block."""
+    from tests import oracle_lib as ol
+    h = _hier(kind)
+    f = _fmax(h)
+    c, fine = _field(h, f, seed=2), _field(h, f, seed=3)
+    u, r = _field(h, f, seed=4), _field(h, f, seed=5)
+    for Lf in range(1, h.nlev):
+        ol.oracle_step(h, ol.STEP_P2C, f, u=c, out=fine, L=Lf)
+    ol.oracle_step(h, ol.STEP_BASE_SOLVE, f, u=u, rhs=r, bc=_bc(kind))
+    owner = _owner(h, part)
+    got = {x[0]: x[3:] for x in two_ranks if x[1] == "vmg" and x[2] == (kind, part)}
+    assert set(got) == {0, 1}, "a rank did not report"
+    for rk in (0, 1):
+        g_fine, g_base = got[rk]
+        mine = owner == rk
+        assert np.array_equal(g_fine, fine[mine])
+        assert np.array_equal(g_base, u[mine])
+        base = h.level[mine] == 0
+        assert np.isfinite(g_base[base]).all()
