@@ -30,7 +30,11 @@ step for GPU ranks:
     owner (the V-cycle's restriction is the converge step);
   - the base-grid solve (mg_dataPrepare, mg_data.F90:179-253): the interior
     of every base block, read by every rank, each of which then solves the
-    base grid itself and keeps its own base blocks.
+    base grid itself and keeps its own base blocks (the same gather serves
+    the isolated boundary's multipole moments, one running sum over the
+    base cells in order, evaluated by every rank);
+  - ordered sums (``gather_blocks``): per-block partials gathered exactly,
+    then folded in block order on every rank.
   Both ends derive the same lists from the hierarchy, so a step's exchange
   is one grouped send/receive per peer of the packed values
   (``torch.distributed`` P2P: gloo between CPU ranks, NCCL between GPUs),
@@ -224,6 +228,21 @@ class HaloExchange:
     def base(self, field):
         """Exchange before the base-grid solve: every base block to every rank."""
         self.exchange(field, ("base",))
+
+    def gather_blocks(self, values):
+        """Every block's value of a per-block array ([nb] float64 torch
+        tensor, this rank's entries set) from its owner: an all-reduce sum
+        in which every other rank adds -0.0, so each entry comes out exactly
+        as its owner had it (signed zeros and NaN included).  The ordered
+        sums of the solve -- the mean of rho (fmg_data_if.F90:59-82) and the
+        level averages of vmg_zeroAverage -- then fold these per-block
+        partials in block order on every rank, the single-rank order."""
+        import torch
+        import torch.distributed as dist
+        mine = torch.from_numpy(self.owner == self.rank).to(values.device)
+        t = torch.where(mine, values, torch.full_like(values, -0.0))
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return t
 
     def exchange(self, field, step: tuple):
         """Send the values of this rank's blocks that other ranks read in

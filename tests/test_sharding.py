@@ -115,6 +115,9 @@ def _worker(rank, world, port, q):
                 owner = _owner(h, part, world)
                 fine, base = _split_vmg(h, owner, rank)
                 q.put((rank, "vmg", (kind, part), fine[owner == rank].copy(), base[owner == rank].copy()))
+        for part in PARTS:
+            h = _hier("periodic")
+            q.put((rank, "mean", part, _split_mean(h, _owner(h, part, world), rank)))
         q.put((rank, "max", sharding.allreduce_max(float(rank + 1))))
     finally:
         dist.destroy_process_group()
@@ -204,6 +207,39 @@ def _split_vmg(h, owner, rank):
     return fine, u
 
 
+def _rho(h):
+    G = h.ni + 4   # two io ghost layers
+    return np.random.default_rng(77).standard_normal((h.nblocks, G, G, G)) + 1.0
+
+
+def _split_mean(h, owner, rank):
+    """The mean of 4 pi G rho over the leaf cells as fmg_make_physvar forms
+    it (fmg_data_if.F90:59-82): per-block sums of this rank's leaf blocks
+    (k, j, i order), gathered, then folded in block order."""
+    import torch
+    from code_only_b200 import abi, sharding
+    ex = sharding.HaloExchange(h, owner, rank, h.ni)
+    four_pi_g = abi.default_params(abi.SFM_BC_PERIODIC).four_pi_G
+    rho, n = _rho(h), h.ni
+    part = np.full(h.nblocks, np.nan)
+    leaf = h.child[:, 0] < 0
+    for b in np.nonzero((owner == rank) & leaf)[0]:
+        s = 0.0
+        for k in range(n):
+            for j in range(n):
+                for i in range(n):
+                    s = s + float(rho[b, k + 2, j + 2, i + 2]) * four_pi_g
+        part[b] = s
+    part = ex.gather_blocks(torch.from_numpy(part)).numpy()
+    mass = vol = 0.0
+    for b in np.nonzero(leaf)[0]:   # blocks are sorted by level
+        hL = float(h.cellwidth[h.level[b]])
+        dv = hL * hL * hL
+        mass = mass + float(part[b]) * dv
+        vol = vol + float(n * n * n) * dv
+    return mass / vol
+
+
 def _run(world=2, timeout=240):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -213,7 +249,7 @@ def _run(world=2, timeout=240):
         p.start()
     out = []
     t0 = time.time()
-    n_msgs = len(CASES) + len(PARTS) * (len(OP_CASES) + len(VMG_CASES)) + 1
+    n_msgs = len(CASES) + len(PARTS) * (len(OP_CASES) + len(VMG_CASES) + 1) + 1
     while len(out) < world * n_msgs and time.time() - t0 < timeout:
         try:
             out.append(q.get(timeout=5))
@@ -254,7 +290,7 @@ def test_two_rank_ghost_fill_is_bitwise(two_ranks, case):
     oracle_ghost_pass(h, ref, f, -1, 0, cubic)         # the whole fill on one rank
     owner = sharding.partition(h, 2)
     got = {r: v for (r, k, ff, c, v, cnt, nbytes) in
-           [x for x in two_ranks if x[1] not in ("max", "op", "vmg")] if (k, ff, c) == case}
+           [x for x in two_ranks if x[1] not in ("max", "op", "vmg", "mean")] if (k, ff, c) == case}
     assert set(got) == {0, 1}, "a rank did not report"
     for r in (0, 1):
         assert np.isfinite(got[r]).all()
@@ -403,3 +439,17 @@ def test_two_rank_vcycle_transfers_are_bitwise(two_ranks, kind, part):
         assert np.array_equal(g_base, u[mine])
         base = h.level[mine] == 0
         assert np.isfinite(g_base[base]).all()
+
+
+@pytest.mark.parametrize("part", PARTS)
+def test_two_rank_mean_is_bitwise(two_ranks, part):
+    """Per-block sums gathered exactly and folded in block order give the
+    oracle's own mean of 4 pi G rho (the solve's rho_mean) to the bit."""
+    from code_only_b200 import abi
+    from tests import oracle_lib as ol
+    h = _hier("periodic")
+    rc, _, _, st, _ = ol.oracle_solve(h, _rho(h), abi.default_params(abi.SFM_BC_PERIODIC), want_g=False)
+    assert rc in (abi.SFM_OK, abi.SFM_ENOTCONVERGED)
+    got = [x[3] for x in two_ranks if x[1] == "mean" and x[2] == part]
+    assert len(got) == 2
+    assert got[0] == got[1] == st.rho_mean
