@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -189,19 +190,58 @@ struct HostHier {
 // ---------------------------------------------------------------------------
 // device memory bookkeeping
 // ---------------------------------------------------------------------------
+// Guard bands (a debug mode, sfm_debug_set_guard_bytes): every device
+// array of a context created while the setting is non-zero sits between two
+// bands of that many bytes filled with kGuardByte; a kernel that writes
+// past either end of an array changes a band (sfm_debug_check_guards counts
+// the changed bytes), and one that reads past it reads NaN (0xFF bytes are
+// a NaN in both float widths), which shows in the results.
+constexpr unsigned char kGuardByte = 0xFF;
+static std::atomic<uint64_t> g_guard_bytes{0};
+
 struct DevMem {
     std::vector<void *> ptrs;
     int64_t bytes = 0;
     cudaError_t err = cudaSuccess;
+    uint64_t guard = g_guard_bytes.load();
+    struct Band { unsigned char *lo, *hi; size_t hiLen; };   // the bands below and above one array
+    std::vector<Band> bands;
     template <class T>
     T *alloc(size_t count) {
         if (count == 0) count = 1;
         void *p = nullptr;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        const size_t payload = count * sizeof(T);
+        if (guard > 0) {   // [band][payload rounded up to 256 B][band]
+            const size_t body = (payload + 255) / 256 * 256;
+            cudaError_t e = cudaMalloc(&p, body + 2 * guard);
+            if (e != cudaSuccess) { err = e; return nullptr; }
+            ptrs.push_back(p);
+            unsigned char *base = static_cast<unsigned char *>(p);
+            e = cudaMemset(base, kGuardByte, guard);
+            if (e == cudaSuccess) e = cudaMemset(base + guard + payload, kGuardByte, body - payload + guard);
+            if (e != cudaSuccess) { err = e; return nullptr; }
+            bands.push_back({base, base + guard + payload, body - payload + guard});
+            bytes += (int64_t)payload;
+            return reinterpret_cast<T *>(base + guard);
+        }
+        cudaError_t e = cudaMalloc(&p, payload);
         if (e != cudaSuccess) { err = e; return nullptr; }
         ptrs.push_back(p);
-        bytes += (int64_t)(count * sizeof(T));
+        bytes += (int64_t)payload;
         return (T *)p;
+    }
+    // bytes of all bands that no longer hold kGuardByte (-1: a copy failed)
+    int64_t guard_violations() const {
+        int64_t bad = 0;
+        std::vector<unsigned char> h;
+        for (const Band &b : bands)
+            for (int side = 0; side < 2; side++) {
+                const size_t len = side ? b.hiLen : guard;
+                h.resize(len);
+                if (cudaMemcpy(h.data(), side ? b.hi : b.lo, len, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+                for (unsigned char v : h) bad += v != kGuardByte;
+            }
+        return bad;
     }
     template <class T>
     T *upload(const std::vector<T> &v) {
@@ -229,6 +269,7 @@ public:
                       double *dump) = 0;
     virtual int adjoint(const double *dJdphi, double *dJdrho, sfm_stats *st, cudaStream_t s) = 0;
     virtual int64_t device_bytes() const = 0;
+    virtual int64_t guard_violations() const = 0;
     virtual int fmg_levels() const = 0;
     virtual void set_wait_polls(uint32_t polls) = 0;
     virtual void set_ghost_merge(bool on) = 0;
@@ -464,6 +505,7 @@ public:
         mem.release();
     }
     int64_t device_bytes() const override { return mem.bytes; }
+    int64_t guard_violations() const override { return mem.guard_violations(); }
     // the iteration graph holds the kernel parameters it was captured with:
     // a new limit drops it, and the next outer iteration captures again
     void set_serial_relax(bool on) override {
@@ -2516,6 +2558,23 @@ int sfm_debug_set_wait_polls(sfm_ctx *c, uint32_t polls) {
     if (!c || !c->s) return SFM_EINVAL;
     c->s->set_wait_polls(polls);
     return SFM_OK;
+}
+
+// Test hooks (not part of include/sfmg.h): guard bands of `bytes` (rounded
+// up to 4 KiB; 0 turns the mode off) around every device array of the
+// contexts created from now on, in this process; and the number of band
+// bytes a context's kernels have changed (-1 if they could not be read).
+int sfm_debug_set_guard_bytes(uint64_t bytes) {
+    if (bytes > ((uint64_t)1 << 30)) return SFM_EINVAL;
+    sfm::g_guard_bytes.store((bytes + 4095) / 4096 * 4096);
+    return SFM_OK;
+}
+int sfm_debug_check_guards(sfm_ctx *c, int64_t *bad_bytes) {
+    if (!c || !c->s || !bad_bytes) return SFM_EINVAL;
+    DeviceGuard dg(c->device);
+    if (cudaDeviceSynchronize() != cudaSuccess) return SFM_ECUDA;
+    *bad_bytes = c->s->guard_violations();
+    return *bad_bytes < 0 ? SFM_ECUDA : SFM_OK;
 }
 
 // Test hook (not part of include/sfmg.h): 1 runs every red-black colour

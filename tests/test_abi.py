@@ -30,6 +30,18 @@ def test_every_declared_symbol_is_exported(sfmg_lib):
         assert hasattr(sfmg_lib, n), n
 
 
+def test_debug_hooks_are_exported(sfmg_lib):
+    """The test hooks that tests/ binds by name (not part of include/sfmg.h)."""
+    for n in ("sfm_debug_set_wait_polls", "sfm_debug_set_serial_relax", "sfm_debug_set_ghost_merge",
+              "sfm_debug_solve", "sfm_debug_set_guard_bytes", "sfm_debug_check_guards"):
+        assert hasattr(sfmg_lib, n), n
+    sfmg_lib.sfm_debug_set_guard_bytes.argtypes = [C.c_uint64]
+    assert sfmg_lib.sfm_debug_set_guard_bytes(1 << 31) == abi.SFM_EINVAL
+    assert sfmg_lib.sfm_debug_set_guard_bytes(0) == abi.SFM_OK
+    sfmg_lib.sfm_debug_check_guards.argtypes = [C.c_void_p, C.c_void_p]
+    assert sfmg_lib.sfm_debug_check_guards(None, None) == abi.SFM_EINVAL
+
+
 def test_default_params_match_reference_constants(sfmg_lib):
     p = abi.SfmParams()
     sfmg_lib.sfm_default_params(C.byref(p))
