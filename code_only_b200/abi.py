@@ -39,7 +39,7 @@ SFM_MAX_HISTORY = 64
 # every exported symbol of include/sfmg.h
 EXPORTED = ("sfm_default_params", "sfm_create", "sfm_solve", "sfm_solve_device",
             "sfm_adjoint", "sfm_destroy", "sfm_strerror", "sfm_info", "sfm_autotune", "sfm_tune_save",
-            "sfm_tune_load", "sfm_uniform_solve_noalloc")
+            "sfm_tune_load", "sfm_uniform_solve_noalloc", "sfm_link_blocks")
 SFM_NOALLOC_MAX_N = 32
 
 
@@ -170,6 +170,10 @@ def load_library(path: Optional[str] = None) -> C.CDLL:
     lib.sfm_tune_load.restype = C.c_int
     lib.sfm_tune_text_check.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t]
     lib.sfm_tune_text_check.restype = C.c_int
+    lib.sfm_link_blocks.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
+    lib.sfm_link_blocks.restype = C.c_int
     if path is None:
         _lib = lib
     return lib

@@ -149,3 +149,35 @@ def fmg_poisson(hierarchy, rho: np.ndarray, psi: np.ndarray, bc: int = abi.SFM_B
     """One-shot form of the reference entry point: returns (psi, g, stats)."""
     with FMGPoisson(hierarchy, bc=bc, **kw) as s:
         return s.solve(rho, psi)
+
+
+def link_blocks(level, ijk, ngb, periodic, nlev: Optional[int] = None, stream: int = 0):
+    """Links of a block hierarchy computed on the device (sfm_link_blocks):
+    the parent, children, same-level face neighbours and physical-boundary
+    flags that the reference's refinement keeps (grid.F90:587-731), from the
+    blocks' AMR levels and integer positions.
+
+    level: int32 [nb], ijk: int32 [nb, 3] -- CUDA tensors of the current
+    device; ngb: base blocks per direction; periodic: one bool or three.
+    Returns (parent [nb], child [nb, 8], nbr [nb, 6], touch [nb, 6]) as CUDA
+    tensors in sfm_hier_desc's conventions."""
+    import torch
+    nb = int(level.shape[0])
+    if ijk.shape != (nb, 3) or level.dtype != torch.int32 or ijk.dtype != torch.int32:
+        raise ValueError("level must be int32 [nb] and ijk int32 [nb, 3]")
+    level, ijk = level.contiguous(), ijk.contiguous()
+    if nlev is None:
+        nlev = int(level.max().item()) + 1 if nb else 0
+    per = (bool(periodic),) * 3 if np.isscalar(periodic) else tuple(bool(v) for v in periodic)
+    dev = level.device
+    parent = torch.empty(nb, dtype=torch.int32, device=dev)
+    child = torch.empty((nb, 8), dtype=torch.int32, device=dev)
+    nbr = torch.empty((nb, 6), dtype=torch.int32, device=dev)
+    touch = torch.empty((nb, 6), dtype=torch.int8, device=dev)
+    lib = abi.load_library()
+    rc = lib.sfm_link_blocks(nb, int(nlev), level.data_ptr(), ijk.data_ptr(), (C.c_int32 * 3)(*[int(v) for v in ngb]),
+                             (C.c_int32 * 3)(*[int(v) for v in per]), parent.data_ptr(), child.data_ptr(),
+                             nbr.data_ptr(), touch.data_ptr(), C.c_void_p(stream))
+    if rc != abi.SFM_OK:
+        raise SFMError(rc, "sfm_link_blocks")
+    return parent, child, nbr, touch

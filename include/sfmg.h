@@ -281,6 +281,33 @@ int sfm_uniform_solve_noalloc(const double *d_rho, double *d_psi, int n, double 
                               double rel_tol, int max_cycles, int *cycles, double *rel_residual,
                               void *stream);
 
+/* Links of a block hierarchy computed on the device from the blocks' levels
+ * and integer positions.  Replaces the link updates the reference runs after
+ * each refinement (update_neighbor, update_neighbor_linklist,
+ * update_parent_linklist; grid.F90:587-731), whose ParentGid / ChildGid /
+ * NeighborGid fmg_make_linklist then reads (fmg_data_if.F90:298-411): the
+ * arrays it fills are sfm_hier_desc's parent, child, nbr and touch, in the
+ * same conventions, so a hierarchy regridded on the device is linked without
+ * a round trip through the host.
+ *   nblocks, nlev   blocks (any order) and AMR levels (nlev <= 16)
+ *   d_level[nb]     AMR level of each block
+ *   d_ijk[3*nb]     integer position of each block on its level, 0 <= i <
+ *                   ngb[0] << level (likewise j, k; ngb[d] << (nlev-1) <= 2^20)
+ *   ngb[3], periodic[3]  base blocks per direction and periodic flags (host)
+ *   outputs d_parent[nb] (-1 on the base level), d_child[8*nb] (child
+ *                   lri + 2 lrj + 4 lrk, -1 for a leaf), d_nbr[6*nb] (face
+ *                   lr + 2 dir, the same-level neighbour, periodic directions
+ *                   wrapping, else -1), d_touch[6*nb] (1 on the physical
+ *                   boundary of a non-periodic direction)
+ *   stream          a cudaStream_t, or NULL; the call waits for it
+ * All arrays are device memory of the current device (else SFM_EINVAL).
+ * Returns SFM_EHIER for a block outside its level's box, a block given
+ * twice, a block above the base level without a parent, or a block with
+ * some but not all of its 8 children. */
+int sfm_link_blocks(int32_t nblocks, int32_t nlev, const int32_t *d_level, const int32_t *d_ijk,
+                    const int32_t ngb[3], const int32_t periodic[3], int32_t *d_parent, int32_t *d_child,
+                    int32_t *d_nbr, int8_t *d_touch, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

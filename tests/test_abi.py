@@ -42,6 +42,23 @@ def test_debug_hooks_are_exported(sfmg_lib):
     assert sfmg_lib.sfm_debug_check_guards(None, None) == abi.SFM_EINVAL
 
 
+def test_link_blocks_argument_checks(sfmg_lib):
+    """sfm_link_blocks rejects bad sizes before any device call, and reports
+    a missing GPU rather than touching the pointers."""
+    ngb = (C.c_int32 * 3)(2, 2, 2)
+    per = (C.c_int32 * 3)(1, 1, 1)
+    dummy = C.c_void_p(16)
+    args = lambda nb, nlev, g: (nb, nlev, dummy, dummy, g, per, dummy, dummy, dummy, dummy, None)
+    assert sfmg_lib.sfm_link_blocks(*args(0, 1, ngb)) == abi.SFM_EINVAL
+    assert sfmg_lib.sfm_link_blocks(*args(8, 17, ngb)) == abi.SFM_EINVAL            # more than 16 levels
+    big = (C.c_int32 * 3)(1 << 16, 2, 2)
+    assert sfmg_lib.sfm_link_blocks(*args(8, 6, big)) == abi.SFM_EINVAL             # positions past 2^20
+    assert sfmg_lib.sfm_link_blocks(8, 1, None, dummy, ngb, per, dummy, dummy, dummy, dummy, None) == abi.SFM_EINVAL
+    import torch
+    if not torch.cuda.is_available():
+        assert sfmg_lib.sfm_link_blocks(*args(8, 1, ngb)) == abi.SFM_EDEVICE
+
+
 def test_default_params_match_reference_constants(sfmg_lib):
     p = abi.SfmParams()
     sfmg_lib.sfm_default_params(C.byref(p))
