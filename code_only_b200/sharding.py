@@ -43,9 +43,10 @@ step for GPU ranks:
 
 Run before each such step, the exchanges make a rank's owned blocks hold
 exactly the values a single rank computes: after the ghost fill, after
-whole red-black sweeps and residuals of the composite operator, and after
-the V-cycle's prolongation and base-grid solve (tests/test_sharding.py,
-world size 2, bit for bit, for Morton-range and alternating owners).  Residual maxima are an
+whole red-black sweeps and residuals of the composite operator, after the
+V-cycle's prolongation and base-grid solve, and through a whole FMG solve
+(tests/test_sharding.py, world size 2, bit for bit, for Morton-range and
+alternating owners).  Residual maxima are an
 all-reduce of one value (``allreduce_max``); the base grid (at most 32^3
 cells) is gathered whole on every rank, where the base-grid solve runs
 redundantly.

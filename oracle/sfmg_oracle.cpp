@@ -122,6 +122,19 @@ struct Oracle {
     // with NPE = 1
     const int8_t *own = nullptr;
     bool mine(int b) const { return !own || own[b]; }
+    // A split run (oracle_solve_split) also calls back before every step
+    // that reads blocks another rank owns, with the array the step reads:
+    //   kind 0 ghost pass (L, dir); 1 converge_c2p of level L (dir = cubic);
+    //   2 flux correction, face fluxes of direction dir; 3 prolongation onto
+    //   L + 1; 4 the base-grid gather; 5 a maximum (one value, in place);
+    //   6 per-block partial sums (nb values, in place) before an ordered sum
+    typedef void (*XchgFn)(void *user, int kind, int f, int L, int dir, double *data, int64_t n);
+    XchgFn xchg = nullptr;
+    void *xuser = nullptr;
+    void xc(int kind, int f, int L, int dir, double *data, int64_t n) {
+        if (xchg) xchg(xuser, kind, f, L, dir, data, n);
+    }
+    void xc_field(int kind, int f, int L, int dir, Arr &A) { xc(kind, f, L, dir, A.d.data(), (int64_t)A.d.size()); }
     double Resh2maxg = 0.0;
     std::vector<double> vmgResmaxg;
 
@@ -305,16 +318,23 @@ struct Oracle {
                     }
         double rhoave = 0.0;
         if (zero_mean) {
+            // per-block sums, then one running sum over the leaves in block order
+            std::vector<double> part(nb, 0.0);
+            for (int b = 0; b < nb; b++) {
+                if (child[8 * b] != Undef || !mine(b)) continue;
+                double s = 0.0;
+                for (int k = 0; k < n; k++)
+                    for (int j = 0; j < n; j++)
+                        for (int i = 0; i < n; i++) s = s + R.at(b, i, j, k);
+                part[b] = s;
+            }
+            xc(6, 0, 0, 0, part.data(), nb);
             double mass = 0.0, vol = 0.0;
             for (int L = 0; L < nlev; L++) {
                 double dv = h(L, 0) * h(L, 0) * h(L, 0);   // dv = h**3 (fmg_data.F90:290)
                 for (int b = lstart[L]; b < lstart[L + 1]; b++) {
                     if (child[8 * b] != Undef) continue;
-                    double s = 0.0;
-                    for (int k = 0; k < n; k++)
-                        for (int j = 0; j < n; j++)
-                            for (int i = 0; i < n; i++) s = s + R.at(b, i, j, k);
-                    mass = mass + s * dv;
+                    mass = mass + part[b] * dv;
                     vol = vol + (double)(n * n * n) * dv;
                 }
             }
@@ -356,7 +376,7 @@ struct Oracle {
         for (int L = 0; L < nlev; L++) {
             double h2 = h(L, f) * h(L, f);
             for (int b = lstart[L]; b < lstart[L + 1]; b++) {
-                if (skip(b)) continue;
+                if (skip(b) || !mine(b)) continue;
                 double bm = 0.0;
                 for (int k = 0; k < n; k++)
                     for (int j = 0; j < n; j++)
@@ -364,6 +384,7 @@ struct Oracle {
                 m = std::max(m, bm * h2);
             }
         }
+        xc(5, f, 0, 0, &m, 1);
         return m;
     }
 
@@ -417,6 +438,7 @@ struct Oracle {
     // =====================================================================
     void converge_c2p_lev(int Lc, int f, int code, bool cubic) {
         Arr &A = F(code, f);
+        xc_field(1, f, Lc, cubic ? 1 : 0, A);
         const int n = nF(f), h2n = n / 2;
         const int Lf = Lc + 1;
         OMP_FOR
@@ -444,6 +466,7 @@ struct Oracle {
     // same-level face copy, full transverse range (fmg_ghfix_samelev, :127-199)
     void samelev(int L, int f, int dir, int code) {
         Arr &A = F(code, f);
+        xc_field(0, f, L, dir, A);
         const int n = nF(f);
         OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++)
@@ -485,6 +508,7 @@ struct Oracle {
     // interpCubic when the transverse buffer has >= 4 cells
     // (interpCubic_checkSize, :738-756), else interp (bilinear).
     void parentlev(int L, int f, int dir, int code, bool cubic) {
+        xc_field(0, f, L, dir, F(code, f));
         if (L <= 0) return;
         Arr &A = F(code, f);
         const int n = nF(f), nb2 = n / 2;
@@ -898,6 +922,7 @@ struct Oracle {
     // quarter becomes the mean of the 4 fine fluxes.  All reads precede all
     // writes, as the reference packs before it unpacks.
     void fluxcorrection(int f) {
+        for (int d = 0; d < 3; d++) xc_field(2, f, 0, d, FL(d, f));
         const int n = nF(f), h2n = n / 2;
         struct Item { int cb, dir, xc, ta0, tb0; std::vector<double> v; };
         std::vector<Item> items;
@@ -954,6 +979,7 @@ struct Oracle {
             poisson_flux(f, ju, bf0);
             resmax = std::max(resmax, relax_colour(f, ju, jrhs, ipass));
         }
+        xc(5, f, 0, 0, &resmax, 1);
         Resh2maxg = resmax;
     }
     // one colour (ipass) of the sweep from the current face fluxes; returns
@@ -1250,6 +1276,7 @@ struct Oracle {
     void vmg_p2c(int Lf, int juf, int juc) {
         const int Lc = Lf - 1;
         Arr &Fo = F(juf, FMax), &C = F(juc, FMax);
+        xc_field(3, FMax, Lc, 0, C);
         const int n = nF(FMax), h2n = n / 2;
         for (int p = lstart[Lc]; p < lstart[Lc + 1]; p++)
             for (int c = 0; c < 8; c++) {
@@ -1267,13 +1294,19 @@ struct Oracle {
         const int n = nF(FMax);
         double ave = 0.0;
         int ngrid = 0;
+        std::vector<double> part(nb, 0.0);   // per-block sums, then one running sum in block order
         for (int b = lstart[L]; b < lstart[L + 1]; b++) {
-            ngrid++;
+            if (!mine(b)) continue;
             double s = 0.0;
             for (int k = 0; k < n; k++)
                 for (int j = 0; j < n; j++)
                     for (int i = 0; i < n; i++) s = s + A.at(b, i, j, k);
-            ave = ave + s;
+            part[b] = s;
+        }
+        xc(6, FMax, L, 0, part.data(), nb);
+        for (int b = lstart[L]; b < lstart[L + 1]; b++) {
+            ngrid++;
+            ave = ave + part[b];
         }
         ave = (ngrid == 0) ? 0.0 : ave / (double)(n * n * n * ngrid);
         for (int b = lstart[L]; b < lstart[L + 1]; b++)
@@ -1328,6 +1361,8 @@ struct Oracle {
     void mg_dataPrepare(int jrhs, int ju) {   // mg_data.F90:179-253: mg SRC, PSI <- base blocks
         const int n = nF(FMax);
         Arr &S = MG(ISRC, 0), &P = MG(IPSI, 0), &R = F(jrhs, FMax), &U = F(ju, FMax);
+        xc_field(4, FMax, 0, 0, R);
+        xc_field(4, FMax, 0, 0, U);
         for (int kb = 0; kb < ngb[2]; kb++)
             for (int jb = 0; jb < ngb[1]; jb++)
                 for (int ib = 0; ib < ngb[0]; ib++) {
@@ -1566,12 +1601,13 @@ struct Oracle {
         const int n = NI;
         double m = 0.0;
         for (int b = 0; b < nb; b++) {
-            if (skip(b)) continue;
+            if (skip(b) || !mine(b)) continue;
             double h2 = h(level[b], 0) * h(level[b], 0);
             for (int k = 0; k < n; k++)
                 for (int j = 0; j < n; j++)
                     for (int i = 0; i < n; i++) m = std::max(m, std::fabs(R.at(b, i, j, k)) * h2);
         }
+        xc(5, 0, 0, 0, &m, 1);
         return m;
     }
 
@@ -2100,6 +2136,27 @@ int oracle_solve(const sfm_hier_desc *h, const sfm_params *p, const double *rho,
     Oracle *o = new Oracle();
     int rc = o->setup(h, p);
     if (rc == SFM_OK) rc = o->solve(rho, psi, g, p->ngh_io, st, stop_stage, dump);
+    delete o;
+    return rc;
+}
+
+// oracle_solve on the blocks with own[b] != 0 only, as one of several
+// ranks: before every step that reads other ranks' blocks the oracle calls
+// xchg(user, kind, f, L, dir, data, n) with the array the step reads (kinds
+// in Oracle::xchg), and the caller fills in the values other ranks own;
+// maxima and ordered sums go through it as well.  Every rank takes the same
+// steps in the same order.  psi and g are valid on the owned blocks.  The
+// isolated boundaries' multipole moments are not split (SFM_EINVAL).
+int oracle_solve_split(const sfm_hier_desc *h, const sfm_params *p, const double *rho, double *psi, double *g,
+                       sfm_stats *st, const int8_t *own, Oracle::XchgFn xchg, void *user) {
+    if (!h || !p || !rho || !own || !xchg) return SFM_EINVAL;
+    if (p->ngh_io < 1 || p->bc != SFM_BC_PERIODIC) return SFM_EINVAL;
+    Oracle *o = new Oracle();
+    int rc = o->setup(h, p);
+    o->own = own;
+    o->xchg = xchg;
+    o->xuser = user;
+    if (rc == SFM_OK) rc = o->solve(rho, psi, g, p->ngh_io, st, 0, nullptr);
     delete o;
     return rc;
 }

@@ -12,6 +12,8 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
 
 _lib = None
+# the exchange callback of oracle_solve_split: (user, kind, f, L, dir, data, n)
+XCHG_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int64)
 
 
 def load_oracle():
@@ -48,6 +50,9 @@ def load_oracle():
     lib.oracle_relax.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_int, C.c_int,
                                  C.c_void_p, C.c_void_p, C.c_void_p]
     lib.oracle_relax.restype = C.c_int
+    lib.oracle_solve_split.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.POINTER(abi.SfmStats), C.c_void_p, XCHG_FN, C.c_void_p]
+    lib.oracle_solve_split.restype = C.c_int
     _lib = lib
     return lib
 
@@ -138,3 +143,30 @@ def oracle_relax(h, u, rhs, f, sweeps):
                           _ptr(u), _ptr(np.ascontiguousarray(rhs)), C.byref(m))
     assert rc == 0, rc
     return m.value
+
+
+def oracle_solve_split(h, rho, params, owner, rank, exchanges):
+    """The oracle's solve on this rank's blocks (owner == rank), the other
+    ranks' values filled in through `exchanges(kind, f, L, d, array)` before
+    every step that reads them (see Oracle::xchg).  Returns (rc, psi, g,
+    stats); psi and g hold the owned blocks' results."""
+    lib = load_oracle()
+    own = np.ascontiguousarray(owner == rank, dtype=np.int8)
+    psi = np.zeros_like(rho)
+    g = np.zeros((h.nblocks, 3) + rho.shape[1:])
+    st = abi.SfmStats()
+    errors = []
+
+    def cb(user, kind, f, L, d, data, n):
+        try:
+            exchanges(kind, f, L, d, np.ctypeslib.as_array(data, shape=(n,)))
+        except Exception as e:   # an exception cannot cross the C frames: record it
+            errors.append(e)
+            raise
+
+    fn = XCHG_FN(cb)
+    rc = lib.oracle_solve_split(abi.HierDesc(h).ref(), C.byref(params), np.ascontiguousarray(rho).ctypes.data,
+                                psi.ctypes.data, g.ctypes.data, C.byref(st), own.ctypes.data, fn, None)
+    if errors:
+        raise errors[0]
+    return rc, psi, g, st

@@ -18,6 +18,10 @@ AMR-level V-cycle: the prolongation onto every level (parent blocks to the
 children's owners) and the base-grid solve (every base block to every
 rank), likewise.
 
+The whole solve: the oracle's fmg_cycle on each rank's blocks
+(oracle_solve_split), which calls back before every step that reads
+another rank's blocks, for every maximum and every ordered sum.
+
 Owners are contiguous Morton ranges per level (sharding.partition) and,
 to put most neighbours, parents and children on the other rank, alternating
 blocks; with alternating owners, turning any one kind of exchange into a
@@ -118,6 +122,13 @@ def _worker(rank, world, port, q):
         for part in PARTS:
             h = _hier("periodic")
             q.put((rank, "mean", part, _split_mean(h, _owner(h, part, world), rank)))
+        for part in PARTS:
+            h = _hier("periodic")
+            owner = _owner(h, part, world)
+            rc, psi, g, st = _split_solve(h, owner, rank)
+            mine = owner == rank
+            q.put((rank, "solve", part, rc, psi[mine].copy(), g[mine].copy(), st.outer_iters, st.rho_mean,
+                   list(st.ratio)[:st.outer_iters], st.true_rel_residual))
         q.put((rank, "max", sharding.allreduce_max(float(rank + 1))))
     finally:
         dist.destroy_process_group()
@@ -240,6 +251,51 @@ def _split_mean(h, owner, rank):
     return mass / vol
 
 
+def _solve_params():
+    from code_only_b200 import abi
+    return abi.default_params(abi.SFM_BC_PERIODIC, rel_tol=1e-5, max_outer=40)   # a few outer iterations
+
+
+def _solve_rho(h):
+    from code_only_b200 import abi, workloads as w
+    return w.block_field(h, abi.default_params(abi.SFM_BC_PERIODIC).ngh_io, w.gaussian_peak)
+
+
+def _split_solve(h, owner, rank):
+    """The oracle's whole solve (fmg_cycle: set-up, outer loop of fmg_lin with
+    the AMR-level V-cycle and the base-grid solve, psi and g) on this rank's
+    blocks, every cross-rank read through the exchanges above; the blocks
+    another rank owns start as NaN in rho and psi."""
+    import torch
+    from code_only_b200 import sharding
+    from tests import oracle_lib as ol
+    fmax = _fmax(h)
+    ex = [sharding.HaloExchange(h, owner, rank, h.ni >> f) for f in range(fmax + 1)]
+    rho = _solve_rho(h)
+    rho[owner != rank] = np.nan
+
+    def exchanges(kind, f, L, d, a):
+        t = torch.from_numpy(a)
+        if kind == 0:
+            ex[f].ghost(t, L, d)
+        elif kind == 1:
+            ex[f].converge(t, L, bool(d))
+        elif kind == 2:
+            ex[f].reflux(t, d)
+        elif kind == 3:
+            ex[f].p2c(t, L)
+        elif kind == 4:
+            ex[f].base(t)
+        elif kind == 5:
+            a[0] = sharding.allreduce_max(float(a[0]))
+        elif kind == 6:
+            a[:] = ex[0].gather_blocks(t).numpy()
+        else:
+            raise ValueError(f"unknown exchange kind {kind}")
+
+    return ol.oracle_solve_split(h, rho, _solve_params(), owner, rank, exchanges)
+
+
 def _run(world=2, timeout=240):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -249,7 +305,7 @@ def _run(world=2, timeout=240):
         p.start()
     out = []
     t0 = time.time()
-    n_msgs = len(CASES) + len(PARTS) * (len(OP_CASES) + len(VMG_CASES) + 1) + 1
+    n_msgs = len(CASES) + len(PARTS) * (len(OP_CASES) + len(VMG_CASES) + 2) + 1
     while len(out) < world * n_msgs and time.time() - t0 < timeout:
         try:
             out.append(q.get(timeout=5))
@@ -290,7 +346,7 @@ def test_two_rank_ghost_fill_is_bitwise(two_ranks, case):
     oracle_ghost_pass(h, ref, f, -1, 0, cubic)         # the whole fill on one rank
     owner = sharding.partition(h, 2)
     got = {r: v for (r, k, ff, c, v, cnt, nbytes) in
-           [x for x in two_ranks if x[1] not in ("max", "op", "vmg", "mean")] if (k, ff, c) == case}
+           [x for x in two_ranks if x[1] not in ("max", "op", "vmg", "mean", "solve")] if (k, ff, c) == case}
     assert set(got) == {0, 1}, "a rank did not report"
     for r in (0, 1):
         assert np.isfinite(got[r]).all()
@@ -453,3 +509,27 @@ def test_two_rank_mean_is_bitwise(two_ranks, part):
     got = [x[3] for x in two_ranks if x[1] == "mean" and x[2] == part]
     assert len(got) == 2
     assert got[0] == got[1] == st.rho_mean
+
+
+@pytest.mark.parametrize("part", PARTS)
+def test_two_rank_solve_is_bitwise(two_ranks, part):
+    """The whole FMG solve split over two ranks -- the oracle's fmg_cycle on
+    each rank's blocks, every read of the other rank's blocks through the
+    exchanges, maxima all-reduced, ordered sums gathered -- gives the
+    single-rank solve bit for bit: psi and g on every owned block, the
+    iteration count, the mean, the residual history."""
+    from tests import oracle_lib as ol
+    h = _hier("periodic")
+    rc0, psi0, g0, st0, _ = ol.oracle_solve(h, _solve_rho(h), _solve_params())
+    owner = _owner(h, part)
+    got = {x[0]: x[3:] for x in two_ranks if x[1] == "solve" and x[2] == part}
+    assert set(got) == {0, 1}, "a rank did not report"
+    for r in (0, 1):
+        rc, psi, g, iters, mean, ratios, trr = got[r]
+        mine = owner == r
+        assert rc == rc0
+        assert iters == st0.outer_iters and mean == st0.rho_mean
+        assert ratios == list(st0.ratio)[:st0.outer_iters]
+        assert trr == st0.true_rel_residual
+        assert np.array_equal(psi, psi0[mine])
+        assert np.array_equal(g, g0[mine])
