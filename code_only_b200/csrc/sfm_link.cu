@@ -164,6 +164,9 @@ extern "C" int sfm_link_blocks(int32_t nblocks, int32_t nlev, const int32_t *d_l
                           (const void *)d_nbr, (const void *)d_touch})
         if (!on_device(p, dev)) return SFM_EINVAL;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return SFM_EINVAL;
+    if (cap != cudaStreamCaptureStatusNone) return SFM_EINVAL;   // the call waits for the stream
     uint64_t slots = 1;
     while (slots < 2 * (uint64_t)nblocks) slots <<= 1;
     LinkTable t{nullptr, nullptr, slots - 1};

@@ -299,7 +299,8 @@ int sfm_uniform_solve_noalloc(const double *d_rho, double *d_psi, int n, double 
  *                   lr + 2 dir, the same-level neighbour, periodic directions
  *                   wrapping, else -1), d_touch[6*nb] (1 on the physical
  *                   boundary of a non-periodic direction)
- *   stream          a cudaStream_t, or NULL; the call waits for it
+ *   stream          a cudaStream_t, or NULL; the call waits for it, so a
+ *                   stream under capture returns SFM_EINVAL
  * All arrays are device memory of the current device (else SFM_EINVAL).
  * Returns SFM_EHIER for a block outside its level's box, a block given
  * twice, a block above the base level without a parent, or a block with
