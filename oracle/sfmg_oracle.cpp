@@ -18,8 +18,12 @@
 // array kept per (AMR level, fmg level, block) for the whole solve exactly as
 // GridLevel()%Block()%{U,Res,Rhs,Rho,Src,Psi,F} are (fmg_data.F90:35-43),
 // with the same loop, fill and pass orders, and with Fortran's left-to-right
-// evaluation of every arithmetic expression.  Single process: every MPI
-// exchange of the reference becomes a local copy (NPE = 1 semantics).
+// evaluation of every arithmetic expression.  One process: every MPI
+// exchange of the reference becomes a local copy (NPE = 1 semantics).  The
+// split run (oracle_solve_split, oracle_step) computes only the blocks a
+// rank owns and hands every cross-rank read, maximum and ordered sum to a
+// caller-supplied exchange, which the tests of the multi-rank partition
+// answer over torch.distributed.
 //
 // Routine map (reference file:line -> function here):
 //   fmg_poisson / fmg_cycle       fmg.F90:63-74,134-233   -> Oracle::solve
