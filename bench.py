@@ -96,8 +96,17 @@ def workload_config(name, h, bc):
         "level_blocks": [int(v) for v in h.level_counts()],
         "bc": "periodic" if bc == 0 else "isolated sphere (multipole l<=4)",
         "rel_tol": REL_TOL,
-        "l2": "inputs larger than L2 (>= 1 GB per field), no flush",
+        "l2": _l2_note(h),
     }
+
+
+def _l2_note(h):
+    """How the timed steps stand to the 126 MB L2: the FP64 level-0 field
+    (one of the solve's arrays) against it."""
+    field = h.nblocks * (h.ni + 2) ** 3 * 8
+    if field > 126 * 2 ** 20:
+        return f"inputs larger than L2 ({field / 2 ** 30:.2f} GiB per FP64 field), no flush"
+    return f"inputs fit in L2 ({field / 2 ** 20:.1f} MiB per FP64 field), no flush: warm-cache figures"
 
 
 def params_for(bc, precision, profile=0):
