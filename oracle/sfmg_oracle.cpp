@@ -468,9 +468,10 @@ struct Oracle {
     // ghost cells (fmg_ghostcell.F90)
     // =====================================================================
     // same-level face copy, full transverse range (fmg_ghfix_samelev, :127-199)
-    void samelev(int L, int f, int dir, int code) {
+    // (hook false: the caller's parentlev of the same pass has just exchanged)
+    void samelev(int L, int f, int dir, int code, bool hook = true) {
         Arr &A = F(code, f);
-        xc_field(0, f, L, dir, A);
+        if (hook) xc_field(0, f, L, dir, A);
         const int n = nF(f);
         OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++)
@@ -589,7 +590,7 @@ struct Oracle {
         for (int L = 0; L < nlev; L++)
             for (int dir = 0; dir < 3; dir++) {
                 parentlev(L, f, dir, code, cubic);
-                samelev(L, f, dir, code);
+                samelev(L, f, dir, code, false);
             }
     }
 
@@ -681,6 +682,7 @@ struct Oracle {
                         if (x * x + y * y + z * z >= rad2) R.at(b, i, j, k) = 0.0;
                     }
         double mom[25];
+        xc_field(4, f, 0, 0, R);   // the moments run over every base block's cells
         multipole_moments(R, mom);
         // potential on the first ghost layer of every boundary-touching block
         for (int b = 0; b < nb; b++)
@@ -729,6 +731,7 @@ struct Oracle {
         }
         const double dv = h0[0] * h0[0] * h0[0];
         double a00 = 0.0;
+        xc_field(4, f, 0, 0, R);   // a running sum over every base block's cells
         for (int b = lstart[0]; b < lstart[1]; b++)
             for (int k = 0; k < n; k++)
                 for (int j = 0; j < n; j++)
@@ -1220,7 +1223,7 @@ struct Oracle {
         if (cubic)
             for (int dir = 0; dir < 3; dir++) {
                 parentlev(Lc + 1, FMax, dir, code, true);
-                samelev(Lc + 1, FMax, dir, code);
+                samelev(Lc + 1, FMax, dir, code, false);
             }
         converge_c2p_lev(Lc, FMax, code, cubic);
     }
@@ -2149,12 +2152,14 @@ int oracle_solve(const sfm_hier_desc *h, const sfm_params *p, const double *rho,
 // xchg(user, kind, f, L, dir, data, n) with the array the step reads (kinds
 // in Oracle::xchg), and the caller fills in the values other ranks own;
 // maxima and ordered sums go through it as well.  Every rank takes the same
-// steps in the same order.  psi and g are valid on the owned blocks.  The
-// isolated boundaries' multipole moments are not split (SFM_EINVAL).
+// steps in the same order.  psi and g are valid on the owned blocks; the
+// isolated boundaries' moments and the cylinders' line density, sums over
+// the base cells in order, are formed by every rank from the base blocks
+// the exchange gathers.
 int oracle_solve_split(const sfm_hier_desc *h, const sfm_params *p, const double *rho, double *psi, double *g,
                        sfm_stats *st, const int8_t *own, Oracle::XchgFn xchg, void *user) {
     if (!h || !p || !rho || !own || !xchg) return SFM_EINVAL;
-    if (p->ngh_io < 1 || p->bc != SFM_BC_PERIODIC) return SFM_EINVAL;
+    if (p->ngh_io < 1) return SFM_EINVAL;
     Oracle *o = new Oracle();
     int rc = o->setup(h, p);
     o->own = own;
