@@ -78,6 +78,29 @@ class SfmStats(C.Structure):
     def history(self):
         return [self.ratio[i] for i in range(min(self.outer_iters, SFM_MAX_HISTORY))]
 
+    def record(self, hierarchy=None) -> dict:
+        """The solve as one structured record (json.dumps gives one line): the
+        outer residual history the reference prints once per iteration
+        ('fmg error = ...', fmg.F90:189), the device time and launches, the
+        smoother's share (filled when the context profiles), the bytes a
+        host-array call moved, and the hierarchy's shape when given."""
+        rec = {
+            "outer_iters": int(self.outer_iters), "converged": bool(self.converged),
+            "residual_history": self.history(), "true_rel_residual": float(self.true_rel_residual),
+            "rho_mean": float(self.rho_mean), "precision": "fp64" if self.elem_bytes == 8 else "mixed",
+            "device_ms": float(self.device_ms), "kernel_launches": int(self.kernel_launches),
+            "smoother": {"ms": float(self.smoother_ms), "launches": int(self.smoother_launches),
+                         "cell_updates": int(self.smoother_cells), "colours_per_launch": int(self.smoother_colours),
+                         "cell_updates_per_s": (float(self.smoother_cells) / (self.smoother_ms * 1e-3)
+                                                if self.smoother_ms > 0 else None)},
+            "host_bytes": {"h2d": int(self.h2d_bytes), "d2h": int(self.d2h_bytes)},
+        }
+        if hierarchy is not None:
+            rec["hierarchy"] = {"levels": int(hierarchy.nlev), "blocks": int(hierarchy.nblocks),
+                                "block_cells": int(hierarchy.ni) ** 3,
+                                "level_blocks": [int(v) for v in hierarchy.level_counts()]}
+        return rec
+
 
 def _ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))

@@ -59,6 +59,22 @@ def test_link_blocks_argument_checks(sfmg_lib):
         assert sfmg_lib.sfm_link_blocks(*args(8, 1, ngb)) == abi.SFM_EDEVICE
 
 
+def test_stats_record_is_one_json_line():
+    import json
+    st = abi.SfmStats()
+    st.outer_iters, st.converged, st.elem_bytes = 3, 1, 4
+    for i, v in enumerate((1e-2, 1e-4, 1e-6)):
+        st.ratio[i] = v
+    st.device_ms, st.smoother_ms, st.smoother_cells = 12.5, 2.0, 4000000
+    h = w.small_periodic(2, 8, 2, 0)
+    rec = st.record(h)
+    assert rec["residual_history"] == [1e-2, 1e-4, 1e-6] and rec["precision"] == "mixed"
+    assert rec["smoother"]["cell_updates_per_s"] == 2e9
+    assert rec["hierarchy"]["blocks"] == h.nblocks and sum(rec["hierarchy"]["level_blocks"]) == h.nblocks
+    line = json.dumps(rec)
+    assert "\n" not in line and json.loads(line) == rec
+
+
 def test_default_params_match_reference_constants(sfmg_lib):
     p = abi.SfmParams()
     sfmg_lib.sfm_default_params(C.byref(p))
