@@ -475,6 +475,18 @@ def oracle_solve_timed(h, rho, bc):
     return dt, st.outer_iters, psi[:, sl, sl, sl].copy(), g[:, :, sl, sl, sl].copy()
 
 
+def oracle_solve_profiled(h, rho, bc):
+    """One complete FP64 oracle solve to 1e-10 with the exclusive time of each
+    routine class.  Returns (seconds, outer iterations, {class: share of the solve})."""
+    from tests.oracle_lib import oracle_profile
+    t = time.perf_counter()
+    rc, secs, total, st = oracle_profile(h, rho, params_for(bc, 0))
+    dt = time.perf_counter() - t
+    if rc not in (0, -5):
+        raise RuntimeError(f"oracle solve failed: {rc}")
+    return dt, st.outer_iters, {k: round(v / total, 4) for k, v in sorted(secs.items(), key=lambda kv: -kv[1])}
+
+
 def cpu_baseline(h, rho, bc):
     """One complete solve of the oracle (CPU restatement of the reference
     algorithm, FP64, OpenMP over blocks) to 1e-10, measured."""
@@ -514,9 +526,12 @@ def run_reference(args):
     h, rho, bc = load_workload(args.workload)
     from tests.oracle_lib import load_oracle
     threads = load_oracle().oracle_threads()
-    samples, iters = [], []
+    samples, iters, shares = [], [], None
     for i in range(args.warmup + args.steps):   # every step one complete FP64 solve
-        dt, n_outer, _, _ = oracle_solve_timed(h, rho, bc)
+        if i == args.warmup + args.steps - 1:   # the last one with the time of each routine class
+            dt, n_outer, shares = oracle_solve_profiled(h, rho, bc)
+        else:
+            dt, n_outer, _, _ = oracle_solve_timed(h, rho, bc)
         iters.append(n_outer)
         if i >= args.warmup:
             samples.append(dt)
@@ -535,6 +550,8 @@ def run_reference(args):
         "e2e": {"value": round(value, 6), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_note": "the Fortran/MPI reference cannot be built in this image; the CPU restatement of "
                           "its algorithm (oracle/) is timed",
+        "cpu_profile": {"shares": shares, "note": "exclusive wall time of each routine class in the last "
+                                                  "step's solve (nested routines counted once)"},
     }
     print(json.dumps(line), flush=True)
 

@@ -48,6 +48,7 @@
 //                                 mg_data.F90:45-559, mg_interpol_cubic.F90:89-125 -> mg_*
 // =============================================================================
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -99,7 +100,39 @@ inline void put3(int dir, int x, int a, int b, int &i, int &j, int &k) {
     else { i = a; j = b; k = x; }
 }
 
+// Exclusive wall time per routine class of a solve (oracle_profile): a
+// scope stack, so time inside a nested timed routine counts for that
+// routine only.  Off (no clock reads) unless a solve is profiled.
+enum ProfClass { kPrOther, kPrGhost, kPrConverge, kPrFlux, kPrReflux, kPrRelax, kPrResid, kPrRestrict,
+                 kPrProlong, kPrBase, kPrBoundary, kPrPsi2g, kPrCount };
+struct Prof {
+    bool on = false;
+    double sec[kPrCount] = {};
+    int stack[64] = {kPrOther};
+    int sp = 0;
+    std::chrono::steady_clock::time_point t0;
+    void charge() {
+        const auto t = std::chrono::steady_clock::now();
+        sec[stack[sp]] += std::chrono::duration<double>(t - t0).count();
+        t0 = t;
+    }
+};
+struct ProfScope {
+    Prof &p;
+    ProfScope(Prof &pr, int k) : p(pr) {
+        if (!p.on) return;
+        p.charge();
+        p.stack[++p.sp] = k;
+    }
+    ~ProfScope() {
+        if (!p.on) return;
+        p.charge();
+        --p.sp;
+    }
+};
+
 struct Oracle {
+    Prof prof;
     // ---------------- hierarchy ----------------
     int nb = 0, nlev = 0, NI = 0, FMax = 0;
     int ngb[3] = {0, 0, 0};
@@ -425,6 +458,7 @@ struct Oracle {
     // fmg_rstrct (fmg.F90:750-778): coarse fmg level f from f-1 within each
     // non-skip block (the cubic form is used by the nonlinear path only)
     void fmg_rstrct(int f, int iuc, int iuf) {
+        ProfScope ps(prof, kPrRestrict);
         Arr &C = F(iuc, f), &Fa = F(iuf, f - 1);
         const int nc = nF(f);
         OMP_FOR
@@ -441,6 +475,7 @@ struct Oracle {
     // fmg_converge_c2p (fmg_converge.F90:73-188)
     // =====================================================================
     void converge_c2p_lev(int Lc, int f, int code, bool cubic) {
+        ProfScope ps(prof, kPrConverge);
         Arr &A = F(code, f);
         xc_field(1, f, Lc, cubic ? 1 : 0, A);
         const int n = nF(f), h2n = n / 2;
@@ -470,6 +505,7 @@ struct Oracle {
     // same-level face copy, full transverse range (fmg_ghfix_samelev, :127-199)
     // (hook false: the caller's parentlev of the same pass has just exchanged)
     void samelev(int L, int f, int dir, int code, bool hook = true) {
+        ProfScope ps(prof, kPrGhost);
         Arr &A = F(code, f);
         if (hook) xc_field(0, f, L, dir, A);
         const int n = nF(f);
@@ -513,6 +549,7 @@ struct Oracle {
     // interpCubic when the transverse buffer has >= 4 cells
     // (interpCubic_checkSize, :738-756), else interp (bilinear).
     void parentlev(int L, int f, int dir, int code, bool cubic) {
+        ProfScope ps(prof, kPrGhost);
         xc_field(0, f, L, dir, F(code, f));
         if (L <= 0) return;
         Arr &A = F(code, f);
@@ -660,6 +697,7 @@ struct Oracle {
     // -zmin, the moments carry the mirror's factor 2 or 0); a no-op for
     // periodic (fmg_boundary_phys_periodic.F90:109-112)
     void boundary_physical_grid(int ju, int jrho) {
+        ProfScope ps(prof, kPrBoundary);
         if (zperiodic()) return boundary_physical_grid_cyl(ju, jrho);
         if (bc != SFM_BC_SPHERE && bc != SFM_BC_ZMIRROR && bc != SFM_BC_SPHERE_MHD_BE) return;
         const int f = 0, n = NI;
@@ -907,6 +945,7 @@ struct Oracle {
     // the face fluxes of every non-skip block from its cells and ghost layer
     // (fmg_poisson.F90:93-119)
     void face_flux(int f, int ju) {
+        ProfScope ps(prof, kPrFlux);
         Arr &U = F(ju, f);
         const int n = nF(f);
         OMP_FOR
@@ -929,6 +968,7 @@ struct Oracle {
     // quarter becomes the mean of the 4 fine fluxes.  All reads precede all
     // writes, as the reference packs before it unpacks.
     void fluxcorrection(int f) {
+        ProfScope ps(prof, kPrReflux);
         for (int d = 0; d < 3; d++) xc_field(2, f, 0, d, FL(d, f));
         const int n = nF(f), h2n = n / 2;
         struct Item { int cb, dir, xc, ta0, tb0; std::vector<double> v; };
@@ -992,6 +1032,7 @@ struct Oracle {
     // one colour (ipass) of the sweep from the current face fluxes; returns
     // the maximum of |resh2| over the blocks it updates
     double relax_colour(int f, int ju, int jrhs, int ipass) {
+        ProfScope ps(prof, kPrRelax);
         const double sixth = 1.0 / 6.0;
         const int n = nF(f);
         Arr &U = F(ju, f), &R = F(jrhs, f);
@@ -1019,6 +1060,7 @@ struct Oracle {
         resid_from_flux(f, jres, jrhs);
     }
     void resid_from_flux(int f, int jres, int jrhs) {
+        ProfScope ps(prof, kPrResid);
         const int n = nF(f);
         Arr &Rs = F(jres, f), &R = F(jrhs, f);
         OMP_FOR
@@ -1090,6 +1132,7 @@ struct Oracle {
 
     // fmg_interp (fmg.F90:786-822)
     void fmg_interp(int f, int iuf, int iuc, bool cubic) {
+        ProfScope ps(prof, kPrProlong);
         int lc = f + 1;
         converge_c2p(lc, iuc, cubic);
         fmg_boundary_u(lc, iuc);
@@ -1188,6 +1231,7 @@ struct Oracle {
     void vmg_poisson_flux(int L, int ju) {   // vmg_poisson.F90:63-94
         vmg_ghostcell(L, ju);
         vmg_boundary_u(L, FMax, ju);
+        ProfScope ps(prof, kPrFlux);
         Arr &U = F(ju, FMax);
         const int n = nF(FMax);
         double hi = 1.0 / h(L, FMax);
@@ -1208,6 +1252,7 @@ struct Oracle {
         Arr &U = F(ju, FMax), &R = F(jrhs, FMax);
         for (int ipass = 1; ipass <= 2; ipass++) {
             vmg_poisson_flux(L, ju);
+            ProfScope ps(prof, kPrRelax);
             for (int b = lstart[L]; b < lstart[L + 1]; b++)
                 for (int k = 0; k < n; k++)
                     for (int j = 0; j < n; j++)
@@ -1281,6 +1326,7 @@ struct Oracle {
     }
     // the prolongation loop of vmg_interp: every child at Lf from its parent
     void vmg_p2c(int Lf, int juf, int juc) {
+        ProfScope ps(prof, kPrProlong);
         const int Lc = Lf - 1;
         Arr &Fo = F(juf, FMax), &C = F(juc, FMax);
         xc_field(3, FMax, Lc, 0, C);
@@ -1557,6 +1603,7 @@ struct Oracle {
         }
     }
     void mg_cycle() {   // mg.F90:42-94 with ju = IPSI, jrho = ISRC
+        ProfScope ps(prof, kPrBase);
         const double errmax = (double)1.e-2f;   // default-real literal (mg.F90:50)
         mg_boundary_fill0(0, IPSI);
         mg_boundary_u(0, IPSI);
@@ -1575,6 +1622,7 @@ struct Oracle {
     // =====================================================================
     void psi2g(int ju, double *g, int gw) {
         poisson_flux(0, ju, false);
+        ProfScope ps(prof, kPrPsi2g);
         Arr &U = F(ju, 0);
         const int n = NI, Gi = NI + 2 * gw;
         const size_t V = (size_t)Gi * Gi * Gi;
@@ -2166,6 +2214,27 @@ int oracle_solve_split(const sfm_hier_desc *h, const sfm_params *p, const double
     o->xchg = xchg;
     o->xuser = user;
     if (rc == SFM_OK) rc = o->solve(rho, psi, g, p->ngh_io, st, 0, nullptr);
+    delete o;
+    return rc;
+}
+
+// oracle_solve with the exclusive wall time of each routine class (seconds)
+// in secs[12]: other, ghost passes, converge, face fluxes, flux correction,
+// relaxation updates, residuals, restriction, prolongation, base grid,
+// physical boundary, psi2g; secs[12] the whole solve.
+int oracle_profile(const sfm_hier_desc *h, const sfm_params *p, const double *rho, double *psi, double *g,
+                   sfm_stats *st, double *secs) {
+    if (!h || !p || !rho || !secs) return SFM_EINVAL;
+    if (p->ngh_io < 1) return SFM_EINVAL;
+    Oracle *o = new Oracle();
+    int rc = o->setup(h, p);
+    const auto t0 = std::chrono::steady_clock::now();
+    o->prof.on = true;
+    o->prof.t0 = t0;
+    if (rc == SFM_OK) rc = o->solve(rho, psi, g, p->ngh_io, st, 0, nullptr);
+    o->prof.charge();
+    for (int k = 0; k < kPrCount; k++) secs[k] = o->prof.sec[k];
+    secs[kPrCount] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     delete o;
     return rc;
 }

@@ -53,6 +53,9 @@ def load_oracle():
     lib.oracle_solve_split.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.POINTER(abi.SfmStats), C.c_void_p, XCHG_FN, C.c_void_p]
     lib.oracle_solve_split.restype = C.c_int
+    lib.oracle_profile.argtypes = [C.POINTER(abi.SfmHierDesc), C.POINTER(abi.SfmParams), C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.POINTER(abi.SfmStats), C.c_void_p]
+    lib.oracle_profile.restype = C.c_int
     _lib = lib
     return lib
 
@@ -170,3 +173,20 @@ def oracle_solve_split(h, rho, params, owner, rank, exchanges):
     if errors:
         raise errors[0]
     return rc, psi, g, st
+
+
+PROFILE_CLASSES = ("other", "ghost passes", "converge", "face fluxes", "flux correction", "relaxation",
+                   "residuals", "restriction", "prolongation", "base grid", "physical boundary", "psi2g")
+
+
+def oracle_profile(h, rho, params):
+    """One oracle solve with the exclusive wall time of each routine class;
+    returns (rc, {class: seconds}, total seconds, stats)."""
+    lib = load_oracle()
+    psi = np.zeros_like(rho)
+    g = np.zeros((h.nblocks, 3) + rho.shape[1:])
+    secs = np.zeros(len(PROFILE_CLASSES) + 1)
+    st = abi.SfmStats()
+    rc = lib.oracle_profile(abi.HierDesc(h).ref(), C.byref(params), np.ascontiguousarray(rho).ctypes.data,
+                            psi.ctypes.data, g.ctypes.data, C.byref(st), secs.ctypes.data)
+    return rc, dict(zip(PROFILE_CLASSES, secs[:-1].tolist())), float(secs[-1]), st

@@ -134,3 +134,18 @@ def test_zero_density_skips_the_loop():
     rho = np.zeros((h.nblocks, 12, 12, 12))        # |resh2max| <= TINY: nfmgmax = 0 (fmg.F90:180)
     rc, psi, g, st, _ = oracle_solve(h, rho, abi.default_params(abi.SFM_BC_PERIODIC))
     assert rc == abi.SFM_OK and st.outer_iters == 0 and np.all(psi == 0.0)
+
+
+def test_profile_accounts_for_the_solve_and_changes_nothing():
+    """oracle_profile times each routine class exclusively: the classes add
+    up to the whole solve, and the solve's results are those of oracle_solve."""
+    from tests.oracle_lib import oracle_profile
+    h = w.small_sphere(2, 8, 3, 2)
+    p = abi.default_params(abi.SFM_BC_SPHERE, rel_tol=1e-10, max_outer=40, zero_mean=0)
+    rho = w.block_field(h, p.ngh_io, w.softened_sphere)
+    rc, secs, total, st = oracle_profile(h, rho, p)
+    rc0, _, _, st0, _ = oracle_solve(h, rho, p)
+    assert rc == rc0 == abi.SFM_OK
+    assert st.outer_iters == st0.outer_iters and st.true_rel_residual == st0.true_rel_residual
+    assert abs(sum(secs.values()) - total) <= 0.01 * total + 1e-4
+    assert secs["ghost passes"] > 0 and secs["relaxation"] > 0 and secs["base grid"] > 0
