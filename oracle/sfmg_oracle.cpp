@@ -119,13 +119,15 @@ struct Prof {
 };
 struct ProfScope {
     Prof &p;
+    bool pushed = false;
     ProfScope(Prof &pr, int k) : p(pr) {
-        if (!p.on) return;
+        if (!p.on || p.sp + 1 >= 64) return;   // deeper nesting is charged to the enclosing class
         p.charge();
         p.stack[++p.sp] = k;
+        pushed = true;
     }
     ~ProfScope() {
-        if (!p.on) return;
+        if (!pushed) return;
         p.charge();
         --p.sp;
     }
