@@ -559,3 +559,49 @@ def test_two_rank_solve_is_bitwise(two_ranks, case):
         assert trr == st0.true_rel_residual
         assert np.array_equal(psi, psi0[mine])
         assert np.array_equal(g, g0[mine])
+
+
+
+def _three_rank_worker(rank, world, port, q):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                      OMP_NUM_THREADS="1")
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        h = _hier("sphere")
+        owner = _owner(h, "alternating", world)
+        u, res, maxima = _split_operator(h, 0, owner, rank)
+        q.put((rank, u[owner == rank].copy(), res[owner == rank].copy(), maxima))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_three_rank_relax_and_residual_are_bitwise():
+    """The same exchanges with three ranks (blocks dealt round-robin, so a
+    block's neighbours, parent and children mostly sit on two other ranks)."""
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_three_rank_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        got = {r: (u, res, m) for r, u, res, m in (q.get(timeout=300) for _ in procs)}
+    finally:
+        for p in procs:
+            p.join(timeout=30)
+            if p.is_alive():
+                p.kill()
+    h = _hier("sphere")
+    u_ref, res_ref, max_ref = _single_rank_operator(h, 0)
+    owner = _owner(h, "alternating", world)
+    skip = (h.level != h.nlev - 1) & (h.child[:, 0] >= 0)
+    for r in range(world):
+        u, res, maxima = got[r]
+        mine = owner == r
+        assert np.array_equal(u, u_ref[mine])
+        assert np.array_equal(res[~skip[mine]], res_ref[mine & ~skip])
+        assert maxima == max_ref
