@@ -60,12 +60,33 @@ import numpy as np
 __all__ = ["partition", "HaloExchange", "allreduce_max"]
 
 
-def partition(h, world: int) -> np.ndarray:
-    """owner[nb]: rank of every block, contiguous Morton ranges per AMR level."""
+def partition(h, world: int, nested: bool = False) -> np.ndarray:
+    """owner[nb]: rank of every block.
+
+    Default: contiguous Morton ranges per AMR level, nearly equal block
+    counts on every level (the reference's per-level assignment).  nested:
+    the base level is cut into Morton ranges of nearly equal weight (a base
+    block weighs as many blocks as its subtree holds) and every block
+    inherits its parent's rank, so the restriction and the prolongation
+    between levels stay on one rank and only faces between subtrees cross
+    ranks -- at the price of whole subtrees as the unit of balance."""
     if world < 1:
         raise ValueError("world must be >= 1")
     owner = np.empty(h.nblocks, dtype=np.int32)
     starts = np.concatenate([[0], np.cumsum(h.level_counts())]).astype(np.int64)
+    if nested:
+        weight = np.ones(h.nblocks, dtype=np.int64)
+        for b in range(h.nblocks - 1, int(starts[1]) - 1, -1):   # children come after their parents
+            weight[h.parent[b]] += weight[b]
+        base = weight[:int(starts[1])]
+        cum = np.concatenate([[0], np.cumsum(base)])
+        target = cum[-1] * np.arange(1, world, dtype=np.int64) / world
+        cuts = np.concatenate([[0], np.searchsorted(cum[1:], target, side="left") + 1, [base.size]])
+        for r in range(world):
+            owner[cuts[r]:cuts[r + 1]] = r
+        for b in range(int(starts[1]), h.nblocks):
+            owner[b] = owner[h.parent[b]]
+        return owner
     for L in range(h.nlev):
         s, e = int(starts[L]), int(starts[L + 1])
         cut = s + (np.arange(world + 1, dtype=np.int64) * (e - s)) // world

@@ -60,6 +60,8 @@ def _owner(h, part, world=2):
     from code_only_b200 import sharding
     if part == "morton":
         return sharding.partition(h, world)
+    if part == "nested":
+        return sharding.partition(h, world, nested=True)
     return (np.arange(h.nblocks) % world).astype(np.int32)
 
 
@@ -255,8 +257,8 @@ def _split_mean(h, owner, rank):
 
 # whole-solve cases: (boundary, owners); the isolated boundaries gather the
 # base blocks for their moments, the z-periodic cylinder for its line density
-SOLVE_CASES = [("periodic", "morton"), ("periodic", "alternating"), ("sphere", "alternating"),
-               ("zmirror", "alternating"), ("cylinder", "alternating")]
+SOLVE_CASES = [("periodic", "morton"), ("periodic", "alternating"), ("periodic", "nested"),
+               ("sphere", "alternating"), ("zmirror", "alternating"), ("cylinder", "alternating")]
 
 
 def _solve_hier(kind):
@@ -346,6 +348,22 @@ def _run(world=2, timeout=900):
 @pytest.fixture(scope="module")
 def two_ranks():
     return _run()
+
+
+def test_nested_partition_keeps_subtrees_together():
+    """partition(nested=True): every block on its parent's rank, so neither
+    the restriction nor the prolongation between levels crosses ranks; the
+    base level is cut by subtree weight."""
+    from code_only_b200 import sharding, workloads as w
+    for h in (_hier("periodic"), _hier("sphere"), w.nested_sphere(5, 8, 8)):
+        for world in (2, 3, 4):
+            owner = sharding.partition(h, world, nested=True)
+            up = h.level > 0
+            assert np.array_equal(owner[up], owner[h.parent[up]])
+            assert set(np.unique(owner)) == set(range(world))
+            for rank in range(world):
+                ex = sharding.HaloExchange(h, owner, rank, h.ni)
+                assert not any(k[0] in ("converge", "p2c") and v for k, v in ex.bytes_per_step().items())
 
 
 def test_partition_is_balanced_and_contiguous():
