@@ -2253,6 +2253,11 @@ static int64_t stage_elems(const sfm_ctx *c) {
 int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g, sfm_stats *st, void *stream) {
     if (!c || !c->s || !d_rho) return SFM_EINVAL;
     DeviceGuard dg(c->device);
+    if (stream) {   // the stopping rule reads the residual on the host: no stream capture
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing((cudaStream_t)stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+            return SFM_EINVAL;
+    }
     if (!device_pointer_on(d_rho, c->device) || (d_psi && !device_pointer_on(d_psi, c->device)) ||
         (d_g && !device_pointer_on(d_g, c->device)))
         return SFM_EINVAL;

@@ -168,7 +168,10 @@ int sfm_solve(sfm_ctx *c, const double *rho, double *psi, double *g, sfm_stats *
 /* Same with DEVICE pointers on the context's device (no host copies).
  * `stream` is a cudaStream_t or NULL for the context's own stream.  Each
  * pointer must be device memory of the context's device (or managed
- * memory); a host pointer or another GPU's memory returns SFM_EINVAL. */
+ * memory); a host pointer or another GPU's memory returns SFM_EINVAL.
+ * The call waits for the stream between outer iterations (the stopping
+ * rule reads the residual on the host), so it cannot be captured into a
+ * caller's graph: a stream under capture returns SFM_EINVAL untouched. */
 int sfm_solve_device(sfm_ctx *c, const double *d_rho, double *d_psi, double *d_g,
                      sfm_stats *st, void *stream);
 

@@ -294,3 +294,35 @@ def test_red_black_sweeps_have_no_intra_colour_race(name):
             psi_ser, g_ser, st_ser = s.solve(rho)
         assert st_par.outer_iters == st_ser.outer_iters
         assert np.array_equal(psi_par, psi_ser) and np.array_equal(g_par, g_ser)
+
+
+def test_solve_device_refuses_a_capturing_stream():
+    """The solve synchronises with the host between outer iterations, so a
+    stream under capture is refused before anything is queued on it, and the
+    caller's capture stays valid."""
+    import torch
+    h = w.small_periodic(2, 8, 2, 0)
+    p = abi.default_params(abi.SFM_BC_PERIODIC)
+    rho = w.block_field(h, p.ngh_io, w.gaussian_peak)
+    with FMGPoisson(h, params=p) as s:
+        rho_d = torch.from_numpy(rho).cuda()
+        psi_d = torch.zeros_like(rho_d)
+        st = abi.SfmStats()
+        stream = torch.cuda.Stream()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            graph.capture_begin()
+            rc = s.lib.sfm_solve_device(s.ctx, C.c_void_p(rho_d.data_ptr()), C.c_void_p(psi_d.data_ptr()), None,
+                                        C.byref(st), C.c_void_p(stream.cuda_stream))
+            psi_d.add_(1.0)   # the capture is still usable
+            graph.capture_end()
+        assert rc == abi.SFM_EINVAL
+        graph.replay()
+        torch.cuda.synchronize()
+        assert float(psi_d.max()) == 1.0
+        # and the same stream, not capturing, solves
+        psi_d.zero_()
+        rc = s.lib.sfm_solve_device(s.ctx, C.c_void_p(rho_d.data_ptr()), C.c_void_p(psi_d.data_ptr()), None,
+                                    C.byref(st), C.c_void_p(stream.cuda_stream))
+        torch.cuda.synchronize()
+        assert rc == abi.SFM_OK
