@@ -57,19 +57,68 @@ from typing import Dict, List, Tuple
 
 import numpy as np
 
-__all__ = ["partition", "HaloExchange", "allreduce_max"]
+__all__ = ["partition", "hilbert_key", "HaloExchange", "allreduce_max"]
 
 
-def partition(h, world: int, nested: bool = False) -> np.ndarray:
+def hilbert_key(ijk: np.ndarray, bits: int) -> np.ndarray:
+    """Index of each integer point (int [m, 3], 0 <= coordinate < 2^bits)
+    along the 3-D Hilbert curve, the curve the reference deals blocks to
+    ranks along (its Peano-Hilbert fillcells, refine.F90:662-706).  The
+    transform is Skilling's (Programming the Hilbert curve, AIP Conf. Proc.
+    707, 2004): axes to transposed index, then the bits interleaved."""
+    X = [np.asarray(ijk[:, d], dtype=np.int64).copy() for d in range(3)]
+    M = 1 << (bits - 1)
+    Q = M
+    while Q > 1:   # inverse undo of the rotations and reflections
+        P = Q - 1
+        for i in range(3):
+            hi = (X[i] & Q) != 0
+            X[0] = np.where(hi, X[0] ^ P, X[0])
+            t = np.where(hi, 0, (X[0] ^ X[i]) & P)
+            X[0] ^= t
+            X[i] ^= t
+        Q >>= 1
+    for i in range(1, 3):   # Gray encode
+        X[i] ^= X[i - 1]
+    t = np.zeros_like(X[0])
+    Q = M
+    while Q > 1:
+        t = np.where((X[2] & Q) != 0, t ^ (Q - 1), t)
+        Q >>= 1
+    for i in range(3):
+        X[i] ^= t
+    key = np.zeros_like(X[0])
+    for bit in range(bits - 1, -1, -1):
+        for i in range(3):
+            key = (key << 1) | ((X[i] >> bit) & 1)
+    return key
+
+
+def _curve_order(h, s: int, e: int, curve: str) -> np.ndarray:
+    """block ids s..e-1 (one AMR level, stored in Morton order) in the order
+    of the chosen space-filling curve"""
+    ids = np.arange(s, e, dtype=np.int64)
+    if curve == "morton":
+        return ids
+    if curve != "hilbert":
+        raise ValueError(f"unknown curve {curve!r}")
+    ijk = np.asarray(h.ijk[s:e], dtype=np.int64)
+    bits = max(1, int(ijk.max()).bit_length()) if e > s else 1
+    return ids[np.argsort(hilbert_key(ijk, bits), kind="stable")]
+
+
+def partition(h, world: int, nested: bool = False, curve: str = "morton") -> np.ndarray:
     """owner[nb]: rank of every block.
 
-    Default: contiguous Morton ranges per AMR level, nearly equal block
-    counts on every level (the reference's per-level assignment).  nested:
-    the base level is cut into Morton ranges of nearly equal weight (a base
-    block weighs as many blocks as its subtree holds) and every block
-    inherits its parent's rank, so the restriction and the prolongation
-    between levels stay on one rank and only faces between subtrees cross
-    ranks -- at the price of whole subtrees as the unit of balance."""
+    Default: the blocks of each AMR level cut into `world` consecutive runs
+    of nearly equal block counts along a space-filling curve (Morton, or
+    Hilbert as the reference deals its blocks, refine.F90:662-706).  nested:
+    the base level is cut along the curve into runs of nearly equal weight
+    (a base block weighs as many blocks as its subtree holds) and every
+    block inherits its parent's rank, so the restriction and the
+    prolongation between levels stay on one rank and only faces between
+    subtrees cross ranks -- at the price of whole subtrees as the unit of
+    balance."""
     if world < 1:
         raise ValueError("world must be >= 1")
     owner = np.empty(h.nblocks, dtype=np.int32)
@@ -78,20 +127,21 @@ def partition(h, world: int, nested: bool = False) -> np.ndarray:
         weight = np.ones(h.nblocks, dtype=np.int64)
         for b in range(h.nblocks - 1, int(starts[1]) - 1, -1):   # children come after their parents
             weight[h.parent[b]] += weight[b]
-        base = weight[:int(starts[1])]
-        cum = np.concatenate([[0], np.cumsum(base)])
+        order = _curve_order(h, 0, int(starts[1]), curve)
+        cum = np.concatenate([[0], np.cumsum(weight[order])])
         target = cum[-1] * np.arange(1, world, dtype=np.int64) / world
-        cuts = np.concatenate([[0], np.searchsorted(cum[1:], target, side="left") + 1, [base.size]])
+        cuts = np.concatenate([[0], np.searchsorted(cum[1:], target, side="left") + 1, [order.size]])
         for r in range(world):
-            owner[cuts[r]:cuts[r + 1]] = r
+            owner[order[cuts[r]:cuts[r + 1]]] = r
         for b in range(int(starts[1]), h.nblocks):
             owner[b] = owner[h.parent[b]]
         return owner
     for L in range(h.nlev):
         s, e = int(starts[L]), int(starts[L + 1])
-        cut = s + (np.arange(world + 1, dtype=np.int64) * (e - s)) // world
+        order = _curve_order(h, s, e, curve)
+        cut = (np.arange(world + 1, dtype=np.int64) * (e - s)) // world
         for r in range(world):
-            owner[cut[r]:cut[r + 1]] = r
+            owner[order[cut[r]:cut[r + 1]]] = r
     return owner
 
 

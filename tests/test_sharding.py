@@ -366,6 +366,34 @@ def test_nested_partition_keeps_subtrees_together():
                 assert not any(k[0] in ("converge", "p2c") and v for k, v in ex.bytes_per_step().items())
 
 
+def test_hilbert_key_is_a_hilbert_curve():
+    """hilbert_key orders the points of a 2^b cube as a Hilbert curve: every
+    point once, each step to a face neighbour, starting at the origin."""
+    from code_only_b200.sharding import hilbert_key
+    for bits in (1, 2, 3, 4):
+        n = 1 << bits
+        g = np.array([(i, j, k) for k in range(n) for j in range(n) for i in range(n)])
+        key = hilbert_key(g, bits)
+        assert sorted(key.tolist()) == list(range(n ** 3))
+        pts = g[np.argsort(key)]
+        assert (pts[0] == 0).all()
+        assert (np.abs(np.diff(pts, axis=0)).sum(axis=1) == 1).all()
+
+
+def test_hilbert_partitions_are_balanced():
+    from code_only_b200 import sharding, workloads as w
+    for h in (_hier("periodic"), w.nested_sphere(5, 8, 8)):
+        for world in (2, 3, 4):
+            o = sharding.partition(h, world, curve="hilbert")
+            for L in range(h.nlev):
+                c = np.bincount(o[h.level == L], minlength=world)
+                assert c.max() - c.min() <= 1
+            on = sharding.partition(h, world, nested=True, curve="hilbert")
+            up = h.level > 0
+            assert np.array_equal(on[up], on[h.parent[up]])
+            assert set(np.unique(on)) == set(range(world))
+
+
 def test_partition_is_balanced_and_contiguous():
     from code_only_b200 import sharding
     h = _hier("periodic")
