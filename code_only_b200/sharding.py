@@ -182,6 +182,7 @@ class HaloExchange:
 
     def __init__(self, h, owner: np.ndarray, rank: int, n: int):
         self.h, self.owner, self.rank, self.n = h, np.asarray(owner), rank, n
+        self._idx_cache = {}
         self.world = int(self.owner.max()) + 1
         G = n + 2
         self.G, self.V = G, G ** 3
@@ -326,7 +327,9 @@ class HaloExchange:
         import torch.distributed as dist
         ops, recvs = [], []
         for (reader, holder), cells in self.needs.get(step, {}).items():
-            idx = torch.from_numpy(cells).to(field.device)
+            if self.rank not in (reader, holder):
+                continue
+            idx = self._index(step, reader, holder, cells, field.device)
             if holder == self.rank:
                 ops.append(dist.P2POp(dist.isend, field[idx].contiguous(), reader))
             elif reader == self.rank:
@@ -338,6 +341,17 @@ class HaloExchange:
                 req.wait()
         for idx, buf in recvs:
             field[idx] = buf
+
+    def _index(self, step, reader, holder, cells, device):
+        """the cell list as an index tensor on `device`, made once per step
+        and device (on a GPU, one upload instead of one per exchange)"""
+        import torch
+        key = (step, reader, holder, str(device))
+        idx = self._idx_cache.get(key)
+        if idx is None:
+            idx = torch.from_numpy(cells).to(device)
+            self._idx_cache[key] = idx
+        return idx
 
     def bytes_per_step(self) -> Dict[tuple, int]:
         """Values this rank receives per step x 8 bytes (FP64)."""
