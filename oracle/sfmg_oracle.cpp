@@ -973,7 +973,11 @@ struct Oracle {
         ProfScope ps(prof, kPrReflux);
         for (int d = 0; d < 3; d++) xc_field(2, f, 0, d, FL(d, f));
         const int n = nF(f), h2n = n / 2;
-        struct Item { int cb, dir, xc, ta0, tb0; std::vector<double> v; };
+        const size_t per = (size_t)h2n * h2n;
+        // the faces, then every face's means into one flat buffer, then the
+        // writes: reads and writes in two phases, as the reference packs
+        // before it unpacks; each face's values are independent of the others'
+        struct Item { int b, cb, dir, xf, xc, ta0, tb0; };
         std::vector<Item> items;
         for (int L = 1; L < nlev; L++)
             for (int b = lstart[L]; b < lstart[L + 1]; b++)
@@ -981,31 +985,34 @@ struct Oracle {
                     for (int lr = 0; lr < 2; lr++) {
                         int fc = lr + 2 * dir;
                         if (!parLev[6 * b + fc] || !mine(nbrGid[6 * b + fc])) continue;
-                        Arr &Ff = FL(dir, f);
-                        int xf = (lr == Left) ? -1 : n - 1;       // Ifs(lr,ndir)
-                        Item it;
-                        it.cb = nbrGid[6 * b + fc];
-                        it.dir = dir;
-                        it.xc = (lr == Left) ? n - 1 : -1;        // Ics(lr,ndir)
                         int ta = (dir == MX) ? MY : MX, tb = (dir == MZ) ? MY : MZ;
-                        it.ta0 = octant[3 * b + ta] * h2n;
-                        it.tb0 = octant[3 * b + tb] * h2n;
-                        it.v.resize((size_t)h2n * h2n);
-                        for (int qc = 0; qc < h2n; qc++)
-                            for (int pc = 0; pc < h2n; pc++) {
-                                int pf = 2 * pc, qf = 2 * qc;
-                                auto ff = [&](int p, int q) { int i, j, k; put3(dir, xf, p, q, i, j, k); return Ff.at(b, i, j, k); };
-                                it.v[(size_t)qc * h2n + pc] =
-                                    (ff(pf, qf) + ff(pf, qf + 1) + ff(pf + 1, qf) + ff(pf + 1, qf + 1)) * 0.25;
-                            }
-                        items.push_back(std::move(it));
+                        items.push_back({b, nbrGid[6 * b + fc], dir,
+                                         (lr == Left) ? -1 : n - 1,        // Ifs(lr,ndir)
+                                         (lr == Left) ? n - 1 : -1,        // Ics(lr,ndir)
+                                         octant[3 * b + ta] * h2n, octant[3 * b + tb] * h2n});
                     }
-        for (auto &it : items) {
+        const int64_t ni = (int64_t)items.size();
+        std::vector<double> v((size_t)ni * per);
+        OMP_FOR
+        for (int64_t q = 0; q < ni; q++) {
+            const Item &it = items[q];
+            Arr &Ff = FL(it.dir, f);
+            for (int qc = 0; qc < h2n; qc++)
+                for (int pc = 0; pc < h2n; pc++) {
+                    int pf = 2 * pc, qf = 2 * qc;
+                    auto ff = [&](int p, int qq) { int i, j, k; put3(it.dir, it.xf, p, qq, i, j, k); return Ff.at(it.b, i, j, k); };
+                    v[(size_t)q * per + (size_t)qc * h2n + pc] =
+                        (ff(pf, qf) + ff(pf, qf + 1) + ff(pf + 1, qf) + ff(pf + 1, qf + 1)) * 0.25;
+                }
+        }
+        OMP_FOR
+        for (int64_t q = 0; q < ni; q++) {
+            const Item &it = items[q];
             Arr &Fc = FL(it.dir, f);
             for (int qc = 0; qc < h2n; qc++)
                 for (int pc = 0; pc < h2n; pc++) {
                     int i, j, k; put3(it.dir, it.xc, pc + it.ta0, qc + it.tb0, i, j, k);
-                    Fc.at(it.cb, i, j, k) = it.v[(size_t)qc * h2n + pc];
+                    Fc.at(it.cb, i, j, k) = v[(size_t)q * per + (size_t)qc * h2n + pc];
                 }
         }
     }
