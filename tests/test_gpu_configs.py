@@ -21,7 +21,7 @@ Tolerances (max norm, relative): FP64 is bit-identical (0.0), the isolated
 boundary included (its multipole moments are summed in the reference's
 order); the mixed path against the FP64 oracle 1e-9 in
 phi (mean removed on periodic boxes, whose constant is free) and in g, at a
-true relative residual <= 1e-10 -- the north-star bar.  Every solve runs to
+true relative residual <= 1e-10 -- the accuracy target of the mixed path.  Every solve runs to
 relative residual 1e-10 as the benchmark does.
 """
 import gc
@@ -135,6 +135,6 @@ def test_jeans6_mixed_within_1e9(jeans6):
 def test_jeans6_mixed_tuned_within_1e9(jeans6):
     """The benchmark's configuration: launch shapes and the mixed path's
     inner-solve schedule tuned on the jeans6 density, then phi and g against
-    the FP64 oracle at the north-star bar."""
+    the FP64 oracle: within 1e-9 at a true relative residual <= 1e-10."""
     h, rho, bc, out = jeans6
     _check_mixed(h, rho, bc, {}, out, tuned=True)
