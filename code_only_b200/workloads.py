@@ -495,12 +495,12 @@ def gaussian_peak(x, y, z):
 
 def config_hierarchy(name: str):
     """(hierarchy, density fn, bc) for a named workload:
-    'uniform64'  : 64^3 periodic, 8^3 blocks of 8^3, Gaussian peak (config 1)
-    'nested5'    : 64^3 base + 4 concentric levels, softened sphere, isolated (config 2)
-    'jeans6'     : 128^3 base periodic Jeans-refined GRF, 6 levels (config 3); the
+    'uniform64'  : 64^3 periodic, 8^3 blocks of 8^3, Gaussian peak
+    'nested5'    : 64^3 base + 4 concentric levels, softened sphere, isolated
+    'jeans6'     : 128^3 base periodic Jeans-refined GRF, 6 levels; the
                    box is 6 length units (G = 1, c_s = 0.2), the smallest size at
                    which this density reaches the sixth level: 133,856 blocks
-    'deep8'      : 256^3 base of 16^3 blocks, 8 levels, GRF + Plummer cores (config 5)
+    'deep8'      : 256^3 base of 16^3 blocks, 8 levels, GRF + Plummer cores
     'uniform256' : 256^3 periodic, 32^3 blocks of 8^3, Gaussian peak: the smallest
                    uniform grid whose FP32 field with ghosts (131 MB) exceeds the
                    126 MB L2, used for kernel profiles of the 8^3-block sweeps

@@ -5,17 +5,17 @@ The small cases of test_gpu_parity.py reach at most an 8^3 base grid.  These
 cases pin what the benchmark workloads run:
 
 * uniform64 -- the 64^3 periodic box of 8^3 blocks with the Gaussian peak,
-  a 16^3 base grid (config 1);
+  a 16^3 base grid;
 * uniform128 and amr_base16 -- the 32^3 base grid of the Jeans-refined cloud,
   whose base-grid CTA keeps its coarse levels in shared memory;
 * nested5 -- base 64^3 plus four concentric levels around a softened
   isothermal sphere, isolated boundary with multipoles l <= 3 (the
-  reference's order) and l <= 4 (config 2);
+  reference's order) and l <= 4;
 * base3_* / base6_sphere -- base boxes whose block counts are not powers of
   two, where the reference replaces the base-grid multigrid by 10 smoother
   sweeps on the base level (UseSerialMg = .FALSE., vmg.F90:85-91,397-402);
 * jeans6 -- the 6-level Jeans-refined turbulent cloud of the benchmark
-  (133,856 blocks), FP64 and mixed precision (config 3).
+  (133,856 blocks), FP64 and mixed precision.
 
 Tolerances (max norm, relative): FP64 is bit-identical (0.0), the isolated
 boundary included (its multipole moments are summed in the reference's

@@ -1,4 +1,4 @@
-"""Guard-band debug mode on the GPU (the bounds check of this build).
+"""Guard-band debug mode on the GPU (the library's bounds check).
 
 With sfm_debug_set_guard_bytes, every device array of a new context sits
 between two bands of 0xFF bytes.  A kernel that writes past either end of an
