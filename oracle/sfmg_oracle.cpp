@@ -1203,15 +1203,18 @@ struct Oracle {
     // =====================================================================
     void vmg_copy(int L, int out, int in) {
         Arr &O = F(out, FMax), &I = F(in, FMax);
+        OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++) std::copy(I.blk(b), I.blk(b) + I.V, O.blk(b));
     }
     void vmg_sub(int L, int out, int a, int bb) {
         Arr &O = F(out, FMax), &A = F(a, FMax), &B = F(bb, FMax);
+        OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++)
             for (size_t q = 0; q < O.V; q++) O.blk(b)[q] = A.blk(b)[q] - B.blk(b)[q];
     }
     void vmg_add(int L, int a, int da, bool onov) {
         Arr &A = F(a, FMax), &D = F(da, FMax);
+        OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++) {
             if (onov && child[8 * b] == Undef) continue;
             for (size_t q = 0; q < A.V; q++) A.blk(b)[q] = A.blk(b)[q] + D.blk(b)[q];
@@ -1219,10 +1222,12 @@ struct Oracle {
     }
     void vmg_boundary_fill0(int L, int code) {
         Arr &A = F(code, FMax);
+        OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++) fill0_faces_block(A, b, nF(FMax));
     }
     void vmg_boundary_extrap(int L, int code) {
         Arr &A = F(code, FMax);
+        OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++) extrap_block(A, b, nF(FMax));
     }
     void vmg_ghostcell(int L, int code) {   // vmg.F90:729-743
@@ -1244,6 +1249,7 @@ struct Oracle {
         Arr &U = F(ju, FMax);
         const int n = nF(FMax);
         double hi = 1.0 / h(L, FMax);
+        OMP_FOR
         for (int b = lstart[L]; b < lstart[L + 1]; b++)
             for (int k = -1; k <= n - 1; k++)
                 for (int j = -1; j <= n - 1; j++)
@@ -1262,6 +1268,9 @@ struct Oracle {
         for (int ipass = 1; ipass <= 2; ipass++) {
             vmg_poisson_flux(L, ju);
             ProfScope ps(prof, kPrRelax);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) reduction(max : resmax)
+#endif
             for (int b = lstart[L]; b < lstart[L + 1]; b++)
                 for (int k = 0; k < n; k++)
                     for (int j = 0; j < n; j++)
