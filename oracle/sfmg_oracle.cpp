@@ -1298,6 +1298,7 @@ struct Oracle {
             Arr &T = F(jtau, FMax);
             vmg_poisson_flux(Lf, ju);
             double hi = 1.0 / h(Lf, FMax);
+            OMP_FOR
             for (int b = lstart[Lf]; b < lstart[Lf + 1]; b++) {
                 std::fill(T.blk(b), T.blk(b) + T.V, 0.0);
                 for (int k = 0; k < n; k++)
@@ -1307,6 +1308,7 @@ struct Oracle {
             converge_c2p_lev(L, FMax, jtau, false);
             vmg_poisson_flux(L, ju);
             hi = 1.0 / h(L, FMax);
+            OMP_FOR
             for (int b = lstart[L]; b < lstart[L + 1]; b++) {
                 if (child[8 * b] == Undef) continue;
                 for (int k = 0; k < n; k++)
@@ -1349,6 +1351,7 @@ struct Oracle {
         Arr &Fo = F(juf, FMax), &C = F(juc, FMax);
         xc_field(3, FMax, Lc, 0, C);
         const int n = nF(FMax), h2n = n / 2;
+        OMP_FOR
         for (int p = lstart[Lc]; p < lstart[Lc + 1]; p++)
             for (int c = 0; c < 8; c++) {
                 int cb = child[8 * p + c];
