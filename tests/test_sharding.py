@@ -275,8 +275,9 @@ def _solve_params(kind="periodic"):
     bc = {"periodic": abi.SFM_BC_PERIODIC, "sphere": abi.SFM_BC_SPHERE, "zmirror": abi.SFM_BC_ZMIRROR,
           "cylinder": abi.SFM_BC_CYL_ZPERIODIC}[kind]
     kw = {} if kind == "periodic" else {"zero_mean": 0}
-    # a few outer iterations on the periodic box, one elsewhere (each rank's
-    # exchanges go through gloo: a split solve costs seconds per iteration)
+    # two outer iterations on the periodic box, one or two elsewhere (each
+    # rank's exchanges go through gloo: a split solve costs seconds per
+    # iteration)
     return abi.default_params(bc, rel_tol=1e-3 if kind == "periodic" else 0.5, max_outer=40, **kw)
 
 
